@@ -1,0 +1,273 @@
+/*
+ * pt_b200.h -- C ABI of the B200 path tracer (libpt_b200.so).
+ *
+ * This is the drop-in boundary for the per-pixel path-tracing integrator of
+ * Neroued/PathTracingTutorial Part_2.  Every entry point returns an int status
+ * (PT_OK == 0); on failure pt_last_error() returns a thread-local message.
+ * No entry point exits the process (the reference's CUDA_CHECK calls exit(1),
+ * Part_2/src/cuda/check.h:6-24).
+ *
+ * Structs below are byte-for-byte layout-compatible with the reference's host
+ * structs so that arrays built for the reference can be passed unchanged:
+ *   pt_vertex          <-> pt::Vertex          Part_2/src/geometry/vertex.h:10-15   (64 B)
+ *   pt_face            <-> pt::TriangleFace    Part_2/src/geometry/vertex.h:17-20   (16 B)
+ *   pt_material        <-> pt::Material        Part_2/src/materials/material.h:8-75 (256 B)
+ *   pt_camera          <-> pt::Camera          Part_2/src/camera/camera.h:12-21     (80 B)
+ *   pt_camera_frame    <-> pt::CameraFrame     Part_2/src/camera/camera.h:25-34     (64 B)
+ *   pt_scene_params    <-> pt::SceneParams     Part_2/src/scene/device_scene.h:19-27 (88 B)
+ *   pt_punctual_light  <-> pt::PunctualLight   Part_2/src/lights/punctual_light.h:14-25 (112 B)
+ *   pt_bvh_node        <-> pt::BVHNode         Part_2/src/accel/bvh_common.h:16-27  (32 B)
+ *   pt_alias_entry     <-> pt::AliasEntry      Part_2/src/lights/light_sampler.h:20-23 (8 B)
+ *   pt_emissive_ref    <-> pt::EmissiveTriangleRef Part_2/src/lights/light_sampler.h:13-18 (16 B)
+ *
+ * Ownership: the library owns every device allocation; the caller owns host
+ * buffers it passes in.  A scene is thread-compatible, not thread-safe.
+ */
+#ifndef PT_B200_H
+#define PT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define PT_OK            0
+#define PT_ERR_INVALID   1  /* bad argument or unsupported input            */
+#define PT_ERR_IO        2  /* file missing, unreadable or malformed          */
+#define PT_ERR_CUDA      3  /* a CUDA runtime call failed                     */
+#define PT_ERR_STATE     4  /* call order violated (e.g. render before build) */
+#define PT_ERR_DEVICE    5  /* a kernel reported an error word (see message)  */
+#define PT_ERR_NOMEM     6  /* host or device allocation failed               */
+
+/* ---- samplers (Part_2/src/scene/device_scene.h:17) ---- */
+#define PT_SAMPLER_PCG   0
+#define PT_SAMPLER_SOBOL 1
+
+/* ---- render flags ---- */
+#define PT_FLAG_WATERTIGHT     1  /* watertight triangle test instead of the reference's Moller-Trumbore */
+#define PT_FLAG_STAGE_TIMING   2  /* record CUDA events around every stage launch                       */
+#define PT_FLAG_NO_GRAPH       4  /* launch stages directly instead of replaying a captured CUDA graph   */
+#define PT_FLAG_COUNT_TRAVERSAL 8 /* count node visits / triangle tests (device counters)               */
+
+/* ---- argument-order of paired sampler draws ----
+ * The reference draws two sampler dimensions inside one call's argument list
+ * (e.g. Part_2/src/integrators/direct_lighting.cuh:63-64,69-70,137-138 and
+ * Part_2/src/materials/disney_bsdf.cuh:350,354,362,368).  C++ leaves the order
+ * unspecified; the two compilers of the reference differ.  PT_ARGS_LTR draws the
+ * first argument first, PT_ARGS_RTL draws the second argument first. */
+#define PT_ARGS_LTR 0
+#define PT_ARGS_RTL 1
+
+/* ---- layout-compatible scene structs ---- */
+typedef struct pt_vertex {
+    float position[3]; float _pad0;
+    float normal[3];   float _pad1;
+    float uv[2];       float _pad2[2];
+    float tangent[4];               /* xyz = tangent, w = handedness */
+} pt_vertex;
+
+typedef struct pt_face {
+    uint32_t v0, v1, v2;
+    int32_t  material_id;
+} pt_face;
+
+typedef struct pt_material {
+    float   base_color[3]; float _pad0;                                  /*   0 */
+    float   metallic, roughness, specular_tint, anisotropic;             /*  16 */
+    float   sheen, sheen_tint, clearcoat, clearcoat_roughness;           /*  32 */
+    float   spec_trans, ior, subsurface, specular_factor;                /*  48 */
+    float   specular_color_r, specular_color_g, specular_color_b,
+            anisotropy_rotation;                                         /*  64 */
+    float   normal_scale; float _pad1[3];                                /*  80 */
+    float   emissive[3]; float _pad2;                                    /*  96 */
+    float   emissive_strength, alpha_cutoff; int32_t alpha_mode;
+    float   base_alpha;                                                  /* 112 */
+    int32_t double_sided; float sheen_color_r, sheen_color_g,
+            sheen_color_b;                                               /* 128 */
+    float   occlusion_strength, thickness_factor, attenuation_distance,
+            att_color_r;                                                 /* 144 */
+    float   att_color_g, att_color_b, uv_offset_x, uv_offset_y;          /* 160 */
+    float   uv_scale_x, uv_scale_y, uv_rotation, _pad3;                  /* 176 */
+    float   _pad4; int32_t base_color_tex, metallic_roughness_tex,
+            normal_tex;                                                  /* 192 */
+    int32_t emissive_tex, occlusion_tex, clearcoat_tex,
+            clearcoat_roughness_tex;                                     /* 208 */
+    int32_t clearcoat_normal_tex, transmission_tex, sheen_color_tex,
+            sheen_roughness_tex;                                         /* 224 */
+    int32_t _pad5; int32_t _pad6[3];                                     /* 240 */
+} pt_material;
+
+typedef struct pt_camera {
+    float   position[3]; float _pad0;
+    float   look_at[3];  float _pad1;
+    float   up[3];       float _pad2;
+    float   fov, aperture, focal_distance;
+    int32_t width, height;
+    int32_t _pad3[3];
+} pt_camera;
+
+typedef struct pt_camera_frame {
+    float position[3], forward[3], right[3], up[3];
+    float tan_half_fov, aspect, aperture, focal_distance;
+} pt_camera_frame;
+
+typedef struct pt_scene_params {
+    pt_camera_frame camera;
+    int32_t width, height, sample_per_frame, target_samples, max_depth, sampler_type;
+} pt_scene_params;
+
+typedef struct pt_punctual_light {
+    float   position[3]; float _pad0;
+    float   range; float _pad1[3];
+    float   color[3]; float _pad2;
+    float   intensity; float _pad3[3];
+    float   direction[3]; float _pad4;
+    float   inner_cone, outer_cone;     /* cosines */
+    int32_t type;                       /* 0 point, 1 directional, 2 spot */
+    float   _pad5, _pad6; float _pad7[3];
+} pt_punctual_light;
+
+typedef struct pt_bvh_node {
+    float    bmin[3]; uint32_t data0;   /* leaf: first | 0x80000000, inner: left  */
+    float    bmax[3]; uint32_t data1;   /* leaf: count,             inner: right */
+} pt_bvh_node;
+
+typedef struct pt_alias_entry { float prob; uint32_t alias; } pt_alias_entry;
+
+typedef struct pt_emissive_ref {
+    uint32_t triangle_index; float selection_pmf; float cdf; float _pad;
+} pt_emissive_ref;
+
+/* ---- render settings (RenderSettings, Part_2/src/scene/scene.h:16-22) ---- */
+typedef struct pt_render_settings {
+    int32_t  spp;               /* targetSamples                                  */
+    int32_t  sample_per_frame;  /* samples per launch (batch)                     */
+    int32_t  max_depth;
+    int32_t  sampler_type;      /* PT_SAMPLER_*                                   */
+    uint32_t pcg_seed;          /* added knob; 0 reproduces the reference seeding */
+    int32_t  arg_order;         /* PT_ARGS_*                                      */
+    int32_t  flags;             /* PT_FLAG_*                                      */
+    int32_t  _reserved;
+} pt_render_settings;
+
+typedef struct pt_scene_info {
+    uint32_t num_vertices, num_faces, num_materials, num_bvh_nodes;
+    uint32_t num_emissive_triangles, num_punctual_lights;
+    int32_t  env_width, env_height;
+    uint32_t bvh_max_depth, num_inner_nodes, num_leaves;
+    uint32_t frame_count;
+    uint64_t device_bytes;
+} pt_scene_info;
+
+typedef struct pt_render_stats {
+    uint64_t camera_rays, extension_rays, shadow_rays;  /* rays traced          */
+    uint64_t node_visits, triangle_tests;               /* closest-hit only     */
+    uint64_t shadow_node_visits, shadow_triangle_tests;
+    uint64_t paths;                                      /* camera samples       */
+    uint64_t extend_launches;
+    double   extend_ms, shade_ms, shadow_ms, other_ms;   /* with PT_FLAG_STAGE_TIMING */
+    double   total_ms;
+} pt_render_stats;
+
+typedef struct pt_hit {
+    float   t;          /* FLT_MAX on miss (SurfaceInteraction::distance)     */
+    int32_t prim;       /* -1 on miss; index into the BVH-ordered face array  */
+    float   u, v;       /* barycentrics of the closest hit                    */
+} pt_hit;
+
+typedef struct pt_scene      pt_scene;
+typedef struct pt_film       pt_film;
+typedef struct pt_integrator pt_integrator;
+
+/* ---- errors / version ---- */
+const char* pt_last_error(void);
+const char* pt_version(void);
+
+/* ---- camera (buildCameraFrame, Part_2/src/camera/camera.h:36-51) ---- */
+int pt_build_camera_frame(const pt_camera* cam, pt_camera_frame* out);
+
+/* ---- scene: load / create (SceneLoader::load, Part_2/src/scene/scene_loader.cpp:240-292) ---- */
+int pt_scene_load_json(const char* path, pt_scene** out);
+int pt_scene_create(const pt_vertex* vertices, uint32_t num_vertices,
+                    const pt_face* faces, uint32_t num_faces,
+                    const pt_material* materials, uint32_t num_materials,
+                    const pt_camera* camera,
+                    const float* env_rgba, int32_t env_width, int32_t env_height,
+                    pt_scene** out);
+int pt_scene_destroy(pt_scene* scene);
+int pt_scene_set_punctual_lights(pt_scene* scene, const pt_punctual_light* lights, uint32_t n);
+int pt_scene_set_render_settings(pt_scene* scene, const pt_render_settings* s);   /* setSpp/setSampler/setMaxDepth */
+int pt_scene_get_render_settings(const pt_scene* scene, pt_render_settings* s);
+int pt_scene_set_camera(pt_scene* scene, const pt_camera* cam);                   /* SceneManager::updateCamera */
+int pt_scene_get_camera(const pt_scene* scene, pt_camera* cam);
+
+/* ---- scene: prep (SceneManager::buildAccel, Part_2/src/scene/scene_manager.cpp:28-41) ----
+ * SAH BVH (reorders faces: triangle ids are BVH-ordered face indices), emissive
+ * triangle and environment alias tables, and the device node layout.  Host only. */
+int pt_scene_build_accel(pt_scene* scene);
+/* ---- scene: upload (SceneManager::uploadToDevice / DeviceScene::uploadFrom,
+ *      Part_2/src/scene/device_scene.cu:8-57) ---- */
+int pt_scene_upload(pt_scene* scene, int32_t device);
+int pt_scene_info_get(const pt_scene* scene, pt_scene_info* info);
+int pt_scene_build_params(const pt_scene* scene, pt_scene_params* out);           /* DeviceScene::buildParams */
+/* Read back host-side prep results (arrays sized from pt_scene_info). */
+int pt_scene_get_vertices(const pt_scene* scene, pt_vertex* out, uint32_t cap);
+int pt_scene_get_faces(const pt_scene* scene, pt_face* out, uint32_t cap);
+int pt_scene_get_materials(const pt_scene* scene, pt_material* out, uint32_t cap);
+int pt_scene_get_bvh(const pt_scene* scene, pt_bvh_node* out, uint32_t cap);
+int pt_scene_get_emissive(const pt_scene* scene, pt_emissive_ref* refs, uint32_t cap_refs,
+                          float* face_pmf, uint32_t cap_pmf,
+                          pt_alias_entry* alias, uint32_t cap_alias);
+int pt_scene_get_env_tables(const pt_scene* scene, float* pmf, pt_alias_entry* alias, uint32_t cap);
+
+/* ---- film (Film, Part_2/src/film/film.h:9-40) ----
+ * Per pixel: compensated FP32 sum (Neumaier), compensation, sample count, and
+ * the mean of the last launch (the reference's "new" surface). */
+int pt_film_create(int32_t width, int32_t height, int32_t device, pt_film** out);
+int pt_film_destroy(pt_film* film);
+int pt_film_clear(pt_film* film);
+int pt_film_download(const pt_film* film, float* host_rgba);       /* Film::downloadAccumulated */
+int pt_film_download_new(const pt_film* film, float* host_rgba);   /* the last launch's mean     */
+
+/* ---- integrator plugin (Integrator, Part_2/src/integrators/integrator.h:10-20) ---- */
+int         pt_integrator_create(const char* name, pt_integrator** out);          /* "path" */
+int         pt_integrator_destroy(pt_integrator* integ);
+const char* pt_integrator_name(const pt_integrator* integ);                       /* "Path" */
+/* Integrator::launch: trace params->sample_per_frame samples per pixel with the
+ * scene's current frame count and fold them into the film.  Asynchronous on
+ * `stream` (a cudaStream_t; NULL = the integrator's own stream). */
+int pt_integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* scene,
+                         const pt_scene_params* params, void* stream);
+int pt_integrator_stats(const pt_integrator* integ, pt_render_stats* out);
+int pt_integrator_reset_stats(pt_integrator* integ);
+
+/* ---- renderer (Renderer, Part_2/src/renderer.h:17-55) ---- */
+int pt_renderer_render_batch(pt_integrator* integ, pt_film* film, pt_scene* scene, void* stream); /* renderBatch */
+int pt_renderer_reset_accumulation(pt_film* film, pt_scene* scene);                               /* resetAccumulation */
+/* render(scene, spp) -> HDR image: build (if needed), upload (if needed), render
+ * spp samples per pixel, write width*height*4 floats (RGBA, row y at y*width*4). */
+int pt_render(pt_scene* scene, int32_t spp, float* out_rgba, int32_t out_is_device,
+              pt_render_stats* stats);
+
+/* ---- diagnostics used by the parity tests (same kernels as the render path) ---- */
+/* rays: n x 8 floats (ox, oy, oz, unused, dx, dy, dz, tmax).  tmax only used by trace_any. */
+int pt_trace_closest(pt_scene* scene, const float* rays, uint32_t n, pt_hit* hits,
+                     int32_t ptrs_are_device);
+int pt_trace_any(pt_scene* scene, const float* rays, uint32_t n, uint8_t* occluded,
+                 int32_t ptrs_are_device);
+/* Sampler streams: out[(y*width + x)*ndims + k] = dimension k of pixel (x,y) for the
+ * sample with (frame_count, sample_in_frame) as the render kernel draws it. */
+int pt_sampler_stream(int32_t sampler_type, int32_t width, int32_t height,
+                      uint32_t frame_count, int32_t sample_per_frame, int32_t sample_in_frame,
+                      uint32_t ndims, uint32_t pcg_seed, int32_t device, float* out_host);
+/* BSDF table: for n (material index, wo, wi, n, t) records evaluate the device
+ * Disney BSDF.  in: n x 13 floats (mat, wo[3], wi[3], N[3], T[3]); out: n x 4 (f.rgb, pdf). */
+int pt_bsdf_eval(pt_scene* scene, const float* in, uint32_t n, float* out_host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PT_B200_H */

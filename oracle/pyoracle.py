@@ -1,0 +1,303 @@
+"""TEST INFRASTRUCTURE: Python access to the CPU oracle (liboracle.so) and to the
+reference's own host-compiled code (_ref/libptref.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  `Oracle` is the restatement (oracle/pt_oracle.cpp); `RefHarness`
+runs the reference's code and exists only where oracle/_ref was built (it is
+built from the reference tree in the development container and travels with
+the repository snapshot as a binary).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libptref.so")
+
+VERTEX = np.dtype([("position", "<f4", 3), ("_pad0", "<f4"), ("normal", "<f4", 3), ("_pad1", "<f4"),
+                   ("uv", "<f4", 2), ("_pad2", "<f4", 2), ("tangent", "<f4", 4)])
+FACE = np.dtype([("v0", "<u4"), ("v1", "<u4"), ("v2", "<u4"), ("material_id", "<i4")])
+NODE = np.dtype([("bmin", "<f4", 3), ("data0", "<u4"), ("bmax", "<f4", 3), ("data1", "<u4")])
+ALIAS = np.dtype([("prob", "<f4"), ("alias", "<u4")])
+EMREF = np.dtype([("triangle_index", "<u4"), ("selection_pmf", "<f4"), ("cdf", "<f4"), ("_pad", "<f4")])
+
+
+class Scene(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("num_vertices", C.c_uint32), ("faces", C.c_void_p),
+                ("num_faces", C.c_uint32), ("materials", C.c_void_p), ("num_materials", C.c_uint32),
+                ("nodes", C.c_void_p), ("num_nodes", C.c_uint32), ("emissive", C.c_void_p),
+                ("num_emissive", C.c_uint32), ("tri_pmf", C.c_void_p), ("tri_alias", C.c_void_p),
+                ("env_rgba", C.c_void_p), ("env_w", C.c_int32), ("env_h", C.c_int32), ("env_pmf", C.c_void_p),
+                ("env_alias", C.c_void_p), ("num_env_texels", C.c_uint32), ("env_tw", C.c_int32),
+                ("env_th", C.c_int32), ("punctual", C.c_void_p), ("num_punctual", C.c_uint32),
+                ("camera_frame", C.c_void_p), ("width", C.c_int32), ("height", C.c_int32)]
+
+
+class RenderArgs(C.Structure):
+    _fields_ = [("sample_per_frame", C.c_int32), ("max_depth", C.c_int32), ("sampler_type", C.c_int32),
+                ("arg_rtl", C.c_int32), ("pcg_seed", C.c_uint32), ("first_frame", C.c_uint32),
+                ("num_frames", C.c_uint32), ("row0", C.c_int32), ("row_step", C.c_int32), ("threads", C.c_int32),
+                ("precision", C.c_int32), ("_pad", C.c_int32)]
+
+
+class Counters(C.Structure):
+    _fields_ = [("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("node_pops", C.c_uint64),
+                ("tri_tests", C.c_uint64), ("shadow_node_pops", C.c_uint64), ("shadow_tri_tests", C.c_uint64),
+                ("paths", C.c_uint64), ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return C.c_void_p(a.ctypes.data)
+
+
+def build(ref: bool = False) -> None:
+    """Compile liboracle.so (and, when the reference tree is present, _ref/libptref.so)."""
+    targets = ["oracle", "ref"] if ref else ["oracle"]
+    r = subprocess.run(["make", "-C", HERE, "-j8", *targets], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
+
+
+class Prepared:
+    """Scene prepared with the oracle's own builder (BVH order, light tables)."""
+
+    def __init__(self, vertices, faces, materials, nodes, depth, em_refs, tri_pmf, tri_alias, env, env_pmf,
+                 env_alias, camera_frame, width, height, punctual=None):
+        self.vertices, self.faces, self.materials, self.nodes, self.depth = vertices, faces, materials, nodes, depth
+        self.em_refs, self.tri_pmf, self.tri_alias = em_refs, tri_pmf, tri_alias
+        self.env, self.env_pmf, self.env_alias = env, env_pmf, env_alias
+        self.camera_frame, self.width, self.height = camera_frame, width, height
+        self.punctual = punctual
+
+    def struct(self) -> Scene:
+        s = Scene()
+        s.vertices, s.num_vertices = _p(self.vertices), len(self.vertices)
+        s.faces, s.num_faces = _p(self.faces), len(self.faces)
+        s.materials, s.num_materials = _p(self.materials), len(self.materials)
+        s.nodes, s.num_nodes = _p(self.nodes), len(self.nodes)
+        s.emissive, s.num_emissive = _p(self.em_refs), len(self.em_refs)
+        s.tri_pmf, s.tri_alias = _p(self.tri_pmf), _p(self.tri_alias)
+        if self.env is not None:
+            s.env_rgba, s.env_h, s.env_w = _p(self.env), self.env.shape[0], self.env.shape[1]
+        if self.env_pmf is not None and len(self.env_pmf):
+            s.env_pmf, s.env_alias, s.num_env_texels = _p(self.env_pmf), _p(self.env_alias), len(self.env_pmf)
+            s.env_tw, s.env_th = self.env.shape[1], self.env.shape[0]
+        if self.punctual is not None and len(self.punctual):
+            s.punctual, s.num_punctual = _p(self.punctual), len(self.punctual)
+        s.camera_frame = _p(self.camera_frame)
+        s.width, s.height = self.width, self.height
+        return s
+
+
+class Oracle:
+    def __init__(self):
+        if not os.path.exists(ORACLE_SO):
+            build()
+        self.L = C.CDLL(ORACLE_SO)
+
+    def build_bvh(self, vertices, faces):
+        v = np.ascontiguousarray(vertices, VERTEX)
+        f = np.ascontiguousarray(faces, FACE).copy()
+        nodes = np.zeros(max(1, 2 * len(f)), NODE)
+        nn, depth = C.c_uint32(), C.c_uint32()
+        rc = self.L.oracle_build_bvh(_p(v), C.c_uint32(len(v)), _p(f), C.c_uint32(len(f)), _p(nodes),
+                                     C.c_uint32(len(nodes)), C.byref(nn), C.byref(depth))
+        assert rc == 0, rc
+        return nodes[:nn.value].copy(), f, depth.value
+
+    def alias_table(self, weights):
+        w = np.ascontiguousarray(weights, np.float32)
+        out = np.zeros(len(w), ALIAS)
+        rc = self.L.oracle_alias_table(_p(w), C.c_uint32(len(w)), _p(out))
+        return out if rc == 0 else np.zeros(0, ALIAS)
+
+    def emissive_tables(self, vertices, faces, materials):
+        f = np.ascontiguousarray(faces, FACE)
+        refs = np.zeros(len(f), EMREF)
+        pmf = np.zeros(len(f), np.float32)
+        alias = np.zeros(len(f), ALIAS)
+        cnt = C.c_uint32()
+        m = np.ascontiguousarray(materials)
+        self.L.oracle_emissive_tables(_p(np.ascontiguousarray(vertices, VERTEX)), _p(f), C.c_uint32(len(f)), _p(m),
+                                      C.c_uint32(len(m)), _p(refs), _p(pmf), _p(alias), C.byref(cnt))
+        return refs[:cnt.value].copy(), pmf, alias[:cnt.value].copy()
+
+    def env_tables(self, env):
+        if env is None:
+            return np.zeros(0, np.float32), np.zeros(0, ALIAS)
+        e = np.ascontiguousarray(env, np.float32)
+        h, w = e.shape[:2]
+        pmf = np.zeros(w * h, np.float32)
+        alias = np.zeros(w * h, ALIAS)
+        rc = self.L.oracle_env_tables(_p(e), C.c_int32(w), C.c_int32(h), _p(pmf), _p(alias))
+        if rc != 0:
+            return np.zeros(0, np.float32), np.zeros(0, ALIAS)
+        return pmf, alias
+
+    def camera_frame(self, camera):
+        out = np.zeros(16, np.float32)
+        self.L.oracle_camera_frame(_p(np.ascontiguousarray(camera)), _p(out))
+        return out
+
+    def sampler_stream(self, sampler, w, h, frame, spf, sif, ndims, pcg_seed=0):
+        out = np.zeros((h, w, ndims), np.float32)
+        self.L.oracle_sampler_stream(C.c_int32(sampler), C.c_int32(w), C.c_int32(h), C.c_uint32(frame),
+                                     C.c_int32(spf), C.c_int32(sif), C.c_uint32(ndims), C.c_uint32(pcg_seed), _p(out))
+        return out
+
+    def trace(self, nodes, vertices, faces, rays, any_hit=False):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = len(rays)
+        hits = np.zeros((n, 4), np.float32)
+        occ = np.zeros(n, np.uint8)
+        cnt = Counters()
+        self.L.oracle_trace(_p(nodes), _p(np.ascontiguousarray(vertices, VERTEX)), _p(np.ascontiguousarray(faces, FACE)),
+                            _p(rays), C.c_uint32(n), C.c_int32(1 if any_hit else 0), _p(hits), _p(occ), C.byref(cnt))
+        return (occ.astype(bool) if any_hit else hits), cnt.as_dict()
+
+    def bsdf_eval(self, materials, records):
+        rec = np.ascontiguousarray(records, np.float32)
+        out = np.zeros((len(rec), 4), np.float32)
+        m = np.ascontiguousarray(materials)
+        self.L.oracle_bsdf_eval(_p(m), C.c_uint32(len(m)), _p(rec), C.c_uint32(len(rec)), _p(out))
+        return out
+
+    def prepare(self, sa) -> Prepared:
+        """Build a SceneArrays (pathtracingtutorial_b200.scenes) with the oracle's own prep."""
+        nodes, faces, depth = self.build_bvh(sa.vertices, sa.faces)
+        refs, pmf, alias = self.emissive_tables(sa.vertices, faces, sa.materials)
+        env_pmf, env_alias = self.env_tables(sa.env)
+        cf = self.camera_frame(sa.camera)
+        env = None if sa.env is None else np.ascontiguousarray(sa.env, np.float32)
+        punct = getattr(sa, "punctual", None)
+        return Prepared(np.ascontiguousarray(sa.vertices, VERTEX), faces, np.ascontiguousarray(sa.materials), nodes,
+                        depth, refs, pmf, alias, env, env_pmf, env_alias, cf, int(sa.camera["width"]),
+                        int(sa.camera["height"]), punct)
+
+    def render(self, prep: Prepared, spf, max_depth, sampler, frames, first_frame=0, precision=64, rtl=1,
+               pcg_seed=0, row0=0, row_step=1, threads=0):
+        """precision 32: the reference's film (H, W, 4).  precision 64: (mean, var) of shape (H, W, 3)."""
+        sc = prep.struct()
+        a = RenderArgs(spf, max_depth, sampler, rtl, pcg_seed, first_frame, frames, row0, row_step, threads,
+                       precision, 0)
+        cnt = Counters()
+        h, w = prep.height, prep.width
+        if precision == 32:
+            out = np.zeros((h, w, 4), np.float32)
+            self.L.oracle_render(C.byref(sc), C.byref(a), _p(out), None, None, C.byref(cnt))
+            return out, cnt.as_dict()
+        mean = np.zeros((h, w, 3), np.float64)
+        var = np.zeros((h, w, 3), np.float64)
+        self.L.oracle_render(C.byref(sc), C.byref(a), None, _p(mean), _p(var), C.byref(cnt))
+        return (mean, var), cnt.as_dict()
+
+
+class RefHarness:
+    """The reference's own code, host compiled (requires oracle/_ref/libptref.so)."""
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REF_SO)
+
+    def __init__(self):
+        self.L = C.CDLL(REF_SO)
+
+    def layout(self):
+        out = np.zeros(256, np.int64)
+        n = self.L.ref_struct_layout(_p(out), C.c_int(256))
+        return out[:n]
+
+    def load_json(self, path):
+        counts = np.zeros(6, np.uint32)
+        cam = np.zeros(80, np.uint8)
+        settings = np.zeros(4, np.int32)
+        rc = self.L.ref_load_json(os.fsencode(path), _p(counts), _p(cam), _p(settings))
+        if rc != 0:
+            raise RuntimeError(f"reference loader failed on {path}")
+        nv, nf, nm, nl, ew, eh = (int(x) for x in counts)
+        v = np.zeros(nv, VERTEX)
+        f = np.zeros(nf, FACE)
+        m = np.zeros(nm * 256, np.uint8)
+        lights = np.zeros(nl * 112, np.uint8)
+        env = np.zeros((eh, ew, 4), np.float32) if ew else None
+        self.L.ref_loaded_arrays(_p(v), _p(f), _p(m), _p(lights), _p(env) if env is not None else None)
+        return {"vertices": v, "faces": f, "materials": m, "lights": lights, "env": env, "camera": cam,
+                "settings": settings}
+
+    def build(self, vertices, faces, materials, env=None):
+        v = np.ascontiguousarray(vertices, VERTEX)
+        f = np.ascontiguousarray(faces, FACE).copy()
+        m = np.ascontiguousarray(materials)
+        nm = m.nbytes // 256
+        ew, eh = (env.shape[1], env.shape[0]) if env is not None else (0, 0)
+        e = np.ascontiguousarray(env, np.float32) if env is not None else None
+        nodes = np.zeros(max(1, 2 * len(f)), NODE)
+        em = np.zeros(max(1, len(f)), EMREF)
+        tp = np.zeros(max(1, len(f)), np.float32)
+        ta = np.zeros(max(1, len(f)), ALIAS)
+        ep = np.zeros(max(1, ew * eh), np.float32)
+        ea = np.zeros(max(1, ew * eh), ALIAS)
+        sizes = np.zeros(5, np.uint32)
+        rc = self.L.ref_build(_p(v), C.c_uint32(len(v)), _p(f), C.c_uint32(len(f)), _p(m), C.c_uint32(nm), _p(e),
+                              C.c_int(ew), C.c_int(eh), _p(nodes), C.c_uint32(len(nodes)), _p(em), _p(tp), _p(ta),
+                              _p(ep), _p(ea), _p(sizes))
+        assert rc == 0, rc
+        n_nodes, n_em, n_env = int(sizes[0]), int(sizes[1]), int(sizes[2])
+        return {"nodes": nodes[:n_nodes].copy(), "faces": f, "emissive": em[:n_em].copy(),
+                "tri_pmf": tp[:len(f)].copy(), "tri_alias": ta[:n_em].copy(), "env_pmf": ep[:n_env].copy(),
+                "env_alias": ea[:n_env].copy()}
+
+    def camera_frame(self, camera):
+        out = np.zeros(16, np.float32)
+        self.L.ref_camera_frame(_p(np.ascontiguousarray(camera)), _p(out))
+        return out
+
+    def sampler_stream(self, sampler, w, h, frame, spf, sif, ndims):
+        out = np.zeros((h, w, ndims), np.float32)
+        self.L.ref_sampler_stream(C.c_int(sampler), C.c_int(w), C.c_int(h), C.c_uint32(frame), C.c_int(spf),
+                                  C.c_int(sif), C.c_uint32(ndims), _p(out))
+        return out
+
+    def trace(self, nodes, vertices, faces, rays, any_hit=False):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = len(rays)
+        hits = np.zeros((n, 4), np.float32)
+        occ = np.zeros(n, np.uint8)
+        self.L.ref_trace(_p(nodes), _p(np.ascontiguousarray(vertices, VERTEX)), _p(np.ascontiguousarray(faces, FACE)),
+                         _p(rays), C.c_uint32(n), C.c_int(1 if any_hit else 0), _p(hits), _p(occ))
+        return occ.astype(bool) if any_hit else hits
+
+    def render(self, vertices, faces, materials, camera, settings, env=None, lights=None, first_frame=0,
+               num_frames=1, row0=0, row_step=1, threads=0):
+        """kernelPathTrace over the selected rows.  Returns (acc, new, stats)."""
+        v = np.ascontiguousarray(vertices, VERTEX)
+        f = np.ascontiguousarray(faces, FACE)
+        m = np.ascontiguousarray(materials)
+        nm = m.nbytes // 256
+        cam = np.ascontiguousarray(camera)
+        w = int(np.frombuffer(cam.tobytes()[60:64], np.int32)[0])
+        h = int(np.frombuffer(cam.tobytes()[64:68], np.int32)[0])
+        ew, eh = (env.shape[1], env.shape[0]) if env is not None else (0, 0)
+        e = np.ascontiguousarray(env, np.float32) if env is not None else None
+        L = np.ascontiguousarray(lights) if lights is not None else None
+        nl = 0 if L is None else L.nbytes // 112
+        st = np.ascontiguousarray(settings, np.int32)
+        acc = np.zeros((h, w, 4), np.float32)
+        new = np.zeros((h, w, 4), np.float32)
+        stats = np.zeros(4, np.float64)
+        self.L.ref_render(_p(v), C.c_uint32(len(v)), _p(f), C.c_uint32(len(f)), _p(m), C.c_uint32(nm), _p(e),
+                          C.c_int(ew), C.c_int(eh), _p(L), C.c_uint32(nl), _p(cam), _p(st), C.c_uint32(first_frame),
+                          C.c_uint32(num_frames), C.c_int(row0), C.c_int(row_step), C.c_int(threads), _p(acc),
+                          _p(new), _p(stats))
+        return acc, new, {"closest_rays": stats[0], "shadow_rays": stats[1], "paths": stats[2], "seconds": stats[3]}

@@ -1,0 +1,449 @@
+"""pathtracingtutorial_b200 -- B200-native path tracer behind the reference's plugin API.
+
+Host-side mirror of Neroued/PathTracingTutorial Part_2's rendering interface
+over the C ABI of libpt_b200.so (include/pt_b200.h):
+
+  SceneManager   load / buildAccel / uploadToDevice / setSpp / setSampler
+                 (Part_2/src/scene/scene_manager.h:11-45)
+  PathIntegrator launch(film, scene, params) / name()   (Part_2/src/integrators/integrator.h:10-20,
+                 path_integrator.h:7-15)
+  Film           clear / download_accumulated            (Part_2/src/film/film.h:9-40)
+  Renderer       render_batch / render_all / save_image / download_current_image /
+                 run_convergence_benchmark / reset_accumulation (Part_2/src/renderer.h:17-55)
+  render(scene, spp) -> HDR image (H, W, 4) float32
+
+Every compute call runs on the GPU through the CUDA library; there is no CPU
+fallback -- the library raises when it is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import (ALIAS_DTYPE, BVH_NODE_DTYPE, CAMERA_DTYPE, EMISSIVE_DTYPE, FACE_DTYPE, HIT_DTYPE,
+                   MATERIAL_DTYPE, PUNCTUAL_DTYPE, VERTEX_DTYPE, PTError, check, lib, ptr)
+from ._ffi import SAMPLER_PCG, SAMPLER_SOBOL, FLAG_WATERTIGHT, FLAG_STAGE_TIMING, FLAG_NO_GRAPH, \
+    FLAG_COUNT_TRAVERSAL, ARGS_LTR, ARGS_RTL
+
+__all__ = ["SceneManager", "PathIntegrator", "Film", "Renderer", "render", "default_material", "make_camera",
+           "trace_closest", "trace_any", "sampler_stream", "bsdf_eval", "write_hdr", "read_hdr",
+           "compute_rmse", "rmse_to_db", "PTError", "VERTEX_DTYPE", "FACE_DTYPE", "MATERIAL_DTYPE",
+           "CAMERA_DTYPE", "PUNCTUAL_DTYPE", "BVH_NODE_DTYPE", "SAMPLER_PCG", "SAMPLER_SOBOL",
+           "FLAG_WATERTIGHT", "FLAG_STAGE_TIMING", "FLAG_NO_GRAPH", "FLAG_COUNT_TRAVERSAL",
+           "ARGS_LTR", "ARGS_RTL"]
+
+# Order in which nvcc's device code evaluates the two sampler draws that the
+# reference takes inside one argument list; the kernels default to it so that
+# they consume dimensions as the reference's GPU build does.
+DEVICE_ARG_ORDER = ARGS_LTR
+
+
+def default_material(**kw) -> np.ndarray:
+    """One Material with the reference's defaults (Part_2/src/materials/material.h:8-75)."""
+    m = np.zeros((), MATERIAL_DTYPE)
+    m["base_color"] = (0.8, 0.8, 0.8)
+    m["roughness"] = 0.5
+    m["sheen_tint"] = 0.5
+    m["clearcoat_roughness"] = 0.03
+    m["ior"] = 1.5
+    m["specular_factor"] = 1.0
+    m["specular_color_r"] = m["specular_color_g"] = m["specular_color_b"] = 1.0
+    m["normal_scale"] = 1.0
+    m["emissive_strength"] = 1.0
+    m["base_alpha"] = 1.0
+    m["sheen_color_r"] = m["sheen_color_g"] = m["sheen_color_b"] = 1.0
+    m["occlusion_strength"] = 1.0
+    m["attenuation_distance"] = 1e30
+    m["att_color_r"] = m["att_color_g"] = m["att_color_b"] = 1.0
+    m["uv_scale_x"] = m["uv_scale_y"] = 1.0
+    for k in ("base_color_tex", "metallic_roughness_tex", "normal_tex", "emissive_tex", "occlusion_tex",
+              "clearcoat_tex", "clearcoat_roughness_tex", "clearcoat_normal_tex", "transmission_tex",
+              "sheen_color_tex", "sheen_roughness_tex"):
+        m[k] = -1
+    for k, v in kw.items():
+        m[k] = v
+    return m
+
+
+def make_camera(position=(0, 0, 4), look_at=(0, 0, 0), up=(0, 1, 0), fov=90.0, aperture=0.0,
+                focal_distance=10.0, width=1600, height=1600) -> np.ndarray:
+    """Camera with the reference's defaults (Part_2/src/camera/camera.h:12-21)."""
+    c = np.zeros((), CAMERA_DTYPE)
+    c["position"], c["look_at"], c["up"] = position, look_at, up
+    c["fov"], c["aperture"], c["focal_distance"] = fov, aperture, focal_distance
+    c["width"], c["height"] = width, height
+    return c
+
+
+class SceneManager:
+    """Scene handle: load or create, buildAccel (host prep), uploadToDevice."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+
+    # -- construction --
+    @classmethod
+    def load(cls, path: str) -> "SceneManager":
+        h = C.c_void_p()
+        check(lib().pt_scene_load_json(os.fsencode(path), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_arrays(cls, vertices: np.ndarray, faces: np.ndarray, materials: np.ndarray,
+                    camera: np.ndarray | None = None, env_rgba: np.ndarray | None = None) -> "SceneManager":
+        v = np.ascontiguousarray(vertices, dtype=VERTEX_DTYPE)
+        f = np.ascontiguousarray(faces, dtype=FACE_DTYPE)
+        m = np.ascontiguousarray(np.atleast_1d(materials), dtype=MATERIAL_DTYPE)
+        cam = None if camera is None else np.ascontiguousarray(camera, dtype=CAMERA_DTYPE)
+        env = None
+        ew = eh = 0
+        if env_rgba is not None:
+            env = np.ascontiguousarray(env_rgba, dtype=np.float32)
+            if env.ndim != 3 or env.shape[2] != 4:
+                raise ValueError("env_rgba must be (H, W, 4)")
+            eh, ew = env.shape[:2]
+        h = C.c_void_p()
+        check(lib().pt_scene_create(ptr(v), len(v), ptr(f), len(f), ptr(m), len(m),
+                                    ptr(cam) if cam is not None else None, ptr(env) if env is not None else None,
+                                    ew, eh, C.byref(h)))
+        return cls(h)
+
+    def close(self) -> None:
+        if self._h:
+            lib().pt_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # -- settings (SceneManager::setSpp / setSampler / setMaxDepth) --
+    def settings(self) -> _ffi.RenderSettings:
+        s = _ffi.RenderSettings()
+        check(lib().pt_scene_get_render_settings(self._h, C.byref(s)))
+        return s
+
+    def update_settings(self, **kw) -> None:
+        s = self.settings()
+        for k, v in kw.items():
+            setattr(s, k, int(v))
+        check(lib().pt_scene_set_render_settings(self._h, C.byref(s)))
+
+    def set_spp(self, spp: int) -> None:
+        self.update_settings(spp=spp)
+
+    def set_sampler(self, sampler: int | str) -> None:
+        if isinstance(sampler, str):
+            sampler = {"pcg": SAMPLER_PCG, "sobol": SAMPLER_SOBOL}[sampler]
+        self.update_settings(sampler_type=sampler)
+
+    def set_max_depth(self, depth: int) -> None:
+        self.update_settings(max_depth=depth)
+
+    @property
+    def camera(self) -> np.ndarray:
+        c = np.zeros((), CAMERA_DTYPE)
+        check(lib().pt_scene_get_camera(self._h, ptr(c)))
+        return c
+
+    def update_camera(self, cam: np.ndarray) -> None:
+        c = np.ascontiguousarray(cam, dtype=CAMERA_DTYPE)
+        check(lib().pt_scene_set_camera(self._h, ptr(c)))
+
+    def set_punctual_lights(self, lights: np.ndarray) -> None:
+        L = np.ascontiguousarray(lights, dtype=PUNCTUAL_DTYPE)
+        check(lib().pt_scene_set_punctual_lights(self._h, ptr(L), len(L)))
+
+    # -- prep / upload --
+    def build_accel(self) -> None:
+        check(lib().pt_scene_build_accel(self._h))
+
+    def upload_to_device(self, device: int = 0) -> None:
+        check(lib().pt_scene_upload(self._h, device))
+
+    def info(self) -> dict:
+        i = _ffi.SceneInfo()
+        check(lib().pt_scene_info_get(self._h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in i._fields_}
+
+    def build_params(self) -> _ffi.SceneParams:
+        p = _ffi.SceneParams()
+        check(lib().pt_scene_build_params(self._h, C.byref(p)))
+        return p
+
+    # -- read back prep results --
+    def vertices(self) -> np.ndarray:
+        out = np.zeros(self.info()["num_vertices"], VERTEX_DTYPE)
+        check(lib().pt_scene_get_vertices(self._h, ptr(out), len(out)))
+        return out
+
+    def faces(self) -> np.ndarray:
+        out = np.zeros(self.info()["num_faces"], FACE_DTYPE)
+        check(lib().pt_scene_get_faces(self._h, ptr(out), len(out)))
+        return out
+
+    def materials(self) -> np.ndarray:
+        out = np.zeros(self.info()["num_materials"], MATERIAL_DTYPE)
+        check(lib().pt_scene_get_materials(self._h, ptr(out), len(out)))
+        return out
+
+    def bvh_nodes(self) -> np.ndarray:
+        out = np.zeros(self.info()["num_bvh_nodes"], BVH_NODE_DTYPE)
+        check(lib().pt_scene_get_bvh(self._h, ptr(out), len(out)))
+        return out
+
+    def emissive_tables(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        info = self.info()
+        refs = np.zeros(info["num_emissive_triangles"], EMISSIVE_DTYPE)
+        pmf = np.zeros(info["num_faces"] if info["num_bvh_nodes"] else 0, np.float32)
+        alias = np.zeros(info["num_emissive_triangles"], ALIAS_DTYPE)
+        check(lib().pt_scene_get_emissive(self._h, ptr(refs), len(refs), ptr(pmf), len(pmf), ptr(alias), len(alias)))
+        return refs, pmf, alias
+
+    def env_tables(self) -> tuple[np.ndarray, np.ndarray]:
+        info = self.info()
+        n = info["env_width"] * info["env_height"]
+        pmf = np.zeros(n, np.float32)
+        alias = np.zeros(n, ALIAS_DTYPE)
+        rc = lib().pt_scene_get_env_tables(self._h, ptr(pmf), ptr(alias), n)
+        check(rc)
+        return pmf, alias
+
+
+class Film:
+    """Device film: compensated accumulation + the last launch's mean."""
+
+    def __init__(self, width: int, height: int, device: int = 0):
+        self.width, self.height, self.device = width, height, device
+        h = C.c_void_p()
+        check(lib().pt_film_create(width, height, device, C.byref(h)))
+        self._h = h
+
+    def clear(self) -> None:
+        check(lib().pt_film_clear(self._h))
+
+    def download_accumulated(self) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        check(lib().pt_film_download(self._h, ptr(out)))
+        return out
+
+    def download_new(self) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        check(lib().pt_film_download_new(self._h, ptr(out)))
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            lib().pt_film_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PathIntegrator:
+    """The "Path" integrator plugin (Integrator::launch / name)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        check(lib().pt_integrator_create(b"path", C.byref(h)))
+        self._h = h
+
+    def name(self) -> str:
+        return lib().pt_integrator_name(self._h).decode()
+
+    def launch(self, film: Film, scene: SceneManager, params: _ffi.SceneParams, stream: int | None = None) -> None:
+        check(lib().pt_integrator_launch(self._h, film._h, scene.handle, C.byref(params),
+                                         C.c_void_p(stream) if stream else None))
+
+    def stats(self) -> dict:
+        s = _ffi.RenderStats()
+        check(lib().pt_integrator_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def reset_stats(self) -> None:
+        check(lib().pt_integrator_reset_stats(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            lib().pt_integrator_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Renderer:
+    """Batch loop over the integrator (Renderer, Part_2/src/renderer.h:17-55)."""
+
+    def __init__(self, scene: SceneManager, integrator: PathIntegrator | None = None, device: int = 0,
+                 stream: int | None = None):
+        self.scene = scene
+        self.integrator = integrator or PathIntegrator()
+        cam = scene.camera
+        self.film = Film(int(cam["width"]), int(cam["height"]), device)
+        self.stream = stream
+        self.last_batch_ms = 0.0
+
+    def render_batch(self) -> int:
+        t0 = time.perf_counter()
+        check(lib().pt_renderer_render_batch(self.integrator._h, self.film._h, self.scene.handle,
+                                             C.c_void_p(self.stream) if self.stream else None))
+        self.last_batch_ms = (time.perf_counter() - t0) * 1e3
+        return self.current_spp()
+
+    def current_spp(self) -> int:
+        return self.scene.info()["frame_count"] * self.scene.settings().sample_per_frame
+
+    def target_spp(self) -> int:
+        return self.scene.settings().spp
+
+    def is_complete(self) -> bool:
+        return self.current_spp() >= self.target_spp()
+
+    def render_all(self) -> None:
+        while not self.is_complete():
+            self.render_batch()
+        self.synchronize()
+
+    def synchronize(self) -> None:
+        import torch  # noqa: plumbing only
+        if torch.cuda.is_available():
+            torch.cuda.synchronize(self.film.device)
+
+    def reset_accumulation(self) -> None:
+        check(lib().pt_renderer_reset_accumulation(self.film._h, self.scene.handle))
+
+    def download_current_image(self) -> np.ndarray:
+        return self.film.download_accumulated()
+
+    def save_image(self, path: str) -> None:
+        write_hdr(path, self.download_current_image())
+
+    def run_convergence_benchmark(self, ref: np.ndarray, checkpoints: list[int]) -> list[dict]:
+        """RMSE / PSNR at spp checkpoints (Renderer::runConvergenceBenchmark, renderer.cu:138-173)."""
+        self.reset_accumulation()
+        out = []
+        nxt = 0
+        t0 = time.perf_counter()
+        while nxt < len(checkpoints):
+            spp = self.render_batch()
+            if spp >= checkpoints[nxt]:
+                img = self.download_current_image()
+                ms = (time.perf_counter() - t0) * 1e3
+                rmse = compute_rmse(img, ref)
+                out.append({"spp": spp, "rmse": rmse, "psnr": rmse_to_db(rmse), "time_ms": ms})
+                nxt += 1
+        return out
+
+
+def render(scene: SceneManager, spp: int, stats: bool = False):
+    """render(scene, spp) -> HDR image (H, W, 4) float32 (and the render stats)."""
+    cam = scene.camera
+    out = np.zeros((int(cam["height"]), int(cam["width"]), 4), np.float32)
+    st = _ffi.RenderStats()
+    check(lib().pt_render(scene.handle, int(spp), ptr(out), 0, C.byref(st)))
+    return (out, st.as_dict()) if stats else out
+
+
+# ---- diagnostics over the same kernels ----
+def trace_closest(scene: SceneManager, origins: np.ndarray, dirs: np.ndarray) -> np.ndarray:
+    rays = _pack_rays(origins, dirs, None)
+    hits = np.zeros(len(rays), HIT_DTYPE)
+    check(lib().pt_trace_closest(scene.handle, ptr(rays), len(rays), ptr(hits), 0))
+    return hits
+
+
+def trace_any(scene: SceneManager, origins: np.ndarray, dirs: np.ndarray, tmax: np.ndarray) -> np.ndarray:
+    rays = _pack_rays(origins, dirs, tmax)
+    occ = np.zeros(len(rays), np.uint8)
+    check(lib().pt_trace_any(scene.handle, ptr(rays), len(rays), ptr(occ), 0))
+    return occ.astype(bool)
+
+
+def _pack_rays(o: np.ndarray, d: np.ndarray, tmax: np.ndarray | None) -> np.ndarray:
+    o = np.asarray(o, np.float32).reshape(-1, 3)
+    d = np.asarray(d, np.float32).reshape(-1, 3)
+    r = np.zeros((len(o), 8), np.float32)
+    r[:, 0:3] = o
+    r[:, 4:7] = d
+    r[:, 7] = np.float32(np.finfo(np.float32).max) if tmax is None else np.asarray(tmax, np.float32)
+    return np.ascontiguousarray(r)
+
+
+def sampler_stream(sampler: int, width: int, height: int, frame: int, spf: int, sample_in_frame: int,
+                   ndims: int, pcg_seed: int = 0, device: int = 0) -> np.ndarray:
+    out = np.zeros((height, width, ndims), np.float32)
+    check(lib().pt_sampler_stream(sampler, width, height, frame, spf, sample_in_frame, ndims, pcg_seed, device,
+                                  ptr(out)))
+    return out
+
+
+def bsdf_eval(scene: SceneManager, records: np.ndarray) -> np.ndarray:
+    """records: (n, 13) = material index, wo, wi, N, T.  Returns (n, 4) = f*|N.L| rgb, pdf."""
+    rec = np.ascontiguousarray(records, np.float32)
+    out = np.zeros((len(rec), 4), np.float32)
+    check(lib().pt_bsdf_eval(scene.handle, ptr(rec), len(rec), ptr(out)))
+    return out
+
+
+# ---- quality metrics (Part_2/src/film/quality_metrics.h:20-39) ----
+def compute_rmse(img: np.ndarray, ref: np.ndarray, channels: int = 3) -> float:
+    d = img[..., :channels].astype(np.float64) - ref[..., :channels].astype(np.float64)
+    return float(np.sqrt(np.mean(d * d))) if d.size else 0.0
+
+
+def rmse_to_db(rmse: float) -> float:
+    return 100.0 if rmse <= 0.0 else -20.0 * math.log10(rmse)
+
+
+# ---- Radiance RGBE files ----
+def write_hdr(path: str, img: np.ndarray, flip_y: bool = True) -> None:
+    """Write (H, W, 3|4) float radiance as flat RGBE; rows flipped like ImageIO::write's default."""
+    rgb = np.asarray(img, np.float32)[..., :3]
+    if flip_y:
+        rgb = rgb[::-1]
+    h, w = rgb.shape[:2]
+    v = rgb.max(axis=2)
+    mant, expo = np.frexp(v)
+    scale = np.where(v > 1e-32, mant * 256.0 / np.where(v > 1e-32, v, 1.0), 0.0)
+    out = np.zeros((h, w, 4), np.uint8)
+    out[..., :3] = np.clip(rgb * scale[..., None], 0, 255).astype(np.uint8)
+    out[..., 3] = np.where(v > 1e-32, expo + 128, 0).astype(np.uint8)
+    with open(path, "wb") as f:
+        f.write(b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n")
+        f.write(f"-Y {h} +X {w}\n".encode())
+        f.write(out.tobytes())
+
+
+def read_hdr(path: str) -> np.ndarray:
+    """Read a flat (non-RLE) RGBE file as written by write_hdr -> (H, W, 4)."""
+    with open(path, "rb") as f:
+        data = f.read()
+    head, _, rest = data.partition(b"\n\n")
+    line, _, pix = rest.partition(b"\n")
+    _, hh, _, ww = line.split()
+    h, w = int(hh), int(ww)
+    px = np.frombuffer(pix[: h * w * 4], np.uint8).reshape(h, w, 4).astype(np.float32)
+    scale = np.where(px[..., 3] > 0, np.ldexp(1.0, px[..., 3].astype(np.int32) - 136), 0.0)
+    out = np.ones((h, w, 4), np.float32)
+    out[..., :3] = px[..., :3] * scale[..., None]
+    return out

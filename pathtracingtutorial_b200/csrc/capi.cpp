@@ -1,0 +1,425 @@
+// capi.cpp -- the extern "C" boundary (include/pt_b200.h).
+//
+// Mirrors the reference's host flow SceneManager::load -> buildAccel ->
+// uploadToDevice -> Renderer::renderAll -> download
+// (Part_2/src/main.cpp:69-78,148-149), but every entry point returns a status
+// code instead of exiting, and the library owns all device memory.
+#include <algorithm>
+#include <cctype>
+#include <cstring>
+#include <exception>
+#include <mutex>
+#include <new>
+#include <unordered_map>
+
+#include "device_api.h"
+#include "engine.h"
+
+namespace ptb {
+
+static thread_local std::string g_error;
+void set_error(const std::string& msg) { g_error = msg; }
+const std::string& get_error() { return g_error; }
+
+}  // namespace ptb
+
+using namespace ptb;
+
+#define PT_GUARD_BEGIN try {
+#define PT_GUARD_END                                                   \
+    }                                                                  \
+    catch (const std::bad_alloc&) { set_error("host allocation failed"); return PT_ERR_NOMEM; } \
+    catch (const std::exception& e) { set_error(e.what()); return PT_ERR_INVALID; }
+
+#define PT_REQUIRE(cond, msg) do { if (!(cond)) { set_error(msg); return PT_ERR_INVALID; } } while (0)
+
+namespace {
+
+// Per-scene render state reused by pt_render (film + integrator).
+struct RenderCache {
+    pt_film*       film = nullptr;
+    pt_integrator* integ = nullptr;
+};
+
+std::mutex g_cache_mu;
+std::unordered_map<pt_scene*, RenderCache>& caches() {
+    static std::unordered_map<pt_scene*, RenderCache> m;
+    return m;
+}
+
+void drop_cache(pt_scene* s) {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto it = caches().find(s);
+    if (it == caches().end()) return;
+    if (it->second.film) { film_free(it->second.film); delete it->second.film; }
+    if (it->second.integ) { integrator_free(it->second.integ); delete it->second.integ; }
+    caches().erase(it);
+}
+
+template <typename T>
+int copy_out(const std::vector<T>& v, T* out, uint32_t cap) {
+    PT_REQUIRE(out || v.empty(), "null output");
+    PT_REQUIRE(cap >= v.size(), "output capacity too small");
+    if (!v.empty()) std::memcpy(out, v.data(), v.size() * sizeof(T));
+    return PT_OK;
+}
+
+void invalidate_build(pt_scene* s) {
+    s->tables = SceneTables{};
+    if (s->dev.uploaded || s->dev.device >= 0) free_scene_device(s);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pt_last_error(void) { return get_error().c_str(); }
+const char* pt_version(void) { return "pt_b200 1.0 (sm_100a wavefront path tracer)"; }
+
+int pt_build_camera_frame(const pt_camera* cam, pt_camera_frame* out) {
+    PT_REQUIRE(cam && out, "null argument");
+    *out = camera_frame(*cam);
+    return PT_OK;
+}
+
+int pt_scene_load_json(const char* path, pt_scene** out) {
+    PT_REQUIRE(path && out, "null argument");
+    PT_GUARD_BEGIN
+    pt_scene* s = new pt_scene();
+    s->host.camera = default_camera();
+    s->host.settings = default_settings();
+    if (!load_json_scene(path, s->host)) {
+        const std::string msg = get_error();
+        delete s;
+        set_error(msg);
+        return PT_ERR_IO;
+    }
+    *out = s;
+    return PT_OK;
+    PT_GUARD_END
+}
+
+int pt_scene_create(const pt_vertex* vertices, uint32_t num_vertices, const pt_face* faces, uint32_t num_faces,
+                    const pt_material* materials, uint32_t num_materials, const pt_camera* camera,
+                    const float* env_rgba, int32_t env_width, int32_t env_height, pt_scene** out) {
+    PT_REQUIRE(out, "null output handle");
+    PT_REQUIRE(num_vertices == 0 || vertices, "vertices is null");
+    PT_REQUIRE(num_faces == 0 || faces, "faces is null");
+    PT_REQUIRE(num_materials == 0 || materials, "materials is null");
+    PT_REQUIRE(env_width >= 0 && env_height >= 0, "negative environment size");
+    PT_REQUIRE((env_width == 0) == (env_height == 0), "environment width and height must both be zero or positive");
+    PT_REQUIRE(env_width == 0 || env_rgba, "environment data is null");
+    PT_GUARD_BEGIN
+    pt_scene* s = new pt_scene();
+    s->host.vertices.assign(vertices, vertices + num_vertices);
+    s->host.faces.assign(faces, faces + num_faces);
+    s->host.materials.assign(materials, materials + num_materials);
+    if (s->host.materials.empty()) s->host.materials.push_back(default_material());
+    s->host.camera = camera ? *camera : default_camera();
+    s->host.settings = default_settings();
+    if (env_width > 0) {
+        s->host.env_w = env_width;
+        s->host.env_h = env_height;
+        s->host.env_rgba.assign(env_rgba, env_rgba + static_cast<size_t>(env_width) * env_height * 4);
+    }
+    *out = s;
+    return PT_OK;
+    PT_GUARD_END
+}
+
+int pt_scene_destroy(pt_scene* scene) {
+    if (!scene) return PT_OK;
+    drop_cache(scene);
+    free_scene_device(scene);
+    delete scene;
+    return PT_OK;
+}
+
+int pt_scene_set_punctual_lights(pt_scene* s, const pt_punctual_light* lights, uint32_t n) {
+    PT_REQUIRE(s && (n == 0 || lights), "null argument");
+    PT_REQUIRE(n <= 64, "at most 64 punctual lights are supported");
+    s->host.punctual.assign(lights, lights + n);
+    if (s->dev.uploaded) free_scene_device(s);
+    return PT_OK;
+}
+
+int pt_scene_set_render_settings(pt_scene* s, const pt_render_settings* st) {
+    PT_REQUIRE(s && st, "null argument");
+    PT_REQUIRE(st->sample_per_frame > 0, "sample_per_frame must be positive");
+    PT_REQUIRE(st->max_depth >= 0, "max_depth must be non-negative");
+    PT_REQUIRE(st->sampler_type == PT_SAMPLER_PCG || st->sampler_type == PT_SAMPLER_SOBOL, "unknown sampler");
+    PT_REQUIRE(st->arg_order == PT_ARGS_LTR || st->arg_order == PT_ARGS_RTL, "unknown arg order");
+    s->host.settings = *st;
+    return PT_OK;
+}
+
+int pt_scene_get_render_settings(const pt_scene* s, pt_render_settings* st) {
+    PT_REQUIRE(s && st, "null argument");
+    *st = s->host.settings;
+    return PT_OK;
+}
+
+int pt_scene_set_camera(pt_scene* s, const pt_camera* cam) {
+    PT_REQUIRE(s && cam, "null argument");
+    PT_REQUIRE(cam->width > 0 && cam->height > 0, "camera resolution must be positive");
+    s->host.camera = *cam;
+    return PT_OK;
+}
+
+int pt_scene_get_camera(const pt_scene* s, pt_camera* cam) {
+    PT_REQUIRE(s && cam, "null argument");
+    *cam = s->host.camera;
+    return PT_OK;
+}
+
+int pt_scene_build_accel(pt_scene* s) {
+    PT_REQUIRE(s, "null scene");
+    PT_GUARD_BEGIN
+    if (s->tables.built) return PT_OK;   // faces are already in BVH order
+    const HostScene& h = s->host;
+    for (size_t i = 0; i < h.faces.size(); ++i) {
+        const pt_face& f = h.faces[i];
+        if (f.material_id < 0 || f.material_id >= static_cast<int>(h.materials.size())) {
+            set_error("face " + std::to_string(i) + " has material id " + std::to_string(f.material_id) +
+                      " outside [0, " + std::to_string(h.materials.size()) + ")");
+            return PT_ERR_INVALID;
+        }
+    }
+    invalidate_build(s);
+    SceneTables& t = s->tables;
+    if (!build_bvh(s->host.vertices, s->host.faces, t.bvh, t.bvh_depth)) return PT_ERR_INVALID;
+    if (t.bvh_depth >= static_cast<uint32_t>(kStackDepth)) {
+        set_error("BVH depth " + std::to_string(t.bvh_depth) + " exceeds the traversal stack (" +
+                  std::to_string(kStackDepth) + ")");
+        return PT_ERR_INVALID;
+    }
+    build_emissive_tables(s->host, t);
+    build_env_tables(s->host, t);
+    if (!build_traversal_layout(s->host, t)) return PT_ERR_INVALID;
+    t.built = true;
+    return PT_OK;
+    PT_GUARD_END
+}
+
+int pt_scene_upload(pt_scene* s, int32_t device) {
+    PT_REQUIRE(s, "null scene");
+    PT_REQUIRE(device >= 0, "device must be >= 0");
+    PT_GUARD_BEGIN
+    drop_cache(s);
+    return upload_scene(s, device);
+    PT_GUARD_END
+}
+
+int pt_scene_info_get(const pt_scene* s, pt_scene_info* info) {
+    PT_REQUIRE(s && info, "null argument");
+    std::memset(info, 0, sizeof(*info));
+    info->num_vertices = static_cast<uint32_t>(s->host.vertices.size());
+    info->num_faces = static_cast<uint32_t>(s->host.faces.size());
+    info->num_materials = static_cast<uint32_t>(s->host.materials.size());
+    info->num_bvh_nodes = static_cast<uint32_t>(s->tables.bvh.size());
+    info->num_emissive_triangles = static_cast<uint32_t>(s->tables.emissive.size());
+    info->num_punctual_lights = static_cast<uint32_t>(s->host.punctual.size());
+    info->env_width = s->host.env_w;
+    info->env_height = s->host.env_h;
+    info->bvh_max_depth = s->tables.bvh_depth;
+    info->num_inner_nodes = static_cast<uint32_t>(s->tables.inner.size());
+    info->num_leaves = s->tables.num_leaves;
+    info->frame_count = s->frame_count;
+    info->device_bytes = s->dev.bytes;
+    return PT_OK;
+}
+
+int pt_scene_build_params(const pt_scene* s, pt_scene_params* out) {
+    PT_REQUIRE(s && out, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    out->camera = camera_frame(s->host.camera);
+    out->width = s->host.camera.width;
+    out->height = s->host.camera.height;
+    out->sample_per_frame = s->host.settings.sample_per_frame;
+    out->target_samples = s->host.settings.spp;
+    out->max_depth = s->host.settings.max_depth;
+    out->sampler_type = s->host.settings.sampler_type;
+    return PT_OK;
+}
+
+int pt_scene_get_vertices(const pt_scene* s, pt_vertex* out, uint32_t cap) {
+    PT_REQUIRE(s, "null scene");
+    return copy_out(s->host.vertices, out, cap);
+}
+int pt_scene_get_faces(const pt_scene* s, pt_face* out, uint32_t cap) {
+    PT_REQUIRE(s, "null scene");
+    return copy_out(s->host.faces, out, cap);
+}
+int pt_scene_get_materials(const pt_scene* s, pt_material* out, uint32_t cap) {
+    PT_REQUIRE(s, "null scene");
+    return copy_out(s->host.materials, out, cap);
+}
+int pt_scene_get_bvh(const pt_scene* s, pt_bvh_node* out, uint32_t cap) {
+    PT_REQUIRE(s, "null scene");
+    return copy_out(s->tables.bvh, out, cap);
+}
+int pt_scene_get_emissive(const pt_scene* s, pt_emissive_ref* refs, uint32_t cap_refs, float* face_pmf,
+                          uint32_t cap_pmf, pt_alias_entry* alias, uint32_t cap_alias) {
+    PT_REQUIRE(s, "null scene");
+    if (int rc = copy_out(s->tables.emissive, refs, cap_refs)) return rc;
+    if (int rc = copy_out(s->tables.tri_pmf, face_pmf, cap_pmf)) return rc;
+    return copy_out(s->tables.tri_alias, alias, cap_alias);
+}
+int pt_scene_get_env_tables(const pt_scene* s, float* pmf, pt_alias_entry* alias, uint32_t cap) {
+    PT_REQUIRE(s, "null scene");
+    if (int rc = copy_out(s->tables.env_pmf, pmf, cap)) return rc;
+    return copy_out(s->tables.env_alias, alias, cap);
+}
+
+// ---- film ----
+int pt_film_create(int32_t width, int32_t height, int32_t device, pt_film** out) {
+    PT_REQUIRE(out && width > 0 && height > 0 && device >= 0, "invalid film arguments");
+    PT_GUARD_BEGIN
+    pt_film* f = new pt_film();
+    f->width = width; f->height = height; f->device = device;
+    if (int rc = film_alloc(f)) { film_free(f); delete f; return rc; }
+    *out = f;
+    return PT_OK;
+    PT_GUARD_END
+}
+int pt_film_destroy(pt_film* f) {
+    if (!f) return PT_OK;
+    film_free(f);
+    delete f;
+    return PT_OK;
+}
+int pt_film_clear(pt_film* f) {
+    PT_REQUIRE(f, "null film");
+    return film_clear(f);
+}
+int pt_film_download(const pt_film* f, float* host_rgba) {
+    PT_REQUIRE(f && host_rgba, "null argument");
+    return film_download(f, host_rgba, false, true);
+}
+int pt_film_download_new(const pt_film* f, float* host_rgba) {
+    PT_REQUIRE(f && host_rgba, "null argument");
+    return film_download(f, host_rgba, true, true);
+}
+
+// ---- integrator ----
+int pt_integrator_create(const char* name, pt_integrator** out) {
+    PT_REQUIRE(out, "null output handle");
+    const std::string n = name ? name : "path";
+    std::string low = n;
+    std::transform(low.begin(), low.end(), low.begin(), [](unsigned char c) { return static_cast<char>(std::tolower(c)); });
+    if (low != "path") { set_error("unknown integrator '" + n + "' (available: path)"); return PT_ERR_INVALID; }
+    PT_GUARD_BEGIN
+    *out = new pt_integrator();
+    return PT_OK;
+    PT_GUARD_END
+}
+int pt_integrator_destroy(pt_integrator* integ) {
+    if (!integ) return PT_OK;
+    integrator_free(integ);
+    delete integ;
+    return PT_OK;
+}
+const char* pt_integrator_name(const pt_integrator* integ) { return integ ? integ->name.c_str() : ""; }
+
+int pt_integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scene_params* params,
+                         void* stream) {
+    PT_REQUIRE(integ && film && s && params, "null argument");
+    PT_GUARD_BEGIN
+    return integrator_launch(integ, film, s, params, stream);
+    PT_GUARD_END
+}
+int pt_integrator_stats(const pt_integrator* integ, pt_render_stats* out) {
+    PT_REQUIRE(integ && out, "null argument");
+    return integrator_stats(integ, out);
+}
+int pt_integrator_reset_stats(pt_integrator* integ) {
+    PT_REQUIRE(integ, "null argument");
+    return integrator_reset_stats(integ);
+}
+
+// ---- renderer ----
+int pt_renderer_render_batch(pt_integrator* integ, pt_film* film, pt_scene* s, void* stream) {
+    PT_REQUIRE(integ && film && s, "null argument");
+    pt_scene_params prm;
+    pt_scene_build_params(s, &prm);
+    if (int rc = pt_integrator_launch(integ, film, s, &prm, stream)) return rc;
+    s->frame_count++;
+    return PT_OK;
+}
+int pt_renderer_reset_accumulation(pt_film* film, pt_scene* s) {
+    PT_REQUIRE(film && s, "null argument");
+    s->frame_count = 0;
+    return film_clear(film);
+}
+
+int pt_render(pt_scene* s, int32_t spp, float* out_rgba, int32_t out_is_device, pt_render_stats* stats) {
+    PT_REQUIRE(s && out_rgba, "null argument");
+    PT_REQUIRE(spp > 0, "spp must be positive");
+    PT_GUARD_BEGIN
+    if (!s->tables.built) {
+        if (int rc = pt_scene_build_accel(s)) return rc;
+    }
+    if (!s->dev.uploaded) {
+        int dev = 0;
+        if (int rc = current_device(&dev)) return rc;
+        if (int rc = upload_scene(s, dev)) return rc;
+    }
+    const int dev = s->dev.device;
+    const int w = s->host.camera.width, h = s->host.camera.height;
+    PT_REQUIRE(w > 0 && h > 0, "camera resolution must be positive");
+    RenderCache rcache;
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        rcache = caches()[s];
+    }
+    if (rcache.film && (rcache.film->width != w || rcache.film->height != h || rcache.film->device != dev)) {
+        film_free(rcache.film); delete rcache.film; rcache.film = nullptr;
+    }
+    if (!rcache.film) {
+        if (int rc = pt_film_create(w, h, dev, &rcache.film)) return rc;
+    }
+    if (!rcache.integ) {
+        if (int rc = pt_integrator_create("path", &rcache.integ)) return rc;
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        caches()[s] = rcache;
+    }
+    if (int rc = pt_renderer_reset_accumulation(rcache.film, s)) return rc;
+    pt_integrator_reset_stats(rcache.integ);
+    const int spf = s->host.settings.sample_per_frame;
+    // Renderer::renderAll: whole batches until frameCount * spf >= spp
+    while (static_cast<int64_t>(s->frame_count) * spf < spp) {
+        if (int rc = pt_renderer_render_batch(rcache.integ, rcache.film, s, nullptr)) return rc;
+    }
+    if (int rc = integrator_check(rcache.integ, true)) return rc;
+    if (int rc = film_download(rcache.film, out_rgba, false, out_is_device == 0)) return rc;
+    if (stats) integrator_stats(rcache.integ, stats);
+    return device_sync(dev);
+    PT_GUARD_END
+}
+
+// ---- diagnostics ----
+int pt_trace_closest(pt_scene* s, const float* rays, uint32_t n, pt_hit* hits, int32_t ptrs_are_device) {
+    PT_REQUIRE(s && (n == 0 || (rays && hits)), "null argument");
+    return trace_rays(s, rays, n, hits, nullptr, false, ptrs_are_device != 0);
+}
+int pt_trace_any(pt_scene* s, const float* rays, uint32_t n, uint8_t* occluded, int32_t ptrs_are_device) {
+    PT_REQUIRE(s && (n == 0 || (rays && occluded)), "null argument");
+    return trace_rays(s, rays, n, nullptr, occluded, true, ptrs_are_device != 0);
+}
+int pt_sampler_stream(int32_t sampler_type, int32_t width, int32_t height, uint32_t frame_count,
+                      int32_t sample_per_frame, int32_t sample_in_frame, uint32_t ndims, uint32_t pcg_seed,
+                      int32_t device, float* out_host) {
+    PT_REQUIRE(out_host, "null output");
+    PT_REQUIRE(width > 0 && height > 0 && sample_per_frame > 0 && ndims > 0, "invalid sizes");
+    PT_REQUIRE(sampler_type == PT_SAMPLER_PCG || sampler_type == PT_SAMPLER_SOBOL, "unknown sampler");
+    return sampler_stream(sampler_type, width, height, frame_count, sample_per_frame, sample_in_frame, ndims,
+                          pcg_seed, device, out_host);
+}
+int pt_bsdf_eval(pt_scene* s, const float* in, uint32_t n, float* out_host) {
+    PT_REQUIRE(s && (n == 0 || (in && out_host)), "null argument");
+    return bsdf_eval(s, in, n, out_host);
+}
+
+}  // extern "C"

@@ -1,0 +1,31 @@
+// device_api.h -- host functions implemented in integrator.cu (CUDA side),
+// called by the C ABI layer in capi.cpp.
+#pragma once
+
+#include "engine.h"
+
+namespace ptb {
+
+DeviceScene device_view(const pt_scene* s);
+void free_scene_device(pt_scene* s);
+int  upload_scene(pt_scene* s, int device);
+
+int  film_alloc(pt_film* f);
+void film_free(pt_film* f);
+int  film_clear(pt_film* f);
+int  film_download(const pt_film* f, float* dst, bool fresh, bool host_ptr);
+
+void integrator_free(pt_integrator* integ);
+int  integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scene_params* prm, void* stream);
+int  integrator_check(pt_integrator* integ, bool sync);
+int  integrator_stats(const pt_integrator* integ, pt_render_stats* out);
+int  integrator_reset_stats(pt_integrator* integ);
+
+int  trace_rays(pt_scene* s, const float* rays, uint32_t n, pt_hit* hits, uint8_t* occl, bool any, bool device_ptrs);
+int  sampler_stream(int type, int w, int h, uint32_t frame, int spf, int sif, uint32_t ndims, uint32_t seed,
+                    int device, float* out_host);
+int  bsdf_eval(pt_scene* s, const float* in, uint32_t n, float* out_host);
+int  current_device(int* dev);
+int  device_sync(int device);
+
+}  // namespace ptb

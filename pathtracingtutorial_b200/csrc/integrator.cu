@@ -1,0 +1,1153 @@
+// integrator.cu -- wavefront path-tracing integrator for sm_100a.
+//
+// Replaces the reference's megakernel kernelPathTrace/pathTrace
+// (Part_2/src/integrators/path.cu:31-255) by stages over structure-of-arrays
+// queues; one sample pass covers every pixel once:
+//
+//   raygen   camera rays for all pixels               (path.cu:31-59, 217-225)
+//   extend   closest-hit traversal of the ray queue   (bvh_traversal.cuh:43-96)
+//   shade    miss/emission MIS, NEE sampling, BSDF sampling, Russian roulette
+//            -> next ray queue + shadow queue         (path.cu:69-199,
+//                                                      direct_lighting.cuh:55-249)
+//   shadow   any-hit traversal of the shadow queue; visible contributions are
+//            added to per-(path, light slot) accumulators (one writer each, so
+//            the result is deterministic)           (bvh_traversal.cuh:98-133)
+//   finalize per-sample firefly clamp and compensated (Neumaier) FP32
+//            accumulation into the film              (path.cu:201-204, 228-241)
+//
+// Kernels grid-stride over a queue length that lives in device memory, so a
+// whole batch (sample_per_frame passes x max_depth bounces) is a fixed launch
+// sequence that is captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "bsdf.h"
+#include "traverse.h"
+
+namespace ptb {
+
+#define PT_CU(call)                                                                      \
+    do {                                                                                 \
+        cudaError_t e__ = (call);                                                        \
+        if (e__ != cudaSuccess) {                                                        \
+            set_error(std::string("CUDA error: ") + cudaGetErrorString(e__) + " in " #call); \
+            return PT_ERR_CUDA;                                                          \
+        }                                                                                \
+    } while (0)
+
+enum StatIdx {
+    kStatCameraRays = 0, kStatExtRays, kStatShadowRays, kStatNodes, kStatTris,
+    kStatShadowNodes, kStatShadowTris, kStatPaths, kStatCount
+};
+
+struct PassState { uint32_t frame; uint32_t pad[3]; };
+
+struct WaveParams {
+    DeviceScene scene;
+    pt_camera_frame cam;
+    int      width, height, npix;
+    int      spf, max_depth, sampler_type, arg_rtl, flags;
+    uint32_t pcg_seed;
+    int      n_slots;
+    uint32_t* queue[2];
+    float4*  ray_o[2];
+    float4*  ray_d[2];
+    float4*  hit;
+    float4*  thr;       // xyz throughput, w last BSDF pdf
+    float4*  lo;        // xyz radiance from emission / env hits, w last-was-delta
+    uint32_t* rng;      // sobol dimension or pcg state
+    float4*  nee;       // n_slots x npix visible NEE contributions
+    uint32_t* sq_path;
+    float4*  sq_o;      // w = slot (bits)
+    float4*  sq_d;      // w = tmax
+    float4*  sq_c;
+    uint32_t* counts;   // [0], [1] path queues, [2] shadow queue
+    unsigned long long* stats;
+    uint32_t* err;
+    PassState* pass;
+    float4*  f_sum;
+    float4*  f_comp;
+    float4*  f_batch;
+    float4*  f_new;
+};
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
+    const uint32_t active = __activemask();
+    const uint32_t ballot = __ballot_sync(active, want);
+    if (!want) return 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(ballot) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(ballot)));
+    base = __shfl_sync(ballot, base, leader);
+    return base + static_cast<uint32_t>(__popc(ballot & ((1u << lane) - 1u)));
+}
+
+__device__ __forceinline__ f3 f3of(float4 v) { return mk(v.x, v.y, v.z); }
+__device__ __forceinline__ float4 f4of(f3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+
+// Equirectangular mapping (Part_2/src/lights/envmap.h:15-33).
+__device__ __forceinline__ void spherical_uv(f3 d, float& u, float& v) {
+    u = atan2f(d.z, d.x) * kInv2Pi + 0.5f;
+    v = 1.0f - (asinf(d.y) * kInvPi + 0.5f);
+}
+__device__ __forceinline__ f3 dir_from_uv(float u, float v) {
+    const float phi = (u - 0.5f) * kTwoPi;
+    const float theta = v * kPi;
+    const float st = sinf(theta);
+    return normalize(mk(cosf(phi) * st, cosf(theta), sinf(phi) * st));
+}
+// Environment radiance: hardware bilinear lookup (wrap, normalized) x 2*pi
+// (envmap.h:36-45; the reference samples the same texture configuration).
+__device__ __forceinline__ f3 env_radiance(const DeviceScene& s, f3 d) {
+    if (s.env_tex == 0) return mk(0.0f);
+    float u, v;
+    spherical_uv(d, u, v);
+    const float4 c = tex2D<float4>(static_cast<cudaTextureObject_t>(s.env_tex), u, v);
+    return mk(c.x, c.y, c.z) * kTwoPi;
+}
+__device__ __forceinline__ bool has_env_light(const DeviceScene& s) {
+    return s.env_tex != 0 && s.env_alias != nullptr && s.num_env_texels > 0 && s.env_w > 0 && s.env_h > 0;
+}
+// environmentPdf (Part_2/src/lights/light_pdf.cuh:12-29)
+__device__ float env_pdf(const DeviceScene& s, f3 d) {
+    if (s.env_tex == 0 || s.env_pmf == nullptr || s.num_env_texels == 0 || s.env_w <= 0 || s.env_h <= 0) return 0.0f;
+    float u, v;
+    spherical_uv(d, u, v);
+    const int x = static_cast<int>(clampf(u * s.env_w, 0.0f, static_cast<float>(s.env_w - 1)));
+    const int y = static_cast<int>(clampf(v * s.env_h, 0.0f, static_cast<float>(s.env_h - 1)));
+    const float st = sqrtf(fmaxf(0.0f, 1.0f - d.y * d.y));
+    if (st <= 1e-5f) return 0.0f;
+    return __ldg(s.env_pmf + (y * s.env_w + x)) * static_cast<float>(s.env_w * s.env_h) / (kTwoPi * kPi * st);
+}
+__device__ __forceinline__ f3 vpos(const DeviceScene& s, uint32_t i) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(s.vertices + i));
+    return mk(a.x, a.y, a.z);
+}
+__device__ __forceinline__ f3 vnrm(const DeviceScene& s, uint32_t i) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(s.vertices + i) + 1);
+    return mk(a.x, a.y, a.z);
+}
+__device__ __forceinline__ pt_face load_face(const DeviceScene& s, uint32_t i) {
+    const uint4 f = __ldg(reinterpret_cast<const uint4*>(s.faces + i));
+    pt_face r; r.v0 = f.x; r.v1 = f.y; r.v2 = f.z; r.material_id = static_cast<int32_t>(f.w);
+    return r;
+}
+// emissiveTrianglePdf (light_pdf.cuh:31-54)
+__device__ float emissive_pdf(const DeviceScene& s, int prim, float dist, f3 dir) {
+    if (prim < 0 || prim >= static_cast<int>(s.num_faces) || s.tri_light_pmf == nullptr) return 0.0f;
+    const float pmf = __ldg(s.tri_light_pmf + prim);
+    if (pmf <= 0.0f) return 0.0f;
+    const pt_face f = load_face(s, prim);
+    const f3 p0 = vpos(s, f.v0), p1 = vpos(s, f.v1), p2 = vpos(s, f.v2);
+    const f3 c = cross(p1 - p0, p2 - p0);
+    const float area = 0.5f * length(c);
+    if (area <= 0.0f) return 0.0f;
+    const float cl = fabsf(dot(normalize(c), -dir));
+    if (cl <= 1e-5f) return 0.0f;
+    return pmf * dist * dist / (area * cl);
+}
+__device__ __forceinline__ uint32_t sample_alias(const pt_alias_entry* t, uint32_t n, float u1, float u2) {
+    uint32_t i = static_cast<uint32_t>(u1 * n);
+    if (i >= n) i = n - 1;
+    const float2 e = __ldg(reinterpret_cast<const float2*>(t + i));
+    return (u2 < e.x) ? i : __float_as_uint(e.y);
+}
+// evaluateDirectLight (direct_lighting.cuh:204-218) without the visibility term.
+__device__ __forceinline__ f3 direct_term(const MatEval& me, f3 wo, f3 wi, f3 n, f3 radiance, float light_pdf) {
+    const BsdfEval b = disney_eval(me, wo, wi, n, true);
+    if (b.pdf <= 0.0f) return mk(0.0f);
+    const float mis = power_heuristic(light_pdf, b.pdf);
+    return radiance * b.f * (mis / (light_pdf + 1e-7f));
+}
+
+__device__ __forceinline__ void emit_shadow(const WaveParams& P, bool want, uint32_t path, uint32_t slot,
+                                            f3 o, f3 d, float tmax, f3 c) {
+    const uint32_t j = warp_append(P.counts + 2, want);
+    if (!want) return;
+    const uint32_t cap = static_cast<uint32_t>(P.npix) * static_cast<uint32_t>(P.n_slots);
+    if (j >= cap) { atomicOr(P.err, kErrQueueOverflow); return; }
+    P.sq_path[j] = path;
+    P.sq_o[j] = make_float4(o.x, o.y, o.z, __uint_as_float(slot));
+    P.sq_d[j] = make_float4(d.x, d.y, d.z, tmax);
+    P.sq_c[j] = make_float4(c.x, c.y, c.z, 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+__global__ void k_begin(PassState* ps, uint32_t frame) { ps->frame = frame; }
+
+__global__ void __launch_bounds__(256) k_raygen(WaveParams P, int sample_in_frame) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.counts[0] = static_cast<uint32_t>(P.npix);
+        P.counts[1] = 0;
+        P.counts[2] = 0;
+        atomicAdd(P.stats + kStatPaths, static_cast<unsigned long long>(P.npix));
+    }
+    const uint32_t frame = P.pass->frame;
+    const uint32_t sidx = frame * static_cast<uint32_t>(P.spf) + static_cast<uint32_t>(sample_in_frame);
+    const pt_camera_frame& c = P.cam;
+    const f3 fwd = ld3(c.forward), rgt = ld3(c.right), cup = ld3(c.up), pos0 = ld3(c.position);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.npix; p += gridDim.x * blockDim.x) {
+        const int x = p % P.width, y = p / P.width;
+        PathRng rng;
+        rng.type = P.sampler_type; rng.px = x; rng.py = y; rng.sample_index = sidx;
+        rng.s = (P.sampler_type == PT_SAMPLER_SOBOL) ? 0u
+                : pcg_seed(x, y, frame, static_cast<uint32_t>(sample_in_frame), P.pcg_seed);
+        const float jx = rng_next(rng);
+        const float jy = rng_next(rng);
+        const float u = (2.0f * (x + jx) / P.width - 1.0f) * c.tan_half_fov * c.aspect;
+        const float v = (2.0f * (y + jy) / P.height - 1.0f) * c.tan_half_fov;
+        f3 pos = pos0;
+        f3 dir = normalize(u * rgt + v * cup + fwd);
+        if (c.aperture > 0.0f) {
+            const f3 focal = pos + dir * (c.focal_distance / dot(dir, fwd));
+            const float lx = rng_next(rng);
+            const float ly = rng_next(rng);
+            const float r = sqrtf(lx) * c.aperture;
+            const float th = kTwoPi * ly;
+            pos = pos + rgt * (r * cosf(th)) + cup * (r * sinf(th));
+            dir = normalize(focal - pos);
+        }
+        dir = normalize(dir);
+        P.queue[0][p] = static_cast<uint32_t>(p);
+        P.ray_o[0][p] = f4of(pos, 0.0f);
+        P.ray_d[0][p] = f4of(dir, 0.0f);
+        P.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        P.lo[p] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        P.rng[p] = rng.s;
+        for (int k = 0; k < P.n_slots; ++k) P.nee[static_cast<size_t>(k) * P.npix + p] = make_float4(0, 0, 0, 0);
+    }
+}
+
+__device__ __forceinline__ void warp_count(unsigned long long* dst, uint32_t v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(__activemask(), v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, static_cast<unsigned long long>(v));
+}
+
+__global__ void __launch_bounds__(128) k_extend(WaveParams P, int q, int depth) {
+    const uint32_t n = P.counts[q];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.counts[q ^ 1] = 0;
+        P.counts[2] = 0;
+        atomicAdd(P.stats + (depth == 0 ? kStatCameraRays : kStatExtRays), static_cast<unsigned long long>(n));
+    }
+    const bool watertight = (P.flags & PT_FLAG_WATERTIGHT) != 0;
+    const bool count = (P.flags & PT_FLAG_COUNT_TRAVERSAL) != 0;
+    uint32_t err = 0;
+    TraceCounters tc{0, 0};
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const float4* __restrict__ ro = P.ray_o[q];
+    const float4* __restrict__ rd = P.ray_d[q];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float4 o = ro[i];
+        const float4 d = rd[i];
+        const RayInv r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+        float t, u, v;
+        const int prim = trace_closest(P.scene, r, watertight, t, u, v, err, tc);
+        P.hit[i] = make_float4(t, __int_as_float(prim), u, v);
+    }
+    if (err) atomicOr(P.err, err);
+    if (count) {
+        warp_count(P.stats + kStatNodes, tc.inner);
+        warp_count(P.stats + kStatTris, tc.tris);
+    }
+}
+
+// One bounce of pathTrace (path.cu:69-199) for path p.  Returns true when the
+// path continues with ray (no, nd).
+__device__ bool shade_path(const WaveParams& P, int depth, bool last, uint32_t p, f3 ro, f3 rd, float4 h,
+                           f3& T, float& last_pdf, bool& last_delta, f3& L, PathRng& rng, f3& no, f3& nd) {
+    const DeviceScene& s = P.scene;
+    const int prim = __float_as_int(h.y);
+    if (prim < 0) {
+        const f3 env = env_radiance(s, rd);
+        if (!is_zero(env)) {
+            float w = 1.0f;
+            if (depth > 0 && !last_delta) w = power_heuristic(last_pdf, env_pdf(s, rd));
+            L += T * env * w;
+        }
+        return false;
+    }
+    const float t = h.x, bu = h.z, bv = h.w;
+    const pt_face f = load_face(s, static_cast<uint32_t>(prim));
+    const f3 hp = ro + t * rd;
+    const float bw = 1.0f - bu - bv;
+    const f3 n = normalize(bw * vnrm(s, f.v0) + bu * vnrm(s, f.v1) + bv * vnrm(s, f.v2));
+    const pt_material& m = s.materials[f.material_id];
+    bool entering = dot(n, rd) < 0.0f;
+    f3 gn;
+    if (m.double_sided && !entering) { gn = -n; entering = true; }
+    else gn = entering ? n : -n;
+    const f3 wo = -rd;
+    const f3 N = gn;   // no normal map without textures
+    if (material_emits(m)) {
+        float w = 1.0f;
+        if (depth > 0 && !last_delta) w = power_heuristic(last_pdf, emissive_pdf(s, prim, t, rd));
+        L += T * material_emission(m) * w;
+        return false;
+    }
+    // alpha (path.cu:136-158); untextured: MASK alpha is 1, BLEND alpha is baseAlpha
+    if (m.alpha_mode == 1) {
+        if (1.0f < m.alpha_cutoff) { no = hp + rd * 1e-4f; nd = normalize(rd); return true; }
+    } else if (m.alpha_mode == 2) {
+        if (rng_next(rng) >= m.base_alpha) { no = hp + rd * 1e-4f; nd = normalize(rd); return true; }
+    }
+    const MatEval me = resolve_material(m);
+    const bool delta_surface = (me.metallic >= 1.0f && me.roughness < 0.01f) ||
+                               (me.spec_trans >= 1.0f && me.roughness < 0.01f);
+    if (!delta_surface) {
+        const bool has_area = s.num_emissive > 0 && s.emissive != nullptr;
+        const bool has_env = has_env_light(s);
+        // area light sample (sampleAreaLight, direct_lighting.cuh:75-121)
+        if (has_area) {
+            float u1, u2;
+            rng_pair(rng, P.arg_rtl, u1, u2);
+            const uint32_t li = sample_alias(s.tri_alias, s.num_emissive, u1, u2);
+            const uint32_t tri = __ldg(&s.emissive[li].triangle_index);
+            const float pmf = __ldg(&s.emissive[li].selection_pmf);
+            const pt_face lf = load_face(s, tri);
+            const float tu = rng_next(rng);
+            const float tv = rng_next(rng);
+            const f3 p0 = vpos(s, lf.v0), p1 = vpos(s, lf.v1), p2 = vpos(s, lf.v2);
+            const float su0 = sqrtf(tu);
+            const float b0 = 1.0f - su0, b1 = tv * su0, b2 = 1.0f - b0 - b1;
+            const f3 lp = p0 * b0 + p1 * b1 + p2 * b2;
+            f3 ln = normalize(vnrm(s, lf.v0) * b0 + vnrm(s, lf.v1) * b1 + vnrm(s, lf.v2) * b2);
+            if (length(ln) == 0.0f) ln = normalize(cross(p1 - p0, p2 - p0));
+            const f3 to = lp - hp;
+            const float d2 = dot(to, to);
+            bool ok = d2 > 1e-8f;
+            float dist = 0.0f, pdf = 0.0f;
+            f3 wi = mk(0.0f), contrib = mk(0.0f);
+            if (ok) {
+                dist = sqrtf(d2);
+                wi = to / dist;
+                ok = fmaxf(0.0f, dot(N, wi)) > 0.0f;
+            }
+            if (ok) {
+                const float area = 0.5f * length(cross(p1 - p0, p2 - p0));
+                const float cl = fabsf(dot(ln, -wi));
+                ok = area > 0.0f && cl > 1e-5f;
+                if (ok) {
+                    pdf = (pmf / area) * d2 / cl;
+                    ok = pdf > 0.0f;
+                }
+            }
+            if (ok) {
+                const f3 le = material_emission(s.materials[lf.material_id]);
+                contrib = T * direct_term(me, wo, wi, N, le, pdf);
+                ok = !is_zero(contrib);
+            }
+            const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
+            emit_shadow(P, ok, p, 0, hp + N * (1e-4f * sg), normalize(wi), dist - 1e-3f, contrib);
+        }
+        // environment sample (sampleEnvironmentLight, direct_lighting.cuh:123-154)
+        if (has_env) {
+            float u1, u2;
+            rng_pair(rng, P.arg_rtl, u1, u2);
+            const uint32_t texel = sample_alias(s.env_alias, s.num_env_texels, u1, u2);
+            const int x = static_cast<int>(texel % static_cast<uint32_t>(s.env_w));
+            const int y = static_cast<int>(texel / static_cast<uint32_t>(s.env_w));
+            float j1, j2;
+            rng_pair(rng, P.arg_rtl, j1, j2);
+            const float uu = (static_cast<float>(x) + j1) / static_cast<float>(s.env_w);
+            const float vv = (static_cast<float>(y) + j2) / static_cast<float>(s.env_h);
+            const f3 wi = dir_from_uv(uu, vv);
+            bool ok = fmaxf(0.0f, dot(N, wi)) > 0.0f;
+            float pdf = 0.0f;
+            f3 contrib = mk(0.0f);
+            if (ok) { pdf = env_pdf(s, wi); ok = pdf > 0.0f; }
+            if (ok) {
+                contrib = T * direct_term(me, wo, wi, N, env_radiance(s, wi), pdf);
+                ok = !is_zero(contrib);
+            }
+            const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
+            emit_shadow(P, ok, p, 1, hp + N * (1e-4f * sg), normalize(wi), FLT_MAX, contrib);
+        }
+        // punctual lights, no MIS (evaluatePunctualLights, direct_lighting.cuh:158-200)
+        for (uint32_t j = 0; j < s.num_punctual; ++j) {
+            const pt_punctual_light& pl = s.punctual[j];
+            f3 wi;
+            float dist = FLT_MAX;
+            f3 inten;
+            bool ok = true;
+            if (pl.type == 0 || pl.type == 2) {
+                const f3 to = ld3(pl.position) - hp;
+                const float d2 = dot(to, to);
+                ok = !(d2 < 1e-8f);
+                dist = sqrtf(d2);
+                wi = to / dist;
+                float att = dist >= pl.range ? 0.0f : 1.0f / (dist * dist + 1e-7f);
+                if (pl.type == 2) {
+                    const float ca = dot(normalize(-to), ld3(pl.direction));
+                    float sa;
+                    if (ca < pl.outer_cone) sa = 0.0f;
+                    else if (ca > pl.inner_cone) sa = 1.0f;
+                    else { const float tt = (ca - pl.outer_cone) / (pl.inner_cone - pl.outer_cone + 1e-7f); sa = tt * tt; }
+                    att *= sa;
+                }
+                inten = ld3(pl.color) * (pl.intensity * att);
+            } else {
+                wi = -ld3(pl.direction);
+                inten = ld3(pl.color) * pl.intensity;
+            }
+            f3 contrib = mk(0.0f);
+            if (ok) ok = dot(N, wi) > 0.0f;
+            if (ok) {
+                contrib = T * (inten * disney_eval(me, wo, wi, N, true).f);
+                ok = !is_zero(contrib);
+            }
+            const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
+            const float tmax = dist < FLT_MAX ? dist - 1e-3f : FLT_MAX;
+            emit_shadow(P, ok, p, 2 + j, hp + N * (1e-4f * sg), normalize(wi), tmax, contrib);
+        }
+    }
+    if (last) return false;   // the sampled continuation would never be traced
+    const BsdfSample bs = disney_sample(me, wo, N, rng, P.arg_rtl, entering);
+    if (!bs.valid) return false;
+    T *= bs.weight;
+    const bool transmitted = dot(bs.wi, gn) < 0.0f;
+    const f3 off = transmitted ? -gn : gn;
+    no = hp + off * 1e-4f;
+    nd = normalize(bs.wi);
+    if (transmitted && me.thickness > 0.0f && me.att_distance < 1e20f) {
+        const float th = me.thickness, ad = me.att_distance;
+        const f3 ac = me.att_color;
+        T *= mk(expf(-th * fmaxf(-logf(fmaxf(ac.x, 1e-6f)), 0.0f) / ad),
+                expf(-th * fmaxf(-logf(fmaxf(ac.y, 1e-6f)), 0.0f) / ad),
+                expf(-th * fmaxf(-logf(fmaxf(ac.z, 1e-6f)), 0.0f) / ad));
+    }
+    last_pdf = bs.pdf;
+    last_delta = bs.delta;
+    if (depth > 2) {
+        const float surv = fminf(max3(T), 0.95f);
+        if (rng_next(rng) >= surv) return false;
+        T = T / surv;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(128) k_shade(WaveParams P, int q, int depth, int sample_in_frame) {
+    const uint32_t n = P.counts[q];
+    const uint32_t sidx = P.pass->frame * static_cast<uint32_t>(P.spf) + static_cast<uint32_t>(sample_in_frame);
+    const bool last = depth == P.max_depth - 1;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t cap = static_cast<uint32_t>(P.npix);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t p = P.queue[q][i];
+        const float4 o4 = P.ray_o[q][i];
+        const float4 d4 = P.ray_d[q][i];
+        const float4 h = P.hit[i];
+        const float4 thr = P.thr[p];
+        const float4 lo = P.lo[p];
+        f3 T = f3of(thr);
+        float last_pdf = thr.w;
+        bool last_delta = lo.w != 0.0f;
+        f3 L = f3of(lo);
+        PathRng rng;
+        rng.type = P.sampler_type;
+        rng.px = static_cast<int>(p % static_cast<uint32_t>(P.width));
+        rng.py = static_cast<int>(p / static_cast<uint32_t>(P.width));
+        rng.sample_index = sidx;
+        rng.s = P.rng[p];
+        f3 no = mk(0.0f), nd = mk(0.0f);
+        const bool cont = shade_path(P, depth, last, p, f3of(o4), f3of(d4), h, T, last_pdf, last_delta, L, rng, no, nd)
+                          && !last;
+        P.thr[p] = f4of(T, last_pdf);
+        P.lo[p] = f4of(L, last_delta ? 1.0f : 0.0f);
+        P.rng[p] = rng.s;
+        const uint32_t j = warp_append(P.counts + (q ^ 1), cont);
+        if (cont) {
+            if (j < cap) {
+                P.queue[q ^ 1][j] = p;
+                P.ray_o[q ^ 1][j] = f4of(no, 0.0f);
+                P.ray_d[q ^ 1][j] = f4of(nd, 0.0f);
+            } else {
+                atomicOr(P.err, kErrQueueOverflow);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) k_shadow(WaveParams P) {
+    const uint32_t n = P.counts[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        atomicAdd(P.stats + kStatShadowRays, static_cast<unsigned long long>(n));
+    const bool watertight = (P.flags & PT_FLAG_WATERTIGHT) != 0;
+    const bool count = (P.flags & PT_FLAG_COUNT_TRAVERSAL) != 0;
+    uint32_t err = 0;
+    TraceCounters tc{0, 0};
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float4 o = P.sq_o[i];
+        const float4 d = P.sq_d[i];
+        const RayInv r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+        if (!trace_any(P.scene, r, d.w, watertight, err, tc)) {
+            const uint32_t slot = __float_as_uint(o.w);
+            const uint32_t path = P.sq_path[i];
+            float4* acc = P.nee + static_cast<size_t>(slot) * P.npix + path;
+            const float4 c = P.sq_c[i];
+            float4 a = *acc;
+            a.x += c.x; a.y += c.y; a.z += c.z;
+            *acc = a;
+        }
+    }
+    if (err) atomicOr(P.err, err);
+    if (count) {
+        warp_count(P.stats + kStatShadowNodes, tc.inner);
+        warp_count(P.stats + kStatShadowTris, tc.tris);
+    }
+}
+
+__device__ __forceinline__ void neumaier(float& s, float& c, float x) {
+    const float t = s + x;
+    if (fabsf(s) >= fabsf(x)) c += (s - t) + x;
+    else c += (x - t) + s;
+    s = t;
+}
+
+__global__ void __launch_bounds__(256) k_finalize(WaveParams P) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.npix; p += gridDim.x * blockDim.x) {
+        f3 L = f3of(P.lo[p]);
+        for (int k = 0; k < P.n_slots; ++k) L += f3of(P.nee[static_cast<size_t>(k) * P.npix + p]);
+        // per-sample firefly clamp (path.cu:201-204); fminf maps NaN to the clamp value as the reference does
+        L = mk(fminf(L.x, 100.0f), fminf(L.y, 100.0f), fminf(L.z, 100.0f));
+        float4 s = P.f_sum[p], c = P.f_comp[p];
+        neumaier(s.x, c.x, L.x);
+        neumaier(s.y, c.y, L.y);
+        neumaier(s.z, c.z, L.z);
+        s.w += 1.0f;
+        P.f_sum[p] = s;
+        P.f_comp[p] = c;
+        float4 b = P.f_batch[p];
+        b.x += L.x; b.y += L.y; b.z += L.z;
+        P.f_batch[p] = b;
+    }
+}
+
+__global__ void k_batch_resolve(WaveParams P) {
+    const float inv_spf = static_cast<float>(P.spf);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.npix; p += gridDim.x * blockDim.x) {
+        const float4 b = P.f_batch[p];
+        P.f_new[p] = make_float4(b.x / inv_spf, b.y / inv_spf, b.z / inv_spf, 1.0f);
+        P.f_batch[p] = make_float4(0, 0, 0, 0);
+    }
+}
+
+__global__ void k_film_mean(const float4* sum, const float4* comp, float4* out, int n) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const float4 s = sum[p], c = comp[p];
+        if (s.w > 0.0f) out[p] = make_float4((s.x + c.x) / s.w, (s.y + c.y) / s.w, (s.z + c.z) / s.w, 1.0f);
+        else out[p] = make_float4(0, 0, 0, 0);
+    }
+}
+
+// ---- diagnostics ----
+__global__ void k_trace_rays(DeviceScene s, const float* rays, uint32_t n, pt_hit* hits, uint8_t* occl,
+                             int any, int watertight, uint32_t* err_out) {
+    uint32_t err = 0;
+    TraceCounters tc{0, 0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 o = reinterpret_cast<const float4*>(rays)[2 * i];
+        const float4 d = reinterpret_cast<const float4*>(rays)[2 * i + 1];
+        const RayInv r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+        if (any) {
+            occl[i] = trace_any(s, r, d.w, watertight != 0, err, tc) ? 1 : 0;
+        } else {
+            pt_hit h;
+            h.prim = trace_closest(s, r, watertight != 0, h.t, h.u, h.v, err, tc);
+            hits[i] = h;
+        }
+    }
+    if (err) atomicOr(err_out, err);
+}
+
+__global__ void k_sampler_stream(int type, int w, int h, uint32_t frame, int spf, int sif, uint32_t ndims,
+                                 uint32_t seed, float* out) {
+    const int npix = w * h;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        PathRng r;
+        r.type = type; r.px = p % w; r.py = p / w;
+        r.sample_index = frame * static_cast<uint32_t>(spf) + static_cast<uint32_t>(sif);
+        r.s = type == PT_SAMPLER_SOBOL ? 0u : pcg_seed(r.px, r.py, frame, static_cast<uint32_t>(sif), seed);
+        for (uint32_t k = 0; k < ndims; ++k) out[static_cast<size_t>(p) * ndims + k] = rng_next(r);
+    }
+}
+
+__global__ void k_bsdf_eval(const pt_material* mats, uint32_t nmat, const float* in, uint32_t n, float* out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* r = in + static_cast<size_t>(i) * 13;
+        const uint32_t mi = static_cast<uint32_t>(r[0]);
+        float* o = out + static_cast<size_t>(i) * 4;
+        if (mi >= nmat) { o[0] = o[1] = o[2] = o[3] = 0.0f; continue; }
+        const MatEval me = resolve_material(mats[mi]);
+        const BsdfEval b = disney_eval(me, mk(r[1], r[2], r[3]), mk(r[4], r[5], r[6]), mk(r[7], r[8], r[9]), true);
+        o[0] = b.f.x; o[1] = b.f.y; o[2] = b.f.z; o[3] = b.pdf;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+struct Wavefront {
+    int device = -1;
+    cudaStream_t own_stream = nullptr;
+    int npix = 0, n_slots = 0;
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    WaveParams base{};
+    // graph cache
+    cudaGraphExec_t graph = nullptr;
+    std::vector<unsigned char> graph_key;
+    cudaStream_t graph_stream = nullptr;
+    // launch shapes
+    int sms = 0;
+    int grid_raygen = 0, grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_finalize = 0;
+    // stats
+    unsigned long long host_stats[kStatCount] = {};
+    double stage_ms[4] = {0, 0, 0, 0};
+    double total_ms = 0.0;
+    uint64_t extend_launches = 0;
+};
+
+namespace {
+
+template <typename T>
+T* carve(char*& cur, size_t count) {
+    const uintptr_t a = (reinterpret_cast<uintptr_t>(cur) + 255) & ~uintptr_t(255);
+    T* p = reinterpret_cast<T*>(a);
+    cur = reinterpret_cast<char*>(a + sizeof(T) * count);
+    return p;
+}
+
+int ensure_device(int device) {
+    int cur = -1;
+    PT_CU(cudaGetDevice(&cur));
+    if (cur != device) PT_CU(cudaSetDevice(device));
+    return PT_OK;
+}
+
+int grid_for(const void* kernel, int block, int sms) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+    return per_sm * sms;
+}
+
+// Size of the wavefront arena for npix paths and n_slots light slots.
+size_t arena_size(int npix, int n_slots) {
+    const size_t P = static_cast<size_t>(npix);
+    const size_t S = P * static_cast<size_t>(n_slots);
+    size_t b = 0;
+    b += 2 * (P * 4 + 256);          // queues
+    b += 4 * (P * 16 + 256);         // ray_o/ray_d x2
+    b += P * 16 + 256;               // hit
+    b += 2 * (P * 16 + 256);         // thr, lo
+    b += P * 4 + 256;                // rng
+    b += S * 16 + 256;               // nee
+    b += S * 4 + 256;                // sq_path
+    b += 3 * (S * 16 + 256);         // sq_o, sq_d, sq_c
+    b += 64 * 4 + 256;               // counts
+    b += kStatCount * 8 + 256;       // stats
+    b += 4 * 4 + 256;                // err
+    b += sizeof(PassState) + 256;
+    return b;
+}
+
+int wavefront_prepare(Wavefront& wf, int device, int npix, int n_slots) {
+    if (wf.device != device) {
+        if (wf.arena) { cudaSetDevice(wf.device); cudaFree(wf.arena); wf.arena = nullptr; wf.arena_bytes = 0; }
+        if (wf.graph) { cudaGraphExecDestroy(wf.graph); wf.graph = nullptr; wf.graph_key.clear(); }
+        if (wf.own_stream) { cudaStreamDestroy(wf.own_stream); wf.own_stream = nullptr; }
+        if (int rc = ensure_device(device)) return rc;
+        PT_CU(cudaStreamCreateWithFlags(&wf.own_stream, cudaStreamNonBlocking));
+        int sms = 0;
+        PT_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        wf.sms = sms;
+        wf.grid_raygen = grid_for(reinterpret_cast<const void*>(k_raygen), 256, sms);
+        wf.grid_extend = grid_for(reinterpret_cast<const void*>(k_extend), 128, sms);
+        wf.grid_shade = grid_for(reinterpret_cast<const void*>(k_shade), 128, sms);
+        wf.grid_shadow = grid_for(reinterpret_cast<const void*>(k_shadow), 128, sms);
+        wf.grid_finalize = grid_for(reinterpret_cast<const void*>(k_finalize), 256, sms);
+        wf.device = device;
+        wf.npix = 0;
+    } else if (int rc = ensure_device(device)) {
+        return rc;
+    }
+    if (wf.npix == npix && wf.n_slots == n_slots && wf.arena) return PT_OK;
+    std::memset(&wf.base, 0, sizeof(wf.base));
+    const size_t need = arena_size(npix, n_slots);
+    if (need > wf.arena_bytes) {
+        if (wf.arena) { cudaFree(wf.arena); wf.arena = nullptr; wf.arena_bytes = 0; }
+        if (cudaMalloc(&wf.arena, need) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cannot allocate " + std::to_string(need) + " bytes of wavefront state");
+            return PT_ERR_NOMEM;
+        }
+        wf.arena_bytes = need;
+    }
+    char* cur = static_cast<char*>(wf.arena);
+    WaveParams& b = wf.base;
+    const size_t P = static_cast<size_t>(npix), S = P * static_cast<size_t>(n_slots);
+    b.queue[0] = carve<uint32_t>(cur, P);
+    b.queue[1] = carve<uint32_t>(cur, P);
+    b.ray_o[0] = carve<float4>(cur, P);
+    b.ray_d[0] = carve<float4>(cur, P);
+    b.ray_o[1] = carve<float4>(cur, P);
+    b.ray_d[1] = carve<float4>(cur, P);
+    b.hit = carve<float4>(cur, P);
+    b.thr = carve<float4>(cur, P);
+    b.lo = carve<float4>(cur, P);
+    b.rng = carve<uint32_t>(cur, P);
+    b.nee = carve<float4>(cur, S);
+    b.sq_path = carve<uint32_t>(cur, S);
+    b.sq_o = carve<float4>(cur, S);
+    b.sq_d = carve<float4>(cur, S);
+    b.sq_c = carve<float4>(cur, S);
+    b.counts = carve<uint32_t>(cur, 64);
+    b.stats = carve<unsigned long long>(cur, kStatCount);
+    b.err = carve<uint32_t>(cur, 4);
+    b.pass = carve<PassState>(cur, 1);
+    PT_CU(cudaMemset(b.counts, 0, 64 * 4));
+    PT_CU(cudaMemset(b.stats, 0, kStatCount * 8));
+    PT_CU(cudaMemset(b.err, 0, 16));
+    PT_CU(cudaMemset(b.pass, 0, sizeof(PassState)));
+    wf.npix = npix;
+    wf.n_slots = n_slots;
+    if (wf.graph) { cudaGraphExecDestroy(wf.graph); wf.graph = nullptr; wf.graph_key.clear(); }
+    return PT_OK;
+}
+
+// Enqueue one batch (all sample passes) on `st`.  When `ev` is non-null,
+// stage events are recorded (ev holds pairs per launch: kind, start, stop).
+struct StageEvent { int kind; cudaEvent_t a, b; };
+
+int enqueue_batch(Wavefront& wf, const WaveParams& P, cudaStream_t st, std::vector<StageEvent>* ev) {
+    auto timed = [&](int kind, auto&& launch) -> int {
+        if (ev) {
+            StageEvent e{kind, nullptr, nullptr};
+            PT_CU(cudaEventCreate(&e.a));
+            PT_CU(cudaEventCreate(&e.b));
+            PT_CU(cudaEventRecord(e.a, st));
+            launch();
+            PT_CU(cudaEventRecord(e.b, st));
+            ev->push_back(e);
+        } else {
+            launch();
+        }
+        return PT_OK;
+    };
+    for (int i = 0; i < P.spf; ++i) {
+        if (int rc = timed(3, [&] { k_raygen<<<wf.grid_raygen, 256, 0, st>>>(P, i); })) return rc;
+        for (int d = 0; d < P.max_depth; ++d) {
+            const int q = d & 1;
+            if (int rc = timed(0, [&] { k_extend<<<wf.grid_extend, 128, 0, st>>>(P, q, d); })) return rc;
+            if (int rc = timed(1, [&] { k_shade<<<wf.grid_shade, 128, 0, st>>>(P, q, d, i); })) return rc;
+            if (int rc = timed(2, [&] { k_shadow<<<wf.grid_shadow, 128, 0, st>>>(P); })) return rc;
+        }
+        if (int rc = timed(3, [&] { k_finalize<<<wf.grid_finalize, 256, 0, st>>>(P); })) return rc;
+    }
+    if (int rc = timed(3, [&] { k_batch_resolve<<<wf.grid_finalize, 256, 0, st>>>(P); })) return rc;
+    PT_CU(cudaGetLastError());
+    return PT_OK;
+}
+
+}  // namespace
+
+DeviceScene device_view(const pt_scene* s) {
+    DeviceScene v;
+    std::memset(&v, 0, sizeof(v));
+    const SceneTables& t = s->tables;
+    const DeviceSceneBuffers& d = s->dev;
+    v.inner = static_cast<const InnerNode*>(d.inner);
+    v.tris = static_cast<const TriRecord*>(d.tris);
+    for (int a = 0; a < 3; ++a) { v.root_lo[a] = t.root_lo[a]; v.root_hi[a] = t.root_hi[a]; }
+    v.root_ref = t.root_ref;
+    v.num_faces = static_cast<uint32_t>(s->host.faces.size());
+    v.vertices = static_cast<const pt_vertex*>(d.vertices);
+    v.faces = static_cast<const pt_face*>(d.faces);
+    v.materials = static_cast<const pt_material*>(d.materials);
+    v.num_materials = static_cast<uint32_t>(s->host.materials.size());
+    v.emissive = static_cast<const pt_emissive_ref*>(d.emissive);
+    v.num_emissive = static_cast<uint32_t>(t.emissive.size());
+    v.tri_light_pmf = static_cast<const float*>(d.tri_pmf);
+    v.tri_alias = static_cast<const pt_alias_entry*>(d.tri_alias);
+    v.env_pmf = static_cast<const float*>(d.env_pmf);
+    v.env_alias = static_cast<const pt_alias_entry*>(d.env_alias);
+    v.num_env_texels = static_cast<uint32_t>(t.env_pmf.size());
+    v.env_w = t.env_w;
+    v.env_h = t.env_h;
+    v.env_tex = d.env_tex;
+    v.punctual = static_cast<const pt_punctual_light*>(d.punctual);
+    v.num_punctual = static_cast<uint32_t>(s->host.punctual.size());
+    return v;
+}
+
+void free_scene_device(pt_scene* s) {
+    DeviceSceneBuffers& d = s->dev;
+    if (d.device >= 0) cudaSetDevice(d.device);
+    if (d.env_tex) cudaDestroyTextureObject(static_cast<cudaTextureObject_t>(d.env_tex));
+    if (d.env_array) cudaFreeArray(static_cast<cudaArray_t>(d.env_array));
+    void* bufs[] = {d.inner, d.tris, d.vertices, d.faces, d.materials, d.emissive, d.tri_pmf,
+                    d.tri_alias, d.env_pmf, d.env_alias, d.punctual};
+    for (void* b : bufs) if (b) cudaFree(b);
+    d = DeviceSceneBuffers{};
+}
+
+int upload_scene(pt_scene* s, int device) {
+    if (!s->tables.built) { set_error("scene not built: call pt_scene_build_accel first"); return PT_ERR_STATE; }
+    free_scene_device(s);
+    if (int rc = ensure_device(device)) return rc;
+    DeviceSceneBuffers& d = s->dev;
+    d.device = device;
+    auto up = [&](void** dst, const void* src, size_t bytes) -> int {
+        if (bytes == 0) { *dst = nullptr; return PT_OK; }
+        if (cudaMalloc(dst, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+            return PT_ERR_NOMEM;
+        }
+        PT_CU(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+        d.bytes += bytes;
+        return PT_OK;
+    };
+    const HostScene& h = s->host;
+    const SceneTables& t = s->tables;
+    int rc = PT_OK;
+    if ((rc = up(&d.inner, t.inner.data(), t.inner.size() * sizeof(InnerNode)))) return rc;
+    if ((rc = up(&d.tris, t.tris.data(), t.tris.size() * sizeof(TriRecord)))) return rc;
+    if ((rc = up(&d.vertices, h.vertices.data(), h.vertices.size() * sizeof(pt_vertex)))) return rc;
+    if ((rc = up(&d.faces, h.faces.data(), h.faces.size() * sizeof(pt_face)))) return rc;
+    if ((rc = up(&d.materials, h.materials.data(), h.materials.size() * sizeof(pt_material)))) return rc;
+    if ((rc = up(&d.emissive, t.emissive.data(), t.emissive.size() * sizeof(pt_emissive_ref)))) return rc;
+    if ((rc = up(&d.tri_pmf, t.tri_pmf.data(), t.tri_pmf.size() * sizeof(float)))) return rc;
+    if ((rc = up(&d.tri_alias, t.tri_alias.data(), t.tri_alias.size() * sizeof(pt_alias_entry)))) return rc;
+    if ((rc = up(&d.env_pmf, t.env_pmf.data(), t.env_pmf.size() * sizeof(float)))) return rc;
+    if ((rc = up(&d.env_alias, t.env_alias.data(), t.env_alias.size() * sizeof(pt_alias_entry)))) return rc;
+    if ((rc = up(&d.punctual, h.punctual.data(), h.punctual.size() * sizeof(pt_punctual_light)))) return rc;
+    if (h.env_w > 0 && h.env_h > 0) {
+        // float4 array, linear filtering, wrap, normalized coordinates
+        // (CudaTexture, Part_2/src/cuda/cuda_texture.cu:39-63)
+        cudaChannelFormatDesc ch = cudaCreateChannelDesc<float4>();
+        cudaArray_t arr = nullptr;
+        PT_CU(cudaMallocArray(&arr, &ch, h.env_w, h.env_h));
+        d.env_array = arr;
+        const size_t pitch = static_cast<size_t>(h.env_w) * 4 * sizeof(float);
+        PT_CU(cudaMemcpy2DToArray(arr, 0, 0, h.env_rgba.data(), pitch, pitch, h.env_h, cudaMemcpyHostToDevice));
+        cudaResourceDesc rd;
+        std::memset(&rd, 0, sizeof(rd));
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = arr;
+        cudaTextureDesc td;
+        std::memset(&td, 0, sizeof(td));
+        td.addressMode[0] = cudaAddressModeWrap;
+        td.addressMode[1] = cudaAddressModeWrap;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 1;
+        cudaTextureObject_t tex = 0;
+        PT_CU(cudaCreateTextureObject(&tex, &rd, &td, nullptr));
+        d.env_tex = tex;
+        d.bytes += static_cast<uint64_t>(h.env_w) * h.env_h * 16;
+    }
+    d.uploaded = true;
+    return PT_OK;
+}
+
+int film_alloc(pt_film* f) {
+    if (int rc = ensure_device(f->device)) return rc;
+    const size_t bytes = static_cast<size_t>(f->width) * f->height * sizeof(float4);
+    void** bufs[] = {&f->sum, &f->comp, &f->batch, &f->fresh, &f->resolve};
+    for (void** b : bufs) {
+        if (cudaMalloc(b, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cannot allocate film buffers");
+            return PT_ERR_NOMEM;
+        }
+        PT_CU(cudaMemset(*b, 0, bytes));
+    }
+    return PT_OK;
+}
+
+void film_free(pt_film* f) {
+    if (f->device >= 0) cudaSetDevice(f->device);
+    void* bufs[] = {f->sum, f->comp, f->batch, f->fresh, f->resolve};
+    for (void* b : bufs) if (b) cudaFree(b);
+    f->sum = f->comp = f->batch = f->fresh = f->resolve = nullptr;
+}
+
+int film_clear(pt_film* f) {
+    if (int rc = ensure_device(f->device)) return rc;
+    const size_t bytes = static_cast<size_t>(f->width) * f->height * sizeof(float4);
+    void* bufs[] = {f->sum, f->comp, f->batch, f->fresh};
+    for (void* b : bufs) PT_CU(cudaMemset(b, 0, bytes));
+    return PT_OK;
+}
+
+int film_download(const pt_film* f, float* host, bool fresh, bool host_ptr) {
+    if (int rc = ensure_device(f->device)) return rc;
+    const int n = f->width * f->height;
+    const size_t bytes = static_cast<size_t>(n) * sizeof(float4);
+    if (fresh) {
+        PT_CU(cudaMemcpy(host, f->fresh, bytes, host_ptr ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice));
+        return PT_OK;
+    }
+    k_film_mean<<<(n + 255) / 256, 256>>>(static_cast<const float4*>(f->sum), static_cast<const float4*>(f->comp),
+                                          static_cast<float4*>(f->resolve), n);
+    PT_CU(cudaGetLastError());
+    PT_CU(cudaMemcpy(host, f->resolve, bytes, host_ptr ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice));
+    return PT_OK;
+}
+
+void integrator_free(pt_integrator* integ) {
+    Wavefront* wf = integ->wf;
+    if (!wf) return;
+    if (wf->device >= 0) cudaSetDevice(wf->device);
+    if (wf->graph) cudaGraphExecDestroy(wf->graph);
+    if (wf->arena) cudaFree(wf->arena);
+    if (wf->own_stream) cudaStreamDestroy(wf->own_stream);
+    delete wf;
+    integ->wf = nullptr;
+}
+
+// Integrator::launch (Part_2/src/integrators/path.cu:244-255).
+int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scene_params* prm, void* stream) {
+    if (!s->dev.uploaded) { set_error("scene not uploaded: call pt_scene_upload first"); return PT_ERR_STATE; }
+    if (film->width != prm->width || film->height != prm->height) { set_error("film size does not match params"); return PT_ERR_INVALID; }
+    if (prm->width <= 0 || prm->height <= 0 || prm->sample_per_frame <= 0 || prm->max_depth < 0) {
+        set_error("invalid scene params"); return PT_ERR_INVALID;
+    }
+    if (film->device != s->dev.device) { set_error("film and scene live on different devices"); return PT_ERR_INVALID; }
+    if (!integ->wf) integ->wf = new Wavefront();
+    Wavefront& wf = *integ->wf;
+    const int npix = prm->width * prm->height;
+    const int n_slots = 2 + static_cast<int>(s->host.punctual.size());
+    if (int rc = wavefront_prepare(wf, s->dev.device, npix, n_slots)) return rc;
+    const pt_render_settings& rs = s->host.settings;
+    // Built byte-wise (padding zeroed) because the bytes key the graph cache.
+    WaveParams P;
+    std::memset(&P, 0, sizeof(P));
+    std::memcpy(&P, &wf.base, sizeof(P));
+    const DeviceScene view = device_view(s);
+    std::memcpy(&P.scene, &view, sizeof(DeviceScene));
+    P.cam = prm->camera;
+    P.width = prm->width; P.height = prm->height; P.npix = npix;
+    P.spf = prm->sample_per_frame;
+    P.max_depth = prm->max_depth;
+    P.sampler_type = prm->sampler_type;
+    P.arg_rtl = rs.arg_order == PT_ARGS_RTL ? 1 : 0;
+    P.flags = rs.flags;
+    P.pcg_seed = rs.pcg_seed;
+    P.n_slots = n_slots;
+    P.f_sum = static_cast<float4*>(film->sum);
+    P.f_comp = static_cast<float4*>(film->comp);
+    P.f_batch = static_cast<float4*>(film->batch);
+    P.f_new = static_cast<float4*>(film->fresh);
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : wf.own_stream;
+    k_begin<<<1, 1, 0, st>>>(P.pass, s->frame_count);
+    PT_CU(cudaGetLastError());
+    const bool timing = (rs.flags & PT_FLAG_STAGE_TIMING) != 0;
+    const bool use_graph = !timing && !(rs.flags & PT_FLAG_NO_GRAPH);
+    if (timing) {
+        std::vector<StageEvent> ev;
+        cudaEvent_t t0, t1;
+        PT_CU(cudaEventCreate(&t0));
+        PT_CU(cudaEventCreate(&t1));
+        PT_CU(cudaEventRecord(t0, st));
+        int rc = enqueue_batch(wf, P, st, &ev);
+        PT_CU(cudaEventRecord(t1, st));
+        PT_CU(cudaEventSynchronize(t1));
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        wf.total_ms += ms;
+        for (StageEvent& e : ev) {
+            float m = 0.0f;
+            cudaEventElapsedTime(&m, e.a, e.b);
+            wf.stage_ms[e.kind] += m;
+            if (e.kind == 0) wf.extend_launches++;
+            cudaEventDestroy(e.a);
+            cudaEventDestroy(e.b);
+        }
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        if (rc) return rc;
+    } else if (use_graph) {
+        std::vector<unsigned char> key(sizeof(WaveParams) + sizeof(cudaStream_t));
+        std::memcpy(key.data(), &P, sizeof(WaveParams));
+        std::memcpy(key.data() + sizeof(WaveParams), &st, sizeof(cudaStream_t));
+        if (!wf.graph || key != wf.graph_key) {
+            if (wf.graph) { cudaGraphExecDestroy(wf.graph); wf.graph = nullptr; }
+            cudaGraph_t g = nullptr;
+            PT_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            const int rc = enqueue_batch(wf, P, st, nullptr);
+            const cudaError_t ec = cudaStreamEndCapture(st, &g);
+            if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+            if (ec != cudaSuccess) { set_error(std::string("graph capture failed: ") + cudaGetErrorString(ec)); return PT_ERR_CUDA; }
+            const cudaError_t ei = cudaGraphInstantiate(&wf.graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ei != cudaSuccess) { wf.graph = nullptr; set_error(std::string("graph instantiate failed: ") + cudaGetErrorString(ei)); return PT_ERR_CUDA; }
+            wf.graph_key = key;
+        }
+        PT_CU(cudaGraphLaunch(wf.graph, st));
+        wf.extend_launches += static_cast<uint64_t>(P.spf) * P.max_depth;
+    } else {
+        if (int rc = enqueue_batch(wf, P, st, nullptr)) return rc;
+        wf.extend_launches += static_cast<uint64_t>(P.spf) * P.max_depth;
+    }
+    return PT_OK;
+}
+
+int integrator_check(pt_integrator* integ, bool sync) {
+    Wavefront* wf = integ->wf;
+    if (!wf || wf->device < 0) return PT_OK;
+    if (int rc = ensure_device(wf->device)) return rc;
+    if (sync) PT_CU(cudaDeviceSynchronize());
+    uint32_t err = 0;
+    PT_CU(cudaMemcpy(&err, wf->base.err, 4, cudaMemcpyDeviceToHost));
+    if (err) {
+        std::string m = "device error word 0x" + std::to_string(err) + ":";
+        if (err & kErrStackOverflow) m += " traversal stack overflow;";
+        if (err & kErrQueueOverflow) m += " queue overflow;";
+        set_error(m);
+        PT_CU(cudaMemset(wf->base.err, 0, 4));
+        return PT_ERR_DEVICE;
+    }
+    return PT_OK;
+}
+
+int integrator_stats(const pt_integrator* integ, pt_render_stats* out) {
+    std::memset(out, 0, sizeof(*out));
+    const Wavefront* wf = integ->wf;
+    if (!wf || wf->device < 0) return PT_OK;
+    if (int rc = ensure_device(wf->device)) return rc;
+    unsigned long long st[kStatCount];
+    PT_CU(cudaMemcpy(st, wf->base.stats, sizeof(st), cudaMemcpyDeviceToHost));
+    out->camera_rays = st[kStatCameraRays];
+    out->extension_rays = st[kStatExtRays];
+    out->shadow_rays = st[kStatShadowRays];
+    out->node_visits = st[kStatNodes];
+    out->triangle_tests = st[kStatTris];
+    out->shadow_node_visits = st[kStatShadowNodes];
+    out->shadow_triangle_tests = st[kStatShadowTris];
+    out->paths = st[kStatPaths];
+    out->extend_launches = wf->extend_launches;
+    out->extend_ms = wf->stage_ms[0];
+    out->shade_ms = wf->stage_ms[1];
+    out->shadow_ms = wf->stage_ms[2];
+    out->other_ms = wf->stage_ms[3];
+    out->total_ms = wf->total_ms;
+    return PT_OK;
+}
+
+int integrator_reset_stats(pt_integrator* integ) {
+    Wavefront* wf = integ->wf;
+    if (!wf || wf->device < 0) return PT_OK;
+    if (int rc = ensure_device(wf->device)) return rc;
+    PT_CU(cudaMemset(wf->base.stats, 0, kStatCount * 8));
+    for (double& d : wf->stage_ms) d = 0.0;
+    wf->total_ms = 0.0;
+    wf->extend_launches = 0;
+    return PT_OK;
+}
+
+// ---- diagnostics ----
+int trace_rays(pt_scene* s, const float* rays, uint32_t n, pt_hit* hits, uint8_t* occl, bool any, bool device_ptrs) {
+    if (!s->dev.uploaded) { set_error("scene not uploaded"); return PT_ERR_STATE; }
+    if (int rc = ensure_device(s->dev.device)) return rc;
+    if (n == 0) return PT_OK;
+    const float* d_rays = rays;
+    void* d_out = any ? static_cast<void*>(occl) : static_cast<void*>(hits);
+    void* tmp_rays = nullptr;
+    void* tmp_out = nullptr;
+    uint32_t* d_err = nullptr;
+    const size_t out_bytes = any ? n : static_cast<size_t>(n) * sizeof(pt_hit);
+    auto cleanup = [&] { if (tmp_rays) cudaFree(tmp_rays); if (tmp_out) cudaFree(tmp_out); if (d_err) cudaFree(d_err); };
+    if (!device_ptrs) {
+        if (cudaMalloc(&tmp_rays, static_cast<size_t>(n) * 32) != cudaSuccess ||
+            cudaMalloc(&tmp_out, out_bytes) != cudaSuccess) {
+            cudaGetLastError(); cleanup(); set_error("cannot allocate ray buffers"); return PT_ERR_NOMEM;
+        }
+        if (cudaMemcpy(tmp_rays, rays, static_cast<size_t>(n) * 32, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cleanup(); set_error("ray upload failed"); return PT_ERR_CUDA;
+        }
+        d_rays = static_cast<const float*>(tmp_rays);
+        d_out = tmp_out;
+    }
+    if (cudaMalloc(&d_err, 4) != cudaSuccess || cudaMemset(d_err, 0, 4) != cudaSuccess) {
+        cudaGetLastError(); cleanup(); set_error("cannot allocate error word"); return PT_ERR_NOMEM;
+    }
+    const DeviceScene v = device_view(s);
+    const int wt = (s->host.settings.flags & PT_FLAG_WATERTIGHT) ? 1 : 0;
+    const int blocks = static_cast<int>(std::min<uint32_t>((n + 127) / 128, 148u * 16u));
+    k_trace_rays<<<blocks, 128>>>(v, d_rays, n, any ? nullptr : static_cast<pt_hit*>(d_out),
+                                  any ? static_cast<uint8_t*>(d_out) : nullptr, any ? 1 : 0, wt, d_err);
+    cudaError_t e = cudaDeviceSynchronize();
+    uint32_t err = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&err, d_err, 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && !device_ptrs)
+        e = cudaMemcpy(any ? static_cast<void*>(occl) : static_cast<void*>(hits), d_out, out_bytes, cudaMemcpyDeviceToHost);
+    cleanup();
+    if (e != cudaSuccess) { set_error(std::string("trace failed: ") + cudaGetErrorString(e)); return PT_ERR_CUDA; }
+    if (err) { set_error("traversal stack overflow"); return PT_ERR_DEVICE; }
+    return PT_OK;
+}
+
+int sampler_stream(int type, int w, int h, uint32_t frame, int spf, int sif, uint32_t ndims, uint32_t seed,
+                   int device, float* out_host) {
+    if (int rc = ensure_device(device)) return rc;
+    const size_t bytes = static_cast<size_t>(w) * h * ndims * sizeof(float);
+    if (bytes == 0) return PT_OK;
+    float* d = nullptr;
+    PT_CU(cudaMalloc(&d, bytes));
+    k_sampler_stream<<<std::min((w * h + 255) / 256, 148 * 8), 256>>>(type, w, h, frame, spf, sif, ndims, seed, d);
+    cudaError_t e = cudaMemcpy(out_host, d, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) { set_error(std::string("sampler stream failed: ") + cudaGetErrorString(e)); return PT_ERR_CUDA; }
+    return PT_OK;
+}
+
+int bsdf_eval(pt_scene* s, const float* in, uint32_t n, float* out_host) {
+    if (!s->dev.uploaded) { set_error("scene not uploaded"); return PT_ERR_STATE; }
+    if (int rc = ensure_device(s->dev.device)) return rc;
+    if (n == 0) return PT_OK;
+    float *din = nullptr, *dout = nullptr;
+    PT_CU(cudaMalloc(&din, static_cast<size_t>(n) * 13 * 4));
+    if (cudaMalloc(&dout, static_cast<size_t>(n) * 4 * 4) != cudaSuccess) { cudaFree(din); cudaGetLastError(); set_error("alloc failed"); return PT_ERR_NOMEM; }
+    cudaError_t e = cudaMemcpy(din, in, static_cast<size_t>(n) * 13 * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_bsdf_eval<<<std::min<uint32_t>((n + 127) / 128, 1184u), 128>>>(
+            static_cast<const pt_material*>(s->dev.materials), static_cast<uint32_t>(s->host.materials.size()), din, n, dout);
+        e = cudaMemcpy(out_host, dout, static_cast<size_t>(n) * 16, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(din);
+    cudaFree(dout);
+    if (e != cudaSuccess) { set_error(std::string("bsdf eval failed: ") + cudaGetErrorString(e)); return PT_ERR_CUDA; }
+    return PT_OK;
+}
+
+}  // namespace ptb
+
+namespace ptb {
+
+int current_device(int* dev) {
+    PT_CU(cudaGetDevice(dev));
+    return PT_OK;
+}
+
+int device_sync(int device) {
+    if (int rc = ensure_device(device)) return rc;
+    PT_CU(cudaDeviceSynchronize());
+    return PT_OK;
+}
+
+}  // namespace ptb

@@ -1,0 +1,289 @@
+// traverse.h -- closest-hit and any-hit BVH traversal (host + device).
+//
+// Semantics are those of the reference's stack traversal
+// (Part_2/src/accel/bvh_traversal.cuh:29-133) and Moller-Trumbore tests
+// (Part_2/src/geometry/triangle.h:13-76), so that hit triangle ids and hit
+// distances are bit-identical to the reference's IEEE (non-contracted) build:
+//
+//  * Box test: the reference's per-axis recurrence with t_min starting at 0
+//    and t_max at the current best distance.  For NaN-free rays (every 1/d
+//    finite) it equals  entry <= best && entry <= exit  with entry/exit the
+//    usual slab max/min, which is what the fast path evaluates; rays with a
+//    zero (or denormal) direction component take the literal recurrence, whose
+//    NaN handling (an axis with a NaN bound is ignored) differs.
+//  * Order: the reference pops the near child first, where "near" comes from
+//    the parent's max-extent axis and the children's centroids compared with
+//    the ray sign (bvh_traversal.cuh:81-92).  Here each inner node stores both
+//    child boxes, so both are tested at the parent with the same best distance
+//    the reference uses when it pops the near child; the far child is pushed
+//    with its entry distance and re-tested against the best distance when
+//    popped.  Visited set and visit order equal the reference's.
+//  * Closest hit keeps the first hit found under strict '<' (ties resolved
+//    exactly as in the reference); any-hit returns on the first triangle with
+//    1e-4 < t < tMax, which is order independent.
+#pragma once
+
+#include "pt_internal.h"
+
+#if !defined(__CUDACC__)
+#include <vector_types.h>
+#endif
+
+namespace ptb {
+
+struct RayInv {
+    float ox, oy, oz;
+    float dx, dy, dz;
+    float ix, iy, iz;
+    int   sx, sy, sz;
+    bool  nan_free;
+};
+
+PT_HD RayInv make_ray_inv(float ox, float oy, float oz, float dx, float dy, float dz) {
+    RayInv r;
+    r.ox = ox; r.oy = oy; r.oz = oz;
+    r.dx = dx; r.dy = dy; r.dz = dz;
+    r.ix = x_rcp(dx); r.iy = x_rcp(dy); r.iz = x_rcp(dz);
+    r.sx = r.ix < 0.0f ? 1 : 0;
+    r.sy = r.iy < 0.0f ? 1 : 0;
+    r.sz = r.iz < 0.0f ? 1 : 0;
+    r.nan_free = fabsf(r.ix) <= FLT_MAX && fabsf(r.iy) <= FLT_MAX && fabsf(r.iz) <= FLT_MAX;
+    return r;
+}
+
+// entry / exit of a box, with the reference's arithmetic.
+PT_HD void box_span(const RayInv& r, float lx, float ly, float lz, float hx, float hy, float hz,
+                    float& entry, float& exit_) {
+    const float t1x = x_mul(x_sub(lx, r.ox), r.ix), t2x = x_mul(x_sub(hx, r.ox), r.ix);
+    const float t1y = x_mul(x_sub(ly, r.oy), r.iy), t2y = x_mul(x_sub(hy, r.oy), r.iy);
+    const float t1z = x_mul(x_sub(lz, r.oz), r.iz), t2z = x_mul(x_sub(hz, r.oz), r.iz);
+    if (r.nan_free) {
+        entry = fmaxf(fmaxf(fminf(t1x, t2x), fminf(t1y, t2y)), fmaxf(fminf(t1z, t2z), 0.0f));
+        exit_ = fminf(fminf(fmaxf(t1x, t2x), fmaxf(t1y, t2y)), fmaxf(t1z, t2z));
+    } else {
+        // literal recurrence (bvh_traversal.cuh:33-39) with t_max starting at +inf
+        float tn = 0.0f, tf = INFINITY;
+        tn = fminf(fmaxf(t1x, tn), fmaxf(t2x, tn)); tf = fmaxf(fminf(t1x, tf), fminf(t2x, tf));
+        tn = fminf(fmaxf(t1y, tn), fmaxf(t2y, tn)); tf = fmaxf(fminf(t1y, tf), fminf(t2y, tf));
+        tn = fminf(fmaxf(t1z, tn), fmaxf(t2z, tn)); tf = fmaxf(fminf(t1z, tf), fminf(t2z, tf));
+        entry = tn; exit_ = tf;
+    }
+}
+
+// Moller-Trumbore on a precomputed record.  Returns t (or -1).  `shadow`
+// selects the reference's shadow acceptance (t > 1e-4) instead of the
+// closest-hit one (t >= 1e-4).
+PT_HD float tri_mt(const RayInv& r, float v0x, float v0y, float v0z,
+                   float e1x, float e1y, float e1z, float e2x, float e2y, float e2z,
+                   bool shadow, float& u_out, float& v_out) {
+    const float px = x_sub(x_mul(r.dy, e2z), x_mul(r.dz, e2y));
+    const float py = x_sub(x_mul(r.dz, e2x), x_mul(r.dx, e2z));
+    const float pz = x_sub(x_mul(r.dx, e2y), x_mul(r.dy, e2x));
+    const float det = x_add(x_add(x_mul(e1x, px), x_mul(e1y, py)), x_mul(e1z, pz));
+    if (fabsf(det) < FLT_EPSILON) return -1.0f;
+    const float inv = x_rcp(det);
+    const float tx = x_sub(r.ox, v0x), ty = x_sub(r.oy, v0y), tz = x_sub(r.oz, v0z);
+    const float u = x_mul(x_add(x_add(x_mul(tx, px), x_mul(ty, py)), x_mul(tz, pz)), inv);
+    if (u < 0.0f || u > 1.0f) return -1.0f;
+    const float qx = x_sub(x_mul(ty, e1z), x_mul(tz, e1y));
+    const float qy = x_sub(x_mul(tz, e1x), x_mul(tx, e1z));
+    const float qz = x_sub(x_mul(tx, e1y), x_mul(ty, e1x));
+    const float v = x_mul(x_add(x_add(x_mul(r.dx, qx), x_mul(r.dy, qy)), x_mul(r.dz, qz)), inv);
+    if (v < 0.0f || x_add(u, v) > 1.0f) return -1.0f;
+    const float t = x_mul(x_add(x_add(x_mul(e2x, qx), x_mul(e2y, qy)), x_mul(e2z, qz)), inv);
+    if (shadow ? !(t > 1e-4f) : (t < 1e-4f)) return -1.0f;
+    u_out = u; v_out = v;
+    return t;
+}
+
+// Watertight ray/triangle test (Woop, Benthin, Wald 2013): shear/scale so the
+// ray is +z, 2D edge functions with a double-precision fallback on exact
+// zeros.  Used when PT_FLAG_WATERTIGHT is set; not bit-comparable with the
+// reference (which has no watertight mode).
+PT_HD float tri_watertight(const RayInv& r, float v0x, float v0y, float v0z,
+                           float e1x, float e1y, float e1z, float e2x, float e2y, float e2z,
+                           bool shadow, float& u_out, float& v_out) {
+    // dominant axis
+    const float adx = fabsf(r.dx), ady = fabsf(r.dy), adz = fabsf(r.dz);
+    int kz = (adx > ady) ? (adx > adz ? 0 : 2) : (ady > adz ? 1 : 2);
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    const float d[3] = {r.dx, r.dy, r.dz};
+    if (d[kz] < 0.0f) { int t = kx; kx = ky; ky = t; }
+    const float sx = d[kx] / d[kz], sy = d[ky] / d[kz], sz = 1.0f / d[kz];
+    const float a[3] = {v0x - r.ox, v0y - r.oy, v0z - r.oz};
+    const float b[3] = {a[0] + e1x, a[1] + e1y, a[2] + e1z};
+    const float c[3] = {a[0] + e2x, a[1] + e2y, a[2] + e2z};
+    const float ax = a[kx] - sx * a[kz], ay = a[ky] - sy * a[kz];
+    const float bx = b[kx] - sx * b[kz], by = b[ky] - sy * b[kz];
+    const float cx = c[kx] - sx * c[kz], cy = c[ky] - sy * c[kz];
+    float U = cx * by - cy * bx;
+    float V = ax * cy - ay * cx;
+    float W = bx * ay - by * ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = (float)((double)cx * (double)by - (double)cy * (double)bx);
+        V = (float)((double)ax * (double)cy - (double)ay * (double)cx);
+        W = (float)((double)bx * (double)ay - (double)by * (double)ax);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return -1.0f;
+    const float det = U + V + W;
+    if (det == 0.0f) return -1.0f;
+    const float az = sz * a[kz], bz = sz * b[kz], cz = sz * c[kz];
+    const float T = U * az + V * bz + W * cz;
+    const float inv = 1.0f / det;
+    const float t = T * inv;
+    if (shadow ? !(t > 1e-4f) : (t < 1e-4f)) return -1.0f;
+    // barycentrics w.r.t. (v0, v1, v2): weight of v1 is V, of v2 is W
+    u_out = V * inv; v_out = W * inv;
+    return t;
+}
+
+struct TraceCounters { uint32_t inner; uint32_t tris; };
+
+#if defined(__CUDA_ARCH__)
+#  define PT_LDG4(p) __ldg(reinterpret_cast<const float4*>(p))
+#  define PT_LDGU4(p) __ldg(reinterpret_cast<const uint4*>(p))
+#else
+#  define PT_LDG4(p) (*reinterpret_cast<const float4*>(p))
+#  define PT_LDGU4(p) (*reinterpret_cast<const uint4*>(p))
+#endif
+
+PT_HD float tri_test(const DeviceScene& s, const RayInv& r, uint32_t ti, bool shadow, bool watertight,
+                     float& u, float& v, bool& last) {
+    const float* base = reinterpret_cast<const float*>(s.tris + ti);
+    const float4 a = PT_LDG4(base);
+    const float4 b = PT_LDG4(base + 4);
+    const float4 c = PT_LDG4(base + 8);
+    last = (__float_as_uint_hd(c.y) & 1u) != 0u;
+    if (watertight)
+        return tri_watertight(r, a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, shadow, u, v);
+    return tri_mt(r, a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, shadow, u, v);
+}
+
+// Closest hit.  Returns prim (BVH-ordered face index) or -1; t = FLT_MAX on miss.
+PT_HD int trace_closest(const DeviceScene& s, const RayInv& r, bool watertight,
+                        float& t_out, float& u_out, float& v_out, uint32_t& err, TraceCounters& cnt) {
+    float best = FLT_MAX;
+    int prim = -1;
+    float bu = 0.0f, bv = 0.0f;
+    t_out = FLT_MAX; u_out = 0.0f; v_out = 0.0f;
+    if (s.num_faces == 0) return -1;
+    float en, ex;
+    box_span(r, s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], en, ex);
+    if (!(en <= best && en <= ex)) return -1;
+    uint32_t stack_ref[kStackDepth];
+    float    stack_t[kStackDepth];
+    int sp = 0;
+    uint32_t ref = s.root_ref;
+    const int sgn[3] = {r.sx, r.sy, r.sz};
+    for (;;) {
+        if (ref & kLeafBit) {
+            uint32_t ti = ref & ~kLeafBit;
+            for (;;) {
+                float u, v; bool last;
+                const float t = tri_test(s, r, ti, false, watertight, u, v, last);
+                ++cnt.tris;
+                if (t >= 0.0f && t < best) { best = t; prim = (int)ti; bu = u; bv = v; }
+                if (last) break;
+                ++ti;
+            }
+        } else {
+            ++cnt.inner;
+            const float* nb = reinterpret_cast<const float*>(s.inner + ref);
+            const float4 q0 = PT_LDG4(nb);
+            const float4 q1 = PT_LDG4(nb + 4);
+            const float4 q2 = PT_LDG4(nb + 8);
+            const uint4  q3 = PT_LDGU4(nb + 12);
+            float e0, x0, e1, x1;
+            box_span(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, e0, x0);
+            box_span(r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, e1, x1);
+            const bool h0 = e0 <= best && e0 <= x0;
+            const bool h1 = e1 <= best && e1 <= x1;
+            const uint32_t axis = q3.z & 3u;
+            const int lt = (int)((q3.z >> 2) & 1u);
+            const bool right_first = sgn[axis] == lt;
+            const uint32_t nref = right_first ? q3.y : q3.x;
+            const uint32_t fref = right_first ? q3.x : q3.y;
+            const bool hn = right_first ? h1 : h0;
+            const bool hf = right_first ? h0 : h1;
+            const float ef = right_first ? e0 : e1;
+            if (hn) {
+                if (hf) {
+                    if (sp >= kStackDepth) { err |= kErrStackOverflow; break; }
+                    stack_ref[sp] = fref; stack_t[sp] = ef; ++sp;
+                }
+                ref = nref;
+                continue;
+            }
+            if (hf) { ref = fref; continue; }
+        }
+        // pop the next deferred child that still passes against the current best
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (stack_t[sp] <= best) { ref = stack_ref[sp]; found = true; break; }
+        }
+        if (!found) break;
+    }
+    if (prim >= 0) { t_out = best; u_out = bu; v_out = bv; }
+    return prim;
+}
+
+// Any hit in (1e-4, tmax).
+PT_HD bool trace_any(const DeviceScene& s, const RayInv& r, float tmax, bool watertight,
+                     uint32_t& err, TraceCounters& cnt) {
+    if (s.num_faces == 0) return false;
+    float en, ex;
+    box_span(r, s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], en, ex);
+    if (!(en <= tmax && en <= ex)) return false;
+    uint32_t stack_ref[kStackDepth];
+    int sp = 0;
+    uint32_t ref = s.root_ref;
+    const int sgn[3] = {r.sx, r.sy, r.sz};
+    for (;;) {
+        if (ref & kLeafBit) {
+            uint32_t ti = ref & ~kLeafBit;
+            for (;;) {
+                float u, v; bool last;
+                const float t = tri_test(s, r, ti, true, watertight, u, v, last);
+                ++cnt.tris;
+                if (t > 0.0f && t < tmax) return true;
+                if (last) break;
+                ++ti;
+            }
+        } else {
+            ++cnt.inner;
+            const float* nb = reinterpret_cast<const float*>(s.inner + ref);
+            const float4 q0 = PT_LDG4(nb);
+            const float4 q1 = PT_LDG4(nb + 4);
+            const float4 q2 = PT_LDG4(nb + 8);
+            const uint4  q3 = PT_LDGU4(nb + 12);
+            float e0, x0, e1, x1;
+            box_span(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, e0, x0);
+            box_span(r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, e1, x1);
+            const bool h0 = e0 <= tmax && e0 <= x0;
+            const bool h1 = e1 <= tmax && e1 <= x1;
+            const uint32_t axis = q3.z & 3u;
+            const int lt = (int)((q3.z >> 2) & 1u);
+            const bool right_first = sgn[axis] == lt;
+            const uint32_t nref = right_first ? q3.y : q3.x;
+            const uint32_t fref = right_first ? q3.x : q3.y;
+            const bool hn = right_first ? h1 : h0;
+            const bool hf = right_first ? h0 : h1;
+            if (hn) {
+                if (hf) {
+                    if (sp >= kStackDepth) { err |= kErrStackOverflow; return false; }
+                    stack_ref[sp++] = fref;
+                }
+                ref = nref;
+                continue;
+            }
+            if (hf) { ref = fref; continue; }
+        }
+        if (sp == 0) break;
+        ref = stack_ref[--sp];
+    }
+    return false;
+}
+
+}  // namespace ptb
