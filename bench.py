@@ -1,0 +1,343 @@
+#!/usr/bin/env python
+"""Benchmark: Mrays/s of the path-tracing hot path on the procedural
+2,048,002-triangle icosphere field (400 displaced subdivision-4 icospheres on a
+ground quad, Disney materials, 2048x1024 synthetic sky with a 5e4 sun lobe),
+1920x1080, 256 spp, max depth 16, Sobol.
+
+One step = one full render of that workload: 64 launches of 4 samples per pixel
+(the reference's Renderer::renderAll over PathIntegrator::launch), scene
+resident in HBM.  Rays = camera + extension + shadow rays traced.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank renders the full workload with disjoint sample
+indices (weak scaling, no data-path collective); value = rays of all ranks /
+max-over-ranks time.  --impl reference times the reference's own CPU
+implementation (its integrator compiled for the host, oracle/_ref) on the
+host cores, on a bounded row sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mrays/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--spp", type=int, default=256, help="samples per pixel of one step (workload: 256)")
+    p.add_argument("--small", action="store_true", help="a small scene for quick checks (not a bench line)")
+    p.add_argument("--cpu-sample-seconds", type=float, default=12.0)
+    return p.parse_args()
+
+
+def workload(small: bool):
+    from pathtracingtutorial_b200 import scenes
+    if small:
+        return scenes.icosphere_field(n_spheres=40, subdiv=3, width=480, height=270, env_size=(512, 256))
+    return scenes.icosphere_field()
+
+
+def config_of(sa, spp):
+    return {"workload": f"icosphere_field {sa.meta['triangles']} tri, {int(sa.camera['width'])}x"
+                        f"{int(sa.camera['height'])}, {spp} spp, depth {sa.max_depth}, sobol, env 2048x1024",
+            "triangles": sa.meta["triangles"], "width": int(sa.camera["width"]), "height": int(sa.camera["height"]),
+            "spp": spp, "max_depth": sa.max_depth, "sampler": "sobol", "sample_per_frame": sa.sample_per_frame,
+            "l2": "inputs larger than L2 (BVH + triangles ~150 MB > 126 MB L2)"}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", HBM_FALLBACK_GBS)), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device, self.rows, self.proc = device, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+def reference_arm(args):
+    """The reference's own CPU integrator on the host cores, bounded sample."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle.pyoracle import RefHarness
+    sa = workload(args.small)
+    cfg = config_of(sa, args.spp)
+    import numpy as np
+    if not RefHarness.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference host build (oracle/_ref) not built"}))
+        return
+    R = RefHarness()
+    cores = os.cpu_count() or 1
+    st = np.array([args.spp, sa.sample_per_frame, sa.max_depth, sa.sampler], np.int32)
+    h = int(sa.camera["height"])
+    # calibrate a row stride so one step is ~cpu_sample_seconds
+    _, _, cal = R.render(sa.vertices, sa.faces, sa.materials, sa.camera, st, sa.env, num_frames=1, row0=0,
+                         row_step=max(1, h // 8), threads=cores)
+    per_row = cal["seconds"] / max(1, len(range(0, h, max(1, h // 8))))
+    rows_per_step = max(1, int(args.cpu_sample_seconds / max(per_row, 1e-6)))
+    stride = max(1, h // rows_per_step)
+    rays = secs = paths = 0.0
+    for k in range(args.warmup + args.steps):
+        _, _, s = R.render(sa.vertices, sa.faces, sa.materials, sa.camera, st, sa.env, first_frame=k,
+                           num_frames=1, row0=k % stride, row_step=stride, threads=cores)
+        if k >= args.warmup:
+            rays += s["closest_rays"] + s["shadow_rays"]
+            secs += s["seconds"]
+            paths += s["paths"]
+    value = rays / secs / 1e6
+    sample = (f"rows y = k mod {stride} (every {stride}th row, {len(range(0, h, stride))} rows x "
+              f"{int(sa.camera['width'])} px), 1 frame of {sa.sample_per_frame} spp per step, {int(paths)} paths")
+    line = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "impl": "reference", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(secs / args.steps * 1e3, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": cfg,
+            "cpu_baseline": {"value": round(value, 3), "unit": METRIC, "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def cpu_baseline(sa, spp, seconds):
+    """Reference CPU path timed on this host (rank 0, N=1): bounded row sample."""
+    import numpy as np
+    from oracle.pyoracle import Oracle, RefHarness
+    cores = os.cpu_count() or 1
+    st = np.array([spp, sa.sample_per_frame, sa.max_depth, sa.sampler], np.int32)
+    h = int(sa.camera["height"])
+    if RefHarness.available():
+        R = RefHarness()
+        _, _, cal = R.render(sa.vertices, sa.faces, sa.materials, sa.camera, st, sa.env, num_frames=1, row0=0,
+                             row_step=max(1, h // 8), threads=cores)
+        per_row = cal["seconds"] / len(range(0, h, max(1, h // 8)))
+        stride = max(1, int(h / max(1.0, seconds / max(per_row, 1e-6))))
+        _, _, s = R.render(sa.vertices, sa.faces, sa.materials, sa.camera, st, sa.env, num_frames=1, row0=1,
+                           row_step=stride, threads=cores)
+        kind = "reference"
+    else:
+        O = Oracle()
+        prep = O.prepare(sa)
+        stride = max(1, h // 16)
+        _, s = O.render(prep, sa.sample_per_frame, sa.max_depth, sa.sampler, frames=1, precision=32, rtl=1,
+                        row0=1, row_step=stride, threads=cores)
+        kind = "port"
+    rays = s["closest_rays"] + s["shadow_rays"]
+    return {"value": round(rays / s["seconds"] / 1e6, 3), "unit": METRIC, "cores": cores, "kind": kind,
+            "sample": f"every {stride}th row of {int(sa.camera['width'])}x{h}, {sa.sample_per_frame} spp "
+                      f"(1 frame), {int(s['paths'])} paths, {int(rays)} rays, {s['seconds']:.1f} s"}
+
+
+def ours(args):
+    import numpy as np
+    import torch
+    import pathtracingtutorial_b200 as pt
+
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sa = workload(args.small)
+    spp = args.spp
+    scene = sa.scene()
+    scene.build_accel()
+    scene.upload_to_device(local)
+    spf = sa.sample_per_frame
+    batches = (spp + spf - 1) // spf
+    stream = torch.cuda.Stream(device=local)
+    handle = stream.cuda_stream
+    renderer = pt.Renderer(scene, device=local, stream=handle)
+    frame0 = rank * batches   # disjoint sample indices per rank
+
+    def step():
+        renderer.reset_accumulation()
+        scene.set_frame_count(frame0)
+        for _ in range(batches):
+            renderer.render_batch()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        renderer.integrator.reset_stats()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clocks:
+            barrier()
+            ev0.record(stream)
+            for _ in range(args.steps):
+                step()
+            ev1.record(stream)
+            barrier()
+        ms = ev0.elapsed_time(ev1)
+    st = renderer.integrator.stats()
+    rays = st["camera_rays"] + st["extension_rays"] + st["shadow_rays"]
+    # whole-job: rays of all ranks over the slowest rank's time
+    t = torch.tensor([ms, rays], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        tmax = t.clone(); dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
+        ms, total_rays = float(tmax[0]), float(t[1])
+    else:
+        total_rays = float(rays)
+    value = total_rays / (ms / 1e3) / 1e6
+
+    # e2e through the public API: host->device scene upload, render, image read back
+    cam = scene.camera
+    img = np.zeros((int(cam["height"]), int(cam["width"]), 4), np.float32)
+    e2e_ms = []
+    e2e_rays = 0
+    for k in range(max(1, min(args.steps, 3)) + 1):
+        barrier()
+        t0 = time.perf_counter()
+        scene.upload_to_device(local)
+        out, sts = pt.render(scene, spp, stats=True)
+        barrier()
+        if k > 0:
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+            e2e_rays = sts["camera_rays"] + sts["extension_rays"] + sts["shadow_rays"]
+    info = scene.info()
+    e2e_val = e2e_rays / (statistics.median(e2e_ms) / 1e3) / 1e6 * world
+
+    # instrumented replica of one step: per-stage CUDA events + traversal counters
+    scene.update_settings(flags=pt.FLAG_STAGE_TIMING | pt.FLAG_COUNT_TRAVERSAL)
+    renderer.integrator.reset_stats()
+    with torch.cuda.stream(stream):
+        step()
+    torch.cuda.synchronize()
+    ist = renderer.integrator.stats()
+    scene.update_settings(flags=0)
+    closest = ist["camera_rays"] + ist["extension_rays"]
+    pops = closest + 2 * ist["node_visits"]
+    alg_bytes = 32.0 * pops + 36.0 * ist["triangle_tests"]
+    launches = max(1, ist["extend_launches"])
+    per_launch_ms = ist["extend_ms"] / launches
+    achieved = alg_bytes / launches / (per_launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "extend_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+    stage_total = ist["extend_ms"] + ist["shade_ms"] + ist["shadow_ms"] + ist["other_ms"]
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    cpu = cpu_baseline(sa, spp, args.cpu_sample_seconds) if world == 1 else None
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_of(sa, spp),
+        "rays_per_step": total_rays / args.steps / world,
+        "ray_classes": {"camera": st["camera_rays"] // args.steps, "extension": st["extension_rays"] // args.steps,
+                        "shadow": st["shadow_rays"] // args.steps},
+        "e2e": {"value": round(e2e_val, 2), "unit": METRIC, "ms_per_step": round(statistics.median(e2e_ms), 2),
+                "h2d_bytes_per_step": int(info["device_bytes"]), "d2h_bytes_per_step": int(img.nbytes),
+                "path": "pt_scene_upload + pt_render (host arrays -> device, 256 spp, image -> host)"},
+        "roofline": {"kernel": "k_extend (closest-hit traversal)", "bound": "hbm", "achieved": round(achieved, 1),
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes / launches,
+                     "avg_launch_ms": round(per_launch_ms, 4), "launches": launches,
+                     "stage_ms": {"extend": round(ist["extend_ms"], 2), "shade": round(ist["shade_ms"], 2),
+                                  "shadow": round(ist["shadow_ms"], 2), "other": round(ist["other_ms"], 2)},
+                     "extend_share": round(ist["extend_ms"] / max(stage_total, 1e-9), 3),
+                     "note": "achieved = (32 B x node pops + 36 B x triangle tests, reference-traversal "
+                             "equivalent) / extend launch time, measured with CUDA events on an instrumented "
+                             "replica of one step"},
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+        "gpu_launches": int(st["kernel_launches"]),
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

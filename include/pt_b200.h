@@ -170,6 +170,7 @@ typedef struct pt_render_stats {
     uint64_t extend_launches;
     double   extend_ms, shade_ms, shadow_ms, other_ms;   /* with PT_FLAG_STAGE_TIMING */
     double   total_ms;
+    uint64_t kernel_launches;                            /* this library's kernels launched */
 } pt_render_stats;
 
 typedef struct pt_hit {
@@ -247,6 +248,8 @@ int pt_integrator_reset_stats(pt_integrator* integ);
 /* ---- renderer (Renderer, Part_2/src/renderer.h:17-55) ---- */
 int pt_renderer_render_batch(pt_integrator* integ, pt_film* film, pt_scene* scene, void* stream); /* renderBatch */
 int pt_renderer_reset_accumulation(pt_film* film, pt_scene* scene);                               /* resetAccumulation */
+/* Frame counter that drives sample indices (DeviceScene::frameCount, device_scene.h:97). */
+int pt_scene_set_frame_count(pt_scene* scene, uint32_t frame_count);
 /* render(scene, spp) -> HDR image: build (if needed), upload (if needed), render
  * spp samples per pixel, write width*height*4 floats (RGBA, row y at y*width*4). */
 int pt_render(pt_scene* scene, int32_t spp, float* out_rgba, int32_t out_is_device,

@@ -158,6 +158,9 @@ class SceneManager:
         check(lib().pt_scene_get_camera(self._h, ptr(c)))
         return c
 
+    def set_frame_count(self, n: int) -> None:
+        check(lib().pt_scene_set_frame_count(self._h, int(n)))
+
     def update_camera(self, cam: np.ndarray) -> None:
         c = np.ascontiguousarray(cam, dtype=CAMERA_DTYPE)
         check(lib().pt_scene_set_camera(self._h, ptr(c)))

@@ -86,7 +86,7 @@ class RenderStats(C.Structure):
                 ("shadow_node_visits", C.c_uint64), ("shadow_triangle_tests", C.c_uint64),
                 ("paths", C.c_uint64), ("extend_launches", C.c_uint64),
                 ("extend_ms", C.c_double), ("shade_ms", C.c_double), ("shadow_ms", C.c_double),
-                ("other_ms", C.c_double), ("total_ms", C.c_double)]
+                ("other_ms", C.c_double), ("total_ms", C.c_double), ("kernel_launches", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -132,6 +132,7 @@ _SIGS = [
     ("pt_integrator_reset_stats", C.c_int, [_P]),
     ("pt_renderer_render_batch", C.c_int, [_P, _P, _P, _P]),
     ("pt_renderer_reset_accumulation", C.c_int, [_P, _P]),
+    ("pt_scene_set_frame_count", C.c_int, [_P, C.c_uint32]),
     ("pt_render", C.c_int, [_P, C.c_int32, _P, C.c_int32, C.POINTER(RenderStats)]),
     ("pt_trace_closest", C.c_int, [_P, _P, C.c_uint32, _P, C.c_int32]),
     ("pt_trace_any", C.c_int, [_P, _P, C.c_uint32, _P, C.c_int32]),

@@ -65,6 +65,7 @@ int copy_out(const std::vector<T>& v, T* out, uint32_t cap) {
 }
 
 void invalidate_build(pt_scene* s) {
+    unpin_host_arrays(s);
     s->tables = SceneTables{};
     if (s->dev.uploaded || s->dev.device >= 0) free_scene_device(s);
 }
@@ -131,6 +132,7 @@ int pt_scene_destroy(pt_scene* scene) {
     if (!scene) return PT_OK;
     drop_cache(scene);
     free_scene_device(scene);
+    unpin_host_arrays(scene);
     delete scene;
     return PT_OK;
 }
@@ -205,7 +207,6 @@ int pt_scene_upload(pt_scene* s, int32_t device) {
     PT_REQUIRE(s, "null scene");
     PT_REQUIRE(device >= 0, "device must be >= 0");
     PT_GUARD_BEGIN
-    drop_cache(s);
     return upload_scene(s, device);
     PT_GUARD_END
 }
@@ -350,6 +351,12 @@ int pt_renderer_reset_accumulation(pt_film* film, pt_scene* s) {
     PT_REQUIRE(film && s, "null argument");
     s->frame_count = 0;
     return film_clear(film);
+}
+
+int pt_scene_set_frame_count(pt_scene* s, uint32_t frame_count) {
+    PT_REQUIRE(s, "null scene");
+    s->frame_count = frame_count;
+    return PT_OK;
 }
 
 int pt_render(pt_scene* s, int32_t spp, float* out_rgba, int32_t out_is_device, pt_render_stats* stats) {

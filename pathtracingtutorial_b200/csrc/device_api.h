@@ -8,6 +8,7 @@ namespace ptb {
 
 DeviceScene device_view(const pt_scene* s);
 void free_scene_device(pt_scene* s);
+void unpin_host_arrays(pt_scene* s);
 int  upload_scene(pt_scene* s, int device);
 
 int  film_alloc(pt_film* f);

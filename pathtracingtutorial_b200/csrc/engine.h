@@ -100,6 +100,7 @@ struct pt_scene {
     ptb::SceneTables        tables;
     ptb::DeviceSceneBuffers dev;
     uint32_t                frame_count = 0;   // DeviceScene::frameCount
+    std::vector<void*>      pinned;            // host arrays page-locked for uploads
 };
 
 struct pt_film {

@@ -236,7 +236,7 @@ __device__ __forceinline__ void warp_count(unsigned long long* dst, uint32_t v) 
 }
 
 __global__ void __launch_bounds__(128) k_extend(WaveParams P, int q, int depth) {
-    const uint32_t n = P.counts[q];
+    const uint32_t n = min(P.counts[q], static_cast<uint32_t>(P.npix));
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.counts[q ^ 1] = 0;
         P.counts[2] = 0;
@@ -439,13 +439,14 @@ __device__ bool shade_path(const WaveParams& P, int depth, bool last, uint32_t p
 }
 
 __global__ void __launch_bounds__(128) k_shade(WaveParams P, int q, int depth, int sample_in_frame) {
-    const uint32_t n = P.counts[q];
+    const uint32_t cap = static_cast<uint32_t>(P.npix);
+    const uint32_t n = min(P.counts[q], cap);
     const uint32_t sidx = P.pass->frame * static_cast<uint32_t>(P.spf) + static_cast<uint32_t>(sample_in_frame);
     const bool last = depth == P.max_depth - 1;
     const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t cap = static_cast<uint32_t>(P.npix);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t p = P.queue[q][i];
+        if (p >= cap) { atomicOr(P.err, kErrQueueOverflow); continue; }
         const float4 o4 = P.ray_o[q][i];
         const float4 d4 = P.ray_d[q][i];
         const float4 h = P.hit[i];
@@ -481,7 +482,7 @@ __global__ void __launch_bounds__(128) k_shade(WaveParams P, int q, int depth, i
 }
 
 __global__ void __launch_bounds__(128) k_shadow(WaveParams P) {
-    const uint32_t n = P.counts[2];
+    const uint32_t n = min(P.counts[2], static_cast<uint32_t>(P.npix) * static_cast<uint32_t>(P.n_slots));
     if (blockIdx.x == 0 && threadIdx.x == 0)
         atomicAdd(P.stats + kStatShadowRays, static_cast<unsigned long long>(n));
     const bool watertight = (P.flags & PT_FLAG_WATERTIGHT) != 0;
@@ -496,6 +497,10 @@ __global__ void __launch_bounds__(128) k_shadow(WaveParams P) {
         if (!trace_any(P.scene, r, d.w, watertight, err, tc)) {
             const uint32_t slot = __float_as_uint(o.w);
             const uint32_t path = P.sq_path[i];
+            if (slot >= static_cast<uint32_t>(P.n_slots) || path >= static_cast<uint32_t>(P.npix)) {
+                err |= kErrQueueOverflow;
+                continue;
+            }
             float4* acc = P.nee + static_cast<size_t>(slot) * P.npix + path;
             const float4 c = P.sq_c[i];
             float4 a = *acc;
@@ -619,6 +624,7 @@ struct Wavefront {
     double stage_ms[4] = {0, 0, 0, 0};
     double total_ms = 0.0;
     uint64_t extend_launches = 0;
+    uint64_t kernel_launches = 0;
 };
 
 namespace {
@@ -804,10 +810,35 @@ void free_scene_device(pt_scene* s) {
     d = DeviceSceneBuffers{};
 }
 
+void unpin_host_arrays(pt_scene* s) {
+    for (void* p : s->pinned) cudaHostUnregister(p);
+    s->pinned.clear();
+    cudaGetLastError();
+}
+
+// Page-lock the large host arrays once so that every upload copies from pinned
+// memory (they are not resized after the build).
+static void pin_host_arrays(pt_scene* s) {
+    if (!s->pinned.empty()) return;
+    auto pin = [&](void* p, size_t bytes) {
+        if (!p || bytes < (1u << 20)) return;
+        if (cudaHostRegister(p, bytes, cudaHostRegisterDefault) == cudaSuccess) s->pinned.push_back(p);
+        else cudaGetLastError();
+    };
+    pin(s->tables.inner.data(), s->tables.inner.size() * sizeof(InnerNode));
+    pin(s->tables.tris.data(), s->tables.tris.size() * sizeof(TriRecord));
+    pin(s->host.vertices.data(), s->host.vertices.size() * sizeof(pt_vertex));
+    pin(s->host.faces.data(), s->host.faces.size() * sizeof(pt_face));
+    pin(s->host.env_rgba.data(), s->host.env_rgba.size() * sizeof(float));
+    pin(s->tables.env_pmf.data(), s->tables.env_pmf.size() * sizeof(float));
+    pin(s->tables.env_alias.data(), s->tables.env_alias.size() * sizeof(pt_alias_entry));
+}
+
 int upload_scene(pt_scene* s, int device) {
     if (!s->tables.built) { set_error("scene not built: call pt_scene_build_accel first"); return PT_ERR_STATE; }
     free_scene_device(s);
     if (int rc = ensure_device(device)) return rc;
+    pin_host_arrays(s);
     DeviceSceneBuffers& d = s->dev;
     d.device = device;
     auto up = [&](void** dst, const void* src, size_t bytes) -> int {
@@ -1004,6 +1035,8 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
         if (int rc = enqueue_batch(wf, P, st, nullptr)) return rc;
         wf.extend_launches += static_cast<uint64_t>(P.spf) * P.max_depth;
     }
+    // k_begin + per pass (raygen, 3 per bounce, finalize) + batch resolve
+    wf.kernel_launches += 1 + static_cast<uint64_t>(P.spf) * (2 + 3 * static_cast<uint64_t>(P.max_depth)) + 1;
     return PT_OK;
 }
 
@@ -1046,6 +1079,7 @@ int integrator_stats(const pt_integrator* integ, pt_render_stats* out) {
     out->shadow_ms = wf->stage_ms[2];
     out->other_ms = wf->stage_ms[3];
     out->total_ms = wf->total_ms;
+    out->kernel_launches = wf->kernel_launches;
     return PT_OK;
 }
 
@@ -1057,6 +1091,7 @@ int integrator_reset_stats(pt_integrator* integ) {
     for (double& d : wf->stage_ms) d = 0.0;
     wf->total_ms = 0.0;
     wf->extend_launches = 0;
+    wf->kernel_launches = 0;
     return PT_OK;
 }
 
