@@ -120,6 +120,24 @@ def dist_env():
     return rank, world, local
 
 
+def shard_first_frame(rank: int, batches: int) -> int:
+    """Rank r renders frames [r * batches, (r + 1) * batches): disjoint sample
+    indices (Sobol index = frame * samplePerFrame + i), no data exchange."""
+    return rank * batches
+
+
+def combine_over_ranks(ms: float, rays: float, dist, device: str):
+    """Max of the per-rank device times, sum of the rays traced."""
+    if dist is None:
+        return ms, float(rays)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    r = torch.tensor([float(rays)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(r, op=dist.ReduceOp.SUM)
+    return float(t[0]), float(r[0])
+
+
 def reference_arm(args):
     """The reference's own CPU integrator on the host cores, bounded sample."""
     rank, world, _ = dist_env()
@@ -222,7 +240,7 @@ def ours(args):
     stream = torch.cuda.Stream(device=local)
     handle = stream.cuda_stream
     renderer = pt.Renderer(scene, device=local, stream=handle)
-    frame0 = rank * batches   # disjoint sample indices per rank
+    frame0 = shard_first_frame(rank, batches)   # disjoint sample indices per rank
 
     def step():
         renderer.reset_accumulation()
@@ -248,13 +266,7 @@ def ours(args):
     st = renderer.integrator.stats()
     rays = st["camera_rays"] + st["extension_rays"] + st["shadow_rays"]
     # whole-job: rays of all ranks over the slowest rank's time
-    t = torch.tensor([ms, rays], dtype=torch.float64, device=f"cuda:{local}")
-    if dist is not None:
-        tmax = t.clone(); dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
-        ms, total_rays = float(tmax[0]), float(t[1])
-    else:
-        total_rays = float(rays)
+    ms, total_rays = combine_over_ranks(ms, rays, dist, f"cuda:{local}")
     value = total_rays / (ms / 1e3) / 1e6
 
     # e2e through the public API: host->device scene upload, render, image read back
