@@ -255,6 +255,31 @@ int pt_scene_set_frame_count(pt_scene* scene, uint32_t frame_count);
 int pt_render(pt_scene* scene, int32_t spp, float* out_rgba, int32_t out_is_device,
               pt_render_stats* stats);
 
+/* ---- batched rendering (no reference counterpart: the reference renders one
+ *      scene per process).  Many scenes of uneven size and sample budget are
+ *      rendered by ONE persistent kernel launch captured in a CUDA graph; launch
+ *      shape and chunking come from the built-in autotuner unless fixed in cfg. */
+typedef struct pt_batch_item {
+    pt_scene* scene;        /* built and uploaded; all items on one device          */
+    int32_t   spp;          /* samples per pixel for this item                       */
+    int32_t   max_depth;    /* < 0: the scene's setting                              */
+    uint32_t  first_frame;  /* frame index of the first sample (sample offset)       */
+    int32_t   _pad;
+    float*    out_rgba;     /* width*height*4 floats (host, or device, 16 B aligned) */
+} pt_batch_item;
+
+typedef struct pt_batch_config {
+    int32_t block_size;     /* 64, 128 or 256 (0: autotune / default)   */
+    int32_t blocks_per_sm;  /* 0: occupancy maximum                     */
+    int32_t chunk_spp;      /* samples per work unit (0: default)       */
+    int32_t autotune;       /* 1: time candidate shapes (cached per batch class) */
+    float   tuned_ms;       /* out: calibration time of the chosen shape */
+    int32_t _pad[3];
+} pt_batch_config;
+
+int pt_render_batch(const pt_batch_item* items, uint32_t n, int32_t out_is_device, pt_batch_config* cfg,
+                    pt_render_stats* stats);
+
 /* ---- diagnostics used by the parity tests (same kernels as the render path) ---- */
 /* rays: n x 8 floats (ox, oy, oz, unused, dx, dy, dz, tmax).  tmax only used by trace_any. */
 int pt_trace_closest(pt_scene* scene, const float* rays, uint32_t n, pt_hit* hits,

@@ -367,6 +367,30 @@ def render(scene: SceneManager, spp: int, stats: bool = False):
     return (out, st.as_dict()) if stats else out
 
 
+def render_batch(items, block_size: int = 0, blocks_per_sm: int = 0, chunk_spp: int = 0, autotune: bool = True):
+    """Render [(scene, spp[, first_frame])...] in one persistent launch.
+    Returns (list of (H, W, 4) images, stats dict, config dict)."""
+    n = len(items)
+    arr = (_ffi.BatchItem * n)()
+    outs = []
+    for k, it in enumerate(items):
+        scene, spp = it[0], it[1]
+        first = it[2] if len(it) > 2 else 0
+        cam = scene.camera
+        img = np.zeros((int(cam["height"]), int(cam["width"]), 4), np.float32)
+        outs.append(img)
+        arr[k].scene = scene.handle
+        arr[k].spp = int(spp)
+        arr[k].max_depth = -1
+        arr[k].first_frame = int(first)
+        arr[k].out_rgba = img.ctypes.data
+    cfg = _ffi.BatchConfig(block_size, blocks_per_sm, chunk_spp, 1 if autotune else 0, 0.0)
+    st = _ffi.RenderStats()
+    check(lib().pt_render_batch(arr, n, 0, C.byref(cfg), C.byref(st)))
+    return outs, st.as_dict(), {"block_size": cfg.block_size, "blocks_per_sm": cfg.blocks_per_sm,
+                                "chunk_spp": cfg.chunk_spp, "tuned_ms": cfg.tuned_ms}
+
+
 # ---- diagnostics over the same kernels ----
 def trace_closest(scene: SceneManager, origins: np.ndarray, dirs: np.ndarray) -> np.ndarray:
     rays = _pack_rays(origins, dirs, None)

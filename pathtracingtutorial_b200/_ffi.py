@@ -92,7 +92,17 @@ class RenderStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-assert C.sizeof(SceneParams) == 88 and C.sizeof(CameraFrame) == 64
+class BatchItem(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("spp", C.c_int32), ("max_depth", C.c_int32), ("first_frame", C.c_uint32),
+                ("_pad", C.c_int32), ("out_rgba", C.c_void_p)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("chunk_spp", C.c_int32),
+                ("autotune", C.c_int32), ("tuned_ms", C.c_float), ("_pad", C.c_int32 * 3)]
+
+
+assert C.sizeof(SceneParams) == 88 and C.sizeof(CameraFrame) == 64 and C.sizeof(BatchItem) == 32
 
 # (name, restype, argtypes) for every entry point declared in include/pt_b200.h
 _P = C.c_void_p
@@ -134,6 +144,7 @@ _SIGS = [
     ("pt_renderer_reset_accumulation", C.c_int, [_P, _P]),
     ("pt_scene_set_frame_count", C.c_int, [_P, C.c_uint32]),
     ("pt_render", C.c_int, [_P, C.c_int32, _P, C.c_int32, C.POINTER(RenderStats)]),
+    ("pt_render_batch", C.c_int, [_P, C.c_uint32, C.c_int32, C.POINTER(BatchConfig), C.POINTER(RenderStats)]),
     ("pt_trace_closest", C.c_int, [_P, _P, C.c_uint32, _P, C.c_int32]),
     ("pt_trace_any", C.c_int, [_P, _P, C.c_uint32, _P, C.c_int32]),
     ("pt_sampler_stream", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_uint32, C.c_int32, C.c_int32,

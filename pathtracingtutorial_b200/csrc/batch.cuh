@@ -1,0 +1,386 @@
+// batch.cuh -- batched rendering of many scenes of uneven size and sample
+// budget in ONE persistent kernel launch, captured in a CUDA graph (included
+// by integrator.cu: it reuses shade_path, the traversal and the camera).
+//
+// Work is a flat list of units (item, pixel, chunk of `chunk_spp` samples),
+// chunk-major within an item so that a warp's 32 consecutive units are 32
+// neighbouring pixels of one chunk.  Warps fetch 32 units at a time from a
+// global counter (dynamic load balance across scenes of 1k..2M triangles and
+// 16..512 spp).  Each thread traces its unit's samples end to end (camera ray,
+// bounces, shadow rays traced inline), sums the clamped sample radiance with
+// Neumaier compensation and stores the chunk partial; a resolve kernel sums
+// the chunks of every pixel in chunk order.  The result is deterministic and
+// independent of the launch shape.  Launch shape (block size, blocks per SM)
+// and chunk size come from the autotuner below.
+
+namespace ptb {
+
+struct BatchItemDev {
+    DeviceScene scene;
+    pt_camera_frame cam;
+    int32_t  width, height, spp, spf, max_depth, sampler, arg_rtl, watertight;
+    uint32_t pcg_seed, first_frame, chunk_spp, chunks;
+    unsigned long long unit_begin;   // first global unit of this item
+    unsigned long long pixel_begin;  // first global pixel of this item
+    float4*  partial;                // chunks x pixels: rgb sum, w = samples
+    float4*  out;                    // pixels: mean, w = 1
+};
+
+__device__ __forceinline__ int find_item(const BatchItemDev* items, int n, unsigned long long u, bool by_pixel) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const unsigned long long b = by_pixel ? __ldg(&items[mid].pixel_begin) : __ldg(&items[mid].unit_begin);
+        if (b <= u) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct BatchCounters { uint32_t camera, ext, shadow; };
+
+// One sample of pathTrace (path.cu:62-206) traced end to end.
+__device__ f3 trace_path_inline(const BatchItemDev& it, int x, int y, PathRng& rng, BatchCounters& bc,
+                                uint32_t& err) {
+    f3 o, d;
+    camera_ray(it.cam, it.width, it.height, x, y, rng, o, d);
+    f3 T = mk(1.0f), L = mk(0.0f);
+    float last_pdf = 0.0f;
+    bool last_delta = true;
+    InlineSink sink{it.scene, it.watertight != 0, mk(0.0f), 0u, 0u, TraceCounters{0, 0}};
+    TraceCounters tc{0, 0};
+    for (int depth = 0; depth < it.max_depth; ++depth) {
+        const RayInv r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+        float t, u, v;
+        const int prim = trace_closest(it.scene, r, it.watertight != 0, t, u, v, err, tc);
+        if (depth == 0) ++bc.camera; else ++bc.ext;
+        const bool last = depth == it.max_depth - 1;
+        f3 no, nd;
+        const bool cont = shade_path(it.scene, it.arg_rtl, depth, last, o, d, make_float4(t, __int_as_float(prim), u, v),
+                                     T, last_pdf, last_delta, L, rng, no, nd, sink);
+        if (!cont || last) break;
+        o = no;
+        d = nd;
+    }
+    err |= sink.err;
+    bc.shadow += sink.rays;
+    L += sink.acc;
+    return mk(fminf(L.x, 100.0f), fminf(L.y, 100.0f), fminf(L.z, 100.0f));
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_batch_persistent(const BatchItemDev* __restrict__ items, int n_items,
+                                                             unsigned long long total_units,
+                                                             unsigned long long* next_unit,
+                                                             unsigned long long* stats, uint32_t* err_out) {
+    const int lane = threadIdx.x & 31;
+    BatchCounters bc{0, 0, 0};
+    uint32_t err = 0;
+    uint32_t paths = 0;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(next_unit, 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total_units) break;
+        const unsigned long long u = base + static_cast<unsigned long long>(lane);
+        if (u < total_units) {
+            const int k = find_item(items, n_items, u, false);
+            const BatchItemDev& it = items[k];
+            const unsigned long long local = u - it.unit_begin;
+            const uint32_t npix = static_cast<uint32_t>(it.width) * static_cast<uint32_t>(it.height);
+            const uint32_t chunk = static_cast<uint32_t>(local / npix);
+            const uint32_t pix = static_cast<uint32_t>(local % npix);
+            const int x = static_cast<int>(pix % static_cast<uint32_t>(it.width));
+            const int y = static_cast<int>(pix / static_cast<uint32_t>(it.width));
+            const uint32_t s0 = chunk * it.chunk_spp;
+            const uint32_t s1 = min(s0 + it.chunk_spp, static_cast<uint32_t>(it.spp));
+            float sx = 0.0f, sy = 0.0f, sz = 0.0f, cx = 0.0f, cy = 0.0f, cz = 0.0f;
+            for (uint32_t s = s0; s < s1; ++s) {
+                const uint32_t frame = it.first_frame + s / static_cast<uint32_t>(it.spf);
+                const uint32_t i = s % static_cast<uint32_t>(it.spf);
+                PathRng rng = make_rng(it.sampler, x, y, frame, static_cast<uint32_t>(it.spf), i, it.pcg_seed);
+                const f3 L = trace_path_inline(it, x, y, rng, bc, err);
+                neumaier(sx, cx, L.x);
+                neumaier(sy, cy, L.y);
+                neumaier(sz, cz, L.z);
+                ++paths;
+            }
+            it.partial[static_cast<size_t>(chunk) * npix + pix] =
+                make_float4(sx + cx, sy + cy, sz + cz, static_cast<float>(s1 - s0));
+        }
+    }
+    warp_count(stats + kStatCameraRays, bc.camera);
+    warp_count(stats + kStatExtRays, bc.ext);
+    warp_count(stats + kStatShadowRays, bc.shadow);
+    warp_count(stats + kStatPaths, paths);
+    if (err) atomicOr(err_out, err);
+}
+
+__global__ void k_batch_resolve(const BatchItemDev* __restrict__ items, int n_items, unsigned long long total_pixels) {
+    for (unsigned long long g = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; g < total_pixels;
+         g += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        const int k = find_item(items, n_items, g, true);
+        const BatchItemDev& it = items[k];
+        const uint32_t npix = static_cast<uint32_t>(it.width) * static_cast<uint32_t>(it.height);
+        const uint32_t pix = static_cast<uint32_t>(g - it.pixel_begin);
+        float sx = 0.0f, sy = 0.0f, sz = 0.0f, cx = 0.0f, cy = 0.0f, cz = 0.0f, n = 0.0f;
+        for (uint32_t c = 0; c < it.chunks; ++c) {
+            const float4 p = it.partial[static_cast<size_t>(c) * npix + pix];
+            neumaier(sx, cx, p.x);
+            neumaier(sy, cy, p.y);
+            neumaier(sz, cz, p.z);
+            n += p.w;
+        }
+        it.out[pix] = n > 0.0f ? make_float4((sx + cx) / n, (sy + cy) / n, (sz + cz) / n, 1.0f)
+                               : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+
+struct BatchPlan {
+    std::vector<BatchItemDev> items;
+    unsigned long long total_units = 0, total_pixels = 0;
+    size_t partial_floats4 = 0, out_floats4 = 0;
+};
+
+int launch_persistent(int block, int grid, const BatchItemDev* d_items, int n, unsigned long long total,
+                      unsigned long long* next, unsigned long long* stats, uint32_t* err, cudaStream_t st) {
+    switch (block) {
+        case 64: k_batch_persistent<64><<<grid, 64, 0, st>>>(d_items, n, total, next, stats, err); break;
+        case 128: k_batch_persistent<128><<<grid, 128, 0, st>>>(d_items, n, total, next, stats, err); break;
+        case 256: k_batch_persistent<256><<<grid, 256, 0, st>>>(d_items, n, total, next, stats, err); break;
+        default: set_error("block size must be 64, 128 or 256"); return PT_ERR_INVALID;
+    }
+    PT_CU(cudaGetLastError());
+    return PT_OK;
+}
+
+int max_blocks_per_sm(int block) {
+    int v = 1;
+    const void* k = block == 64 ? reinterpret_cast<const void*>(k_batch_persistent<64>)
+                  : block == 128 ? reinterpret_cast<const void*>(k_batch_persistent<128>)
+                                 : reinterpret_cast<const void*>(k_batch_persistent<256>);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k, block, 0) != cudaSuccess || v < 1) { cudaGetLastError(); v = 1; }
+    return v;
+}
+
+BatchPlan make_plan(const pt_batch_item* in, uint32_t n, uint32_t chunk_spp, int cap_spp) {
+    BatchPlan plan;
+    plan.items.resize(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        const pt_scene* s = in[k].scene;
+        BatchItemDev& it = plan.items[k];
+        std::memset(&it, 0, sizeof(it));
+        it.scene = device_view(s);
+        it.cam = camera_frame(s->host.camera);
+        it.width = s->host.camera.width;
+        it.height = s->host.camera.height;
+        it.spp = cap_spp > 0 ? std::min(cap_spp, in[k].spp) : in[k].spp;
+        it.spf = s->host.settings.sample_per_frame;
+        it.max_depth = in[k].max_depth >= 0 ? in[k].max_depth : s->host.settings.max_depth;
+        it.sampler = s->host.settings.sampler_type;
+        it.arg_rtl = s->host.settings.arg_order == PT_ARGS_RTL ? 1 : 0;
+        it.watertight = (s->host.settings.flags & PT_FLAG_WATERTIGHT) ? 1 : 0;
+        it.pcg_seed = s->host.settings.pcg_seed;
+        it.first_frame = in[k].first_frame;
+        it.chunk_spp = chunk_spp;
+        it.chunks = (static_cast<uint32_t>(it.spp) + chunk_spp - 1) / chunk_spp;
+        const unsigned long long npix = static_cast<unsigned long long>(it.width) * it.height;
+        it.unit_begin = plan.total_units;
+        it.pixel_begin = plan.total_pixels;
+        plan.total_units += npix * it.chunks;
+        plan.total_pixels += npix;
+        plan.partial_floats4 += npix * it.chunks;
+        plan.out_floats4 += npix;
+    }
+    return plan;
+}
+
+struct BatchTune { int block, blocks_per_sm, chunk_spp; double ms; };
+std::mutex g_tune_mu;
+std::vector<std::pair<std::string, BatchTune>> g_tune_cache;
+
+std::string tune_key(int device, const pt_batch_item* items, uint32_t n) {
+    uint64_t tris = 0, pix = 0, spp = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        tris += items[k].scene->host.faces.size();
+        pix += static_cast<uint64_t>(items[k].scene->host.camera.width) * items[k].scene->host.camera.height;
+        spp += static_cast<uint64_t>(items[k].spp);
+    }
+    auto lg = [](uint64_t v) { int b = 0; while (v > 1) { v >>= 1; ++b; } return b; };
+    return std::to_string(device) + ":" + std::to_string(n) + ":" + std::to_string(lg(tris)) + ":" +
+           std::to_string(lg(pix)) + ":" + std::to_string(lg(spp / std::max<uint32_t>(n, 1)));
+}
+
+}  // namespace
+
+// Renders every item; stats accumulate over the batch.
+int render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batch_config* cfg, pt_render_stats* stats) {
+    if (n == 0) return PT_OK;
+    const int device = in[0].scene->dev.device;
+    for (uint32_t k = 0; k < n; ++k) {
+        if (!in[k].scene || !in[k].scene->dev.uploaded) { set_error("batch item " + std::to_string(k) + ": scene not uploaded"); return PT_ERR_STATE; }
+        if (in[k].scene->dev.device != device) { set_error("batch items must live on one device"); return PT_ERR_INVALID; }
+        if (in[k].spp <= 0 || !in[k].out_rgba) { set_error("batch item " + std::to_string(k) + ": invalid spp or output"); return PT_ERR_INVALID; }
+    }
+    if (int rc = ensure_device(device)) return rc;
+    int sms = 0;
+    PT_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    cudaStream_t st;
+    PT_CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct Guard { std::vector<void*> bufs; cudaStream_t st; ~Guard() { for (void* b : bufs) cudaFree(b); cudaStreamDestroy(st); } } g{{}, st};
+    auto alloc = [&](size_t bytes) -> void* {
+        void* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+        g.bufs.push_back(p);
+        return p;
+    };
+    unsigned long long* d_misc = static_cast<unsigned long long*>(alloc(64 * 8));
+    if (!d_misc) { set_error("batch: allocation failed"); return PT_ERR_NOMEM; }
+    unsigned long long* d_next = d_misc;
+    unsigned long long* d_stats = d_misc + 8;
+    uint32_t* d_err = reinterpret_cast<uint32_t*>(d_misc + 32);
+
+    // ---- pick the launch shape (autotuner) ----
+    BatchTune tune{cfg && cfg->block_size ? cfg->block_size : 128,
+                   cfg && cfg->blocks_per_sm ? cfg->blocks_per_sm : 0,
+                   cfg && cfg->chunk_spp ? cfg->chunk_spp : 8, 0.0};
+    const bool autotune = !cfg || cfg->autotune;
+    const std::string key = tune_key(device, in, n);
+    bool cached = false;
+    if (autotune) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        for (auto& kv : g_tune_cache) if (kv.first == key) { tune = kv.second; cached = true; }
+    }
+    if (autotune && !cached) {
+        // time candidate shapes on a calibration batch: every item capped at 8 spp
+        std::vector<BatchTune> cands;
+        for (int block : {64, 128, 256}) {
+            const int mx = max_blocks_per_sm(block);
+            for (int bps : {mx, std::max(1, mx / 2)}) cands.push_back({block, bps, 8, 0.0});
+        }
+        BatchPlan cal = make_plan(in, n, 8, 8);
+        BatchItemDev* d_items = static_cast<BatchItemDev*>(alloc(cal.items.size() * sizeof(BatchItemDev)));
+        float4* part = static_cast<float4*>(alloc(cal.partial_floats4 * sizeof(float4)));
+        if (!d_items || !part) { set_error("batch: calibration allocation failed"); return PT_ERR_NOMEM; }
+        size_t off = 0;
+        for (auto& it : cal.items) {
+            it.partial = part + off;
+            it.out = nullptr;
+            off += static_cast<size_t>(it.width) * it.height * it.chunks;
+        }
+        PT_CU(cudaMemcpyAsync(d_items, cal.items.data(), cal.items.size() * sizeof(BatchItemDev), cudaMemcpyHostToDevice, st));
+        cudaEvent_t e0, e1;
+        PT_CU(cudaEventCreate(&e0));
+        PT_CU(cudaEventCreate(&e1));
+        double best = 1e30;
+        for (BatchTune& c : cands) {
+            for (int rep = 0; rep < 2; ++rep) {
+                PT_CU(cudaMemsetAsync(d_next, 0, 8, st));
+                PT_CU(cudaEventRecord(e0, st));
+                if (int rc = launch_persistent(c.block, c.blocks_per_sm * sms, d_items, static_cast<int>(n),
+                                               cal.total_units, d_next, d_stats, d_err, st)) return rc;
+                PT_CU(cudaEventRecord(e1, st));
+                PT_CU(cudaEventSynchronize(e1));
+                float ms = 0.0f;
+                PT_CU(cudaEventElapsedTime(&ms, e0, e1));
+                c.ms = ms;   // second repetition counts (first is warm-up)
+            }
+            if (c.ms < best) { best = c.ms; tune = c; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        // chunk size: larger chunks amortise the per-unit setup; bounded by the partial buffer
+        uint64_t pix = 0, spp_max = 0;
+        for (uint32_t k = 0; k < n; ++k) {
+            pix += static_cast<uint64_t>(in[k].scene->host.camera.width) * in[k].scene->host.camera.height;
+            spp_max = std::max<uint64_t>(spp_max, static_cast<uint64_t>(in[k].spp));
+        }
+        tune.chunk_spp = 16;
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache.emplace_back(key, tune);
+    }
+    if (tune.blocks_per_sm <= 0) tune.blocks_per_sm = max_blocks_per_sm(tune.block);
+
+    // ---- the batch itself: one persistent launch + resolve, captured in a graph ----
+    BatchPlan plan = make_plan(in, n, static_cast<uint32_t>(tune.chunk_spp), 0);
+    BatchItemDev* d_items = static_cast<BatchItemDev*>(alloc(plan.items.size() * sizeof(BatchItemDev)));
+    float4* part = static_cast<float4*>(alloc(plan.partial_floats4 * sizeof(float4)));
+    float4* outs = out_is_device ? nullptr : static_cast<float4*>(alloc(plan.out_floats4 * sizeof(float4)));
+    if (!d_items || !part || (!out_is_device && !outs)) { set_error("batch: allocation failed (partials)"); return PT_ERR_NOMEM; }
+    size_t off = 0, ooff = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        BatchItemDev& it = plan.items[k];
+        it.partial = part + off;
+        off += static_cast<size_t>(it.width) * it.height * it.chunks;
+        it.out = out_is_device ? reinterpret_cast<float4*>(in[k].out_rgba) : outs + ooff;
+        ooff += static_cast<size_t>(it.width) * it.height;
+    }
+    PT_CU(cudaMemcpyAsync(d_items, plan.items.data(), plan.items.size() * sizeof(BatchItemDev), cudaMemcpyHostToDevice, st));
+    PT_CU(cudaMemsetAsync(d_stats, 0, 24 * 8, st));
+    PT_CU(cudaMemsetAsync(d_err, 0, 4, st));
+    PT_CU(cudaStreamSynchronize(st));
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    PT_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(d_next, 0, 8, st);
+    int rc = launch_persistent(tune.block, tune.blocks_per_sm * sms, d_items, static_cast<int>(n), plan.total_units,
+                               d_next, d_stats, d_err, st);
+    k_batch_resolve<<<sms * 8, 256, 0, st>>>(d_items, static_cast<int>(n), plan.total_pixels);
+    const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+    if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+    if (ec != cudaSuccess) { set_error(std::string("batch graph capture: ") + cudaGetErrorString(ec)); return PT_ERR_CUDA; }
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) { set_error(std::string("batch graph instantiate: ") + cudaGetErrorString(ei)); return PT_ERR_CUDA; }
+    cudaEvent_t e0, e1;
+    PT_CU(cudaEventCreate(&e0));
+    PT_CU(cudaEventCreate(&e1));
+    PT_CU(cudaEventRecord(e0, st));
+    const cudaError_t el = cudaGraphLaunch(exec, st);
+    PT_CU(cudaEventRecord(e1, st));
+    const cudaError_t es = cudaStreamSynchronize(st);
+    cudaGraphExecDestroy(exec);
+    if (el != cudaSuccess || es != cudaSuccess) {
+        set_error(std::string("batch launch: ") + cudaGetErrorString(el != cudaSuccess ? el : es));
+        cudaEventDestroy(e0); cudaEventDestroy(e1);
+        return PT_ERR_CUDA;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    uint32_t err = 0;
+    PT_CU(cudaMemcpy(&err, d_err, 4, cudaMemcpyDeviceToHost));
+    if (err) { set_error("batch: device error word " + std::to_string(err)); return PT_ERR_DEVICE; }
+    if (!out_is_device) {
+        for (uint32_t k = 0; k < n; ++k) {
+            const BatchItemDev& it = plan.items[k];
+            PT_CU(cudaMemcpy(in[k].out_rgba, it.out, static_cast<size_t>(it.width) * it.height * sizeof(float4),
+                             cudaMemcpyDeviceToHost));
+        }
+    }
+    if (stats) {
+        unsigned long long s[kStatCount];
+        PT_CU(cudaMemcpy(s, d_stats, sizeof(s), cudaMemcpyDeviceToHost));
+        std::memset(stats, 0, sizeof(*stats));
+        stats->camera_rays = s[kStatCameraRays];
+        stats->extension_rays = s[kStatExtRays];
+        stats->shadow_rays = s[kStatShadowRays];
+        stats->paths = s[kStatPaths];
+        stats->total_ms = ms;
+        stats->kernel_launches = 2;
+    }
+    if (cfg) {
+        cfg->block_size = tune.block;
+        cfg->blocks_per_sm = tune.blocks_per_sm;
+        cfg->chunk_spp = tune.chunk_spp;
+        cfg->tuned_ms = static_cast<float>(tune.ms);
+    }
+    return PT_OK;
+}
+
+}  // namespace ptb

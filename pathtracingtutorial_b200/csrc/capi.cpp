@@ -406,6 +406,14 @@ int pt_render(pt_scene* s, int32_t spp, float* out_rgba, int32_t out_is_device, 
     PT_GUARD_END
 }
 
+int pt_render_batch(const pt_batch_item* items, uint32_t n, int32_t out_is_device, pt_batch_config* cfg,
+                    pt_render_stats* stats) {
+    PT_REQUIRE(n == 0 || items, "null items");
+    PT_GUARD_BEGIN
+    return render_batch(items, n, out_is_device, cfg, stats);
+    PT_GUARD_END
+}
+
 // ---- diagnostics ----
 int pt_trace_closest(pt_scene* s, const float* rays, uint32_t n, pt_hit* hits, int32_t ptrs_are_device) {
     PT_REQUIRE(s && (n == 0 || (rays && hits)), "null argument");

@@ -26,6 +26,7 @@ int  trace_rays(pt_scene* s, const float* rays, uint32_t n, pt_hit* hits, uint8_
 int  sampler_stream(int type, int w, int h, uint32_t frame, int spf, int sif, uint32_t ndims, uint32_t seed,
                     int device, float* out_host);
 int  bsdf_eval(pt_scene* s, const float* in, uint32_t n, float* out_host);
+int  render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batch_config* cfg, pt_render_stats* stats);
 int  current_device(int* dev);
 int  device_sync(int device);
 

@@ -187,6 +187,39 @@ __device__ __forceinline__ void emit_shadow(const WaveParams& P, bool want, uint
 // ---------------------------------------------------------------------------
 __global__ void k_begin(PassState* ps, uint32_t frame) { ps->frame = frame; }
 
+// Sampler for pixel (x, y), sample (frame, i) (kernelPathTrace, path.cu:217-225).
+__device__ __forceinline__ PathRng make_rng(int type, int x, int y, uint32_t frame, uint32_t spf, uint32_t i,
+                                            uint32_t user_seed) {
+    PathRng rng;
+    rng.type = type; rng.px = x; rng.py = y; rng.sample_index = frame * spf + i;
+    rng.s = (type == PT_SAMPLER_SOBOL) ? 0u : pcg_seed(x, y, frame, i, user_seed);
+    return rng;
+}
+
+// Camera ray for pixel (x, y): 2 jitter draws, +2 lens draws with aperture
+// (emitRay, path.cu:31-59).  The direction is renormalised as Ray's
+// constructor does (core/ray.h:13).
+__device__ __forceinline__ void camera_ray(const pt_camera_frame& c, int width, int height, int x, int y,
+                                           PathRng& rng, f3& pos, f3& dir) {
+    const f3 fwd = ld3(c.forward), rgt = ld3(c.right), cup = ld3(c.up);
+    const float jx = rng_next(rng);
+    const float jy = rng_next(rng);
+    const float u = (2.0f * (x + jx) / width - 1.0f) * c.tan_half_fov * c.aspect;
+    const float v = (2.0f * (y + jy) / height - 1.0f) * c.tan_half_fov;
+    pos = ld3(c.position);
+    dir = normalize(u * rgt + v * cup + fwd);
+    if (c.aperture > 0.0f) {
+        const f3 focal = pos + dir * (c.focal_distance / dot(dir, fwd));
+        const float lx = rng_next(rng);
+        const float ly = rng_next(rng);
+        const float r = sqrtf(lx) * c.aperture;
+        const float th = kTwoPi * ly;
+        pos = pos + rgt * (r * cosf(th)) + cup * (r * sinf(th));
+        dir = normalize(focal - pos);
+    }
+    dir = normalize(dir);
+}
+
 __global__ void __launch_bounds__(256) k_raygen(WaveParams P, int sample_in_frame) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.counts[0] = static_cast<uint32_t>(P.npix);
@@ -195,31 +228,12 @@ __global__ void __launch_bounds__(256) k_raygen(WaveParams P, int sample_in_fram
         atomicAdd(P.stats + kStatPaths, static_cast<unsigned long long>(P.npix));
     }
     const uint32_t frame = P.pass->frame;
-    const uint32_t sidx = frame * static_cast<uint32_t>(P.spf) + static_cast<uint32_t>(sample_in_frame);
-    const pt_camera_frame& c = P.cam;
-    const f3 fwd = ld3(c.forward), rgt = ld3(c.right), cup = ld3(c.up), pos0 = ld3(c.position);
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.npix; p += gridDim.x * blockDim.x) {
         const int x = p % P.width, y = p / P.width;
-        PathRng rng;
-        rng.type = P.sampler_type; rng.px = x; rng.py = y; rng.sample_index = sidx;
-        rng.s = (P.sampler_type == PT_SAMPLER_SOBOL) ? 0u
-                : pcg_seed(x, y, frame, static_cast<uint32_t>(sample_in_frame), P.pcg_seed);
-        const float jx = rng_next(rng);
-        const float jy = rng_next(rng);
-        const float u = (2.0f * (x + jx) / P.width - 1.0f) * c.tan_half_fov * c.aspect;
-        const float v = (2.0f * (y + jy) / P.height - 1.0f) * c.tan_half_fov;
-        f3 pos = pos0;
-        f3 dir = normalize(u * rgt + v * cup + fwd);
-        if (c.aperture > 0.0f) {
-            const f3 focal = pos + dir * (c.focal_distance / dot(dir, fwd));
-            const float lx = rng_next(rng);
-            const float ly = rng_next(rng);
-            const float r = sqrtf(lx) * c.aperture;
-            const float th = kTwoPi * ly;
-            pos = pos + rgt * (r * cosf(th)) + cup * (r * sinf(th));
-            dir = normalize(focal - pos);
-        }
-        dir = normalize(dir);
+        PathRng rng = make_rng(P.sampler_type, x, y, frame, static_cast<uint32_t>(P.spf),
+                               static_cast<uint32_t>(sample_in_frame), P.pcg_seed);
+        f3 pos, dir;
+        camera_ray(P.cam, P.width, P.height, x, y, rng, pos, dir);
         P.queue[0][p] = static_cast<uint32_t>(p);
         P.ray_o[0][p] = f4of(pos, 0.0f);
         P.ray_d[0][p] = f4of(dir, 0.0f);
@@ -264,11 +278,37 @@ __global__ void __launch_bounds__(128) k_extend(WaveParams P, int q, int depth) 
     }
 }
 
-// One bounce of pathTrace (path.cu:69-199) for path p.  Returns true when the
-// path continues with ray (no, nd).
-__device__ bool shade_path(const WaveParams& P, int depth, bool last, uint32_t p, f3 ro, f3 rd, float4 h,
-                           f3& T, float& last_pdf, bool& last_delta, f3& L, PathRng& rng, f3& no, f3& nd) {
-    const DeviceScene& s = P.scene;
+// Shadow-ray sinks for shade_path: the wavefront queues a shadow ray per light
+// slot; the persistent (batched) kernel traces it on the spot.
+struct QueueSink {
+    const WaveParams& P;
+    uint32_t path;
+    __device__ __forceinline__ void emit(bool want, uint32_t slot, f3 o, f3 d, float tmax, f3 c) {
+        emit_shadow(P, want, path, slot, o, d, tmax, c);
+    }
+};
+
+struct InlineSink {
+    const DeviceScene& s;
+    bool watertight;
+    f3 acc;
+    uint32_t err;
+    uint32_t rays;
+    TraceCounters tc;
+    __device__ __forceinline__ void emit(bool want, uint32_t, f3 o, f3 d, float tmax, f3 c) {
+        if (!want) return;
+        ++rays;
+        const RayInv r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+        if (!trace_any(s, r, tmax, watertight, err, tc)) acc += c;
+    }
+};
+
+// One bounce of pathTrace (path.cu:69-199).  Returns true when the path
+// continues with ray (no, nd).  Shadow rays go to `sink`.
+template <class Sink>
+__device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool last, f3 ro, f3 rd, float4 h,
+                           f3& T, float& last_pdf, bool& last_delta, f3& L, PathRng& rng, f3& no, f3& nd,
+                           Sink& sink) {
     const int prim = __float_as_int(h.y);
     if (prim < 0) {
         const f3 env = env_radiance(s, rd);
@@ -312,7 +352,7 @@ __device__ bool shade_path(const WaveParams& P, int depth, bool last, uint32_t p
         // area light sample (sampleAreaLight, direct_lighting.cuh:75-121)
         if (has_area) {
             float u1, u2;
-            rng_pair(rng, P.arg_rtl, u1, u2);
+            rng_pair(rng, arg_rtl, u1, u2);
             const uint32_t li = sample_alias(s.tri_alias, s.num_emissive, u1, u2);
             const uint32_t tri = __ldg(&s.emissive[li].triangle_index);
             const float pmf = __ldg(&s.emissive[li].selection_pmf);
@@ -350,17 +390,17 @@ __device__ bool shade_path(const WaveParams& P, int depth, bool last, uint32_t p
                 ok = !is_zero(contrib);
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
-            emit_shadow(P, ok, p, 0, hp + N * (1e-4f * sg), normalize(wi), dist - 1e-3f, contrib);
+            sink.emit(ok, 0, hp + N * (1e-4f * sg), normalize(wi), dist - 1e-3f, contrib);
         }
         // environment sample (sampleEnvironmentLight, direct_lighting.cuh:123-154)
         if (has_env) {
             float u1, u2;
-            rng_pair(rng, P.arg_rtl, u1, u2);
+            rng_pair(rng, arg_rtl, u1, u2);
             const uint32_t texel = sample_alias(s.env_alias, s.num_env_texels, u1, u2);
             const int x = static_cast<int>(texel % static_cast<uint32_t>(s.env_w));
             const int y = static_cast<int>(texel / static_cast<uint32_t>(s.env_w));
             float j1, j2;
-            rng_pair(rng, P.arg_rtl, j1, j2);
+            rng_pair(rng, arg_rtl, j1, j2);
             const float uu = (static_cast<float>(x) + j1) / static_cast<float>(s.env_w);
             const float vv = (static_cast<float>(y) + j2) / static_cast<float>(s.env_h);
             const f3 wi = dir_from_uv(uu, vv);
@@ -373,7 +413,7 @@ __device__ bool shade_path(const WaveParams& P, int depth, bool last, uint32_t p
                 ok = !is_zero(contrib);
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
-            emit_shadow(P, ok, p, 1, hp + N * (1e-4f * sg), normalize(wi), FLT_MAX, contrib);
+            sink.emit(ok, 1, hp + N * (1e-4f * sg), normalize(wi), FLT_MAX, contrib);
         }
         // punctual lights, no MIS (evaluatePunctualLights, direct_lighting.cuh:158-200)
         for (uint32_t j = 0; j < s.num_punctual; ++j) {
@@ -410,11 +450,11 @@ __device__ bool shade_path(const WaveParams& P, int depth, bool last, uint32_t p
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
             const float tmax = dist < FLT_MAX ? dist - 1e-3f : FLT_MAX;
-            emit_shadow(P, ok, p, 2 + j, hp + N * (1e-4f * sg), normalize(wi), tmax, contrib);
+            sink.emit(ok, 2 + j, hp + N * (1e-4f * sg), normalize(wi), tmax, contrib);
         }
     }
     if (last) return false;   // the sampled continuation would never be traced
-    const BsdfSample bs = disney_sample(me, wo, N, rng, P.arg_rtl, entering);
+    const BsdfSample bs = disney_sample(me, wo, N, rng, arg_rtl, entering);
     if (!bs.valid) return false;
     T *= bs.weight;
     const bool transmitted = dot(bs.wi, gn) < 0.0f;
@@ -463,8 +503,9 @@ __global__ void __launch_bounds__(128) k_shade(WaveParams P, int q, int depth, i
         rng.sample_index = sidx;
         rng.s = P.rng[p];
         f3 no = mk(0.0f), nd = mk(0.0f);
-        const bool cont = shade_path(P, depth, last, p, f3of(o4), f3of(d4), h, T, last_pdf, last_delta, L, rng, no, nd)
-                          && !last;
+        QueueSink sink{P, p};
+        const bool cont = shade_path(P.scene, P.arg_rtl, depth, last, f3of(o4), f3of(d4), h, T, last_pdf,
+                                     last_delta, L, rng, no, nd, sink) && !last;
         P.thr[p] = f4of(T, last_pdf);
         P.lo[p] = f4of(L, last_delta ? 1.0f : 0.0f);
         P.rng[p] = rng.s;
@@ -1186,3 +1227,5 @@ int device_sync(int device) {
 }
 
 }  // namespace ptb
+
+#include "batch.cuh"

@@ -286,11 +286,34 @@ def icosphere_field(n_spheres: int = 400, subdiv: int = 4, width: int = 1920, he
            np.zeros((len(pos), 4), np.float32), tri, sph_mat))
     b.add(g)
     v, f = b.arrays()
-    env = sky_env(*env_size)
+    env = sky_env(*env_size) if env_size is not None else None
     cam = make_camera(position=(0.0, 7.0, 32.0), look_at=(0.0, 0.5, 0.0), fov=50.0, width=width, height=height)
     return SceneArrays(f"icosphere_field_{len(f)}tri", v, f, mats, cam, env, spp=spp, sample_per_frame=4,
                        max_depth=max_depth, sampler=SAMPLER_SOBOL,
                        meta={"triangles": int(len(f)), "spheres": n_spheres, "subdiv": subdiv})
+
+
+def uneven_batch(n_scenes: int = 64, seed: int = 3, env_size=(1024, 512), max_depth: int = 12,
+                 tri_range=(1_000, 2_000_000)):
+    """Uneven batch: scenes generated like icosphere_field with triangle counts
+    log-uniform in tri_range, resolutions drawn from {256^2, 512^2, 1024^2,
+    1280x720}, spp uniform in 16..512, depth 12.  One shared sky (env_size)."""
+    rng = np.random.default_rng(seed)
+    env = sky_env(*env_size)
+    res = [(256, 256), (512, 512), (1024, 1024), (1280, 720)]
+    out = []
+    for k in range(n_scenes):
+        target = float(np.exp(rng.uniform(np.log(tri_range[0]), np.log(tri_range[1]))))
+        sub = next(s for s in (1, 2, 3, 4) if target / (20 * 4 ** s) <= 400 or s == 4)
+        n_sph = max(1, int(round(target / (20 * 4 ** sub))))
+        w, h = res[int(rng.integers(0, len(res)))]
+        spp = int(rng.integers(16, 513))
+        sa = icosphere_field(n_spheres=n_sph, subdiv=sub, width=w, height=h, spp=spp, max_depth=max_depth,
+                             seed=int(rng.integers(0, 2 ** 31)), env_size=None)
+        sa.env = env
+        sa.name = f"batch{k:02d}_{len(sa.faces)}tri_{w}x{h}_{spp}spp"
+        out.append(sa)
+    return out
 
 
 # ---------------------------------------------------------------------------
