@@ -280,6 +280,36 @@ typedef struct pt_batch_config {
 int pt_render_batch(const pt_batch_item* items, uint32_t n, int32_t out_is_device, pt_batch_config* cfg,
                     pt_render_stats* stats);
 
+/* ---- learned path guiding (no reference counterpart).  A hash-grid + MLP
+ *      network (BF16 tensor-core kernels) learns the incident radiance per
+ *      position online from the integrator's own samples; while attached, the
+ *      integrator draws directions from it or the BSDF by one-sample MIS
+ *      (mixture probability 0.5), which keeps the estimator's expectation.
+ *      Vertices with delta lobes (roughness < 0.01) are never guided. */
+#define PT_GUIDE_OFF   0
+#define PT_GUIDE_USE   1   /* sample with the network, do not train      */
+#define PT_GUIDE_TRAIN 2   /* sample with it and train after every pass  */
+typedef struct pt_guide pt_guide;
+int pt_guide_create(pt_scene* scene, uint32_t seed, pt_guide** out);   /* scene must be uploaded */
+int pt_guide_destroy(pt_guide* guide);
+int pt_guide_set_learning_rate(pt_guide* guide, float lr);
+/* steps taken and samples used by the last step (synchronises the device) */
+int pt_guide_info(const pt_guide* guide, uint32_t* steps, uint32_t* last_samples);
+int pt_integrator_set_guide(pt_integrator* integ, pt_guide* guide, int32_t mode);
+/* Evaluate the learned directional density q(dir | pos) for n queries
+ * (pos[3], dir[3] floats each) -> out[n].  Diagnostic / checkpoint check. */
+int pt_guide_eval(pt_guide* guide, const float* pos_dir, uint32_t n, float* out_pdf);
+/* Parameters as used by the kernels: weights (13312 floats: layers 32->64,
+ * 64->64, 64->64, 64->48 row-major [out][in], BF16 values) and, if grid is not
+ * NULL, the hash grid (16 levels x 2^19 entries x 2 features, FP16 values);
+ * meta = {lo[3], inv_extent[3], scale[16], dense_limit}. */
+int pt_guide_get_params(const pt_guide* guide, float* weights, float* grid, float* meta);
+/* One backward pass (no optimiser step) over n samples given as n x 8 floats
+ * (normalised position[3], weight, direction[3], 0); returns the weight
+ * gradient (13312 floats) and, if grid_grad is not NULL, the hash-grid
+ * gradient (16 x 2^19 x 2 floats). */
+int pt_guide_backward(pt_guide* guide, const float* samples, uint32_t n, float* weight_grad, float* grid_grad);
+
 /* ---- diagnostics used by the parity tests (same kernels as the render path) ---- */
 /* rays: n x 8 floats (ox, oy, oz, unused, dx, dy, dz, tmax).  tmax only used by trace_any. */
 int pt_trace_closest(pt_scene* scene, const float* rays, uint32_t n, pt_hit* hits,

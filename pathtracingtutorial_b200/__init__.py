@@ -367,6 +367,96 @@ def render(scene: SceneManager, spp: int, stats: bool = False):
     return (out, st.as_dict()) if stats else out
 
 
+class Guide:
+    """Learned directional guide (hash grid + MLP + 8-lobe vMF mixture) for one scene."""
+
+    OFF, USE, TRAIN = _ffi.GUIDE_OFF, _ffi.GUIDE_USE, _ffi.GUIDE_TRAIN
+
+    def __init__(self, scene: SceneManager, seed: int = 1, lr: float | None = None):
+        h = C.c_void_p()
+        check(lib().pt_guide_create(scene.handle, seed, C.byref(h)))
+        self._h = h
+        if lr is not None:
+            check(lib().pt_guide_set_learning_rate(self._h, float(lr)))
+
+    def attach(self, integrator: PathIntegrator, mode: int) -> None:
+        check(lib().pt_integrator_set_guide(integrator._h, self._h if mode else None, mode))
+
+    def info(self) -> dict:
+        steps, samples = C.c_uint32(), C.c_uint32()
+        check(lib().pt_guide_info(self._h, C.byref(steps), C.byref(samples)))
+        return {"steps": steps.value, "last_samples": samples.value}
+
+    def pdf(self, pos: np.ndarray, dirs: np.ndarray) -> np.ndarray:
+        q = np.ascontiguousarray(np.concatenate([np.asarray(pos, np.float32).reshape(-1, 3),
+                                                 np.asarray(dirs, np.float32).reshape(-1, 3)], 1))
+        out = np.zeros(len(q), np.float32)
+        check(lib().pt_guide_eval(self._h, ptr(q), len(q), ptr(out)))
+        return out
+
+    N_WEIGHTS = 13312
+    GRID_SHAPE = (16, 1 << 19, 2)
+
+    def params(self, with_grid: bool = True) -> dict:
+        """The network as the kernels use it: BF16 weights and FP16 grid values
+        widened to float32, plus the position normalisation and level scales."""
+        w = np.zeros(self.N_WEIGHTS, np.float32)
+        grid = np.zeros(self.GRID_SHAPE, np.float32) if with_grid else None
+        meta = np.zeros(6 + 16 + 1, np.float32)
+        check(lib().pt_guide_get_params(self._h, ptr(w), ptr(grid) if with_grid else None, ptr(meta)))
+        return {"weights": w, "grid": grid, "lo": meta[0:3].copy(), "inv_extent": meta[3:6].copy(),
+                "scale": meta[6:22].copy(), "dense_limit": int(meta[22])}
+
+    def backward(self, pos01: np.ndarray, weight: np.ndarray, dirs: np.ndarray, with_grid: bool = True):
+        """Gradient of mean(-weight * log q(dir | pos)) over the given samples
+        (positions already normalised to [0,1]^3), computed by the training
+        kernel without an optimiser step.  Returns (weight_grad, grid_grad)."""
+        n = len(weight)
+        s = np.zeros((n, 8), np.float32)
+        s[:, 0:3] = np.asarray(pos01, np.float32).reshape(-1, 3)
+        s[:, 3] = np.asarray(weight, np.float32)
+        s[:, 4:7] = np.asarray(dirs, np.float32).reshape(-1, 3)
+        gw = np.zeros(self.N_WEIGHTS, np.float32)
+        gg = np.zeros(self.GRID_SHAPE, np.float32) if with_grid else None
+        check(lib().pt_guide_backward(self._h, ptr(s), n, ptr(gw), ptr(gg) if with_grid else None))
+        return gw, gg
+
+    def close(self) -> None:
+        if self._h:
+            lib().pt_guide_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def render_guided(scene: SceneManager, train_spp: int, spp: int, guide: Guide | None = None, seed: int = 1,
+                  device: int = 0, stream: int | None = None, first_frame: int = 0):
+    """Train a guide online for train_spp samples per pixel (those samples are
+    discarded), then render spp samples per pixel sampling with it.
+    Returns (image, guide, render stats)."""
+    g = guide or Guide(scene, seed)
+    r = Renderer(scene, device=device, stream=stream)
+    spf = scene.settings().sample_per_frame
+    g.attach(r.integrator, Guide.TRAIN)
+    r.reset_accumulation()
+    scene.set_frame_count(first_frame + 100000)   # training samples are independent of the image's
+    for _ in range((train_spp + spf - 1) // spf):
+        r.render_batch()
+    g.attach(r.integrator, Guide.USE)
+    r.reset_accumulation()
+    scene.set_frame_count(first_frame)
+    r.integrator.reset_stats()
+    for _ in range((spp + spf - 1) // spf):
+        r.render_batch()
+    r.synchronize()
+    img = r.download_current_image()
+    return img, g, r.integrator.stats()
+
+
 def render_batch(items, block_size: int = 0, blocks_per_sm: int = 0, chunk_spp: int = 0, autotune: bool = True):
     """Render [(scene, spp[, first_frame])...] in one persistent launch.
     Returns (list of (H, W, 4) images, stats dict, config dict)."""

@@ -18,6 +18,7 @@ PT_OK, PT_ERR_INVALID, PT_ERR_IO, PT_ERR_CUDA, PT_ERR_STATE, PT_ERR_DEVICE, PT_E
 SAMPLER_PCG, SAMPLER_SOBOL = 0, 1
 FLAG_WATERTIGHT, FLAG_STAGE_TIMING, FLAG_NO_GRAPH, FLAG_COUNT_TRAVERSAL = 1, 2, 4, 8
 ARGS_LTR, ARGS_RTL = 0, 1
+GUIDE_OFF, GUIDE_USE, GUIDE_TRAIN = 0, 1, 2
 
 VERTEX_DTYPE = np.dtype([("position", "<f4", 3), ("_pad0", "<f4"), ("normal", "<f4", 3), ("_pad1", "<f4"),
                          ("uv", "<f4", 2), ("_pad2", "<f4", 2), ("tangent", "<f4", 4)])
@@ -145,6 +146,14 @@ _SIGS = [
     ("pt_scene_set_frame_count", C.c_int, [_P, C.c_uint32]),
     ("pt_render", C.c_int, [_P, C.c_int32, _P, C.c_int32, C.POINTER(RenderStats)]),
     ("pt_render_batch", C.c_int, [_P, C.c_uint32, C.c_int32, C.POINTER(BatchConfig), C.POINTER(RenderStats)]),
+    ("pt_guide_create", C.c_int, [_P, C.c_uint32, C.POINTER(_P)]),
+    ("pt_guide_destroy", C.c_int, [_P]),
+    ("pt_guide_set_learning_rate", C.c_int, [_P, C.c_float]),
+    ("pt_guide_info", C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    ("pt_integrator_set_guide", C.c_int, [_P, _P, C.c_int32]),
+    ("pt_guide_eval", C.c_int, [_P, _P, C.c_uint32, _P]),
+    ("pt_guide_get_params", C.c_int, [_P, _P, _P, _P]),
+    ("pt_guide_backward", C.c_int, [_P, _P, C.c_uint32, _P, _P]),
     ("pt_trace_closest", C.c_int, [_P, _P, C.c_uint32, _P, C.c_int32]),
     ("pt_trace_any", C.c_int, [_P, _P, C.c_uint32, _P, C.c_int32]),
     ("pt_sampler_stream", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_uint32, C.c_int32, C.c_int32,

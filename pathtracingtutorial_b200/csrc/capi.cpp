@@ -414,6 +414,46 @@ int pt_render_batch(const pt_batch_item* items, uint32_t n, int32_t out_is_devic
     PT_GUARD_END
 }
 
+// ---- learned guiding ----
+int pt_guide_create(pt_scene* scene, uint32_t seed, pt_guide** out) {
+    PT_REQUIRE(scene && out, "null argument");
+    PT_GUARD_BEGIN
+    return guide_create(scene, seed, out);
+    PT_GUARD_END
+}
+int pt_guide_destroy(pt_guide* guide) {
+    if (guide) guide_destroy(guide);
+    return PT_OK;
+}
+int pt_guide_set_learning_rate(pt_guide* guide, float lr) {
+    PT_REQUIRE(guide && lr > 0.0f, "invalid argument");
+    guide_set_lr(guide, lr);
+    return PT_OK;
+}
+int pt_guide_info(const pt_guide* guide, uint32_t* steps, uint32_t* last_samples) {
+    PT_REQUIRE(guide, "null guide");
+    return guide_info(guide, steps, last_samples);
+}
+int pt_integrator_set_guide(pt_integrator* integ, pt_guide* guide, int32_t mode) {
+    PT_REQUIRE(integ, "null integrator");
+    PT_REQUIRE(mode == PT_GUIDE_OFF || mode == PT_GUIDE_USE || mode == PT_GUIDE_TRAIN, "unknown guide mode");
+    PT_REQUIRE(guide || mode == PT_GUIDE_OFF, "a guide is required for this mode");
+    return integrator_set_guide(integ, mode == PT_GUIDE_OFF ? nullptr : guide, mode);
+}
+int pt_guide_eval(pt_guide* guide, const float* pos_dir, uint32_t n, float* out_pdf) {
+    PT_REQUIRE(guide && (n == 0 || (pos_dir && out_pdf)), "null argument");
+    return guide_eval(guide, pos_dir, n, out_pdf);
+}
+
+int pt_guide_get_params(const pt_guide* guide, float* weights, float* grid, float* meta) {
+    PT_REQUIRE(guide && weights, "null argument");
+    return guide_get_params(guide, weights, grid, meta);
+}
+int pt_guide_backward(pt_guide* guide, const float* samples, uint32_t n, float* weight_grad, float* grid_grad) {
+    PT_REQUIRE(guide && weight_grad && (n == 0 || samples), "null argument");
+    return guide_backward(guide, samples, n, weight_grad, grid_grad);
+}
+
 // ---- diagnostics ----
 int pt_trace_closest(pt_scene* s, const float* rays, uint32_t n, pt_hit* hits, int32_t ptrs_are_device) {
     PT_REQUIRE(s && (n == 0 || (rays && hits)), "null argument");

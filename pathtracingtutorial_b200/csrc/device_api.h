@@ -27,6 +27,14 @@ int  sampler_stream(int type, int w, int h, uint32_t frame, int spf, int sif, ui
                     int device, float* out_host);
 int  bsdf_eval(pt_scene* s, const float* in, uint32_t n, float* out_host);
 int  render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batch_config* cfg, pt_render_stats* stats);
+int  guide_create(pt_scene* s, uint32_t seed, pt_guide** out);
+void guide_destroy(pt_guide* g);
+void guide_set_lr(pt_guide* g, float lr);
+int  guide_info(const pt_guide* g, uint32_t* steps, uint32_t* samples);
+int  integrator_set_guide(pt_integrator* integ, pt_guide* g, int mode);
+int  guide_eval(pt_guide* g, const float* qd, uint32_t n, float* out);
+int  guide_get_params(const pt_guide* g, float* weights, float* grid, float* meta);
+int  guide_backward(pt_guide* g, const float* samples, uint32_t n, float* wgrad, float* ggrad);
 int  current_device(int* dev);
 int  device_sync(int device);
 

@@ -1,0 +1,643 @@
+// guide.cuh -- learned path guiding (no reference counterpart; included by
+// integrator.cu).
+//
+// A position-conditioned directional distribution q(w | x) is learned online
+// from the tracer's own samples and mixed with BSDF sampling by one-sample MIS:
+// with probability alpha the direction is drawn from q, otherwise from the
+// BSDF, and every sample is weighted by f / (alpha q + (1 - alpha) p_bsdf), so
+// the estimator keeps the expectation of the BSDF-only integrator wherever
+// p_bsdf > 0.  Vertices that can produce delta samples (roughness < 0.01) are
+// never guided.
+//
+// Network: multi-resolution hash-grid encoding of the position (16 levels x 2
+// features, 2^19 FP16 entries per level, trilinear) -> 3 hidden layers of 64
+// (ReLU) -> 40 outputs = 8 von Mises-Fisher lobes x (mean direction 3,
+// concentration 1, mixture logit 1).  BF16 weights, FP32 accumulation on the
+// tensor cores (mma.sync m16n8k16): each warp carries 16 queries through all
+// layers in registers (an accumulator fragment pair is the next layer's A
+// fragment), weights sit in shared memory with padded rows.
+//
+// Training minimises the KL divergence from the normalised incident radiance
+// to q with the one-sample estimate  -L_in(w) / p(w) * log q(w | x)  per
+// recorded path vertex; the backward pass runs on the tensor cores too
+// (dX = dY W and dW = dY^T X per CTA tile), the hash-grid gradient is scattered
+// with FP32 atomics, and Adam updates FP32 master copies.
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+namespace ptb {
+
+constexpr int kGLevels = 16;
+constexpr int kGFeat = 2;
+constexpr int kGLog2T = 19;
+constexpr int kGTable = 1 << kGLog2T;
+constexpr int kGIn = kGLevels * kGFeat;   // 32
+constexpr int kGHid = 64;
+constexpr int kGLobes = 8;
+constexpr int kGOut = 40;                 // used outputs
+constexpr int kGOutPad = 48;              // 6 n-tiles of 8
+constexpr int kGMix = 40;                 // floats per mixture: 8 x (mu xyz, kappa) + 8 weights
+constexpr float kGuideAlpha = 0.5f;
+
+// layer l: out x in, row-major, rows padded to in + 8 bf16 in shared memory
+__host__ __device__ constexpr int g_in(int l) { return l == 0 ? kGIn : kGHid; }
+__host__ __device__ constexpr int g_out(int l) { return l == 3 ? kGOutPad : kGHid; }
+__host__ __device__ constexpr int g_woff(int l) {   // offset of layer l in the packed (unpadded) weights
+    return l == 0 ? 0 : (l == 1 ? kGHid * kGIn : (l == 2 ? kGHid * kGIn + kGHid * kGHid : kGHid * kGIn + 2 * kGHid * kGHid));
+}
+constexpr int kGWeights = kGHid * kGIn + 2 * kGHid * kGHid + kGOutPad * kGHid;   // 13312
+__host__ __device__ constexpr int g_sld(int l) { return g_in(l) + 8; }               // padded smem row
+__host__ __device__ constexpr int g_soff(int l) {
+    return l == 0 ? 0 : (l == 1 ? kGHid * g_sld(0) : (l == 2 ? kGHid * g_sld(0) + kGHid * g_sld(1)
+                                                              : kGHid * g_sld(0) + 2 * kGHid * g_sld(1)));
+}
+constexpr int kGSmemW = kGHid * (kGIn + 8) + 2 * kGHid * (kGHid + 8) + kGOutPad * (kGHid + 8);   // bf16 elements
+
+struct GuideNet {
+    __half2*        grid;        // kGLevels * kGTable (inference copy)
+    float2*         grid_master; // FP32 master
+    float2*         grid_grad;
+    float2*         grid_m;
+    float2*         grid_v;
+    __nv_bfloat16*  w;           // kGWeights (inference copy), layer-packed [out][in]
+    float*          w_master;
+    float*          w_grad;
+    float*          w_m;
+    float*          w_v;
+    float           lo[3];       // scene bounds (positions mapped to [0,1]^3)
+    float           inv_ext[3];
+    float           scale[kGLevels];
+    uint32_t        dense_limit; // levels with (res+1)^3 <= table use direct indexing
+};
+
+// ---------------------------------------------------------------------------
+// mma helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Y(16 x OUT) = X(16 x IN) W^T for one warp; X given as A fragments per k-tile,
+// W in shared memory ([out][in], padded rows).  acc[nt][4] = C fragments.
+template <int IN, int OUT>
+__device__ __forceinline__ void warp_layer(const uint32_t (&a)[IN / 16][4], const __nv_bfloat16* W,
+                                           float (&acc)[OUT / 8][4]) {
+    constexpr int LD = IN + 8;
+    const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < OUT / 8; ++nt) {
+        acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
+        const __nv_bfloat16* row = W + (nt * 8 + g) * LD + 2 * c;
+#pragma unroll
+        for (int kt = 0; kt < IN / 16; ++kt) {
+            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(row + kt * 16);
+            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(row + kt * 16 + 8);
+            mma_bf16(acc[nt], a[kt], b0, b1);
+        }
+    }
+}
+
+// C fragments (with ReLU) -> A fragments of the next layer.
+template <int N>
+__device__ __forceinline__ void relu_to_a(const float (&acc)[N / 8][4], uint32_t (&a)[N / 16][4]) {
+#pragma unroll
+    for (int kt = 0; kt < N / 16; ++kt) {
+        a[kt][0] = pack_bf16(fmaxf(acc[2 * kt][0], 0.0f), fmaxf(acc[2 * kt][1], 0.0f));
+        a[kt][1] = pack_bf16(fmaxf(acc[2 * kt][2], 0.0f), fmaxf(acc[2 * kt][3], 0.0f));
+        a[kt][2] = pack_bf16(fmaxf(acc[2 * kt + 1][0], 0.0f), fmaxf(acc[2 * kt + 1][1], 0.0f));
+        a[kt][3] = pack_bf16(fmaxf(acc[2 * kt + 1][2], 0.0f), fmaxf(acc[2 * kt + 1][3], 0.0f));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Hash-grid encoding
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t grid_index(const GuideNet& net, int level, uint32_t x, uint32_t y, uint32_t z) {
+    const uint32_t res = static_cast<uint32_t>(net.scale[level]) + 2u;
+    if (static_cast<uint32_t>(level) < net.dense_limit) return (x + y * res + z * res * res) & (kGTable - 1);
+    return (x ^ (y * 2654435761u) ^ (z * 805459861u)) & (kGTable - 1);
+}
+
+// Trilinear features of one level at normalised position p.
+__device__ __forceinline__ float2 encode_level(const GuideNet& net, int level, f3 p) {
+    const float s = net.scale[level];
+    const float fx = p.x * s + 0.5f, fy = p.y * s + 0.5f, fz = p.z * s + 0.5f;
+    const float bx = floorf(fx), by = floorf(fy), bz = floorf(fz);
+    const float tx = fx - bx, ty = fy - by, tz = fz - bz;
+    const uint32_t ix = static_cast<uint32_t>(bx), iy = static_cast<uint32_t>(by), iz = static_cast<uint32_t>(bz);
+    const __half2* tab = net.grid + static_cast<size_t>(level) * kGTable;
+    float2 r = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int cidx = 0; cidx < 8; ++cidx) {
+        const uint32_t cx = cidx & 1, cy = (cidx >> 1) & 1, cz = (cidx >> 2) & 1;
+        const float w = (cx ? tx : 1.0f - tx) * (cy ? ty : 1.0f - ty) * (cz ? tz : 1.0f - tz);
+        const float2 e = __half22float2(tab[grid_index(net, level, ix + cx, iy + cy, iz + cz)]);
+        r.x += w * e.x;
+        r.y += w * e.y;
+    }
+    return r;
+}
+
+__device__ __forceinline__ f3 guide_normalise(const GuideNet& net, f3 x) {
+    return mk(fminf(fmaxf((x.x - net.lo[0]) * net.inv_ext[0], 0.0f), 1.0f),
+              fminf(fmaxf((x.y - net.lo[1]) * net.inv_ext[1], 0.0f), 1.0f),
+              fminf(fmaxf((x.z - net.lo[2]) * net.inv_ext[2], 0.0f), 1.0f));
+}
+
+// A fragments of the encoded inputs for this warp's rows g and g+8.
+__device__ __forceinline__ void encode_a(const GuideNet& net, f3 p0, f3 p1, uint32_t (&a)[2][4]) {
+    const int c = threadIdx.x & 3;
+#pragma unroll
+    for (int kt = 0; kt < 2; ++kt) {
+        const int la = 8 * kt + c, lb = 8 * kt + 4 + c;
+        const float2 e0a = encode_level(net, la, p0), e1a = encode_level(net, la, p1);
+        const float2 e0b = encode_level(net, lb, p0), e1b = encode_level(net, lb, p1);
+        a[kt][0] = pack_bf16(e0a.x, e0a.y);
+        a[kt][1] = pack_bf16(e1a.x, e1a.y);
+        a[kt][2] = pack_bf16(e0b.x, e0b.y);
+        a[kt][3] = pack_bf16(e1b.x, e1b.y);
+    }
+}
+
+__device__ __forceinline__ void load_weights_smem(const GuideNet& net, __nv_bfloat16* sw) {
+    for (int l = 0; l < 4; ++l) {
+        const int in = g_in(l), out = g_out(l), ld = g_sld(l);
+        for (int i = threadIdx.x; i < out * in; i += blockDim.x) {
+            const int o = i / in, k = i % in;
+            sw[g_soff(l) + o * ld + k] = net.w[g_woff(l) + i];
+        }
+    }
+    __syncthreads();
+}
+
+// Forward of one warp's 16 rows; leaves the (linear) outputs in out[6][4].
+__device__ __forceinline__ void warp_forward(const GuideNet& net, const __nv_bfloat16* sw, f3 p0, f3 p1,
+                                             float (&out)[6][4]) {
+    uint32_t a0[2][4];
+    encode_a(net, p0, p1, a0);
+    float h[8][4];
+    uint32_t a[4][4];
+    warp_layer<kGIn, kGHid>(a0, sw + g_soff(0), h);
+    relu_to_a<kGHid>(h, a);
+    warp_layer<kGHid, kGHid>(a, sw + g_soff(1), h);
+    relu_to_a<kGHid>(h, a);
+    warp_layer<kGHid, kGHid>(a, sw + g_soff(2), h);
+    relu_to_a<kGHid>(h, a);
+    warp_layer<kGHid, kGOutPad>(a, sw + g_soff(3), out);
+}
+
+// ---------------------------------------------------------------------------
+// vMF mixture: raw outputs -> (mu, kappa) x 8, weights x 8
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float softplusf(float x) { return x > 15.0f ? x : log1pf(expf(x)); }
+
+__device__ __forceinline__ void raw_to_mixture(const float* raw, float* mix) {
+    float mx = -1e30f;
+    for (int k = 0; k < kGLobes; ++k) mx = fmaxf(mx, raw[5 * k + 4]);
+    float sum = 0.0f;
+    for (int k = 0; k < kGLobes; ++k) {
+        f3 m = mk(raw[5 * k], raw[5 * k + 1], raw[5 * k + 2]);
+        const float l = length(m);
+        m = l > 1e-12f ? m / l : mk(0.0f, 0.0f, 1.0f);
+        mix[4 * k] = m.x; mix[4 * k + 1] = m.y; mix[4 * k + 2] = m.z;
+        mix[4 * k + 3] = fminf(softplusf(raw[5 * k + 3]) + 1e-3f, 5e3f);
+        const float e = expf(raw[5 * k + 4] - mx);
+        mix[32 + k] = e;
+        sum += e;
+    }
+    for (int k = 0; k < kGLobes; ++k) mix[32 + k] /= sum;
+}
+
+// vMF density on the sphere for cos(angle to the mean) c.
+__device__ __forceinline__ float vmf_pdf(float kappa, float c) {
+    if (kappa < 1e-4f) return 0.25f * kInvPi;
+    return kappa / (kTwoPi * (1.0f - expf(-2.0f * kappa))) * expf(kappa * (c - 1.0f));
+}
+
+__device__ __forceinline__ float mix_pdf(const float* mix, f3 w) {
+    float q = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kGLobes; ++k)
+        q += mix[32 + k] * vmf_pdf(mix[4 * k + 3], mix[4 * k] * w.x + mix[4 * k + 1] * w.y + mix[4 * k + 2] * w.z);
+    return q;
+}
+
+__device__ __forceinline__ f3 mix_sample(const float* mix, float u0, float u1, float u2) {
+    int k = 0;
+    float acc = mix[32];
+    while (k < kGLobes - 1 && u0 >= acc) { ++k; acc += mix[32 + k]; }
+    const f3 mu = mk(mix[4 * k], mix[4 * k + 1], mix[4 * k + 2]);
+    const float kappa = mix[4 * k + 3];
+    float c;
+    if (kappa < 1e-4f) c = 1.0f - 2.0f * u1;
+    else c = fminf(fmaxf(1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * kappa)) / kappa, -1.0f), 1.0f);
+    const float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
+    const float phi = kTwoPi * u2;
+    const Frame fr = make_frame(mu);
+    return normalize(to_world(fr, mk(s * cosf(phi), s * sinf(phi), c)));
+}
+
+// ---------------------------------------------------------------------------
+// Inference over a ray queue: position = hit point of queue entry i.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_guide_infer(GuideNet net, const uint32_t* counts, int q, uint32_t cap,
+                                                     const float4* ray_o, const float4* ray_d, const float4* hit,
+                                                     float* mix_out) {
+    extern __shared__ __align__(16) unsigned char g_smem[];
+    __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(g_smem);
+    float* srow = reinterpret_cast<float*>(g_smem + kGSmemW * sizeof(__nv_bfloat16));   // per warp 16 x 48
+    load_weights_smem(net, sw);
+    const uint32_t n = min(counts[q], cap);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+    float* my = srow + warp * 16 * kGOutPad;
+    const uint32_t tiles = (n + 15) / 16;
+    for (uint32_t tile = blockIdx.x * (blockDim.x >> 5) + warp; tile < tiles; tile += gridDim.x * (blockDim.x >> 5)) {
+        const uint32_t r0 = tile * 16 + g, r1 = r0 + 8;
+        auto pos = [&](uint32_t r) {
+            if (r >= n) return mk(0.5f);
+            const float4 o = ray_o[r], d = ray_d[r], h = hit[r];
+            const float t = __float_as_int(h.y) >= 0 ? h.x : 0.0f;
+            return guide_normalise(net, mk(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z));
+        };
+        float out[6][4];
+        warp_forward(net, sw, pos(r0), pos(r1), out);
+#pragma unroll
+        for (int nt = 0; nt < 6; ++nt) {
+            my[g * kGOutPad + nt * 8 + 2 * c] = out[nt][0];
+            my[g * kGOutPad + nt * 8 + 2 * c + 1] = out[nt][1];
+            my[(g + 8) * kGOutPad + nt * 8 + 2 * c] = out[nt][2];
+            my[(g + 8) * kGOutPad + nt * 8 + 2 * c + 1] = out[nt][3];
+        }
+        __syncwarp();
+        if (lane < 16) {
+            const uint32_t r = tile * 16 + lane;
+            if (r < n) {
+                float mix[kGMix];
+                raw_to_mixture(my + lane * kGOutPad, mix);
+                float4* dst = reinterpret_cast<float4*>(mix_out + static_cast<size_t>(r) * kGMix);
+#pragma unroll
+                for (int k = 0; k < kGMix / 4; ++k) dst[k] = make_float4(mix[4 * k], mix[4 * k + 1], mix[4 * k + 2], mix[4 * k + 3]);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace ptb
+
+namespace ptb {
+
+// ---------------------------------------------------------------------------
+// Training
+// ---------------------------------------------------------------------------
+// One training sample: normalised position (w = weight L_in / p), direction.
+struct GuideSample { float4 pos_w; float4 dir; };
+
+// d(-w log q(dir)) / d(raw outputs) for one row (raw: 48 floats, out: 48 floats).
+__device__ void mixture_grad(const float* raw, f3 dir, float w, float* d) {
+    float mix[kGMix];
+    raw_to_mixture(raw, mix);
+    float v[kGLobes];
+    float q = 0.0f;
+    for (int k = 0; k < kGLobes; ++k) {
+        const float c = mix[4 * k] * dir.x + mix[4 * k + 1] * dir.y + mix[4 * k + 2] * dir.z;
+        v[k] = vmf_pdf(mix[4 * k + 3], c);
+        q += mix[32 + k] * v[k];
+    }
+    q = fmaxf(q, 1e-12f);
+    const float gq = -w / q;
+    for (int k = 0; k < kGLobes; ++k) {
+        const float pi = mix[32 + k], kap = mix[4 * k + 3];
+        const f3 mu = mk(mix[4 * k], mix[4 * k + 1], mix[4 * k + 2]);
+        const float c = dot(mu, dir);
+        // mixture logit
+        d[5 * k + 4] = -w * pi * (v[k] / q - 1.0f);
+        // concentration: d log v / d kappa = 1/kappa - 2/(e^{2kappa} - 1) + c - 1
+        const float dl = (kap > 1e-3f ? 1.0f / kap - 2.0f / expm1f(fminf(2.0f * kap, 80.0f)) : 1.0f) + c - 1.0f;
+        const float r = raw[5 * k + 3];
+        const float sig = 1.0f / (1.0f + expf(-r));
+        d[5 * k + 3] = kap >= 5e3f ? 0.0f : gq * pi * v[k] * dl * sig;
+        // mean direction through the normalisation
+        const f3 m = mk(raw[5 * k], raw[5 * k + 1], raw[5 * k + 2]);
+        const float ml = fmaxf(length(m), 1e-12f);
+        const f3 dm = (dir - c * mu) * (gq * pi * kap * v[k] / ml);
+        d[5 * k] = dm.x; d[5 * k + 1] = dm.y; d[5 * k + 2] = dm.z;
+    }
+    for (int j = kGOut; j < kGOutPad; ++j) d[j] = 0.0f;
+}
+
+// Per-warp shared scratch for the backward pass (bf16):
+//   XT0 [32][16], HT1..3 [64][16]      inputs of layers 0..3, transposed
+//   DY  [16][64+8]                      row-major upstream gradient
+//   DYT [64][16+8]                      transposed upstream gradient
+// plus a float [16][48] tile for the outputs.
+constexpr int kGWarpScratch = (kGIn * 16 + 3 * kGHid * 16) * 2 + 16 * (kGHid + 8) * 2 + kGHid * (16 + 8) * 2 +
+                              16 * kGOutPad * 4;
+
+// store 16 rows of A-fragment data (row-major 16 x K, bf16 pairs) transposed into T[K][16]
+template <int K>
+__device__ __forceinline__ void store_t(const uint32_t (&a)[K / 16][4], __nv_bfloat16* T) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+#pragma unroll
+    for (int kt = 0; kt < K / 16; ++kt) {
+        const __nv_bfloat162 v0 = *reinterpret_cast<const __nv_bfloat162*>(&a[kt][0]);
+        const __nv_bfloat162 v1 = *reinterpret_cast<const __nv_bfloat162*>(&a[kt][1]);
+        const __nv_bfloat162 v2 = *reinterpret_cast<const __nv_bfloat162*>(&a[kt][2]);
+        const __nv_bfloat162 v3 = *reinterpret_cast<const __nv_bfloat162*>(&a[kt][3]);
+        const int k0 = kt * 16 + 2 * c;
+        T[(k0) * 16 + g] = v0.x;     T[(k0 + 1) * 16 + g] = v0.y;
+        T[(k0) * 16 + g + 8] = v1.x; T[(k0 + 1) * 16 + g + 8] = v1.y;
+        T[(k0 + 8) * 16 + g] = v2.x; T[(k0 + 9) * 16 + g] = v2.y;
+        T[(k0 + 8) * 16 + g + 8] = v3.x; T[(k0 + 9) * 16 + g + 8] = v3.y;
+    }
+}
+
+// dW[out][in] += DYT[out][16] . XT[in][16]^T  (K = the warp's 16 rows), into FP32 shared dW.
+template <int OUT, int IN>
+__device__ __forceinline__ void accum_dw(const __nv_bfloat16* DYT, const __nv_bfloat16* XT, float* sdw) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < OUT / 16; ++mt) {
+        uint32_t a[4];
+        const __nv_bfloat16* r0 = DYT + (mt * 16 + g) * 24 + 2 * c;
+        const __nv_bfloat16* r1 = DYT + (mt * 16 + g + 8) * 24 + 2 * c;
+        a[0] = *reinterpret_cast<const uint32_t*>(r0);
+        a[1] = *reinterpret_cast<const uint32_t*>(r1);
+        a[2] = *reinterpret_cast<const uint32_t*>(r0 + 8);
+        a[3] = *reinterpret_cast<const uint32_t*>(r1 + 8);
+#pragma unroll
+        for (int nt = 0; nt < IN / 8; ++nt) {
+            const __nv_bfloat16* xb = XT + (nt * 8 + g) * 16 + 2 * c;
+            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(xb);
+            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(xb + 8);
+            float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            mma_bf16(acc, a, b0, b1);
+            const int m0 = mt * 16 + g, n0 = nt * 8 + 2 * c;
+            atomicAdd(&sdw[m0 * IN + n0], acc[0]);
+            atomicAdd(&sdw[m0 * IN + n0 + 1], acc[1]);
+            atomicAdd(&sdw[(m0 + 8) * IN + n0], acc[2]);
+            atomicAdd(&sdw[(m0 + 8) * IN + n0 + 1], acc[3]);
+        }
+    }
+}
+
+// dX(16 x IN) = DY(16 x OUT) . W(OUT x IN), with W^T in shared memory ([in][out], padded rows).
+template <int OUT, int IN>
+__device__ __forceinline__ void back_dx(const __nv_bfloat16* DY, const __nv_bfloat16* WT, float (&acc)[IN / 8][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+    uint32_t a[OUT / 16][4];
+#pragma unroll
+    for (int kt = 0; kt < OUT / 16; ++kt) {
+        const __nv_bfloat16* r0 = DY + g * (kGHid + 8) + kt * 16 + 2 * c;
+        const __nv_bfloat16* r1 = DY + (g + 8) * (kGHid + 8) + kt * 16 + 2 * c;
+        a[kt][0] = *reinterpret_cast<const uint32_t*>(r0);
+        a[kt][1] = *reinterpret_cast<const uint32_t*>(r1);
+        a[kt][2] = *reinterpret_cast<const uint32_t*>(r0 + 8);
+        a[kt][3] = *reinterpret_cast<const uint32_t*>(r1 + 8);
+    }
+#pragma unroll
+    for (int nt = 0; nt < IN / 8; ++nt) {
+        acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
+        const __nv_bfloat16* row = WT + (nt * 8 + g) * (OUT + 8) + 2 * c;
+#pragma unroll
+        for (int kt = 0; kt < OUT / 16; ++kt) {
+            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(row + kt * 16);
+            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(row + kt * 16 + 8);
+            mma_bf16(acc[nt], a[kt], b0, b1);
+        }
+    }
+}
+
+// write a C-fragment tile (16 x N, optionally masked by a ReLU input held as
+// transposed bf16 HT[N][16]) as the next upstream gradient: DY row-major and DYT
+template <int N>
+__device__ __forceinline__ void store_dy(const float (&acc)[N / 8][4], const __nv_bfloat16* HT, __nv_bfloat16* DY,
+                                         __nv_bfloat16* DYT) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < N / 8; ++nt) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int row = g + (e >= 2 ? 8 : 0), col = nt * 8 + 2 * c + (e & 1);
+            float v = acc[nt][e];
+            if (HT && __bfloat162float(HT[col * 16 + row]) <= 0.0f) v = 0.0f;
+            const __nv_bfloat16 b = __float2bfloat16_rn(v);
+            DY[row * (kGHid + 8) + col] = b;
+            DYT[col * 24 + row] = b;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSample* __restrict__ samples,
+                                                     const uint32_t* count, uint32_t cap) {
+    const uint32_t n = min(*count, cap);
+    if (n == 0) return;
+    const float inv_n = 1.0f / static_cast<float>(n);
+    extern __shared__ __align__(16) unsigned char g_smem[];
+    __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(g_smem);                       // W  [out][in+8]
+    __nv_bfloat16* swt = sw + kGSmemW;                                                 // WT [in][out+8]
+    float* sdw = reinterpret_cast<float*>(swt + kGSmemW + 64);                         // dW fp32, packed
+    unsigned char* scratch0 = reinterpret_cast<unsigned char*>(sdw + kGWeights);
+    load_weights_smem(net, sw);
+    // transposed weights: layer l, WT[in][out] with row length out + 8
+    for (int l = 0; l < 4; ++l) {
+        const int in = g_in(l), out = g_out(l);
+        const int woff = l == 0 ? 0 : (l == 1 ? kGIn * (kGHid + 8) : (l == 2 ? kGIn * (kGHid + 8) + kGHid * (kGHid + 8)
+                                                                             : kGIn * (kGHid + 8) + 2 * kGHid * (kGHid + 8)));
+        for (int i = threadIdx.x; i < out * in; i += blockDim.x) {
+            const int o = i / in, k = i % in;
+            swt[woff + k * (out + 8) + o] = net.w[g_woff(l) + i];
+        }
+    }
+    for (int i = threadIdx.x; i < kGWeights; i += blockDim.x) sdw[i] = 0.0f;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+    unsigned char* my = scratch0 + warp * kGWarpScratch;
+    __nv_bfloat16* XT0 = reinterpret_cast<__nv_bfloat16*>(my);
+    __nv_bfloat16* HT1 = XT0 + kGIn * 16;
+    __nv_bfloat16* HT2 = HT1 + kGHid * 16;
+    __nv_bfloat16* HT3 = HT2 + kGHid * 16;
+    __nv_bfloat16* DY = HT3 + kGHid * 16;
+    __nv_bfloat16* DYT = DY + 16 * (kGHid + 8);
+    float* OUT = reinterpret_cast<float*>(DYT + kGHid * 24);
+    const __nv_bfloat16* WT0 = swt;
+    const __nv_bfloat16* WT1 = swt + kGIn * (kGHid + 8);
+    const __nv_bfloat16* WT2 = WT1 + kGHid * (kGHid + 8);
+    const __nv_bfloat16* WT3 = WT2 + kGHid * (kGHid + 8);
+    const uint32_t tiles = (n + 15) / 16;
+    for (uint32_t tile = blockIdx.x * 4 + warp; tile < tiles; tile += gridDim.x * 4) {
+        const uint32_t r0 = tile * 16 + g, r1 = r0 + 8;
+        const GuideSample s0 = r0 < n ? samples[r0] : GuideSample{make_float4(0.5f, 0.5f, 0.5f, 0.0f), make_float4(0, 0, 1, 0)};
+        const GuideSample s1 = r1 < n ? samples[r1] : GuideSample{make_float4(0.5f, 0.5f, 0.5f, 0.0f), make_float4(0, 0, 1, 0)};
+        const f3 p0 = mk(s0.pos_w.x, s0.pos_w.y, s0.pos_w.z), p1 = mk(s1.pos_w.x, s1.pos_w.y, s1.pos_w.z);
+        // forward, keeping every layer's input
+        uint32_t a0[2][4];
+        encode_a(net, p0, p1, a0);
+        store_t<kGIn>(a0, XT0);
+        float h[8][4];
+        uint32_t a[4][4];
+        warp_layer<kGIn, kGHid>(a0, sw + g_soff(0), h);
+        relu_to_a<kGHid>(h, a);
+        store_t<kGHid>(a, HT1);
+        warp_layer<kGHid, kGHid>(a, sw + g_soff(1), h);
+        relu_to_a<kGHid>(h, a);
+        store_t<kGHid>(a, HT2);
+        warp_layer<kGHid, kGHid>(a, sw + g_soff(2), h);
+        relu_to_a<kGHid>(h, a);
+        store_t<kGHid>(a, HT3);
+        float out[6][4];
+        warp_layer<kGHid, kGOutPad>(a, sw + g_soff(3), out);
+#pragma unroll
+        for (int nt = 0; nt < 6; ++nt) {
+            OUT[g * kGOutPad + nt * 8 + 2 * c] = out[nt][0];
+            OUT[g * kGOutPad + nt * 8 + 2 * c + 1] = out[nt][1];
+            OUT[(g + 8) * kGOutPad + nt * 8 + 2 * c] = out[nt][2];
+            OUT[(g + 8) * kGOutPad + nt * 8 + 2 * c + 1] = out[nt][3];
+        }
+        __syncwarp();
+        // loss gradient per row (lanes 0..15), scaled by 1/n
+        if (lane < 16) {
+            const uint32_t r = tile * 16 + lane;
+            float d[kGOutPad];
+            if (r < n) {
+                const GuideSample s = samples[r];
+                mixture_grad(OUT + lane * kGOutPad, mk(s.dir.x, s.dir.y, s.dir.z), s.pos_w.w * inv_n, d);
+            } else {
+                for (int j = 0; j < kGOutPad; ++j) d[j] = 0.0f;
+            }
+            for (int j = 0; j < kGOutPad; ++j) {
+                const __nv_bfloat16 b = __float2bfloat16_rn(d[j]);
+                DY[lane * (kGHid + 8) + j] = b;
+                DYT[j * 24 + lane] = b;
+            }
+        }
+        __syncwarp();
+        // layer 3 (48 x 64)
+        accum_dw<kGOutPad, kGHid>(DYT, HT3, sdw + g_woff(3));
+        float dh[8][4];
+        back_dx<kGOutPad, kGHid>(DY, WT3, dh);
+        __syncwarp();
+        store_dy<kGHid>(dh, HT3, DY, DYT);
+        __syncwarp();
+        // layer 2
+        accum_dw<kGHid, kGHid>(DYT, HT2, sdw + g_woff(2));
+        back_dx<kGHid, kGHid>(DY, WT2, dh);
+        __syncwarp();
+        store_dy<kGHid>(dh, HT2, DY, DYT);
+        __syncwarp();
+        // layer 1
+        accum_dw<kGHid, kGHid>(DYT, HT1, sdw + g_woff(1));
+        back_dx<kGHid, kGHid>(DY, WT1, dh);
+        __syncwarp();
+        store_dy<kGHid>(dh, HT1, DY, DYT);
+        __syncwarp();
+        // layer 0: dW0 and the gradient of the encoding
+        accum_dw<kGHid, kGIn>(DYT, XT0, sdw + g_woff(0));
+        float dx[4][4];
+        back_dx<kGHid, kGIn>(DY, WT0, dx);
+        __syncwarp();
+        // scatter the input gradient to the hash grid (levels c, 4+c, 8+c, 12+c)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const int level = nt * 4 + c;
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const uint32_t r = half ? r1 : r0;
+                if (r >= n) continue;
+                const f3 p = half ? p1 : p0;
+                const float gx = dx[nt][2 * half], gy = dx[nt][2 * half + 1];
+                const float sc = net.scale[level];
+                const float fx = p.x * sc + 0.5f, fy = p.y * sc + 0.5f, fz = p.z * sc + 0.5f;
+                const float bx = floorf(fx), by = floorf(fy), bz = floorf(fz);
+                const float tx = fx - bx, ty = fy - by, tz = fz - bz;
+                const uint32_t ix = static_cast<uint32_t>(bx), iy = static_cast<uint32_t>(by), iz = static_cast<uint32_t>(bz);
+                float2* gg = net.grid_grad + static_cast<size_t>(level) * kGTable;
+                for (int cidx = 0; cidx < 8; ++cidx) {
+                    const uint32_t cx = cidx & 1, cy = (cidx >> 1) & 1, cz = (cidx >> 2) & 1;
+                    const float w = (cx ? tx : 1.0f - tx) * (cy ? ty : 1.0f - ty) * (cz ? tz : 1.0f - tz);
+                    atomicAdd(&gg[grid_index(net, level, ix + cx, iy + cy, iz + cz)], make_float2(w * gx, w * gy));
+                }
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kGWeights; i += blockDim.x)
+        if (sdw[i] != 0.0f) atomicAdd(&net.w_grad[i], sdw[i]);
+}
+
+// Adam on the MLP weights (FP32 master -> BF16 copy) and the hash grid
+// (FP32 master -> FP16 copy); gradients are cleared.
+// dynamic shared memory of the two network kernels (4 warps per CTA)
+constexpr int kGInferSmem = kGSmemW * 2 + 4 * 16 * kGOutPad * 4;
+constexpr int kGTrainSmem = (2 * kGSmemW + 64) * 2 + kGWeights * 4 + 4 * kGWarpScratch;
+static_assert(kGTrainSmem <= 227 * 1024, "training kernel shared memory");
+static_assert(((2 * kGSmemW + 64) * 2) % 16 == 0 && (kGWeights * 4) % 16 == 0 && kGWarpScratch % 16 == 0,
+              "shared memory carve alignment");
+
+// Host-side state of one guide: the network, its optimiser state and the
+// buffers the wavefront fills (mixtures per queue entry, training records and
+// samples).  Owned by pt_guide.
+struct GuideState {
+    int          device = -1;
+    GuideNet     net{};
+    void*        params = nullptr;    // grid + weights + Adam state (one allocation)
+    size_t       param_bytes = 0;
+    void*        work = nullptr;      // mixtures, records, samples, counters
+    size_t       work_bytes = 0;
+    int          npix = 0, depth = 0;
+    float*       mix = nullptr;
+    float4*      rec = nullptr;
+    GuideSample* samples = nullptr;
+    uint32_t     sample_cap = 0;
+    uint32_t*    counters = nullptr;  // [0] samples, [1] step
+    int          mode = 0;            // 0 off, PT_GUIDE_USE, PT_GUIDE_TRAIN
+    float        lr = 1e-2f;
+};
+
+// Step counter ++ and sample buffer reset, between a training step and Adam.
+__global__ void k_guide_step(uint32_t* step, uint32_t* sample_count) {
+    *step += 1u;
+    *sample_count = 0u;
+}
+
+__global__ void k_guide_adam(GuideNet net, const uint32_t* step, float lr_w, float lr_g, float b1, float b2, float eps) {
+    const float t = static_cast<float>(*step);
+    const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
+    const size_t nw = kGWeights;
+    const size_t ng = static_cast<size_t>(kGLevels) * kGTable;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < nw + ng;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        if (i < nw) {
+            const float gr = net.w_grad[i];
+            const float m = b1 * net.w_m[i] + (1.0f - b1) * gr;
+            const float v = b2 * net.w_v[i] + (1.0f - b2) * gr * gr;
+            net.w_m[i] = m; net.w_v[i] = v; net.w_grad[i] = 0.0f;
+            const float p = net.w_master[i] - lr_w * (m / bc1) / (sqrtf(v / bc2) + eps);
+            net.w_master[i] = p;
+            net.w[i] = __float2bfloat16_rn(p);
+        } else {
+            const size_t j = i - nw;
+            const float2 gr = net.grid_grad[j];
+            if (gr.x == 0.0f && gr.y == 0.0f && net.grid_m[j].x == 0.0f && net.grid_m[j].y == 0.0f) continue;
+            float2 m = net.grid_m[j], v = net.grid_v[j], p = net.grid_master[j];
+            m.x = b1 * m.x + (1.0f - b1) * gr.x; m.y = b1 * m.y + (1.0f - b1) * gr.y;
+            v.x = b2 * v.x + (1.0f - b2) * gr.x * gr.x; v.y = b2 * v.y + (1.0f - b2) * gr.y * gr.y;
+            p.x -= lr_g * (m.x / bc1) / (sqrtf(v.x / bc2) + eps);
+            p.y -= lr_g * (m.y / bc1) / (sqrtf(v.y / bc2) + eps);
+            net.grid_m[j] = m; net.grid_v[j] = v; net.grid_master[j] = p; net.grid_grad[j] = make_float2(0.0f, 0.0f);
+            net.grid[j] = __floats2half2_rn(p.x, p.y);
+        }
+    }
+}
+
+}  // namespace ptb

@@ -29,6 +29,8 @@
 #include "engine.h"
 #include "bsdf.h"
 #include "traverse.h"
+#include "guide.cuh"
+#include "guide_host.cuh"
 
 namespace ptb {
 
@@ -75,6 +77,9 @@ struct WaveParams {
     float4*  f_comp;
     float4*  f_batch;
     float4*  f_new;
+    // learned guiding (null when off)
+    const float* gmix;   // queue-ordered mixtures, kGMix floats per entry
+    float4*  grec;       // training records [depth][npix][4]
 };
 
 // ---------------------------------------------------------------------------
@@ -163,12 +168,24 @@ __device__ __forceinline__ uint32_t sample_alias(const pt_alias_entry* t, uint32
     return (u2 < e.x) ? i : __float_as_uint(e.y);
 }
 // evaluateDirectLight (direct_lighting.cuh:204-218) without the visibility term.
-__device__ __forceinline__ f3 direct_term(const MatEval& me, f3 wo, f3 wi, f3 n, f3 radiance, float light_pdf) {
+// At a guided vertex the directional strategy is the guide/BSDF mixture, so
+// its pdf (alpha q + (1 - alpha) p_bsdf) enters the power heuristic.
+__device__ __forceinline__ f3 direct_term(const MatEval& me, f3 wo, f3 wi, f3 n, f3 radiance, float light_pdf,
+                                          const float* gmix) {
     const BsdfEval b = disney_eval(me, wo, wi, n, true);
     if (b.pdf <= 0.0f) return mk(0.0f);
-    const float mis = power_heuristic(light_pdf, b.pdf);
+    const float dir_pdf = gmix ? kGuideAlpha * mix_pdf(gmix, wi) + (1.0f - kGuideAlpha) * b.pdf : b.pdf;
+    const float mis = power_heuristic(light_pdf, dir_pdf);
     return radiance * b.f * (mis / (light_pdf + 1e-7f));
 }
+
+// Guiding inputs of one shaded vertex: its mixture (nullptr = plain BSDF
+// sampling) and, while training, the record slot that receives
+// (position, direction, pdf, throughput after the vertex).
+struct GuideVertex {
+    const float* mix;
+    float4* rec;
+};
 
 __device__ __forceinline__ void emit_shadow(const WaveParams& P, bool want, uint32_t path, uint32_t slot,
                                             f3 o, f3 d, float tmax, f3 c) {
@@ -308,7 +325,7 @@ struct InlineSink {
 template <class Sink>
 __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool last, f3 ro, f3 rd, float4 h,
                            f3& T, float& last_pdf, bool& last_delta, f3& L, PathRng& rng, f3& no, f3& nd,
-                           Sink& sink) {
+                           Sink& sink, GuideVertex gv = GuideVertex{nullptr, nullptr}) {
     const int prim = __float_as_int(h.y);
     if (prim < 0) {
         const f3 env = env_radiance(s, rd);
@@ -346,6 +363,8 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
     const MatEval me = resolve_material(m);
     const bool delta_surface = (me.metallic >= 1.0f && me.roughness < 0.01f) ||
                                (me.spec_trans >= 1.0f && me.roughness < 0.01f);
+    // guided vertex: a mixture is available and no lobe can be a delta
+    const float* gmix = (gv.mix != nullptr && me.roughness >= 0.01f) ? gv.mix : nullptr;
     if (!delta_surface) {
         const bool has_area = s.num_emissive > 0 && s.emissive != nullptr;
         const bool has_env = has_env_light(s);
@@ -386,7 +405,7 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
             }
             if (ok) {
                 const f3 le = material_emission(s.materials[lf.material_id]);
-                contrib = T * direct_term(me, wo, wi, N, le, pdf);
+                contrib = T * direct_term(me, wo, wi, N, le, pdf, gmix);
                 ok = !is_zero(contrib);
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
@@ -409,7 +428,7 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
             f3 contrib = mk(0.0f);
             if (ok) { pdf = env_pdf(s, wi); ok = pdf > 0.0f; }
             if (ok) {
-                contrib = T * direct_term(me, wo, wi, N, env_radiance(s, wi), pdf);
+                contrib = T * direct_term(me, wo, wi, N, env_radiance(s, wi), pdf, gmix);
                 ok = !is_zero(contrib);
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
@@ -454,7 +473,30 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
         }
     }
     if (last) return false;   // the sampled continuation would never be traced
-    const BsdfSample bs = disney_sample(me, wo, N, rng, arg_rtl, entering);
+    BsdfSample bs;
+    if (gmix) {
+        // one-sample MIS between the learned mixture and the BSDF
+        const float sel = rng_next(rng);
+        if (sel < kGuideAlpha) {
+            const float u0 = rng_next(rng), u1 = rng_next(rng), u2 = rng_next(rng);
+            bs.wi = mix_sample(gmix, u0, u1, u2);
+            const BsdfEval ev = disney_eval(me, wo, bs.wi, N, entering);
+            const float p = kGuideAlpha * mix_pdf(gmix, bs.wi) + (1.0f - kGuideAlpha) * ev.pdf;
+            bs.valid = p > 0.0f && !is_zero(ev.f);
+            bs.pdf = p;
+            bs.weight = bs.valid ? ev.f / p : mk(0.0f);
+            bs.delta = false;
+        } else {
+            bs = disney_sample(me, wo, N, rng, arg_rtl, entering);
+            if (bs.valid) {
+                const float p = kGuideAlpha * mix_pdf(gmix, bs.wi) + (1.0f - kGuideAlpha) * bs.pdf;
+                bs.weight = bs.weight * ((bs.pdf + 1e-7f) / p);
+                bs.pdf = p;
+            }
+        }
+    } else {
+        bs = disney_sample(me, wo, N, rng, arg_rtl, entering);
+    }
     if (!bs.valid) return false;
     T *= bs.weight;
     const bool transmitted = dot(bs.wi, gn) < 0.0f;
@@ -474,6 +516,13 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
         const float surv = fminf(max3(T), 0.95f);
         if (rng_next(rng) >= surv) return false;
         T = T / surv;
+    }
+    if (gv.rec && !bs.delta) {
+        // training record: where, which way, with which pdf, and the throughput
+        // that scales everything found along this direction
+        gv.rec[0] = make_float4(hp.x, hp.y, hp.z, bs.pdf);
+        gv.rec[1] = make_float4(nd.x, nd.y, nd.z, 1.0f);
+        gv.rec[2] = make_float4(T.x, T.y, T.z, 0.0f);
     }
     return true;
 }
@@ -504,8 +553,23 @@ __global__ void __launch_bounds__(128) k_shade(WaveParams P, int q, int depth, i
         rng.s = P.rng[p];
         f3 no = mk(0.0f), nd = mk(0.0f);
         QueueSink sink{P, p};
+        GuideVertex gv{P.gmix ? P.gmix + static_cast<size_t>(i) * kGMix : nullptr, nullptr};
+        if (P.grec) {
+            gv.rec = P.grec + (static_cast<size_t>(depth) * P.npix + p) * 4;
+            gv.rec[1].w = 0.0f;
+            if (depth > 0) {
+                // radiance gathered through the previous vertex: the part of the
+                // final estimate that did not arrive along its sampled direction
+                float4* prev = P.grec + (static_cast<size_t>(depth - 1) * P.npix + p) * 4;
+                if (prev[1].w != 0.0f) {
+                    f3 S = L;
+                    for (int k = 0; k < P.n_slots; ++k) S += f3of(P.nee[static_cast<size_t>(k) * P.npix + p]);
+                    prev[3] = f4of(S, 0.0f);
+                }
+            }
+        }
         const bool cont = shade_path(P.scene, P.arg_rtl, depth, last, f3of(o4), f3of(d4), h, T, last_pdf,
-                                     last_delta, L, rng, no, nd, sink) && !last;
+                                     last_delta, L, rng, no, nd, sink, gv) && !last;
         P.thr[p] = f4of(T, last_pdf);
         P.lo[p] = f4of(L, last_delta ? 1.0f : 0.0f);
         P.rng[p] = rng.s;
@@ -582,12 +646,47 @@ __global__ void __launch_bounds__(256) k_finalize(WaveParams P) {
     }
 }
 
-__global__ void k_batch_resolve(WaveParams P) {
-    const float inv_spf = static_cast<float>(P.spf);
+__global__ void k_frame_resolve(WaveParams P) {
+    const float spf = static_cast<float>(P.spf);
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.npix; p += gridDim.x * blockDim.x) {
         const float4 b = P.f_batch[p];
-        P.f_new[p] = make_float4(b.x / inv_spf, b.y / inv_spf, b.z / inv_spf, 1.0f);
+        P.f_new[p] = make_float4(b.x / spf, b.y / spf, b.z / spf, 1.0f);
         P.f_batch[p] = make_float4(0, 0, 0, 0);
+    }
+}
+
+// Turn this pass's guide records into training samples: for each recorded
+// vertex, the incident radiance along its sampled direction is the part of the
+// path's final estimate gathered after it, divided by the throughput after it
+// (luminance, clamped like a sample); weight = L_in / p.  Records are cleared.
+__global__ void __launch_bounds__(256) k_guide_collect(WaveParams P, GuideNet net, GuideSample* out,
+                                                       uint32_t* count, uint32_t cap) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.npix; p += gridDim.x * blockDim.x) {
+        f3 Lf = f3of(P.lo[p]);
+        for (int k = 0; k < P.n_slots; ++k) Lf += f3of(P.nee[static_cast<size_t>(k) * P.npix + p]);
+        for (int d = 0; d + 1 < P.max_depth; ++d) {
+            float4* r = P.grec + (static_cast<size_t>(d) * P.npix + p) * 4;
+            const float4 r1 = r[1];
+            float w = 0.0f;
+            float4 r0 = make_float4(0, 0, 0, 0);
+            if (r1.w != 0.0f) {
+                r[1].w = 0.0f;
+                r0 = r[0];
+                const f3 Ta = f3of(r[2]);
+                const f3 S = f3of(r[3]);
+                const f3 Lin = mk(Ta.x > 0.0f ? (Lf.x - S.x) / Ta.x : 0.0f, Ta.y > 0.0f ? (Lf.y - S.y) / Ta.y : 0.0f,
+                                  Ta.z > 0.0f ? (Lf.z - S.z) / Ta.z : 0.0f);
+                const float lum = fminf(fmaxf(luminance(Lin), 0.0f), 100.0f);
+                w = r0.w > 0.0f ? lum / r0.w : 0.0f;
+                if (!(w < 1e30f)) w = 0.0f;
+            }
+            const bool want = w > 0.0f;
+            const uint32_t j = warp_append(count, want);
+            if (want && j < cap) {
+                const f3 x = guide_normalise(net, mk(r0.x, r0.y, r0.z));
+                out[j] = GuideSample{make_float4(x.x, x.y, x.z, w), make_float4(r1.x, r1.y, r1.z, 0.0f)};
+            }
+        }
     }
 }
 
@@ -662,7 +761,8 @@ struct Wavefront {
     int grid_raygen = 0, grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_finalize = 0;
     // stats
     unsigned long long host_stats[kStatCount] = {};
-    double stage_ms[4] = {0, 0, 0, 0};
+    double stage_ms[5] = {0, 0, 0, 0, 0};   // extend, shade, shadow, other, guide
+    GuideState* guide = nullptr;           // not owned
     double total_ms = 0.0;
     uint64_t extend_launches = 0;
     uint64_t kernel_launches = 0;
@@ -779,7 +879,10 @@ int wavefront_prepare(Wavefront& wf, int device, int npix, int n_slots) {
 // stage events are recorded (ev holds pairs per launch: kind, start, stop).
 struct StageEvent { int kind; cudaEvent_t a, b; };
 
-int enqueue_batch(Wavefront& wf, const WaveParams& P, cudaStream_t st, std::vector<StageEvent>* ev) {
+int enqueue_batch(Wavefront& wf, const WaveParams& P, cudaStream_t st, std::vector<StageEvent>* ev,
+                  GuideState* gs = nullptr) {
+    const bool infer = gs && gs->mode != 0 && P.gmix;
+    const bool train = infer && P.grec;
     auto timed = [&](int kind, auto&& launch) -> int {
         if (ev) {
             StageEvent e{kind, nullptr, nullptr};
@@ -799,12 +902,30 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, cudaStream_t st, std::vect
         for (int d = 0; d < P.max_depth; ++d) {
             const int q = d & 1;
             if (int rc = timed(0, [&] { k_extend<<<wf.grid_extend, 128, 0, st>>>(P, q, d); })) return rc;
+            if (infer) {
+                if (int rc = timed(4, [&] {
+                        k_guide_infer<<<wf.sms * 4, 128, kGInferSmem, st>>>(gs->net, P.counts, q,
+                                                                            static_cast<uint32_t>(P.npix), P.ray_o[q],
+                                                                            P.ray_d[q], P.hit, gs->mix);
+                    })) return rc;
+            }
             if (int rc = timed(1, [&] { k_shade<<<wf.grid_shade, 128, 0, st>>>(P, q, d, i); })) return rc;
             if (int rc = timed(2, [&] { k_shadow<<<wf.grid_shadow, 128, 0, st>>>(P); })) return rc;
         }
         if (int rc = timed(3, [&] { k_finalize<<<wf.grid_finalize, 256, 0, st>>>(P); })) return rc;
+        if (train) {
+            if (int rc = timed(4, [&] {
+                    k_guide_collect<<<wf.grid_finalize, 256, 0, st>>>(P, gs->net, gs->samples, gs->counters,
+                                                                      gs->sample_cap);
+                    k_guide_train<<<wf.sms, 128, kGTrainSmem, st>>>(gs->net, gs->samples, gs->counters,
+                                                                     gs->sample_cap);
+                    k_guide_step<<<1, 1, 0, st>>>(gs->counters + 1, gs->counters);
+                    k_guide_adam<<<wf.sms * 8, 256, 0, st>>>(gs->net, gs->counters + 1, gs->lr, gs->lr, 0.9f,
+                                                             0.99f, 1e-10f);
+                })) return rc;
+        }
     }
-    if (int rc = timed(3, [&] { k_batch_resolve<<<wf.grid_finalize, 256, 0, st>>>(P); })) return rc;
+    if (int rc = timed(3, [&] { k_frame_resolve<<<wf.grid_finalize, 256, 0, st>>>(P); })) return rc;
     PT_CU(cudaGetLastError());
     return PT_OK;
 }
@@ -1025,6 +1146,13 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     P.f_comp = static_cast<float4*>(film->comp);
     P.f_batch = static_cast<float4*>(film->batch);
     P.f_new = static_cast<float4*>(film->fresh);
+    GuideState* gs = wf.guide;
+    if (gs && gs->mode != 0) {
+        if (gs->device != s->dev.device) { set_error("guide and scene live on different devices"); return PT_ERR_INVALID; }
+        if (int rc = guide_prepare_work(*gs, npix, prm->max_depth)) return rc;
+        P.gmix = gs->mix;
+        P.grec = gs->mode == PT_GUIDE_TRAIN ? gs->rec : nullptr;
+    }
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : wf.own_stream;
     k_begin<<<1, 1, 0, st>>>(P.pass, s->frame_count);
     PT_CU(cudaGetLastError());
@@ -1036,7 +1164,7 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
         PT_CU(cudaEventCreate(&t0));
         PT_CU(cudaEventCreate(&t1));
         PT_CU(cudaEventRecord(t0, st));
-        int rc = enqueue_batch(wf, P, st, &ev);
+        int rc = enqueue_batch(wf, P, st, &ev, gs);
         PT_CU(cudaEventRecord(t1, st));
         PT_CU(cudaEventSynchronize(t1));
         float ms = 0.0f;
@@ -1061,7 +1189,7 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
             if (wf.graph) { cudaGraphExecDestroy(wf.graph); wf.graph = nullptr; }
             cudaGraph_t g = nullptr;
             PT_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            const int rc = enqueue_batch(wf, P, st, nullptr);
+            const int rc = enqueue_batch(wf, P, st, nullptr, gs);
             const cudaError_t ec = cudaStreamEndCapture(st, &g);
             if (rc) { if (g) cudaGraphDestroy(g); return rc; }
             if (ec != cudaSuccess) { set_error(std::string("graph capture failed: ") + cudaGetErrorString(ec)); return PT_ERR_CUDA; }
@@ -1073,11 +1201,12 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
         PT_CU(cudaGraphLaunch(wf.graph, st));
         wf.extend_launches += static_cast<uint64_t>(P.spf) * P.max_depth;
     } else {
-        if (int rc = enqueue_batch(wf, P, st, nullptr)) return rc;
+        if (int rc = enqueue_batch(wf, P, st, nullptr, gs)) return rc;
         wf.extend_launches += static_cast<uint64_t>(P.spf) * P.max_depth;
     }
     // k_begin + per pass (raygen, 3 per bounce, finalize) + batch resolve
     wf.kernel_launches += 1 + static_cast<uint64_t>(P.spf) * (2 + 3 * static_cast<uint64_t>(P.max_depth)) + 1;
+    if (P.gmix) wf.kernel_launches += static_cast<uint64_t>(P.spf) * (P.max_depth + (P.grec ? 4 : 0));
     return PT_OK;
 }
 
@@ -1118,7 +1247,7 @@ int integrator_stats(const pt_integrator* integ, pt_render_stats* out) {
     out->extend_ms = wf->stage_ms[0];
     out->shade_ms = wf->stage_ms[1];
     out->shadow_ms = wf->stage_ms[2];
-    out->other_ms = wf->stage_ms[3];
+    out->other_ms = wf->stage_ms[3] + wf->stage_ms[4];
     out->total_ms = wf->total_ms;
     out->kernel_launches = wf->kernel_launches;
     return PT_OK;
@@ -1229,3 +1358,149 @@ int device_sync(int device) {
 }  // namespace ptb
 
 #include "batch.cuh"
+
+// ---------------------------------------------------------------------------
+// Guide handles
+// ---------------------------------------------------------------------------
+struct pt_guide {
+    ptb::GuideState g;
+};
+
+namespace ptb {
+
+__global__ void __launch_bounds__(128) k_guide_eval(GuideNet net, const float* qd, uint32_t n, float* out) {
+    extern __shared__ __align__(16) unsigned char g_smem[];
+    __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(g_smem);
+    float* srow = reinterpret_cast<float*>(g_smem + kGSmemW * sizeof(__nv_bfloat16));
+    load_weights_smem(net, sw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+    float* my = srow + warp * 16 * kGOutPad;
+    const uint32_t tiles = (n + 15) / 16;
+    for (uint32_t tile = blockIdx.x * 4 + warp; tile < tiles; tile += gridDim.x * 4) {
+        auto pos = [&](uint32_t r) {
+            return r < n ? guide_normalise(net, mk(qd[6 * r], qd[6 * r + 1], qd[6 * r + 2])) : mk(0.5f);
+        };
+        float o[6][4];
+        warp_forward(net, sw, pos(tile * 16 + g), pos(tile * 16 + g + 8), o);
+#pragma unroll
+        for (int nt = 0; nt < 6; ++nt) {
+            my[g * kGOutPad + nt * 8 + 2 * c] = o[nt][0];
+            my[g * kGOutPad + nt * 8 + 2 * c + 1] = o[nt][1];
+            my[(g + 8) * kGOutPad + nt * 8 + 2 * c] = o[nt][2];
+            my[(g + 8) * kGOutPad + nt * 8 + 2 * c + 1] = o[nt][3];
+        }
+        __syncwarp();
+        if (lane < 16 && tile * 16 + lane < n) {
+            const uint32_t r = tile * 16 + lane;
+            float mix[kGMix];
+            raw_to_mixture(my + lane * kGOutPad, mix);
+            out[r] = mix_pdf(mix, normalize(mk(qd[6 * r + 3], qd[6 * r + 4], qd[6 * r + 5])));
+        }
+        __syncwarp();
+    }
+}
+
+int guide_create(pt_scene* s, uint32_t seed, pt_guide** out) {
+    if (!s->dev.uploaded) { set_error("guide: scene not uploaded"); return PT_ERR_STATE; }
+    pt_guide* h = new pt_guide();
+    const int rc = guide_init(h->g, s->dev.device, s->tables.root_lo, s->tables.root_hi, seed);
+    if (rc) { guide_free(h->g); delete h; return rc; }
+    *out = h;
+    return PT_OK;
+}
+
+void guide_destroy(pt_guide* h) {
+    guide_free(h->g);
+    delete h;
+}
+
+void guide_set_lr(pt_guide* h, float lr) { h->g.lr = lr; }
+
+int guide_info(const pt_guide* h, uint32_t* steps, uint32_t* samples) {
+    uint32_t c[2] = {0, 0};
+    if (h->g.counters) {
+        if (int rc = ensure_device(h->g.device)) return rc;
+        PT_CU(cudaDeviceSynchronize());
+        PT_CU(cudaMemcpy(c, h->g.counters, sizeof(c), cudaMemcpyDeviceToHost));
+    }
+    if (steps) *steps = c[1];
+    if (samples) *samples = c[0];
+    return PT_OK;
+}
+
+int integrator_set_guide(pt_integrator* integ, pt_guide* h, int mode) {
+    if (!integ->wf) integ->wf = new Wavefront();
+    integ->wf->guide = h ? &h->g : nullptr;
+    if (h) h->g.mode = mode;
+    if (integ->wf->graph) { cudaGraphExecDestroy(integ->wf->graph); integ->wf->graph = nullptr; integ->wf->graph_key.clear(); }
+    return PT_OK;
+}
+
+int guide_get_params(const pt_guide* h, float* weights, float* grid, float* meta) {
+    if (int rc = ensure_device(h->g.device)) return rc;
+    PT_CU(cudaDeviceSynchronize());
+    std::vector<__nv_bfloat16> wb(kGWeights);
+    PT_CU(cudaMemcpy(wb.data(), h->g.net.w, kGWeights * sizeof(__nv_bfloat16), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < kGWeights; ++i) weights[i] = __bfloat162float(wb[i]);
+    if (grid) {
+        const size_t ng = static_cast<size_t>(kGLevels) * kGTable;
+        std::vector<__half2> gh(ng);
+        PT_CU(cudaMemcpy(gh.data(), h->g.net.grid, ng * sizeof(__half2), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < ng; ++i) {
+            const float2 v = __half22float2(gh[i]);
+            grid[2 * i] = v.x;
+            grid[2 * i + 1] = v.y;
+        }
+    }
+    if (meta) {
+        for (int a = 0; a < 3; ++a) { meta[a] = h->g.net.lo[a]; meta[3 + a] = h->g.net.inv_ext[a]; }
+        for (int l = 0; l < kGLevels; ++l) meta[6 + l] = h->g.net.scale[l];
+        meta[6 + kGLevels] = static_cast<float>(h->g.net.dense_limit);
+    }
+    return PT_OK;
+}
+
+int guide_backward(pt_guide* h, const float* samples, uint32_t n, float* wgrad, float* ggrad) {
+    if (int rc = ensure_device(h->g.device)) return rc;
+    GuideSample* ds = nullptr;
+    uint32_t* dn = nullptr;
+    PT_CU(cudaMalloc(&ds, std::max<size_t>(n, 1) * sizeof(GuideSample)));
+    if (cudaMalloc(&dn, 4) != cudaSuccess) { cudaFree(ds); cudaGetLastError(); set_error("alloc"); return PT_ERR_NOMEM; }
+    const size_t ng = static_cast<size_t>(kGLevels) * kGTable;
+    cudaError_t e = cudaMemcpy(ds, samples, static_cast<size_t>(n) * sizeof(GuideSample), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dn, &n, 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(h->g.net.w_grad, 0, kGWeights * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(h->g.net.grid_grad, 0, ng * sizeof(float2));
+    if (e == cudaSuccess) {
+        k_guide_train<<<148, 128, kGTrainSmem>>>(h->g.net, ds, dn, n);
+        e = cudaDeviceSynchronize();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(wgrad, h->g.net.w_grad, kGWeights * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && ggrad) e = cudaMemcpy(ggrad, h->g.net.grid_grad, ng * sizeof(float2), cudaMemcpyDeviceToHost);
+    // leave the optimiser state as it was
+    cudaMemset(h->g.net.w_grad, 0, kGWeights * sizeof(float));
+    cudaMemset(h->g.net.grid_grad, 0, ng * sizeof(float2));
+    cudaFree(ds);
+    cudaFree(dn);
+    if (e != cudaSuccess) { set_error(std::string("guide backward: ") + cudaGetErrorString(e)); return PT_ERR_CUDA; }
+    return PT_OK;
+}
+
+int guide_eval(pt_guide* h, const float* qd, uint32_t n, float* out) {
+    if (int rc = ensure_device(h->g.device)) return rc;
+    if (n == 0) return PT_OK;
+    float *dq = nullptr, *dout = nullptr;
+    PT_CU(cudaMalloc(&dq, static_cast<size_t>(n) * 24));
+    if (cudaMalloc(&dout, static_cast<size_t>(n) * 4) != cudaSuccess) { cudaFree(dq); cudaGetLastError(); set_error("alloc"); return PT_ERR_NOMEM; }
+    cudaError_t e = cudaMemcpy(dq, qd, static_cast<size_t>(n) * 24, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_guide_eval<<<148, 128, kGInferSmem>>>(h->g.net, dq, n, dout);
+        e = cudaMemcpy(out, dout, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(dq);
+    cudaFree(dout);
+    if (e != cudaSuccess) { set_error(std::string("guide eval: ") + cudaGetErrorString(e)); return PT_ERR_CUDA; }
+    return PT_OK;
+}
+
+}  // namespace ptb

@@ -1,0 +1,169 @@
+"""Learned guiding: the FP64 CPU restatement of the network is checked by
+finite differences; the CUDA forward and backward (BF16 tensor cores, FP32
+accumulation) are checked against it; guided rendering stays unbiased against
+the plain integrator and lowers the error at equal sample count."""
+import numpy as np
+import pytest
+
+from oracle import guide_ref
+
+
+def _samples(n, seed, concentrated=False):
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(0.0, 1.0, (n, 3))
+    d = rng.normal(size=(n, 3))
+    if concentrated:
+        d[:, 2] = np.abs(d[:, 2]) * 3.0
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    w = rng.exponential(1.0, n)
+    return pos.astype(np.float32), w.astype(np.float32), d.astype(np.float32)
+
+
+@pytest.mark.parametrize("table_log2", [10, 13])
+def test_oracle_backward_matches_finite_differences(table_log2):
+    prm = guide_ref.random_params(table_log2, seed=3)
+    pos, w, d = _samples(48, 1)
+    gw, gg = guide_ref.backward(prm, pos, w, d)
+    rng = np.random.default_rng(7)
+    h = 1e-6
+
+    def fd_weight(i):
+        p1, p2 = dict(prm), dict(prm)
+        p1["weights"] = prm["weights"].copy(); p1["weights"][i] += h
+        p2["weights"] = prm["weights"].copy(); p2["weights"][i] -= h
+        return (guide_ref.loss(p1, pos, w, d) - guide_ref.loss(p2, pos, w, d)) / (2 * h)
+
+    def fd_grid(l, e, f):
+        p1, p2 = dict(prm), dict(prm)
+        p1["grid"] = prm["grid"].copy(); p1["grid"][l, e, f] += h
+        p2["grid"] = prm["grid"].copy(); p2["grid"][l, e, f] -= h
+        return (guide_ref.loss(p1, pos, w, d) - guide_ref.loss(p2, pos, w, d)) / (2 * h)
+
+    used = [i for i in range(guide_ref.N_WEIGHTS) if not (i >= 10240 and (i - 10240) // 64 >= 40)]
+    scale_w = np.abs(gw).max()
+    for i in rng.choice(used, 24, replace=False):
+        assert abs(fd_weight(i) - gw[i]) <= 1e-5 * scale_w + 1e-4 * abs(gw[i]), i
+    nz = np.argwhere(gg != 0)
+    scale_g = np.abs(gg).max()
+    for l, e, f in nz[rng.choice(len(nz), 24, replace=False)]:
+        assert abs(fd_grid(l, e, f) - gg[l, e, f]) <= 1e-5 * scale_g + 1e-4 * abs(gg[l, e, f]), (l, e, f)
+
+
+def test_oracle_pdf_normalised():
+    """q(. | x) integrates to one over the sphere (Fibonacci quadrature)."""
+    prm = guide_ref.random_params(10, seed=4, feature_scale=0.5)
+    m = 200_000
+    k = np.arange(m) + 0.5
+    z = 1 - 2 * k / m
+    phi = np.pi * (1 + 5 ** 0.5) * k
+    r = np.sqrt(1 - z * z)
+    dirs = np.stack([r * np.cos(phi), r * np.sin(phi), z], 1)
+    for p in ([0.3, 0.6, 0.2], [0.9, 0.1, 0.5]):
+        q = guide_ref.pdf(prm, np.tile(np.array(p, np.float32), (m, 1)), dirs)
+        assert abs(q.mean() * 4 * np.pi - 1.0) < 2e-3
+
+
+# ---------------------------------------------------------------------------
+# GPU: kernels against the FP64 restatement
+# ---------------------------------------------------------------------------
+
+def _scene(sa):
+    s = sa.scene()
+    s.build_accel()
+    s.upload_to_device(0)
+    return s
+
+
+def _render_from(s, spp, first_frame):
+    """Plain render of spp samples per pixel starting at an arbitrary frame
+    (independent of the frames pt.render uses)."""
+    import pathtracingtutorial_b200 as pt
+    r = pt.Renderer(s)
+    r.reset_accumulation()
+    s.set_frame_count(first_frame)
+    spf = s.settings().sample_per_frame
+    for _ in range((spp + spf - 1) // spf):
+        r.render_batch()
+    r.synchronize()
+    return r.download_current_image()
+
+
+def _layer_rel(a, b):
+    out = []
+    for o, (r, c) in zip(guide_ref.LAYER_OFFSETS, guide_ref.LAYER_SHAPES):
+        x, y = a[o:o + r * c], b[o:o + r * c]
+        out.append(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-30))
+    return out
+
+
+def _check_gradients(g, seed, concentrated):
+    prm = g.params()
+    pos, w, d = _samples(4096, seed, concentrated)
+    gw, gg = g.backward(pos, w, d)
+    rw, rg = guide_ref.backward(prm, pos, w, d)
+    rel = _layer_rel(gw, rw)
+    # BF16 activations and upstream gradients (8-bit mantissa), FP32 accumulation
+    assert max(rel) < 0.05, rel
+    cos = float(gw @ rw / (np.linalg.norm(gw) * np.linalg.norm(rw)))
+    assert cos > 0.998, cos
+    relg = np.linalg.norm(gg - rg) / np.linalg.norm(rg)
+    assert relg < 0.05, relg
+    return rel, relg
+
+
+@pytest.mark.gpu
+def test_guide_gradients_match_fp64_oracle_at_init():
+    import pathtracingtutorial_b200 as pt
+    from pathtracingtutorial_b200 import scenes
+    s = _scene(scenes.cornell_box(width=32, height=32, spp=4))
+    g = pt.Guide(s, seed=5)
+    _check_gradients(g, 11, False)
+    g.close()
+
+
+@pytest.mark.gpu
+def test_guide_forward_and_gradients_after_training():
+    import pathtracingtutorial_b200 as pt
+    from pathtracingtutorial_b200 import scenes
+    sa = scenes.hidden_light_room(width=64, height=64, n_boxes=40, box_subdiv=2, spp=8, max_depth=8)
+    s = _scene(sa)
+    img, g, _ = pt.render_guided(s, train_spp=64, spp=8)
+    assert g.info()["steps"] > 0
+    prm = g.params()
+    # forward: pdf at world positions inside the scene bounds
+    rng = np.random.default_rng(2)
+    lo, inv = prm["lo"].astype(np.float64), prm["inv_extent"].astype(np.float64)
+    p01 = rng.uniform(0.05, 0.95, (2048, 3)).astype(np.float32)
+    world = (lo + p01 / inv).astype(np.float32)
+    d = rng.normal(size=(2048, 3)); d /= np.linalg.norm(d, axis=1, keepdims=True)
+    q_gpu = g.pdf(world, d.astype(np.float32)).astype(np.float64)
+    pn = np.clip((world - prm["lo"]) * prm["inv_extent"], 0, 1).astype(np.float32)
+    q_ref = guide_ref.pdf(prm, pn, d)
+    rel = np.abs(q_gpu - q_ref) / q_ref
+    assert np.median(rel) < 0.02 and np.quantile(rel, 0.99) < 0.15, (np.median(rel), np.quantile(rel, 0.99))
+    _check_gradients(g, 12, True)
+    g.close()
+
+
+@pytest.mark.gpu
+def test_guided_render_unbiased_and_lower_error():
+    """Guided vs plain on the hidden-light room at equal samples per pixel:
+    both agree in the mean with a high-spp plain render, and the trained
+    guide lowers the relative MSE."""
+    import pathtracingtutorial_b200 as pt
+    from pathtracingtutorial_b200 import scenes
+    sa = scenes.hidden_light_room(width=64, height=64, n_boxes=40, box_subdiv=2, spp=64, max_depth=10)
+    s = _scene(sa)
+    ref = _render_from(s, 8192, 1_000_000)[..., :3].astype(np.float64)
+    plain = pt.render(s, 64)[..., :3].astype(np.float64)
+    guided, g, _ = pt.render_guided(s, train_spp=256, spp=64)
+    guided = guided[..., :3].astype(np.float64)
+
+    def relmse(x):
+        return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    m_ref, m_plain, m_guided = ref.mean(), plain.mean(), guided.mean()
+    assert abs(m_plain / m_ref - 1) < 0.03
+    assert abs(m_guided / m_ref - 1) < 0.03, (m_guided, m_ref)
+    assert relmse(guided) < relmse(plain), (relmse(guided), relmse(plain))
+    g.close()
