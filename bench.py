@@ -43,6 +43,8 @@ def parse_args():
     p.add_argument("--spp", type=int, default=256, help="samples per pixel of one step (workload: 256)")
     p.add_argument("--small", action="store_true", help="a small scene for quick checks (not a bench line)")
     p.add_argument("--cpu-sample-seconds", type=float, default=12.0)
+    p.add_argument("--no-cpu-baseline", action="store_true",
+                   help="skip the CPU baseline leg (profiling runs; the line then carries cpu_baseline null)")
     return p.parse_args()
 
 
@@ -243,10 +245,10 @@ def ours(args):
     frame0 = shard_first_frame(rank, batches)   # disjoint sample indices per rank
 
     def step():
+        # Renderer::renderAll over `batches` frames: one graph-captured launch
         renderer.reset_accumulation()
         scene.set_frame_count(frame0)
-        for _ in range(batches):
-            renderer.render_batch()
+        renderer.render_frames(batches)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -312,7 +314,7 @@ def ours(args):
         if dist is not None:
             dist.destroy_process_group()
         return
-    cpu = cpu_baseline(sa, spp, args.cpu_sample_seconds) if world == 1 else None
+    cpu = cpu_baseline(sa, spp, args.cpu_sample_seconds) if world == 1 and not args.no_cpu_baseline else None
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,

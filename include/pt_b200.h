@@ -150,7 +150,9 @@ typedef struct pt_render_settings {
     uint32_t pcg_seed;          /* added knob; 0 reproduces the reference seeding */
     int32_t  arg_order;         /* PT_ARGS_*                                      */
     int32_t  flags;             /* PT_FLAG_*                                      */
-    int32_t  _reserved;
+    int32_t  paths_in_flight;   /* added: wavefront path slots (0 = 2^23); samples of a
+                                   frame run concurrently while they fit.  Results do
+                                   not depend on it. */
 } pt_render_settings;
 
 typedef struct pt_scene_info {
@@ -247,6 +249,10 @@ int pt_integrator_reset_stats(pt_integrator* integ);
 
 /* ---- renderer (Renderer, Part_2/src/renderer.h:17-55) ---- */
 int pt_renderer_render_batch(pt_integrator* integ, pt_film* film, pt_scene* scene, void* stream); /* renderBatch */
+/* Added: `frames` consecutive renderBatch calls in one launch (one CUDA graph);
+ * identical film, frame counter and "new" image (the last frame's). */
+int pt_renderer_render_frames(pt_integrator* integ, pt_film* film, pt_scene* scene, uint32_t frames,
+                              void* stream);
 int pt_renderer_reset_accumulation(pt_film* film, pt_scene* scene);                               /* resetAccumulation */
 /* Frame counter that drives sample indices (DeviceScene::frameCount, device_scene.h:97). */
 int pt_scene_set_frame_count(pt_scene* scene, uint32_t frame_count);

@@ -124,7 +124,19 @@ public:
         check(pt_scene_set_frame_count(scene_.handle(), scene_.info().frame_count + 1));
         return currentSpp();
     }
-    void renderAll() { while (!isComplete()) renderBatch(); }
+    // Renderer::renderAll; with this library's path integrator the remaining
+    // frames run as one launch (pt_renderer_render_frames, same result).
+    void renderAll(void* stream = nullptr) {
+        if (auto* pi = dynamic_cast<PathIntegrator*>(integrator_.get())) {
+            const uint32_t spf = static_cast<uint32_t>(scene_.settings().sample_per_frame);
+            const uint32_t cur = currentSpp(), tgt = targetSpp();
+            if (cur < tgt)
+                check(pt_renderer_render_frames(pi->handle(), film_->handle(), scene_.handle(),
+                                                (tgt - cur + spf - 1) / spf, stream));
+            return;
+        }
+        while (!isComplete()) renderBatch(stream);
+    }
     uint32_t currentSpp() const { return scene_.info().frame_count * scene_.settings().sample_per_frame; }
     uint32_t targetSpp() const { return static_cast<uint32_t>(scene_.settings().spp); }
     bool isComplete() const { return currentSpp() >= targetSpp(); }

@@ -18,7 +18,10 @@ The model, for a position p in [0,1]^3 and a direction w:
   loss = mean_i  -weight_i log max(q_i(w_i), 1e-12).
 Everything here is float64; the weights and grid values are the kernels' own
 (BF16 / FP16 values widened to float), so the difference to the GPU is the
-kernels' arithmetic only.
+kernels' arithmetic only.  With bf16=True the values the kernels store as BF16
+(every layer's input, and the upstream gradient entering every layer's
+backward) are rounded to BF16 at the same points, which leaves only the
+kernels' FP32 accumulation order and FP32 transcendentals as differences.
 """
 from __future__ import annotations
 
@@ -32,6 +35,13 @@ LAYER_SHAPES = [(HIDDEN, 2 * N_LEVELS), (HIDDEN, HIDDEN), (HIDDEN, HIDDEN), (OUT
 LAYER_OFFSETS = [0, 2048, 6144, 10240]
 N_WEIGHTS = 13312
 P1, P2 = np.uint64(2654435761), np.uint64(805459861)
+
+
+def to_bf16(x: np.ndarray) -> np.ndarray:
+    """Round to the nearest BF16 value (ties to even), returned as float64."""
+    b = np.asarray(x, np.float64).astype(np.float32).view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    return b.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
 def layers(weights: np.ndarray) -> list[np.ndarray]:
@@ -100,20 +110,22 @@ def vmf(kappa, c):
     return kappa / (2 * np.pi * -np.expm1(-2 * kappa)) * np.exp(kappa * (c - 1))
 
 
-def forward(params: dict, p: np.ndarray):
+def forward(params: dict, p: np.ndarray, bf16: bool = False):
+    q = to_bf16 if bf16 else (lambda a: a)
     W = layers(params["weights"])
     x, corners = encode(params, p)
+    x = q(x)
     acts = [x]
     h = x
     for l in range(3):
-        h = np.maximum(W[l] @ h.T, 0).T
+        h = q(np.maximum(W[l] @ h.T, 0).T)
         acts.append(h)
     raw = (W[3] @ h.T).T
     return raw, acts, corners
 
 
-def pdf(params: dict, p: np.ndarray, dirs: np.ndarray) -> np.ndarray:
-    raw, _, _ = forward(params, p)
+def pdf(params: dict, p: np.ndarray, dirs: np.ndarray, bf16: bool = False) -> np.ndarray:
+    raw, _, _ = forward(params, p, bf16)
     mu, kappa, pi, _, _ = mixture(raw)
     c = np.einsum("nkj,nj->nk", mu, dirs)
     return (pi * vmf(kappa, c)).sum(axis=1)
@@ -124,15 +136,16 @@ def loss(params: dict, p: np.ndarray, weight: np.ndarray, dirs: np.ndarray) -> f
     return float(np.mean(-np.asarray(weight, np.float64) * np.log(np.maximum(q, 1e-12))))
 
 
-def backward(params: dict, p: np.ndarray, weight: np.ndarray, dirs: np.ndarray):
+def backward(params: dict, p: np.ndarray, weight: np.ndarray, dirs: np.ndarray, bf16: bool = False):
     """Gradient of loss() with respect to the packed weights (13312,) and the
     grid (same shape as params["grid"])."""
+    rq = to_bf16 if bf16 else (lambda a: a)
     p = np.asarray(p, np.float64)
     dirs = np.asarray(dirs, np.float64)
     n = len(p)
     w = np.asarray(weight, np.float64) / n
     W = layers(params["weights"])
-    raw, acts, corners = forward(params, p)
+    raw, acts, corners = forward(params, p, bf16)
     mu, kappa, pi, ml, clipped = mixture(raw)
     c = np.einsum("nkj,nj->nk", mu, dirs)
     v = vmf(kappa, c)
@@ -154,12 +167,12 @@ def backward(params: dict, p: np.ndarray, weight: np.ndarray, dirs: np.ndarray):
     d[:, :5 * LOBES] = dr.reshape(n, 5 * LOBES)
     # MLP backward
     gW = [None] * 4
-    dy = d
+    dy = rq(d)
     for l in (3, 2, 1, 0):
         gW[l] = dy.T @ acts[l]
         dx = dy @ W[l]
         if l > 0:
-            dx = dx * (acts[l] > 0)
+            dx = rq(dx * (acts[l] > 0))
         dy = dx
     gW[3][40:, :] = 0.0
     gw_flat = np.concatenate([g.ravel() for g in gW])

@@ -313,6 +313,15 @@ class Renderer:
         self.last_batch_ms = (time.perf_counter() - t0) * 1e3
         return self.current_spp()
 
+    def render_frames(self, frames: int) -> int:
+        """`frames` renderBatch calls in one launch (same result as calling
+        render_batch that many times)."""
+        t0 = time.perf_counter()
+        check(lib().pt_renderer_render_frames(self.integrator._h, self.film._h, self.scene.handle, int(frames),
+                                              C.c_void_p(self.stream) if self.stream else None))
+        self.last_batch_ms = (time.perf_counter() - t0) * 1e3
+        return self.current_spp()
+
     def current_spp(self) -> int:
         return self.scene.info()["frame_count"] * self.scene.settings().sample_per_frame
 
@@ -323,8 +332,10 @@ class Renderer:
         return self.current_spp() >= self.target_spp()
 
     def render_all(self) -> None:
-        while not self.is_complete():
-            self.render_batch()
+        spf = self.scene.settings().sample_per_frame
+        left = -(-(self.target_spp() - self.current_spp()) // spf)
+        if left > 0:
+            self.render_frames(left)
         self.synchronize()
 
     def synchronize(self) -> None:

@@ -70,7 +70,7 @@ class SceneParams(C.Structure):
 class RenderSettings(C.Structure):
     _fields_ = [("spp", C.c_int32), ("sample_per_frame", C.c_int32), ("max_depth", C.c_int32),
                 ("sampler_type", C.c_int32), ("pcg_seed", C.c_uint32), ("arg_order", C.c_int32),
-                ("flags", C.c_int32), ("_reserved", C.c_int32)]
+                ("flags", C.c_int32), ("paths_in_flight", C.c_int32)]
 
 
 class SceneInfo(C.Structure):
@@ -142,6 +142,7 @@ _SIGS = [
     ("pt_integrator_stats", C.c_int, [_P, C.POINTER(RenderStats)]),
     ("pt_integrator_reset_stats", C.c_int, [_P]),
     ("pt_renderer_render_batch", C.c_int, [_P, _P, _P, _P]),
+    ("pt_renderer_render_frames", C.c_int, [_P, _P, _P, C.c_uint32, _P]),
     ("pt_renderer_reset_accumulation", C.c_int, [_P, _P]),
     ("pt_scene_set_frame_count", C.c_int, [_P, C.c_uint32]),
     ("pt_render", C.c_int, [_P, C.c_int32, _P, C.c_int32, C.POINTER(RenderStats)]),

@@ -326,7 +326,7 @@ int pt_integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const
                          void* stream) {
     PT_REQUIRE(integ && film && s && params, "null argument");
     PT_GUARD_BEGIN
-    return integrator_launch(integ, film, s, params, stream);
+    return integrator_launch(integ, film, s, params, 1, stream);
     PT_GUARD_END
 }
 int pt_integrator_stats(const pt_integrator* integ, pt_render_stats* out) {
@@ -340,11 +340,17 @@ int pt_integrator_reset_stats(pt_integrator* integ) {
 
 // ---- renderer ----
 int pt_renderer_render_batch(pt_integrator* integ, pt_film* film, pt_scene* s, void* stream) {
+    return pt_renderer_render_frames(integ, film, s, 1, stream);
+}
+int pt_renderer_render_frames(pt_integrator* integ, pt_film* film, pt_scene* s, uint32_t frames, void* stream) {
     PT_REQUIRE(integ && film && s, "null argument");
+    PT_REQUIRE(frames >= 1 && frames <= (1u << 20), "frame count out of range");
     pt_scene_params prm;
     pt_scene_build_params(s, &prm);
-    if (int rc = pt_integrator_launch(integ, film, s, &prm, stream)) return rc;
-    s->frame_count++;
+    PT_GUARD_BEGIN
+    if (int rc = integrator_launch(integ, film, s, &prm, static_cast<int>(frames), stream)) return rc;
+    PT_GUARD_END
+    s->frame_count += frames;
     return PT_OK;
 }
 int pt_renderer_reset_accumulation(pt_film* film, pt_scene* s) {
@@ -395,10 +401,10 @@ int pt_render(pt_scene* s, int32_t spp, float* out_rgba, int32_t out_is_device, 
     if (int rc = pt_renderer_reset_accumulation(rcache.film, s)) return rc;
     pt_integrator_reset_stats(rcache.integ);
     const int spf = s->host.settings.sample_per_frame;
-    // Renderer::renderAll: whole batches until frameCount * spf >= spp
-    while (static_cast<int64_t>(s->frame_count) * spf < spp) {
-        if (int rc = pt_renderer_render_batch(rcache.integ, rcache.film, s, nullptr)) return rc;
-    }
+    // Renderer::renderAll: whole batches until frameCount * spf >= spp, here
+    // all of them in one launch (the same samples, in the same order)
+    const int64_t frames = (static_cast<int64_t>(spp) + spf - 1) / spf;
+    if (int rc = pt_renderer_render_frames(rcache.integ, rcache.film, s, static_cast<uint32_t>(frames), nullptr)) return rc;
     if (int rc = integrator_check(rcache.integ, true)) return rc;
     if (int rc = film_download(rcache.film, out_rgba, false, out_is_device == 0)) return rc;
     if (stats) integrator_stats(rcache.integ, stats);

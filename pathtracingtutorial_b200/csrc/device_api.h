@@ -17,7 +17,8 @@ int  film_clear(pt_film* f);
 int  film_download(const pt_film* f, float* dst, bool fresh, bool host_ptr);
 
 void integrator_free(pt_integrator* integ);
-int  integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scene_params* prm, void* stream);
+int  integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scene_params* prm, int nframes,
+                       void* stream);
 int  integrator_check(pt_integrator* integ, bool sync);
 int  integrator_stats(const pt_integrator* integ, pt_render_stats* out);
 int  integrator_reset_stats(pt_integrator* integ);

@@ -39,6 +39,7 @@ constexpr int kGOut = 40;                 // used outputs
 constexpr int kGOutPad = 48;              // 6 n-tiles of 8
 constexpr int kGMix = 40;                 // floats per mixture: 8 x (mu xyz, kappa) + 8 weights
 constexpr float kGuideAlpha = 0.5f;
+constexpr int kGuideMinibatches = 4;       // optimiser steps per wavefront pass
 
 // layer l: out x in, row-major, rows padded to in + 8 bf16 in shared memory
 __host__ __device__ constexpr int g_in(int l) { return l == 0 ? kGIn : kGHid; }
@@ -437,10 +438,31 @@ __device__ __forceinline__ void store_dy(const float (&acc)[N / 8][4], const __n
     }
 }
 
-__global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSample* __restrict__ samples,
-                                                     const uint32_t* count, uint32_t cap) {
-    const uint32_t n = min(*count, cap);
-    if (n == 0) return;
+// Sample range of minibatch mb of nmb over the first n samples.
+__host__ __device__ __forceinline__ void minibatch_range(uint32_t n, int mb, int nmb, uint32_t& lo, uint32_t& hi) {
+    lo = static_cast<uint32_t>(static_cast<uint64_t>(n) * mb / nmb);
+    hi = static_cast<uint32_t>(static_cast<uint64_t>(n) * (mb + 1) / nmb);
+}
+
+// Optimiser steps taken for the first mb minibatches (the empty ones take none).
+__host__ __device__ __forceinline__ uint32_t steps_before(uint32_t n, int mb, int nmb) {
+    uint32_t k = 0;
+    for (int i = 0; i < mb; ++i) {
+        uint32_t lo, hi;
+        minibatch_range(n, i, nmb, lo, hi);
+        k += hi > lo ? 1u : 0u;
+    }
+    return k;
+}
+
+// Gradient of the mean loss over minibatch mb (of nmb) of the collected samples.
+__global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSample* __restrict__ samples_all,
+                                                     const uint32_t* count, uint32_t cap, int mb, int nmb) {
+    uint32_t b0, b1;
+    minibatch_range(min(*count, cap), mb, nmb, b0, b1);
+    if (b1 <= b0) return;
+    const GuideSample* __restrict__ samples = samples_all + b0;
+    const uint32_t n = b1 - b0;
     const float inv_n = 1.0f / static_cast<float>(n);
     extern __shared__ __align__(16) unsigned char g_smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(g_smem);                       // W  [out][in+8]
@@ -604,14 +626,22 @@ struct GuideState {
     float        lr = 1e-2f;
 };
 
-// Step counter ++ and sample buffer reset, between a training step and Adam.
-__global__ void k_guide_step(uint32_t* step, uint32_t* sample_count) {
-    *step += 1u;
-    *sample_count = 0u;
+// After a pass's minibatches: advance the step counter (counters[1]) by the
+// steps taken and empty the sample buffer (counters[0]).
+__global__ void k_guide_step(uint32_t* counters, uint32_t cap, int nmb) {
+    counters[1] += steps_before(min(counters[0], cap), nmb, nmb);
+    counters[0] = 0u;
 }
 
-__global__ void k_guide_adam(GuideNet net, const uint32_t* step, float lr_w, float lr_g, float b1, float b2, float eps) {
-    const float t = static_cast<float>(*step);
+// Adam step for minibatch mb (skipped when it is empty); the step number is
+// the counter plus the non-empty minibatches before it, plus one.
+__global__ void k_guide_adam(GuideNet net, const uint32_t* count, uint32_t cap, int mb, int nmb, const uint32_t* step,
+                             float lr_w, float lr_g, float b1, float b2, float eps) {
+    const uint32_t n = min(*count, cap);
+    uint32_t lo, hi;
+    minibatch_range(n, mb, nmb, lo, hi);
+    if (hi <= lo) return;
+    const float t = static_cast<float>(*step + steps_before(n, mb, nmb) + 1u);
     const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
     const size_t nw = kGWeights;
     const size_t ng = static_cast<size_t>(kGLevels) * kGTable;

@@ -54,6 +54,7 @@ struct WaveParams {
     DeviceScene scene;
     pt_camera_frame cam;
     int      width, height, npix;
+    int      npath;     // path slots: npix x lanes (lanes = samples per pixel in flight)
     int      spf, max_depth, sampler_type, arg_rtl, flags;
     uint32_t pcg_seed;
     int      n_slots;
@@ -64,7 +65,7 @@ struct WaveParams {
     float4*  thr;       // xyz throughput, w last BSDF pdf
     float4*  lo;        // xyz radiance from emission / env hits, w last-was-delta
     uint32_t* rng;      // sobol dimension or pcg state
-    float4*  nee;       // n_slots x npix visible NEE contributions
+    float4*  nee;       // n_slots x npath visible NEE contributions
     uint32_t* sq_path;
     float4*  sq_o;      // w = slot (bits)
     float4*  sq_d;      // w = tmax
@@ -79,7 +80,7 @@ struct WaveParams {
     float4*  f_new;
     // learned guiding (null when off)
     const float* gmix;   // queue-ordered mixtures, kGMix floats per entry
-    float4*  grec;       // training records [depth][npix][4]
+    float4*  grec;       // training records [depth][npath][4]
 };
 
 // ---------------------------------------------------------------------------
@@ -191,7 +192,7 @@ __device__ __forceinline__ void emit_shadow(const WaveParams& P, bool want, uint
                                             f3 o, f3 d, float tmax, f3 c) {
     const uint32_t j = warp_append(P.counts + 2, want);
     if (!want) return;
-    const uint32_t cap = static_cast<uint32_t>(P.npix) * static_cast<uint32_t>(P.n_slots);
+    const uint32_t cap = static_cast<uint32_t>(P.npath) * static_cast<uint32_t>(P.n_slots);
     if (j >= cap) { atomicOr(P.err, kErrQueueOverflow); return; }
     P.sq_path[j] = path;
     P.sq_o[j] = make_float4(o.x, o.y, o.z, __uint_as_float(slot));
@@ -237,18 +238,23 @@ __device__ __forceinline__ void camera_ray(const pt_camera_frame& c, int width, 
     dir = normalize(dir);
 }
 
-__global__ void __launch_bounds__(256) k_raygen(WaveParams P, int sample_in_frame) {
+// Paths of one pass: for every pixel the samples s0 .. s0+count-1 counted
+// from the first sample of frame P.pass->frame (so a pass may span frames);
+// path p = lane * npix + pixel takes sample s0 + lane.
+__global__ void __launch_bounds__(256) k_raygen(WaveParams P, int s0, int count) {
+    const int n = P.npix * count;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        P.counts[0] = static_cast<uint32_t>(P.npix);
+        P.counts[0] = static_cast<uint32_t>(n);
         P.counts[1] = 0;
         P.counts[2] = 0;
-        atomicAdd(P.stats + kStatPaths, static_cast<unsigned long long>(P.npix));
+        atomicAdd(P.stats + kStatPaths, static_cast<unsigned long long>(n));
     }
     const uint32_t frame = P.pass->frame;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.npix; p += gridDim.x * blockDim.x) {
-        const int x = p % P.width, y = p / P.width;
-        PathRng rng = make_rng(P.sampler_type, x, y, frame, static_cast<uint32_t>(P.spf),
-                               static_cast<uint32_t>(sample_in_frame), P.pcg_seed);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int pix = p % P.npix, rel = s0 + p / P.npix;
+        const int x = pix % P.width, y = pix / P.width;
+        PathRng rng = make_rng(P.sampler_type, x, y, frame + static_cast<uint32_t>(rel / P.spf),
+                               static_cast<uint32_t>(P.spf), static_cast<uint32_t>(rel % P.spf), P.pcg_seed);
         f3 pos, dir;
         camera_ray(P.cam, P.width, P.height, x, y, rng, pos, dir);
         P.queue[0][p] = static_cast<uint32_t>(p);
@@ -257,7 +263,7 @@ __global__ void __launch_bounds__(256) k_raygen(WaveParams P, int sample_in_fram
         P.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
         P.lo[p] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         P.rng[p] = rng.s;
-        for (int k = 0; k < P.n_slots; ++k) P.nee[static_cast<size_t>(k) * P.npix + p] = make_float4(0, 0, 0, 0);
+        for (int k = 0; k < P.n_slots; ++k) P.nee[static_cast<size_t>(k) * P.npath + p] = make_float4(0, 0, 0, 0);
     }
 }
 
@@ -267,7 +273,7 @@ __device__ __forceinline__ void warp_count(unsigned long long* dst, uint32_t v) 
 }
 
 __global__ void __launch_bounds__(128) k_extend(WaveParams P, int q, int depth) {
-    const uint32_t n = min(P.counts[q], static_cast<uint32_t>(P.npix));
+    const uint32_t n = min(P.counts[q], static_cast<uint32_t>(P.npath));
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.counts[q ^ 1] = 0;
         P.counts[2] = 0;
@@ -280,13 +286,31 @@ __global__ void __launch_bounds__(128) k_extend(WaveParams P, int q, int depth) 
     const uint32_t stride = gridDim.x * blockDim.x;
     const float4* __restrict__ ro = P.ray_o[q];
     const float4* __restrict__ rd = P.ray_d[q];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const float4 o = ro[i];
-        const float4 d = rd[i];
-        const RayInv r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
-        float t, u, v;
-        const int prim = trace_closest(P.scene, r, watertight, t, u, v, err, tc);
-        P.hit[i] = make_float4(t, __int_as_float(prim), u, v);
+    // one node per iteration; a lane takes its next ray (i + stride) as soon
+    // as its current one is done
+    StepStack stk;
+    ClosestWalk w;
+    bool active = false;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    for (;;) {
+        if (!active) {
+            if (i >= n) break;
+            const float4 o = ro[i];
+            const float4 d = rd[i];
+            w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+            active = closest_begin(P.scene, w);
+            if (!active) {
+                P.hit[i] = make_float4(FLT_MAX, __int_as_float(-1), 0.0f, 0.0f);
+                i += stride;
+                continue;
+            }
+        }
+        if (!closest_step(P.scene, w, stk, watertight, err, tc)) {
+            P.hit[i] = w.prim >= 0 ? make_float4(w.best, __int_as_float(w.prim), w.bu, w.bv)
+                                   : make_float4(FLT_MAX, __int_as_float(-1), 0.0f, 0.0f);
+            i += stride;
+            active = false;
+        }
     }
     if (err) atomicOr(P.err, err);
     if (count) {
@@ -527,10 +551,10 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
     return true;
 }
 
-__global__ void __launch_bounds__(128) k_shade(WaveParams P, int q, int depth, int sample_in_frame) {
-    const uint32_t cap = static_cast<uint32_t>(P.npix);
+__global__ void __launch_bounds__(128) k_shade(WaveParams P, int q, int depth, int s0) {
+    const uint32_t cap = static_cast<uint32_t>(P.npath);
     const uint32_t n = min(P.counts[q], cap);
-    const uint32_t sidx = P.pass->frame * static_cast<uint32_t>(P.spf) + static_cast<uint32_t>(sample_in_frame);
+    const uint32_t sidx0 = P.pass->frame * static_cast<uint32_t>(P.spf) + static_cast<uint32_t>(s0);
     const bool last = depth == P.max_depth - 1;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -547,23 +571,24 @@ __global__ void __launch_bounds__(128) k_shade(WaveParams P, int q, int depth, i
         f3 L = f3of(lo);
         PathRng rng;
         rng.type = P.sampler_type;
-        rng.px = static_cast<int>(p % static_cast<uint32_t>(P.width));
-        rng.py = static_cast<int>(p / static_cast<uint32_t>(P.width));
-        rng.sample_index = sidx;
+        const uint32_t pix = p % static_cast<uint32_t>(P.npix);
+        rng.px = static_cast<int>(pix % static_cast<uint32_t>(P.width));
+        rng.py = static_cast<int>(pix / static_cast<uint32_t>(P.width));
+        rng.sample_index = sidx0 + p / static_cast<uint32_t>(P.npix);
         rng.s = P.rng[p];
         f3 no = mk(0.0f), nd = mk(0.0f);
         QueueSink sink{P, p};
         GuideVertex gv{P.gmix ? P.gmix + static_cast<size_t>(i) * kGMix : nullptr, nullptr};
         if (P.grec) {
-            gv.rec = P.grec + (static_cast<size_t>(depth) * P.npix + p) * 4;
+            gv.rec = P.grec + (static_cast<size_t>(depth) * P.npath + p) * 4;
             gv.rec[1].w = 0.0f;
             if (depth > 0) {
                 // radiance gathered through the previous vertex: the part of the
                 // final estimate that did not arrive along its sampled direction
-                float4* prev = P.grec + (static_cast<size_t>(depth - 1) * P.npix + p) * 4;
+                float4* prev = P.grec + (static_cast<size_t>(depth - 1) * P.npath + p) * 4;
                 if (prev[1].w != 0.0f) {
                     f3 S = L;
-                    for (int k = 0; k < P.n_slots; ++k) S += f3of(P.nee[static_cast<size_t>(k) * P.npix + p]);
+                    for (int k = 0; k < P.n_slots; ++k) S += f3of(P.nee[static_cast<size_t>(k) * P.npath + p]);
                     prev[3] = f4of(S, 0.0f);
                 }
             }
@@ -587,7 +612,7 @@ __global__ void __launch_bounds__(128) k_shade(WaveParams P, int q, int depth, i
 }
 
 __global__ void __launch_bounds__(128) k_shadow(WaveParams P) {
-    const uint32_t n = min(P.counts[2], static_cast<uint32_t>(P.npix) * static_cast<uint32_t>(P.n_slots));
+    const uint32_t n = min(P.counts[2], static_cast<uint32_t>(P.npath) * static_cast<uint32_t>(P.n_slots));
     if (blockIdx.x == 0 && threadIdx.x == 0)
         atomicAdd(P.stats + kStatShadowRays, static_cast<unsigned long long>(n));
     const bool watertight = (P.flags & PT_FLAG_WATERTIGHT) != 0;
@@ -595,22 +620,38 @@ __global__ void __launch_bounds__(128) k_shadow(WaveParams P) {
     uint32_t err = 0;
     TraceCounters tc{0, 0};
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const float4 o = P.sq_o[i];
-        const float4 d = P.sq_d[i];
-        const RayInv r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
-        if (!trace_any(P.scene, r, d.w, watertight, err, tc)) {
-            const uint32_t slot = __float_as_uint(o.w);
-            const uint32_t path = P.sq_path[i];
-            if (slot >= static_cast<uint32_t>(P.n_slots) || path >= static_cast<uint32_t>(P.npix)) {
-                err |= kErrQueueOverflow;
-                continue;
+    uint32_t stk[kStackDepth];
+    AnyWalk w;
+    bool active = false;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    for (;;) {
+        bool done = false;
+        if (!active) {
+            if (i >= n) break;
+            const float4 o = P.sq_o[i];
+            const float4 d = P.sq_d[i];
+            w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+            w.tmax = d.w;
+            active = any_begin(P.scene, w);
+            done = !active;
+        }
+        if (!done) done = !any_step(P.scene, w, stk, watertight, err, tc);
+        if (done) {
+            if (!w.hit) {
+                const uint32_t slot = __float_as_uint(P.sq_o[i].w);
+                const uint32_t path = P.sq_path[i];
+                if (slot < static_cast<uint32_t>(P.n_slots) && path < static_cast<uint32_t>(P.npath)) {
+                    float4* acc = P.nee + static_cast<size_t>(slot) * P.npath + path;
+                    const float4 c = P.sq_c[i];
+                    float4 a = *acc;
+                    a.x += c.x; a.y += c.y; a.z += c.z;
+                    *acc = a;
+                } else {
+                    err |= kErrQueueOverflow;
+                }
             }
-            float4* acc = P.nee + static_cast<size_t>(slot) * P.npix + path;
-            const float4 c = P.sq_c[i];
-            float4 a = *acc;
-            a.x += c.x; a.y += c.y; a.z += c.z;
-            *acc = a;
+            i += stride;
+            active = false;
         }
     }
     if (err) atomicOr(P.err, err);
@@ -627,31 +668,32 @@ __device__ __forceinline__ void neumaier(float& s, float& c, float x) {
     s = t;
 }
 
-__global__ void __launch_bounds__(256) k_finalize(WaveParams P) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.npix; p += gridDim.x * blockDim.x) {
-        f3 L = f3of(P.lo[p]);
-        for (int k = 0; k < P.n_slots; ++k) L += f3of(P.nee[static_cast<size_t>(k) * P.npix + p]);
-        // per-sample firefly clamp (path.cu:201-204); fminf maps NaN to the clamp value as the reference does
-        L = mk(fminf(L.x, 100.0f), fminf(L.y, 100.0f), fminf(L.z, 100.0f));
-        float4 s = P.f_sum[p], c = P.f_comp[p];
-        neumaier(s.x, c.x, L.x);
-        neumaier(s.y, c.y, L.y);
-        neumaier(s.z, c.z, L.z);
-        s.w += 1.0f;
-        P.f_sum[p] = s;
-        P.f_comp[p] = c;
-        float4 b = P.f_batch[p];
-        b.x += L.x; b.y += L.y; b.z += L.z;
-        P.f_batch[p] = b;
-    }
-}
-
-__global__ void k_frame_resolve(WaveParams P) {
+// Adds the pass's samples to the film, per pixel in sample order (the order
+// of one-sample-per-pass rendering, so the sums do not depend on the lanes);
+// a completed frame's mean becomes the "new" image (the reference's surfNew).
+__global__ void __launch_bounds__(256) k_finalize(WaveParams P, int s0, int count) {
     const float spf = static_cast<float>(P.spf);
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.npix; p += gridDim.x * blockDim.x) {
-        const float4 b = P.f_batch[p];
-        P.f_new[p] = make_float4(b.x / spf, b.y / spf, b.z / spf, 1.0f);
-        P.f_batch[p] = make_float4(0, 0, 0, 0);
+    for (int pix = blockIdx.x * blockDim.x + threadIdx.x; pix < P.npix; pix += gridDim.x * blockDim.x) {
+        float4 s = P.f_sum[pix], c = P.f_comp[pix], b = P.f_batch[pix];
+        for (int lane = 0; lane < count; ++lane) {
+            const int p = lane * P.npix + pix;
+            f3 L = f3of(P.lo[p]);
+            for (int k = 0; k < P.n_slots; ++k) L += f3of(P.nee[static_cast<size_t>(k) * P.npath + p]);
+            // per-sample firefly clamp (path.cu:201-204); fminf maps NaN to the clamp value as the reference does
+            L = mk(fminf(L.x, 100.0f), fminf(L.y, 100.0f), fminf(L.z, 100.0f));
+            neumaier(s.x, c.x, L.x);
+            neumaier(s.y, c.y, L.y);
+            neumaier(s.z, c.z, L.z);
+            s.w += 1.0f;
+            b.x += L.x; b.y += L.y; b.z += L.z;
+            if ((s0 + lane) % P.spf == P.spf - 1) {
+                P.f_new[pix] = make_float4(b.x / spf, b.y / spf, b.z / spf, 1.0f);
+                b = make_float4(0, 0, 0, 0);
+            }
+        }
+        P.f_sum[pix] = s;
+        P.f_comp[pix] = c;
+        P.f_batch[pix] = b;
     }
 }
 
@@ -659,13 +701,13 @@ __global__ void k_frame_resolve(WaveParams P) {
 // vertex, the incident radiance along its sampled direction is the part of the
 // path's final estimate gathered after it, divided by the throughput after it
 // (luminance, clamped like a sample); weight = L_in / p.  Records are cleared.
-__global__ void __launch_bounds__(256) k_guide_collect(WaveParams P, GuideNet net, GuideSample* out,
+__global__ void __launch_bounds__(256) k_guide_collect(WaveParams P, int npaths, GuideNet net, GuideSample* out,
                                                        uint32_t* count, uint32_t cap) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P.npix; p += gridDim.x * blockDim.x) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npaths; p += gridDim.x * blockDim.x) {
         f3 Lf = f3of(P.lo[p]);
-        for (int k = 0; k < P.n_slots; ++k) Lf += f3of(P.nee[static_cast<size_t>(k) * P.npix + p]);
+        for (int k = 0; k < P.n_slots; ++k) Lf += f3of(P.nee[static_cast<size_t>(k) * P.npath + p]);
         for (int d = 0; d + 1 < P.max_depth; ++d) {
-            float4* r = P.grec + (static_cast<size_t>(d) * P.npix + p) * 4;
+            float4* r = P.grec + (static_cast<size_t>(d) * P.npath + p) * 4;
             const float4 r1 = r[1];
             float w = 0.0f;
             float4 r0 = make_float4(0, 0, 0, 0);
@@ -706,12 +748,26 @@ __global__ void k_trace_rays(DeviceScene s, const float* rays, uint32_t n, pt_hi
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 o = reinterpret_cast<const float4*>(rays)[2 * i];
         const float4 d = reinterpret_cast<const float4*>(rays)[2 * i + 1];
-        const RayInv r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+        // the step-wise walks the wavefront kernels use
         if (any) {
-            occl[i] = trace_any(s, r, d.w, watertight != 0, err, tc) ? 1 : 0;
+            AnyWalk w;
+            w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+            w.tmax = d.w;
+            uint32_t stk[kStackDepth];
+            if (any_begin(s, w))
+                while (any_step(s, w, stk, watertight != 0, err, tc)) {}
+            occl[i] = w.hit ? 1 : 0;
         } else {
+            ClosestWalk w;
+            w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+            StepStack stk;
+            if (closest_begin(s, w))
+                while (closest_step(s, w, stk, watertight != 0, err, tc)) {}
             pt_hit h;
-            h.prim = trace_closest(s, r, watertight != 0, h.t, h.u, h.v, err, tc);
+            h.prim = w.prim;
+            h.t = w.prim >= 0 ? w.best : FLT_MAX;
+            h.u = w.prim >= 0 ? w.bu : 0.0f;
+            h.v = w.prim >= 0 ? w.bv : 0.0f;
             hits[i] = h;
         }
     }
@@ -748,7 +804,7 @@ __global__ void k_bsdf_eval(const pt_material* mats, uint32_t nmat, const float*
 struct Wavefront {
     int device = -1;
     cudaStream_t own_stream = nullptr;
-    int npix = 0, n_slots = 0;
+    int npath = 0, n_slots = 0;   // path slots the arena holds
     void* arena = nullptr;
     size_t arena_bytes = 0;
     WaveParams base{};
@@ -791,9 +847,9 @@ int grid_for(const void* kernel, int block, int sms) {
     return per_sm * sms;
 }
 
-// Size of the wavefront arena for npix paths and n_slots light slots.
-size_t arena_size(int npix, int n_slots) {
-    const size_t P = static_cast<size_t>(npix);
+// Size of the wavefront arena for npath path slots and n_slots light slots.
+size_t arena_size(int npath, int n_slots) {
+    const size_t P = static_cast<size_t>(npath);
     const size_t S = P * static_cast<size_t>(n_slots);
     size_t b = 0;
     b += 2 * (P * 4 + 256);          // queues
@@ -811,7 +867,7 @@ size_t arena_size(int npix, int n_slots) {
     return b;
 }
 
-int wavefront_prepare(Wavefront& wf, int device, int npix, int n_slots) {
+int wavefront_prepare(Wavefront& wf, int device, int npath, int n_slots) {
     if (wf.device != device) {
         if (wf.arena) { cudaSetDevice(wf.device); cudaFree(wf.arena); wf.arena = nullptr; wf.arena_bytes = 0; }
         if (wf.graph) { cudaGraphExecDestroy(wf.graph); wf.graph = nullptr; wf.graph_key.clear(); }
@@ -827,13 +883,13 @@ int wavefront_prepare(Wavefront& wf, int device, int npix, int n_slots) {
         wf.grid_shadow = grid_for(reinterpret_cast<const void*>(k_shadow), 128, sms);
         wf.grid_finalize = grid_for(reinterpret_cast<const void*>(k_finalize), 256, sms);
         wf.device = device;
-        wf.npix = 0;
+        wf.npath = 0;
     } else if (int rc = ensure_device(device)) {
         return rc;
     }
-    if (wf.npix == npix && wf.n_slots == n_slots && wf.arena) return PT_OK;
+    if (wf.npath == npath && wf.n_slots == n_slots && wf.arena) return PT_OK;
     std::memset(&wf.base, 0, sizeof(wf.base));
-    const size_t need = arena_size(npix, n_slots);
+    const size_t need = arena_size(npath, n_slots);
     if (need > wf.arena_bytes) {
         if (wf.arena) { cudaFree(wf.arena); wf.arena = nullptr; wf.arena_bytes = 0; }
         if (cudaMalloc(&wf.arena, need) != cudaSuccess) {
@@ -845,7 +901,7 @@ int wavefront_prepare(Wavefront& wf, int device, int npix, int n_slots) {
     }
     char* cur = static_cast<char*>(wf.arena);
     WaveParams& b = wf.base;
-    const size_t P = static_cast<size_t>(npix), S = P * static_cast<size_t>(n_slots);
+    const size_t P = static_cast<size_t>(npath), S = P * static_cast<size_t>(n_slots);
     b.queue[0] = carve<uint32_t>(cur, P);
     b.queue[1] = carve<uint32_t>(cur, P);
     b.ray_o[0] = carve<float4>(cur, P);
@@ -869,7 +925,7 @@ int wavefront_prepare(Wavefront& wf, int device, int npix, int n_slots) {
     PT_CU(cudaMemset(b.stats, 0, kStatCount * 8));
     PT_CU(cudaMemset(b.err, 0, 16));
     PT_CU(cudaMemset(b.pass, 0, sizeof(PassState)));
-    wf.npix = npix;
+    wf.npath = npath;
     wf.n_slots = n_slots;
     if (wf.graph) { cudaGraphExecDestroy(wf.graph); wf.graph = nullptr; wf.graph_key.clear(); }
     return PT_OK;
@@ -879,7 +935,7 @@ int wavefront_prepare(Wavefront& wf, int device, int npix, int n_slots) {
 // stage events are recorded (ev holds pairs per launch: kind, start, stop).
 struct StageEvent { int kind; cudaEvent_t a, b; };
 
-int enqueue_batch(Wavefront& wf, const WaveParams& P, cudaStream_t st, std::vector<StageEvent>* ev,
+int enqueue_batch(Wavefront& wf, const WaveParams& P, int nframes, cudaStream_t st, std::vector<StageEvent>* ev,
                   GuideState* gs = nullptr) {
     const bool infer = gs && gs->mode != 0 && P.gmix;
     const bool train = infer && P.grec;
@@ -897,35 +953,41 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, cudaStream_t st, std::vect
         }
         return PT_OK;
     };
-    for (int i = 0; i < P.spf; ++i) {
-        if (int rc = timed(3, [&] { k_raygen<<<wf.grid_raygen, 256, 0, st>>>(P, i); })) return rc;
+    const int lanes = std::max(1, P.npath / std::max(P.npix, 1));
+    const int total = P.spf * nframes;
+    for (int s0 = 0; s0 < total; s0 += lanes) {
+        const int count = std::min(lanes, total - s0);
+        if (int rc = timed(3, [&] { k_raygen<<<wf.grid_raygen, 256, 0, st>>>(P, s0, count); })) return rc;
         for (int d = 0; d < P.max_depth; ++d) {
             const int q = d & 1;
             if (int rc = timed(0, [&] { k_extend<<<wf.grid_extend, 128, 0, st>>>(P, q, d); })) return rc;
             if (infer) {
                 if (int rc = timed(4, [&] {
                         k_guide_infer<<<wf.sms * 4, 128, kGInferSmem, st>>>(gs->net, P.counts, q,
-                                                                            static_cast<uint32_t>(P.npix), P.ray_o[q],
+                                                                            static_cast<uint32_t>(P.npath), P.ray_o[q],
                                                                             P.ray_d[q], P.hit, gs->mix);
                     })) return rc;
             }
-            if (int rc = timed(1, [&] { k_shade<<<wf.grid_shade, 128, 0, st>>>(P, q, d, i); })) return rc;
+            if (int rc = timed(1, [&] { k_shade<<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0); })) return rc;
             if (int rc = timed(2, [&] { k_shadow<<<wf.grid_shadow, 128, 0, st>>>(P); })) return rc;
         }
-        if (int rc = timed(3, [&] { k_finalize<<<wf.grid_finalize, 256, 0, st>>>(P); })) return rc;
+        if (int rc = timed(3, [&] { k_finalize<<<wf.grid_finalize, 256, 0, st>>>(P, s0, count); })) return rc;
         if (train) {
             if (int rc = timed(4, [&] {
-                    k_guide_collect<<<wf.grid_finalize, 256, 0, st>>>(P, gs->net, gs->samples, gs->counters,
-                                                                      gs->sample_cap);
-                    k_guide_train<<<wf.sms, 128, kGTrainSmem, st>>>(gs->net, gs->samples, gs->counters,
-                                                                     gs->sample_cap);
-                    k_guide_step<<<1, 1, 0, st>>>(gs->counters + 1, gs->counters);
-                    k_guide_adam<<<wf.sms * 8, 256, 0, st>>>(gs->net, gs->counters + 1, gs->lr, gs->lr, 0.9f,
-                                                             0.99f, 1e-10f);
+                    k_guide_collect<<<wf.grid_finalize, 256, 0, st>>>(P, P.npix * count, gs->net, gs->samples,
+                                                                      gs->counters, gs->sample_cap);
+                    // kGuideMinibatches optimiser steps over this pass's samples
+                    for (int mb = 0; mb < kGuideMinibatches; ++mb) {
+                        k_guide_train<<<wf.sms, 128, kGTrainSmem, st>>>(gs->net, gs->samples, gs->counters,
+                                                                         gs->sample_cap, mb, kGuideMinibatches);
+                        k_guide_adam<<<wf.sms * 8, 256, 0, st>>>(gs->net, gs->counters, gs->sample_cap, mb,
+                                                                 kGuideMinibatches, gs->counters + 1, gs->lr, gs->lr,
+                                                                 0.9f, 0.99f, 1e-10f);
+                    }
+                    k_guide_step<<<1, 1, 0, st>>>(gs->counters, gs->sample_cap, kGuideMinibatches);
                 })) return rc;
         }
     }
-    if (int rc = timed(3, [&] { k_frame_resolve<<<wf.grid_finalize, 256, 0, st>>>(P); })) return rc;
     PT_CU(cudaGetLastError());
     return PT_OK;
 }
@@ -1114,19 +1176,30 @@ void integrator_free(pt_integrator* integ) {
 }
 
 // Integrator::launch (Part_2/src/integrators/path.cu:244-255).
-int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scene_params* prm, void* stream) {
+int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scene_params* prm, int nframes,
+                      void* stream) {
     if (!s->dev.uploaded) { set_error("scene not uploaded: call pt_scene_upload first"); return PT_ERR_STATE; }
     if (film->width != prm->width || film->height != prm->height) { set_error("film size does not match params"); return PT_ERR_INVALID; }
     if (prm->width <= 0 || prm->height <= 0 || prm->sample_per_frame <= 0 || prm->max_depth < 0) {
         set_error("invalid scene params"); return PT_ERR_INVALID;
     }
     if (film->device != s->dev.device) { set_error("film and scene live on different devices"); return PT_ERR_INVALID; }
+    if (nframes < 1) { set_error("frame count must be positive"); return PT_ERR_INVALID; }
     if (!integ->wf) integ->wf = new Wavefront();
     Wavefront& wf = *integ->wf;
     const int npix = prm->width * prm->height;
     const int n_slots = 2 + static_cast<int>(s->host.punctual.size());
-    if (int rc = wavefront_prepare(wf, s->dev.device, npix, n_slots)) return rc;
     const pt_render_settings& rs = s->host.settings;
+    // samples per pixel in flight per pass: as many of the launch's as the path
+    // budget holds (a guide's per-path records cap it lower)
+    GuideState* gs = wf.guide;
+    const bool guided = gs && gs->mode != 0;
+    int64_t budget = rs.paths_in_flight > 0 ? rs.paths_in_flight : kDefaultPathsInFlight;
+    if (guided) budget = std::min<int64_t>(budget, kGuidedPathsInFlight);
+    const int64_t total = static_cast<int64_t>(prm->sample_per_frame) * nframes;
+    const int lanes = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(total, budget / npix)));
+    const int npath = npix * lanes;
+    if (int rc = wavefront_prepare(wf, s->dev.device, npath, n_slots)) return rc;
     // Built byte-wise (padding zeroed) because the bytes key the graph cache.
     WaveParams P;
     std::memset(&P, 0, sizeof(P));
@@ -1134,7 +1207,7 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     const DeviceScene view = device_view(s);
     std::memcpy(&P.scene, &view, sizeof(DeviceScene));
     P.cam = prm->camera;
-    P.width = prm->width; P.height = prm->height; P.npix = npix;
+    P.width = prm->width; P.height = prm->height; P.npix = npix; P.npath = npath;
     P.spf = prm->sample_per_frame;
     P.max_depth = prm->max_depth;
     P.sampler_type = prm->sampler_type;
@@ -1146,10 +1219,9 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     P.f_comp = static_cast<float4*>(film->comp);
     P.f_batch = static_cast<float4*>(film->batch);
     P.f_new = static_cast<float4*>(film->fresh);
-    GuideState* gs = wf.guide;
-    if (gs && gs->mode != 0) {
+    if (guided) {
         if (gs->device != s->dev.device) { set_error("guide and scene live on different devices"); return PT_ERR_INVALID; }
-        if (int rc = guide_prepare_work(*gs, npix, prm->max_depth)) return rc;
+        if (int rc = guide_prepare_work(*gs, npath, prm->max_depth)) return rc;
         P.gmix = gs->mix;
         P.grec = gs->mode == PT_GUIDE_TRAIN ? gs->rec : nullptr;
     }
@@ -1164,7 +1236,7 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
         PT_CU(cudaEventCreate(&t0));
         PT_CU(cudaEventCreate(&t1));
         PT_CU(cudaEventRecord(t0, st));
-        int rc = enqueue_batch(wf, P, st, &ev, gs);
+        int rc = enqueue_batch(wf, P, nframes, st, &ev, gs);
         PT_CU(cudaEventRecord(t1, st));
         PT_CU(cudaEventSynchronize(t1));
         float ms = 0.0f;
@@ -1182,14 +1254,15 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
         cudaEventDestroy(t1);
         if (rc) return rc;
     } else if (use_graph) {
-        std::vector<unsigned char> key(sizeof(WaveParams) + sizeof(cudaStream_t));
+        std::vector<unsigned char> key(sizeof(WaveParams) + sizeof(cudaStream_t) + sizeof(int));
         std::memcpy(key.data(), &P, sizeof(WaveParams));
         std::memcpy(key.data() + sizeof(WaveParams), &st, sizeof(cudaStream_t));
+        std::memcpy(key.data() + sizeof(WaveParams) + sizeof(cudaStream_t), &nframes, sizeof(int));
         if (!wf.graph || key != wf.graph_key) {
             if (wf.graph) { cudaGraphExecDestroy(wf.graph); wf.graph = nullptr; }
             cudaGraph_t g = nullptr;
             PT_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            const int rc = enqueue_batch(wf, P, st, nullptr, gs);
+            const int rc = enqueue_batch(wf, P, nframes, st, nullptr, gs);
             const cudaError_t ec = cudaStreamEndCapture(st, &g);
             if (rc) { if (g) cudaGraphDestroy(g); return rc; }
             if (ec != cudaSuccess) { set_error(std::string("graph capture failed: ") + cudaGetErrorString(ec)); return PT_ERR_CUDA; }
@@ -1199,14 +1272,14 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
             wf.graph_key = key;
         }
         PT_CU(cudaGraphLaunch(wf.graph, st));
-        wf.extend_launches += static_cast<uint64_t>(P.spf) * P.max_depth;
     } else {
-        if (int rc = enqueue_batch(wf, P, st, nullptr, gs)) return rc;
-        wf.extend_launches += static_cast<uint64_t>(P.spf) * P.max_depth;
+        if (int rc = enqueue_batch(wf, P, nframes, st, nullptr, gs)) return rc;
     }
-    // k_begin + per pass (raygen, 3 per bounce, finalize) + batch resolve
-    wf.kernel_launches += 1 + static_cast<uint64_t>(P.spf) * (2 + 3 * static_cast<uint64_t>(P.max_depth)) + 1;
-    if (P.gmix) wf.kernel_launches += static_cast<uint64_t>(P.spf) * (P.max_depth + (P.grec ? 4 : 0));
+    // k_begin + per pass (raygen, 3 per bounce, finalize)
+    const uint64_t passes = static_cast<uint64_t>((total + lanes - 1) / lanes);
+    if (!timing) wf.extend_launches += passes * static_cast<uint64_t>(P.max_depth);
+    wf.kernel_launches += 1 + passes * (2 + 3 * static_cast<uint64_t>(P.max_depth));
+    if (P.gmix) wf.kernel_launches += passes * (P.max_depth + (P.grec ? 2 + 2 * kGuideMinibatches : 0));
     return PT_OK;
 }
 
@@ -1472,7 +1545,7 @@ int guide_backward(pt_guide* h, const float* samples, uint32_t n, float* wgrad, 
     if (e == cudaSuccess) e = cudaMemset(h->g.net.w_grad, 0, kGWeights * sizeof(float));
     if (e == cudaSuccess) e = cudaMemset(h->g.net.grid_grad, 0, ng * sizeof(float2));
     if (e == cudaSuccess) {
-        k_guide_train<<<148, 128, kGTrainSmem>>>(h->g.net, ds, dn, n);
+        k_guide_train<<<148, 128, kGTrainSmem>>>(h->g.net, ds, dn, n, 0, 1);
         e = cudaDeviceSynchronize();
     }
     if (e == cudaSuccess) e = cudaMemcpy(wgrad, h->g.net.w_grad, kGWeights * sizeof(float), cudaMemcpyDeviceToHost);

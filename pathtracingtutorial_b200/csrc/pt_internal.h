@@ -36,6 +36,11 @@ constexpr float kTwoPi  = 6.28318530717958647692f;
 // far children, so it needs at most (tree depth) entries.  Scenes whose BVH is
 // deeper than this are rejected at build time, and the kernels still guard.
 constexpr int kStackDepth = 64;
+// Default path slots of the wavefront (pt_render_settings.paths_in_flight = 0):
+// about 260 B of path state each with two light slots (8.7 GB).  With a
+// guide attached the training records (64 B per path and bounce) cap it.
+constexpr int64_t kDefaultPathsInFlight = int64_t(1) << 25;
+constexpr int64_t kGuidedPathsInFlight = int64_t(1) << 22;
 
 // Device error word bits.
 enum : uint32_t {

@@ -286,4 +286,155 @@ PT_HD bool trace_any(const DeviceScene& s, const RayInv& r, float tmax, bool wat
     return false;
 }
 
+#if defined(__CUDACC__)
+// ---------------------------------------------------------------------------
+// Step-wise traversal for the wavefront kernels: one call processes one node
+// (an inner node's two child boxes, or all triangles of a leaf) and picks the
+// next one, so a lane whose ray is finished can take its next ray while the
+// other lanes of the warp keep traversing (no lane waits for the warp's
+// longest ray).  Visit order, tests and results are those of trace_closest /
+// trace_any above.
+// ---------------------------------------------------------------------------
+struct StepStack {
+    uint32_t ref[kStackDepth];
+    float    t[kStackDepth];
+};
+
+struct ClosestWalk {
+    RayInv   r;
+    float    best, bu, bv;
+    int      prim;
+    uint32_t ref;
+    int      sp;
+};
+
+// Root test; false when the ray misses the scene box (or the scene is empty).
+__device__ __forceinline__ bool closest_begin(const DeviceScene& s, ClosestWalk& w) {
+    w.best = FLT_MAX; w.prim = -1; w.bu = 0.0f; w.bv = 0.0f; w.sp = 0;
+    if (s.num_faces == 0) return false;
+    float en, ex;
+    box_span(w.r, s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], en, ex);
+    if (!(en <= w.best && en <= ex)) return false;
+    w.ref = s.root_ref;
+    return true;
+}
+
+// One node; false when the traversal is complete.
+__device__ __forceinline__ bool closest_step(const DeviceScene& s, ClosestWalk& w, StepStack& st, bool watertight,
+                                             uint32_t& err, TraceCounters& cnt) {
+    if (w.ref & kLeafBit) {
+        uint32_t ti = w.ref & ~kLeafBit;
+        for (;;) {
+            float u, v; bool last;
+            const float t = tri_test(s, w.r, ti, false, watertight, u, v, last);
+            ++cnt.tris;
+            if (t >= 0.0f && t < w.best) { w.best = t; w.prim = static_cast<int>(ti); w.bu = u; w.bv = v; }
+            if (last) break;
+            ++ti;
+        }
+    } else {
+        ++cnt.inner;
+        const float* nb = reinterpret_cast<const float*>(s.inner + w.ref);
+        const float4 q0 = PT_LDG4(nb);
+        const float4 q1 = PT_LDG4(nb + 4);
+        const float4 q2 = PT_LDG4(nb + 8);
+        const uint4  q3 = PT_LDGU4(nb + 12);
+        float e0, x0, e1, x1;
+        box_span(w.r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, e0, x0);
+        box_span(w.r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, e1, x1);
+        const bool h0 = e0 <= w.best && e0 <= x0;
+        const bool h1 = e1 <= w.best && e1 <= x1;
+        const uint32_t axis = q3.z & 3u;
+        const int lt = static_cast<int>((q3.z >> 2) & 1u);
+        const int sg = axis == 0 ? w.r.sx : (axis == 1 ? w.r.sy : w.r.sz);
+        const bool right_first = sg == lt;
+        const uint32_t nref = right_first ? q3.y : q3.x;
+        const uint32_t fref = right_first ? q3.x : q3.y;
+        const bool hn = right_first ? h1 : h0;
+        const bool hf = right_first ? h0 : h1;
+        const float ef = right_first ? e0 : e1;
+        if (hn) {
+            if (hf) {
+                if (w.sp >= kStackDepth) { err |= kErrStackOverflow; return false; }
+                st.ref[w.sp] = fref; st.t[w.sp] = ef; ++w.sp;
+            }
+            w.ref = nref;
+            return true;
+        }
+        if (hf) { w.ref = fref; return true; }
+    }
+    while (w.sp > 0) {
+        --w.sp;
+        if (st.t[w.sp] <= w.best) { w.ref = st.ref[w.sp]; return true; }
+    }
+    return false;
+}
+
+struct AnyWalk {
+    RayInv   r;
+    float    tmax;
+    uint32_t ref;
+    int      sp;
+    bool     hit;
+};
+
+__device__ __forceinline__ bool any_begin(const DeviceScene& s, AnyWalk& w) {
+    w.sp = 0; w.hit = false;
+    if (s.num_faces == 0) return false;
+    float en, ex;
+    box_span(w.r, s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], en, ex);
+    if (!(en <= w.tmax && en <= ex)) return false;
+    w.ref = s.root_ref;
+    return true;
+}
+
+// One node; false when the traversal is complete (w.hit tells the result).
+__device__ __forceinline__ bool any_step(const DeviceScene& s, AnyWalk& w, uint32_t* stack, bool watertight,
+                                         uint32_t& err, TraceCounters& cnt) {
+    if (w.ref & kLeafBit) {
+        uint32_t ti = w.ref & ~kLeafBit;
+        for (;;) {
+            float u, v; bool last;
+            const float t = tri_test(s, w.r, ti, true, watertight, u, v, last);
+            ++cnt.tris;
+            if (t > 0.0f && t < w.tmax) { w.hit = true; return false; }
+            if (last) break;
+            ++ti;
+        }
+    } else {
+        ++cnt.inner;
+        const float* nb = reinterpret_cast<const float*>(s.inner + w.ref);
+        const float4 q0 = PT_LDG4(nb);
+        const float4 q1 = PT_LDG4(nb + 4);
+        const float4 q2 = PT_LDG4(nb + 8);
+        const uint4  q3 = PT_LDGU4(nb + 12);
+        float e0, x0, e1, x1;
+        box_span(w.r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, e0, x0);
+        box_span(w.r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, e1, x1);
+        const bool h0 = e0 <= w.tmax && e0 <= x0;
+        const bool h1 = e1 <= w.tmax && e1 <= x1;
+        const uint32_t axis = q3.z & 3u;
+        const int lt = static_cast<int>((q3.z >> 2) & 1u);
+        const int sg = axis == 0 ? w.r.sx : (axis == 1 ? w.r.sy : w.r.sz);
+        const bool right_first = sg == lt;
+        const uint32_t nref = right_first ? q3.y : q3.x;
+        const uint32_t fref = right_first ? q3.x : q3.y;
+        const bool hn = right_first ? h1 : h0;
+        const bool hf = right_first ? h0 : h1;
+        if (hn) {
+            if (hf) {
+                if (w.sp >= kStackDepth) { err |= kErrStackOverflow; return false; }
+                stack[w.sp++] = fref;
+            }
+            w.ref = nref;
+            return true;
+        }
+        if (hf) { w.ref = fref; return true; }
+    }
+    if (w.sp == 0) return false;
+    w.ref = stack[--w.sp];
+    return true;
+}
+#endif  // __CUDACC__
+
 }  // namespace ptb

@@ -6,9 +6,14 @@ Radiance is compared with the FP64 oracle:
     two estimates differ only by FP32-vs-FP64 rounding and the rare branch it
     flips, so the bound is tight (median relative error < 1e-4; whole-image
     relMSE < 1e-3);
-  * independent: disjoint sample indices -- per-pixel z-scores of the
-    difference must look standard normal (mean |z| < 1, |z| > 5 in < 0.5 % of
-    channels) and the image means agree within 4 standard errors.
+  * independent: disjoint sample indices -- the squared per-pixel
+    differences must add up to at most their expected value (the sum of both
+    estimates' variances; ratio < 1.4, and > 0.6 for the independent PCG
+    sampler -- Sobol's stratification makes the error smaller than the
+    variance predicts), and the means of the image and of its four quadrants
+    agree within 4 standard errors.  (Per-pixel or per-tile z-scores are not
+    used: with a few dozen samples the variance estimates of heavy-tailed
+    pixels are too noisy for a normal test.)
 """
 import numpy as np
 import pytest
@@ -156,19 +161,25 @@ def test_radiance_correlated_with_fp64_oracle(oracle, name, spp):
 @pytest.mark.parametrize("name", ["cornell", "spheres"])
 def test_radiance_independent_samples_unbiased(oracle, name):
     sa = SCENES[name]()
-    spp = 32
+    spp = 64
     img = pt.render(_scene(sa), spp)[..., :3].astype(np.float64)
     # oracle on disjoint sample indices (frames 1000.. instead of 0..)
-    mean, var, _ = _oracle_mean(oracle, sa, frames=32, first_frame=1000)
-    n_ref = 32 * sa.sample_per_frame
-    se = np.sqrt(var / spp + var / n_ref)
-    live = se > 0
-    z = (img - mean)[live] / se[live]
-    assert np.mean(np.abs(z)) < 1.0, np.mean(np.abs(z))
-    assert np.mean(np.abs(z) > 5) < 5e-3
-    diff = img.mean() - mean.mean()
-    se_mean = np.sqrt((var.mean() / spp + var.mean() / n_ref) / img[..., 0].size)
-    assert abs(diff) < 4 * se_mean * np.sqrt(3) + 1e-6, (diff, se_mean)
+    frames = 64 // sa.sample_per_frame
+    mean, var, _ = _oracle_mean(oracle, sa, frames=frames, first_frame=1000)
+    n_ref = frames * sa.sample_per_frame
+    var = np.maximum(var, 0.0)
+    # (1) squared differences against their expectation
+    ratio = ((img - mean) ** 2).sum() / (var * (1.0 / spp + 1.0 / n_ref)).sum()
+    lo = 0.6 if sa.sampler == pt.SAMPLER_PCG else 0.0
+    assert lo < ratio < 1.4, ratio
+    # (2) means of the image and of its quadrants
+    h, w = img.shape[0], img.shape[1]
+    for ys, xs in [(slice(0, h), slice(0, w)), (slice(0, h // 2), slice(0, w // 2)), (slice(0, h // 2), slice(w // 2, w)),
+                   (slice(h // 2, h), slice(0, w // 2)), (slice(h // 2, h), slice(w // 2, w))]:
+        a, m, v = img[ys, xs], mean[ys, xs], var[ys, xs]
+        diff = a.mean() - m.mean()
+        se_mean = np.sqrt((v.mean() / spp + v.mean() / n_ref) / a[..., 0].size)
+        assert abs(diff) < 4 * se_mean * np.sqrt(3) + 1e-6, (diff, se_mean)
 
 
 def test_render_deterministic_and_graph_equivalent():
