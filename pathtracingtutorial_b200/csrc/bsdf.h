@@ -257,6 +257,18 @@ PT_HD BsdfEval disney_eval(const MatEval& m, f3 wo, f3 wi, f3 n, bool entering) 
 
 struct BsdfSample { f3 wi; f3 weight; float pdf; bool delta; bool valid; };
 
+#if defined(__CUDA_ARCH__)
+// Device code calls the BSDF through one out-of-line copy: inlined at every
+// call site (NEE per light type, BSDF sampling, guided MIS) the shading kernel
+// outgrows the instruction cache.
+__device__ __noinline__ BsdfEval disney_eval_call(const MatEval& m, f3 wo, f3 wi, f3 n, bool entering) {
+    return disney_eval(m, wo, wi, n, entering);
+}
+#  define PT_BSDF_EVAL disney_eval_call
+#else
+#  define PT_BSDF_EVAL disney_eval
+#endif
+
 // One-lobe importance sample.  Draws 1 + 2 dimensions, none when N.V < 1e-5
 // (the reference returns before its first draw, disney_bsdf.cuh:332-333).
 PT_HD BsdfSample disney_sample(const MatEval& m, f3 wo, f3 n, PathRng& rng, int rtl, bool entering) {
@@ -299,7 +311,7 @@ PT_HD BsdfSample disney_sample(const MatEval& m, f3 wo, f3 n, PathRng& rng, int 
             delta = m.roughness < 0.01f;
         }
     }
-    const BsdfEval ev = disney_eval(m, wo, wi, n, entering);
+    const BsdfEval ev = PT_BSDF_EVAL(m, wo, wi, n, entering);
     if (ev.pdf <= 0.0f) return r;
     r.wi = wi; r.pdf = ev.pdf; r.delta = delta; r.valid = true;
     if (delta) {
@@ -314,6 +326,16 @@ PT_HD BsdfSample disney_sample(const MatEval& m, f3 wo, f3 n, PathRng& rng, int 
     }
     return r;
 }
+
+#if defined(__CUDA_ARCH__)
+__device__ __noinline__ BsdfSample disney_sample_call(const MatEval& m, f3 wo, f3 n, PathRng& rng, int rtl,
+                                                      bool entering) {
+    return disney_sample(m, wo, n, rng, rtl, entering);
+}
+#  define PT_BSDF_SAMPLE disney_sample_call
+#else
+#  define PT_BSDF_SAMPLE disney_sample
+#endif
 
 PT_HD float power_heuristic(float a, float b) {
     const float a2 = a * a, b2 = b * b, s = a2 + b2;

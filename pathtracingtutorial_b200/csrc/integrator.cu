@@ -173,7 +173,7 @@ __device__ __forceinline__ uint32_t sample_alias(const pt_alias_entry* t, uint32
 // its pdf (alpha q + (1 - alpha) p_bsdf) enters the power heuristic.
 __device__ __forceinline__ f3 direct_term(const MatEval& me, f3 wo, f3 wi, f3 n, f3 radiance, float light_pdf,
                                           const float* gmix) {
-    const BsdfEval b = disney_eval(me, wo, wi, n, true);
+    const BsdfEval b = PT_BSDF_EVAL(me, wo, wi, n, true);
     if (b.pdf <= 0.0f) return mk(0.0f);
     const float dir_pdf = gmix ? kGuideAlpha * mix_pdf(gmix, wi) + (1.0f - kGuideAlpha) * b.pdf : b.pdf;
     const float mis = power_heuristic(light_pdf, dir_pdf);
@@ -286,32 +286,17 @@ __global__ void __launch_bounds__(128) k_extend(WaveParams P, int q, int depth) 
     const uint32_t stride = gridDim.x * blockDim.x;
     const float4* __restrict__ ro = P.ray_o[q];
     const float4* __restrict__ rd = P.ray_d[q];
-    // one node per iteration; a lane takes its next ray (i + stride) as soon
-    // as its current one is done
-    StepStack stk;
-    ClosestWalk w;
-    bool active = false;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    for (;;) {
-        if (!active) {
-            if (i >= n) break;
-            const float4 o = ro[i];
-            const float4 d = rd[i];
-            w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
-            active = closest_begin(P.scene, w);
-            if (!active) {
-                P.hit[i] = make_float4(FLT_MAX, __int_as_float(-1), 0.0f, 0.0f);
-                i += stride;
-                continue;
-            }
-        }
-        if (!closest_step(P.scene, w, stk, watertight, err, tc)) {
-            P.hit[i] = w.prim >= 0 ? make_float4(w.best, __int_as_float(w.prim), w.bu, w.bv)
-                                   : make_float4(FLT_MAX, __int_as_float(-1), 0.0f, 0.0f);
-            i += stride;
-            active = false;
-        }
-    }
+    float4* __restrict__ hit = P.hit;
+    closest_loop(P.scene, blockIdx.x * blockDim.x + threadIdx.x, n, stride, watertight, err, tc,
+                 [&](uint32_t i, RayInv& r) {
+                     const float4 o = ro[i];
+                     const float4 d = rd[i];
+                     r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+                 },
+                 [&](uint32_t i, const ClosestWalk& w) {
+                     hit[i] = w.prim >= 0 ? make_float4(w.best, __int_as_float(w.prim), w.bu, w.bv)
+                                          : make_float4(FLT_MAX, __int_as_float(-1), 0.0f, 0.0f);
+                 });
     if (err) atomicOr(P.err, err);
     if (count) {
         warp_count(P.stats + kStatNodes, tc.inner);
@@ -488,7 +473,7 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
             f3 contrib = mk(0.0f);
             if (ok) ok = dot(N, wi) > 0.0f;
             if (ok) {
-                contrib = T * (inten * disney_eval(me, wo, wi, N, true).f);
+                contrib = T * (inten * PT_BSDF_EVAL(me, wo, wi, N, true).f);
                 ok = !is_zero(contrib);
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
@@ -504,14 +489,14 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
         if (sel < kGuideAlpha) {
             const float u0 = rng_next(rng), u1 = rng_next(rng), u2 = rng_next(rng);
             bs.wi = mix_sample(gmix, u0, u1, u2);
-            const BsdfEval ev = disney_eval(me, wo, bs.wi, N, entering);
+            const BsdfEval ev = PT_BSDF_EVAL(me, wo, bs.wi, N, entering);
             const float p = kGuideAlpha * mix_pdf(gmix, bs.wi) + (1.0f - kGuideAlpha) * ev.pdf;
             bs.valid = p > 0.0f && !is_zero(ev.f);
             bs.pdf = p;
             bs.weight = bs.valid ? ev.f / p : mk(0.0f);
             bs.delta = false;
         } else {
-            bs = disney_sample(me, wo, N, rng, arg_rtl, entering);
+            bs = PT_BSDF_SAMPLE(me, wo, N, rng, arg_rtl, entering);
             if (bs.valid) {
                 const float p = kGuideAlpha * mix_pdf(gmix, bs.wi) + (1.0f - kGuideAlpha) * bs.pdf;
                 bs.weight = bs.weight * ((bs.pdf + 1e-7f) / p);
@@ -519,7 +504,7 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
             }
         }
     } else {
-        bs = disney_sample(me, wo, N, rng, arg_rtl, entering);
+        bs = PT_BSDF_SAMPLE(me, wo, N, rng, arg_rtl, entering);
     }
     if (!bs.valid) return false;
     T *= bs.weight;
@@ -551,7 +536,9 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
     return true;
 }
 
-__global__ void __launch_bounds__(128) k_shade(WaveParams P, int q, int depth, int s0) {
+// 5 blocks of 128 per SM (96 registers): the register-limited occupancy of 4
+// left too few warps to cover the material and vertex fetches.
+__global__ void __launch_bounds__(128, 5) k_shade(WaveParams P, int q, int depth, int s0) {
     const uint32_t cap = static_cast<uint32_t>(P.npath);
     const uint32_t n = min(P.counts[q], cap);
     const uint32_t sidx0 = P.pass->frame * static_cast<uint32_t>(P.spf) + static_cast<uint32_t>(s0);
@@ -620,40 +607,27 @@ __global__ void __launch_bounds__(128) k_shadow(WaveParams P) {
     uint32_t err = 0;
     TraceCounters tc{0, 0};
     const uint32_t stride = gridDim.x * blockDim.x;
-    uint32_t stk[kStackDepth];
-    AnyWalk w;
-    bool active = false;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    for (;;) {
-        bool done = false;
-        if (!active) {
-            if (i >= n) break;
-            const float4 o = P.sq_o[i];
-            const float4 d = P.sq_d[i];
-            w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
-            w.tmax = d.w;
-            active = any_begin(P.scene, w);
-            done = !active;
-        }
-        if (!done) done = !any_step(P.scene, w, stk, watertight, err, tc);
-        if (done) {
-            if (!w.hit) {
-                const uint32_t slot = __float_as_uint(P.sq_o[i].w);
-                const uint32_t path = P.sq_path[i];
-                if (slot < static_cast<uint32_t>(P.n_slots) && path < static_cast<uint32_t>(P.npath)) {
-                    float4* acc = P.nee + static_cast<size_t>(slot) * P.npath + path;
-                    const float4 c = P.sq_c[i];
-                    float4 a = *acc;
-                    a.x += c.x; a.y += c.y; a.z += c.z;
-                    *acc = a;
-                } else {
-                    err |= kErrQueueOverflow;
-                }
-            }
-            i += stride;
-            active = false;
-        }
-    }
+    any_loop(P.scene, blockIdx.x * blockDim.x + threadIdx.x, n, stride, watertight, err, tc,
+             [&](uint32_t i, AnyWalk& w) {
+                 const float4 o = P.sq_o[i];
+                 const float4 d = P.sq_d[i];
+                 w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+                 w.tmax = d.w;
+             },
+             [&](uint32_t i, bool occluded) {
+                 if (occluded) return;
+                 const uint32_t slot = __float_as_uint(P.sq_o[i].w);
+                 const uint32_t path = P.sq_path[i];
+                 if (slot < static_cast<uint32_t>(P.n_slots) && path < static_cast<uint32_t>(P.npath)) {
+                     float4* acc = P.nee + static_cast<size_t>(slot) * P.npath + path;
+                     const float4 c = P.sq_c[i];
+                     float4 a = *acc;
+                     a.x += c.x; a.y += c.y; a.z += c.z;
+                     *acc = a;
+                 } else {
+                     err |= kErrQueueOverflow;
+                 }
+             });
     if (err) atomicOr(P.err, err);
     if (count) {
         warp_count(P.stats + kStatShadowNodes, tc.inner);
@@ -743,33 +717,33 @@ __global__ void k_film_mean(const float4* sum, const float4* comp, float4* out, 
 // ---- diagnostics ----
 __global__ void k_trace_rays(DeviceScene s, const float* rays, uint32_t n, pt_hit* hits, uint8_t* occl,
                              int any, int watertight, uint32_t* err_out) {
+    // the warp-scheduled loops of the wavefront kernels
     uint32_t err = 0;
     TraceCounters tc{0, 0};
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 o = reinterpret_cast<const float4*>(rays)[2 * i];
-        const float4 d = reinterpret_cast<const float4*>(rays)[2 * i + 1];
-        // the step-wise walks the wavefront kernels use
-        if (any) {
-            AnyWalk w;
-            w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
-            w.tmax = d.w;
-            uint32_t stk[kStackDepth];
-            if (any_begin(s, w))
-                while (any_step(s, w, stk, watertight != 0, err, tc)) {}
-            occl[i] = w.hit ? 1 : 0;
-        } else {
-            ClosestWalk w;
-            w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
-            StepStack stk;
-            if (closest_begin(s, w))
-                while (closest_step(s, w, stk, watertight != 0, err, tc)) {}
-            pt_hit h;
-            h.prim = w.prim;
-            h.t = w.prim >= 0 ? w.best : FLT_MAX;
-            h.u = w.prim >= 0 ? w.bu : 0.0f;
-            h.v = w.prim >= 0 ? w.bv : 0.0f;
-            hits[i] = h;
-        }
+    const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    const float4* r4 = reinterpret_cast<const float4*>(rays);
+    if (any) {
+        any_loop(s, first, n, stride, watertight != 0, err, tc,
+                 [&](uint32_t i, AnyWalk& w) {
+                     const float4 o = r4[2 * i], d = r4[2 * i + 1];
+                     w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+                     w.tmax = d.w;
+                 },
+                 [&](uint32_t i, bool occluded) { occl[i] = occluded ? 1 : 0; });
+    } else {
+        closest_loop(s, first, n, stride, watertight != 0, err, tc,
+                     [&](uint32_t i, RayInv& r) {
+                         const float4 o = r4[2 * i], d = r4[2 * i + 1];
+                         r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+                     },
+                     [&](uint32_t i, const ClosestWalk& w) {
+                         pt_hit h;
+                         h.prim = w.prim;
+                         h.t = w.prim >= 0 ? w.best : FLT_MAX;
+                         h.u = w.prim >= 0 ? w.bu : 0.0f;
+                         h.v = w.prim >= 0 ? w.bv : 0.0f;
+                         hits[i] = h;
+                     });
     }
     if (err) atomicOr(err_out, err);
 }

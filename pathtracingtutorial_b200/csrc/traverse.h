@@ -288,12 +288,13 @@ PT_HD bool trace_any(const DeviceScene& s, const RayInv& r, float tmax, bool wat
 
 #if defined(__CUDACC__)
 // ---------------------------------------------------------------------------
-// Step-wise traversal for the wavefront kernels: one call processes one node
-// (an inner node's two child boxes, or all triangles of a leaf) and picks the
-// next one, so a lane whose ray is finished can take its next ray while the
-// other lanes of the warp keep traversing (no lane waits for the warp's
-// longest ray).  Visit order, tests and results are those of trace_closest /
-// trace_any above.
+// Warp-scheduled traversal for the wavefront kernels.  Each lane walks its own
+// ray with the visit order, tests and results of trace_closest / trace_any
+// above, but the warp alternates two phases: all lanes that stand on inner
+// nodes step through inner nodes until each reaches a leaf, then all lanes
+// at a leaf test its triangles together.  A lane whose ray is finished takes
+// its next ray (i + stride) at once instead of waiting for the warp's longest
+// ray.  All 32 lanes of the warp must call these loops.
 // ---------------------------------------------------------------------------
 struct StepStack {
     uint32_t ref[kStackDepth];
@@ -319,55 +320,91 @@ __device__ __forceinline__ bool closest_begin(const DeviceScene& s, ClosestWalk&
     return true;
 }
 
-// One node; false when the traversal is complete.
-__device__ __forceinline__ bool closest_step(const DeviceScene& s, ClosestWalk& w, StepStack& st, bool watertight,
-                                             uint32_t& err, TraceCounters& cnt) {
-    if (w.ref & kLeafBit) {
-        uint32_t ti = w.ref & ~kLeafBit;
-        for (;;) {
-            float u, v; bool last;
-            const float t = tri_test(s, w.r, ti, false, watertight, u, v, last);
-            ++cnt.tris;
-            if (t >= 0.0f && t < w.best) { w.best = t; w.prim = static_cast<int>(ti); w.bu = u; w.bv = v; }
-            if (last) break;
-            ++ti;
-        }
-    } else {
-        ++cnt.inner;
-        const float* nb = reinterpret_cast<const float*>(s.inner + w.ref);
-        const float4 q0 = PT_LDG4(nb);
-        const float4 q1 = PT_LDG4(nb + 4);
-        const float4 q2 = PT_LDG4(nb + 8);
-        const uint4  q3 = PT_LDGU4(nb + 12);
-        float e0, x0, e1, x1;
-        box_span(w.r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, e0, x0);
-        box_span(w.r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, e1, x1);
-        const bool h0 = e0 <= w.best && e0 <= x0;
-        const bool h1 = e1 <= w.best && e1 <= x1;
-        const uint32_t axis = q3.z & 3u;
-        const int lt = static_cast<int>((q3.z >> 2) & 1u);
-        const int sg = axis == 0 ? w.r.sx : (axis == 1 ? w.r.sy : w.r.sz);
-        const bool right_first = sg == lt;
-        const uint32_t nref = right_first ? q3.y : q3.x;
-        const uint32_t fref = right_first ? q3.x : q3.y;
-        const bool hn = right_first ? h1 : h0;
-        const bool hf = right_first ? h0 : h1;
-        const float ef = right_first ? e0 : e1;
-        if (hn) {
-            if (hf) {
-                if (w.sp >= kStackDepth) { err |= kErrStackOverflow; return false; }
-                st.ref[w.sp] = fref; st.t[w.sp] = ef; ++w.sp;
-            }
-            w.ref = nref;
-            return true;
-        }
-        if (hf) { w.ref = fref; return true; }
-    }
+// Next deferred child that still passes against the current best; false at the end.
+__device__ __forceinline__ bool closest_pop(ClosestWalk& w, const StepStack& st) {
     while (w.sp > 0) {
         --w.sp;
         if (st.t[w.sp] <= w.best) { w.ref = st.ref[w.sp]; return true; }
     }
     return false;
+}
+
+// Inner node w.ref: both child boxes, then the next node; false at the end.
+__device__ __forceinline__ bool closest_inner(const DeviceScene& s, ClosestWalk& w, StepStack& st, uint32_t& err,
+                                              TraceCounters& cnt) {
+    ++cnt.inner;
+    const float* nb = reinterpret_cast<const float*>(s.inner + w.ref);
+    const float4 q0 = PT_LDG4(nb);
+    const float4 q1 = PT_LDG4(nb + 4);
+    const float4 q2 = PT_LDG4(nb + 8);
+    const uint4  q3 = PT_LDGU4(nb + 12);
+    float e0, x0, e1, x1;
+    box_span(w.r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, e0, x0);
+    box_span(w.r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, e1, x1);
+    const bool h0 = e0 <= w.best && e0 <= x0;
+    const bool h1 = e1 <= w.best && e1 <= x1;
+    const uint32_t axis = q3.z & 3u;
+    const int lt = static_cast<int>((q3.z >> 2) & 1u);
+    const int sg = axis == 0 ? w.r.sx : (axis == 1 ? w.r.sy : w.r.sz);
+    const bool right_first = sg == lt;
+    const uint32_t nref = right_first ? q3.y : q3.x;
+    const uint32_t fref = right_first ? q3.x : q3.y;
+    const bool hn = right_first ? h1 : h0;
+    const bool hf = right_first ? h0 : h1;
+    const float ef = right_first ? e0 : e1;
+    if (hn) {
+        if (hf) {
+            if (w.sp >= kStackDepth) { err |= kErrStackOverflow; return false; }
+            st.ref[w.sp] = fref; st.t[w.sp] = ef; ++w.sp;
+        }
+        w.ref = nref;
+        return true;
+    }
+    if (hf) { w.ref = fref; return true; }
+    return closest_pop(w, st);
+}
+
+// Leaf w.ref: its triangles, then the next node; false at the end.
+__device__ __forceinline__ bool closest_leaf(const DeviceScene& s, ClosestWalk& w, StepStack& st, bool watertight,
+                                             TraceCounters& cnt) {
+    uint32_t ti = w.ref & ~kLeafBit;
+    for (;;) {
+        float u, v; bool last;
+        const float t = tri_test(s, w.r, ti, false, watertight, u, v, last);
+        ++cnt.tris;
+        if (t >= 0.0f && t < w.best) { w.best = t; w.prim = static_cast<int>(ti); w.bu = u; w.bv = v; }
+        if (last) break;
+        ++ti;
+    }
+    return closest_pop(w, st);
+}
+
+// Closest hits of rays first, first + stride, ... < n.  fetch(i, RayInv&)
+// loads ray i; done(i, const ClosestWalk&) stores its result (prim < 0: miss).
+template <class Fetch, class Done>
+__device__ __forceinline__ void closest_loop(const DeviceScene& s, uint32_t i, uint32_t n, uint32_t stride,
+                                             bool watertight, uint32_t& err, TraceCounters& cnt, Fetch&& fetch,
+                                             Done&& done) {
+    StepStack st;
+    ClosestWalk w;
+    bool have = false;
+    for (;;) {
+        while (!have && i < n) {
+            fetch(i, w.r);
+            if (closest_begin(s, w)) { have = true; }
+            else { done(i, w); i += stride; }
+        }
+        if (!__any_sync(0xffffffffu, have)) break;
+        bool fin = false;
+        if (have) {
+            while (!(w.ref & kLeafBit)) {
+                if (!closest_inner(s, w, st, err, cnt)) { fin = true; break; }
+            }
+        }
+        __syncwarp();
+        if (have && !fin) fin = !closest_leaf(s, w, st, watertight, cnt);
+        if (fin) { done(i, w); i += stride; have = false; }
+    }
 }
 
 struct AnyWalk {
@@ -388,52 +425,83 @@ __device__ __forceinline__ bool any_begin(const DeviceScene& s, AnyWalk& w) {
     return true;
 }
 
-// One node; false when the traversal is complete (w.hit tells the result).
-__device__ __forceinline__ bool any_step(const DeviceScene& s, AnyWalk& w, uint32_t* stack, bool watertight,
-                                         uint32_t& err, TraceCounters& cnt) {
-    if (w.ref & kLeafBit) {
-        uint32_t ti = w.ref & ~kLeafBit;
-        for (;;) {
-            float u, v; bool last;
-            const float t = tri_test(s, w.r, ti, true, watertight, u, v, last);
-            ++cnt.tris;
-            if (t > 0.0f && t < w.tmax) { w.hit = true; return false; }
-            if (last) break;
-            ++ti;
+__device__ __forceinline__ bool any_inner(const DeviceScene& s, AnyWalk& w, uint32_t* stack, uint32_t& err,
+                                          TraceCounters& cnt) {
+    ++cnt.inner;
+    const float* nb = reinterpret_cast<const float*>(s.inner + w.ref);
+    const float4 q0 = PT_LDG4(nb);
+    const float4 q1 = PT_LDG4(nb + 4);
+    const float4 q2 = PT_LDG4(nb + 8);
+    const uint4  q3 = PT_LDGU4(nb + 12);
+    float e0, x0, e1, x1;
+    box_span(w.r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, e0, x0);
+    box_span(w.r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, e1, x1);
+    const bool h0 = e0 <= w.tmax && e0 <= x0;
+    const bool h1 = e1 <= w.tmax && e1 <= x1;
+    const uint32_t axis = q3.z & 3u;
+    const int lt = static_cast<int>((q3.z >> 2) & 1u);
+    const int sg = axis == 0 ? w.r.sx : (axis == 1 ? w.r.sy : w.r.sz);
+    const bool right_first = sg == lt;
+    const uint32_t nref = right_first ? q3.y : q3.x;
+    const uint32_t fref = right_first ? q3.x : q3.y;
+    const bool hn = right_first ? h1 : h0;
+    const bool hf = right_first ? h0 : h1;
+    if (hn) {
+        if (hf) {
+            if (w.sp >= kStackDepth) { err |= kErrStackOverflow; return false; }
+            stack[w.sp++] = fref;
         }
-    } else {
-        ++cnt.inner;
-        const float* nb = reinterpret_cast<const float*>(s.inner + w.ref);
-        const float4 q0 = PT_LDG4(nb);
-        const float4 q1 = PT_LDG4(nb + 4);
-        const float4 q2 = PT_LDG4(nb + 8);
-        const uint4  q3 = PT_LDGU4(nb + 12);
-        float e0, x0, e1, x1;
-        box_span(w.r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, e0, x0);
-        box_span(w.r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, e1, x1);
-        const bool h0 = e0 <= w.tmax && e0 <= x0;
-        const bool h1 = e1 <= w.tmax && e1 <= x1;
-        const uint32_t axis = q3.z & 3u;
-        const int lt = static_cast<int>((q3.z >> 2) & 1u);
-        const int sg = axis == 0 ? w.r.sx : (axis == 1 ? w.r.sy : w.r.sz);
-        const bool right_first = sg == lt;
-        const uint32_t nref = right_first ? q3.y : q3.x;
-        const uint32_t fref = right_first ? q3.x : q3.y;
-        const bool hn = right_first ? h1 : h0;
-        const bool hf = right_first ? h0 : h1;
-        if (hn) {
-            if (hf) {
-                if (w.sp >= kStackDepth) { err |= kErrStackOverflow; return false; }
-                stack[w.sp++] = fref;
-            }
-            w.ref = nref;
-            return true;
-        }
-        if (hf) { w.ref = fref; return true; }
+        w.ref = nref;
+        return true;
+    }
+    if (hf) { w.ref = fref; return true; }
+    if (w.sp == 0) return false;
+    w.ref = stack[--w.sp];
+    return true;
+}
+
+__device__ __forceinline__ bool any_leaf(const DeviceScene& s, AnyWalk& w, uint32_t* stack, bool watertight,
+                                         TraceCounters& cnt) {
+    uint32_t ti = w.ref & ~kLeafBit;
+    for (;;) {
+        float u, v; bool last;
+        const float t = tri_test(s, w.r, ti, true, watertight, u, v, last);
+        ++cnt.tris;
+        if (t > 0.0f && t < w.tmax) { w.hit = true; return false; }
+        if (last) break;
+        ++ti;
     }
     if (w.sp == 0) return false;
     w.ref = stack[--w.sp];
     return true;
+}
+
+// Any-hit tests of rays first, first + stride, ... < n.  fetch(i, AnyWalk&)
+// sets r and tmax; done(i, bool occluded) consumes the result.
+template <class Fetch, class Done>
+__device__ __forceinline__ void any_loop(const DeviceScene& s, uint32_t i, uint32_t n, uint32_t stride,
+                                         bool watertight, uint32_t& err, TraceCounters& cnt, Fetch&& fetch,
+                                         Done&& done) {
+    uint32_t stack[kStackDepth];
+    AnyWalk w;
+    bool have = false;
+    for (;;) {
+        while (!have && i < n) {
+            fetch(i, w);
+            if (any_begin(s, w)) { have = true; }
+            else { done(i, false); i += stride; }
+        }
+        if (!__any_sync(0xffffffffu, have)) break;
+        bool fin = false;
+        if (have) {
+            while (!(w.ref & kLeafBit)) {
+                if (!any_inner(s, w, stack, err, cnt)) { fin = true; break; }
+            }
+        }
+        __syncwarp();
+        if (have && !fin) fin = !any_leaf(s, w, stack, watertight, cnt);
+        if (fin) { done(i, w.hit); i += stride; have = false; }
+    }
 }
 #endif  // __CUDACC__
 
