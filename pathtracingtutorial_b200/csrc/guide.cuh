@@ -621,16 +621,17 @@ struct GuideState {
     float4*      rec = nullptr;
     GuideSample* samples = nullptr;
     uint32_t     sample_cap = 0;
-    uint32_t*    counters = nullptr;  // [0] samples, [1] step
+    uint32_t*    counters = nullptr;  // [0] samples collected in the current pass (work buffer)
+    uint32_t*    step = nullptr;      // optimiser steps taken (with the parameters: survives work resizes)
     int          mode = 0;            // 0 off, PT_GUIDE_USE, PT_GUIDE_TRAIN
     float        lr = 1e-2f;
 };
 
-// After a pass's minibatches: advance the step counter (counters[1]) by the
-// steps taken and empty the sample buffer (counters[0]).
-__global__ void k_guide_step(uint32_t* counters, uint32_t cap, int nmb) {
-    counters[1] += steps_before(min(counters[0], cap), nmb, nmb);
-    counters[0] = 0u;
+// After a pass's minibatches: advance the step counter by the steps taken
+// and empty the sample buffer.
+__global__ void k_guide_step(uint32_t* sample_count, uint32_t* step, uint32_t cap, int nmb) {
+    *step += steps_before(min(*sample_count, cap), nmb, nmb);
+    *sample_count = 0u;
 }
 
 // Adam step for minibatch mb (skipped when it is empty); the step number is

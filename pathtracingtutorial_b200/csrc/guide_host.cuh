@@ -20,6 +20,7 @@ inline void guide_free(GuideState& g) {
     if (g.params) cudaFree(g.params);
     if (g.work) cudaFree(g.work);
     g.params = g.work = nullptr;
+    g.step = g.counters = nullptr;
     g.param_bytes = g.work_bytes = 0;
     g.npix = g.depth = 0;
 }
@@ -53,7 +54,8 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     const size_t off_w = off_v + al(ng * sizeof(float2));
     const size_t off_wm = off_w + al(kGWeights * sizeof(__nv_bfloat16));
     const size_t wf = al(kGWeights * sizeof(float));
-    const size_t total = off_wm + 4 * wf;
+    const size_t off_step = off_wm + 4 * wf;
+    const size_t total = off_step + 256;
     if (!guide_cuda_ok(cudaMalloc(&g.params, total), "parameter allocation")) return PT_ERR_NOMEM;
     g.param_bytes = total;
     char* base = static_cast<char*>(g.params);
@@ -67,6 +69,7 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     g.net.w_grad = reinterpret_cast<float*>(base + off_wm + wf);
     g.net.w_m = reinterpret_cast<float*>(base + off_wm + 2 * wf);
     g.net.w_v = reinterpret_cast<float*>(base + off_wm + 3 * wf);
+    g.step = reinterpret_cast<uint32_t*>(base + off_step);
     // host-side initial values
     std::mt19937 rng(seed);
     std::vector<float> gm(2 * ng);
@@ -92,6 +95,7 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
               guide_cuda_ok(cudaMemcpy(g.net.w, wb.data(), kGWeights * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice), "upload") &&
               guide_cuda_ok(cudaMemcpy(g.net.w_master, w.data(), kGWeights * sizeof(float), cudaMemcpyHostToDevice), "upload") &&
               guide_cuda_ok(cudaMemset(g.net.w_grad, 0, 3 * wf), "clear") &&
+              guide_cuda_ok(cudaMemset(g.step, 0, 256), "clear") &&
               guide_cuda_ok(cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kGTrainSmem), "smem") &&
               guide_cuda_ok(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kGInferSmem), "smem");
     return ok ? PT_OK : PT_ERR_CUDA;

@@ -955,10 +955,10 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int nframes, cudaStream_t 
                         k_guide_train<<<wf.sms, 128, kGTrainSmem, st>>>(gs->net, gs->samples, gs->counters,
                                                                          gs->sample_cap, mb, kGuideMinibatches);
                         k_guide_adam<<<wf.sms * 8, 256, 0, st>>>(gs->net, gs->counters, gs->sample_cap, mb,
-                                                                 kGuideMinibatches, gs->counters + 1, gs->lr, gs->lr,
+                                                                 kGuideMinibatches, gs->step, gs->lr, gs->lr,
                                                                  0.9f, 0.99f, 1e-10f);
                     }
-                    k_guide_step<<<1, 1, 0, st>>>(gs->counters, gs->sample_cap, kGuideMinibatches);
+                    k_guide_step<<<1, 1, 0, st>>>(gs->counters, gs->step, gs->sample_cap, kGuideMinibatches);
                 })) return rc;
         }
     }
@@ -1169,7 +1169,8 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     GuideState* gs = wf.guide;
     const bool guided = gs && gs->mode != 0;
     int64_t budget = rs.paths_in_flight > 0 ? rs.paths_in_flight : kDefaultPathsInFlight;
-    if (guided) budget = std::min<int64_t>(budget, kGuidedPathsInFlight);
+    if (guided) budget = std::min<int64_t>(budget, gs->mode == PT_GUIDE_TRAIN ? kTrainingPathsInFlight
+                                                                              : kGuidedPathsInFlight);
     const int64_t total = static_cast<int64_t>(prm->sample_per_frame) * nframes;
     const int lanes = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(total, budget / npix)));
     const int npath = npix * lanes;
@@ -1465,11 +1466,10 @@ void guide_set_lr(pt_guide* h, float lr) { h->g.lr = lr; }
 
 int guide_info(const pt_guide* h, uint32_t* steps, uint32_t* samples) {
     uint32_t c[2] = {0, 0};
-    if (h->g.counters) {
-        if (int rc = ensure_device(h->g.device)) return rc;
-        PT_CU(cudaDeviceSynchronize());
-        PT_CU(cudaMemcpy(c, h->g.counters, sizeof(c), cudaMemcpyDeviceToHost));
-    }
+    if (int rc = ensure_device(h->g.device)) return rc;
+    PT_CU(cudaDeviceSynchronize());
+    if (h->g.step) PT_CU(cudaMemcpy(&c[1], h->g.step, 4, cudaMemcpyDeviceToHost));
+    if (h->g.counters) PT_CU(cudaMemcpy(&c[0], h->g.counters, 4, cudaMemcpyDeviceToHost));
     if (steps) *steps = c[1];
     if (samples) *samples = c[0];
     return PT_OK;

@@ -41,6 +41,9 @@ constexpr int kStackDepth = 64;
 // guide attached the training records (64 B per path and bounce) cap it.
 constexpr int64_t kDefaultPathsInFlight = int64_t(1) << 25;
 constexpr int64_t kGuidedPathsInFlight = int64_t(1) << 22;
+// While a guide trains, passes stay small: every pass ends with optimiser
+// steps, so smaller passes mean more steps per sample.
+constexpr int64_t kTrainingPathsInFlight = int64_t(1) << 20;
 
 // Device error word bits.
 enum : uint32_t {
