@@ -280,8 +280,17 @@ typedef struct pt_batch_config {
     int32_t chunk_spp;      /* samples per work unit (0: default)       */
     int32_t autotune;       /* 1: time candidate shapes (cached per batch class) */
     float   tuned_ms;       /* out: calibration time of the chosen shape */
-    int32_t _pad[3];
+    int32_t mode;           /* PT_BATCH_AUTO / _PERSISTENT / _WAVEFRONT; out: the mode used */
+    int32_t paths_in_flight;/* wavefront mode: path slots shared by all items (0: 2^25) */
+    int32_t _pad;
 } pt_batch_config;
+/* Batch modes.  PERSISTENT: one persistent kernel traces whole paths of all
+ * items (dynamic work fetch).  WAVEFRONT: every item runs the wavefront
+ * integrator on its share of the path slots, the items as parallel branches
+ * of one CUDA graph.  AUTO: the autotuner times both on a calibration batch. */
+#define PT_BATCH_AUTO       0
+#define PT_BATCH_PERSISTENT 1
+#define PT_BATCH_WAVEFRONT  2
 
 int pt_render_batch(const pt_batch_item* items, uint32_t n, int32_t out_is_device, pt_batch_config* cfg,
                     pt_render_stats* stats);
@@ -299,8 +308,12 @@ typedef struct pt_guide pt_guide;
 int pt_guide_create(pt_scene* scene, uint32_t seed, pt_guide** out);   /* scene must be uploaded */
 int pt_guide_destroy(pt_guide* guide);
 int pt_guide_set_learning_rate(pt_guide* guide, float lr);
+/* probability of drawing the continuation from the network (default 0.5) */
+int pt_guide_set_alpha(pt_guide* guide, float alpha);
 /* steps taken and samples used by the last step (synchronises the device) */
 int pt_guide_info(const pt_guide* guide, uint32_t* steps, uint32_t* last_samples);
+/* mean training loss -w log q(dir | pos) over the last training pass (synchronises) */
+int pt_guide_loss(const pt_guide* guide, float* loss);
 int pt_integrator_set_guide(pt_integrator* integ, pt_guide* guide, int32_t mode);
 /* Evaluate the learned directional density q(dir | pos) for n queries
  * (pos[3], dir[3] floats each) -> out[n].  Diagnostic / checkpoint check. */

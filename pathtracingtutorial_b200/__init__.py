@@ -383,12 +383,14 @@ class Guide:
 
     OFF, USE, TRAIN = _ffi.GUIDE_OFF, _ffi.GUIDE_USE, _ffi.GUIDE_TRAIN
 
-    def __init__(self, scene: SceneManager, seed: int = 1, lr: float | None = None):
+    def __init__(self, scene: SceneManager, seed: int = 1, lr: float | None = None, alpha: float | None = None):
         h = C.c_void_p()
         check(lib().pt_guide_create(scene.handle, seed, C.byref(h)))
         self._h = h
         if lr is not None:
             check(lib().pt_guide_set_learning_rate(self._h, float(lr)))
+        if alpha is not None:
+            check(lib().pt_guide_set_alpha(self._h, float(alpha)))
 
     def attach(self, integrator: PathIntegrator, mode: int) -> None:
         check(lib().pt_integrator_set_guide(integrator._h, self._h if mode else None, mode))
@@ -397,6 +399,12 @@ class Guide:
         steps, samples = C.c_uint32(), C.c_uint32()
         check(lib().pt_guide_info(self._h, C.byref(steps), C.byref(samples)))
         return {"steps": steps.value, "last_samples": samples.value}
+
+    def loss(self) -> float:
+        """Mean training loss -w log q(dir | pos) of the last training pass."""
+        v = C.c_float()
+        check(lib().pt_guide_loss(self._h, C.byref(v)))
+        return v.value
 
     def pdf(self, pos: np.ndarray, dirs: np.ndarray) -> np.ndarray:
         q = np.ascontiguousarray(np.concatenate([np.asarray(pos, np.float32).reshape(-1, 3),
@@ -468,8 +476,14 @@ def render_guided(scene: SceneManager, train_spp: int, spp: int, guide: Guide | 
     return img, g, r.integrator.stats()
 
 
-def render_batch(items, block_size: int = 0, blocks_per_sm: int = 0, chunk_spp: int = 0, autotune: bool = True):
-    """Render [(scene, spp[, first_frame])...] in one persistent launch.
+BATCH_AUTO, BATCH_PERSISTENT, BATCH_WAVEFRONT = _ffi.BATCH_AUTO, _ffi.BATCH_PERSISTENT, _ffi.BATCH_WAVEFRONT
+
+
+def render_batch(items, block_size: int = 0, blocks_per_sm: int = 0, chunk_spp: int = 0, autotune: bool = True,
+                 mode: int = BATCH_AUTO, paths_in_flight: int = 0):
+    """Render [(scene, spp[, first_frame])...] in one graph launch: one
+    persistent kernel over all items, or every item's wavefront as a parallel
+    graph branch (mode; AUTO lets the autotuner time both).
     Returns (list of (H, W, 4) images, stats dict, config dict)."""
     n = len(items)
     arr = (_ffi.BatchItem * n)()
@@ -485,11 +499,13 @@ def render_batch(items, block_size: int = 0, blocks_per_sm: int = 0, chunk_spp: 
         arr[k].max_depth = -1
         arr[k].first_frame = int(first)
         arr[k].out_rgba = img.ctypes.data
-    cfg = _ffi.BatchConfig(block_size, blocks_per_sm, chunk_spp, 1 if autotune else 0, 0.0)
+    cfg = _ffi.BatchConfig(block_size, blocks_per_sm, chunk_spp, 1 if autotune else 0, 0.0, int(mode),
+                           int(paths_in_flight), 0)
     st = _ffi.RenderStats()
     check(lib().pt_render_batch(arr, n, 0, C.byref(cfg), C.byref(st)))
     return outs, st.as_dict(), {"block_size": cfg.block_size, "blocks_per_sm": cfg.blocks_per_sm,
-                                "chunk_spp": cfg.chunk_spp, "tuned_ms": cfg.tuned_ms}
+                                "chunk_spp": cfg.chunk_spp, "tuned_ms": cfg.tuned_ms, "mode": cfg.mode,
+                                "paths_in_flight": cfg.paths_in_flight}
 
 
 # ---- diagnostics over the same kernels ----

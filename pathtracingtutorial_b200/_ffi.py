@@ -100,7 +100,11 @@ class BatchItem(C.Structure):
 
 class BatchConfig(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("chunk_spp", C.c_int32),
-                ("autotune", C.c_int32), ("tuned_ms", C.c_float), ("_pad", C.c_int32 * 3)]
+                ("autotune", C.c_int32), ("tuned_ms", C.c_float), ("mode", C.c_int32),
+                ("paths_in_flight", C.c_int32), ("_pad", C.c_int32)]
+
+
+BATCH_AUTO, BATCH_PERSISTENT, BATCH_WAVEFRONT = 0, 1, 2
 
 
 assert C.sizeof(SceneParams) == 88 and C.sizeof(CameraFrame) == 64 and C.sizeof(BatchItem) == 32
@@ -150,7 +154,9 @@ _SIGS = [
     ("pt_guide_create", C.c_int, [_P, C.c_uint32, C.POINTER(_P)]),
     ("pt_guide_destroy", C.c_int, [_P]),
     ("pt_guide_set_learning_rate", C.c_int, [_P, C.c_float]),
+    ("pt_guide_set_alpha", C.c_int, [_P, C.c_float]),
     ("pt_guide_info", C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    ("pt_guide_loss", C.c_int, [_P, C.POINTER(C.c_float)]),
     ("pt_integrator_set_guide", C.c_int, [_P, _P, C.c_int32]),
     ("pt_guide_eval", C.c_int, [_P, _P, C.c_uint32, _P]),
     ("pt_guide_get_params", C.c_int, [_P, _P, _P, _P]),

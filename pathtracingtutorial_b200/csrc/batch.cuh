@@ -199,7 +199,186 @@ BatchPlan make_plan(const pt_batch_item* in, uint32_t n, uint32_t chunk_spp, int
     return plan;
 }
 
-struct BatchTune { int block, blocks_per_sm, chunk_spp; double ms; };
+// ---- wavefront mode: every item runs the wavefront integrator as one branch
+//      of a single CUDA graph (branches run concurrently) ----
+struct BatchSlot {
+    const pt_scene* scene = nullptr;
+    int             dup = 0;          // k-th item of the batch with this scene
+    pt_integrator*  integ = nullptr;
+    pt_film*        film = nullptr;
+};
+std::mutex g_slot_mu;
+// one integrator + film per scene, reused across batches (heap cells: the
+// addresses handed out stay valid while the list grows)
+std::vector<std::unique_ptr<BatchSlot>> g_slots;
+std::vector<std::pair<int, std::vector<cudaStream_t>>> g_side_streams;   // per device
+constexpr int kBatchBranches = 16;
+
+void slot_release(BatchSlot& sl) {
+    if (sl.integ) { integrator_free(sl.integ); delete sl.integ; }
+    if (sl.film) { film_free(sl.film); delete sl.film; }
+    sl = BatchSlot{};
+}
+
+// Integrator and film for the dup-th batch item rendering scene s (its camera
+// size, its device); caller holds g_slot_mu.
+int batch_slot(const pt_scene* s, int dup, BatchSlot*& out) {
+    const int w = s->host.camera.width, h = s->host.camera.height, dev = s->dev.device;
+    out = nullptr;
+    for (auto& cell : g_slots) {
+        BatchSlot& sl = *cell;
+        if (sl.scene != s || sl.dup != dup) continue;
+        if (sl.film->width == w && sl.film->height == h && sl.film->device == dev) { out = &sl; return PT_OK; }
+        slot_release(sl);
+        sl.scene = s;
+        out = &sl;
+        break;
+    }
+    if (!out) {
+        g_slots.push_back(std::make_unique<BatchSlot>());
+        out = g_slots.back().get();
+        out->scene = s;
+        out->dup = dup;
+    }
+    out->integ = new pt_integrator();
+    out->film = new pt_film();
+    out->film->width = w; out->film->height = h; out->film->device = dev;
+    return film_alloc(out->film);
+}
+
+int side_streams(int device, std::vector<cudaStream_t>*& out) {
+    for (auto& kv : g_side_streams) if (kv.first == device) { out = &kv.second; return PT_OK; }
+    g_side_streams.emplace_back(device, std::vector<cudaStream_t>(kBatchBranches, nullptr));
+    out = &g_side_streams.back().second;
+    for (cudaStream_t& x : *out) PT_CU(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    return PT_OK;
+}
+
+__global__ void k_batch_film_mean(const float4* sum, const float4* comp, float4* out, int n) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const float4 s = sum[p], c = comp[p];
+        out[p] = s.w > 0.0f ? make_float4((s.x + c.x) / s.w, (s.y + c.y) / s.w, (s.z + c.z) / s.w, 1.0f)
+                            : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// Renders the batch in wavefront mode: the path slots (budget) are shared
+// among the items in proportion to their work (pixels x spp), every item gets
+// at least one sample per pixel in flight.  Returns the graph's device time.
+// write_out = false (calibration) skips the output.
+int batch_wavefront(const pt_batch_item* in, uint32_t n, int out_is_device, int64_t budget, bool write_out,
+                    cudaStream_t st, float* ms_out, pt_render_stats* stats) {
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    const int device = in[0].scene->dev.device;
+    std::vector<cudaStream_t>* side = nullptr;
+    if (int rc = side_streams(device, side)) return rc;
+    double work_total = 0.0;
+    for (uint32_t k = 0; k < n; ++k)
+        work_total += static_cast<double>(in[k].scene->host.camera.width) * in[k].scene->host.camera.height * in[k].spp;
+    std::vector<BatchSlot*> slots(n, nullptr);
+    std::vector<WaveParams> P(n);
+    std::vector<int64_t> total(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        pt_scene* s = in[k].scene;
+        int dup = 0;   // items sharing a scene need their own wavefront and film
+        for (uint32_t j = 0; j < k; ++j) dup += in[j].scene == s ? 1 : 0;
+        if (int rc = batch_slot(s, dup, slots[k])) return rc;
+        pt_scene_params prm;
+        if (int rc = pt_scene_build_params(s, &prm)) return rc;
+        if (in[k].max_depth >= 0) prm.max_depth = in[k].max_depth;
+        const int64_t npix = static_cast<int64_t>(prm.width) * prm.height;
+        total[k] = in[k].spp;
+        const double share = static_cast<double>(budget) * (static_cast<double>(npix) * in[k].spp / work_total);
+        const int64_t item_budget = std::max<int64_t>(npix, static_cast<int64_t>(share));
+        int lanes = 1;
+        if (int rc = prepare_wave(slots[k]->integ, slots[k]->film, s, &prm, total[k], item_budget, P[k], lanes)) return rc;
+        if (int rc = film_clear(slots[k]->film)) return rc;
+        if (int rc = integrator_reset_stats(slots[k]->integ)) return rc;
+    }
+    PT_CU(cudaDeviceSynchronize());
+    cudaEvent_t fork = nullptr, e0 = nullptr, e1 = nullptr;
+    std::vector<cudaEvent_t> join(kBatchBranches, nullptr);
+    struct EvGuard { std::vector<cudaEvent_t*> ev; ~EvGuard() { for (auto* e : ev) if (*e) cudaEventDestroy(*e); } } eg;
+    eg.ev = {&fork, &e0, &e1};
+    PT_CU(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    PT_CU(cudaEventCreate(&e0));
+    PT_CU(cudaEventCreate(&e1));
+    for (cudaEvent_t& e : join) { PT_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)); eg.ev.push_back(&e); }
+    const int branches = static_cast<int>(std::min<uint32_t>(n, kBatchBranches));
+    cudaGraph_t graph = nullptr;
+    PT_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = PT_OK;
+    cudaError_t ce = cudaEventRecord(fork, st);
+    for (int j = 0; j < branches && ce == cudaSuccess; ++j) ce = cudaStreamWaitEvent((*side)[j], fork, 0);
+    for (uint32_t k = 0; k < n && ce == cudaSuccess && rc == PT_OK; ++k) {
+        cudaStream_t bs = (*side)[k % branches];
+        Wavefront& wf = *slots[k]->integ->wf;
+        k_begin<<<1, 1, 0, bs>>>(P[k].pass, in[k].first_frame);
+        rc = enqueue_batch(wf, P[k], total[k], bs, nullptr, nullptr);
+        if (rc == PT_OK && write_out) {
+            const int np = P[k].npix;
+            float4* out = out_is_device ? reinterpret_cast<float4*>(in[k].out_rgba)
+                                        : static_cast<float4*>(slots[k]->film->resolve);
+            k_batch_film_mean<<<std::min((np + 255) / 256, wf.sms * 8), 256, 0, bs>>>(
+                P[k].f_sum, P[k].f_comp, out, np);
+        }
+    }
+    for (int j = 0; j < branches && ce == cudaSuccess; ++j) {
+        ce = cudaEventRecord(join[j], (*side)[j]);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, join[j], 0);
+    }
+    const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+    if (rc != PT_OK || ce != cudaSuccess || ec != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (rc == PT_OK) {
+            set_error(std::string("batch graph capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ec));
+            rc = PT_ERR_CUDA;
+        }
+        return rc;
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) { set_error(std::string("batch graph instantiate: ") + cudaGetErrorString(ei)); return PT_ERR_CUDA; }
+    PT_CU(cudaEventRecord(e0, st));
+    const cudaError_t el = cudaGraphLaunch(exec, st);
+    PT_CU(cudaEventRecord(e1, st));
+    const cudaError_t es = cudaStreamSynchronize(st);
+    cudaGraphExecDestroy(exec);
+    if (el != cudaSuccess || es != cudaSuccess) {
+        set_error(std::string("batch launch: ") + cudaGetErrorString(el != cudaSuccess ? el : es));
+        return PT_ERR_CUDA;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms_out) *ms_out = ms;
+    pt_render_stats sum;
+    std::memset(&sum, 0, sizeof(sum));
+    for (uint32_t k = 0; k < n; ++k) {
+        if (int rc2 = integrator_check(slots[k]->integ, false)) return rc2;
+        pt_render_stats s1;
+        if (int rc2 = integrator_stats(slots[k]->integ, &s1)) return rc2;
+        sum.camera_rays += s1.camera_rays; sum.extension_rays += s1.extension_rays;
+        sum.shadow_rays += s1.shadow_rays; sum.paths += s1.paths;
+        if (write_out && !out_is_device)
+            PT_CU(cudaMemcpy(in[k].out_rgba, slots[k]->film->resolve,
+                             static_cast<size_t>(P[k].npix) * sizeof(float4), cudaMemcpyDeviceToHost));
+    }
+    if (stats) {
+        *stats = sum;
+        stats->total_ms = ms;
+        uint64_t launches = 0;
+        for (uint32_t k = 0; k < n; ++k) {
+            const int lanes = std::max(1, P[k].npath / std::max(P[k].npix, 1));
+            const uint64_t passes = static_cast<uint64_t>((total[k] + lanes - 1) / lanes);
+            launches += 1 + passes * (2 + 3 * static_cast<uint64_t>(P[k].max_depth)) + (write_out ? 1 : 0);
+        }
+        stats->kernel_launches = launches;
+    }
+    return PT_OK;
+}
+
+struct BatchTune { int block, blocks_per_sm, chunk_spp; double ms; int mode; };
 std::mutex g_tune_mu;
 std::vector<std::pair<std::string, BatchTune>> g_tune_cache;
 
@@ -244,12 +423,30 @@ int render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batc
     unsigned long long* d_stats = d_misc + 8;
     uint32_t* d_err = reinterpret_cast<uint32_t*>(d_misc + 32);
 
-    // ---- pick the launch shape (autotuner) ----
+    const int req_mode = cfg ? cfg->mode : PT_BATCH_AUTO;
+    if (req_mode != PT_BATCH_AUTO && req_mode != PT_BATCH_PERSISTENT && req_mode != PT_BATCH_WAVEFRONT) {
+        set_error("unknown batch mode");
+        return PT_ERR_INVALID;
+    }
+    const int64_t budget = cfg && cfg->paths_in_flight > 0 ? cfg->paths_in_flight : kDefaultPathsInFlight;
+    auto run_wavefront = [&](float tuned_ms) -> int {
+        float ms = 0.0f;
+        if (int rc = batch_wavefront(in, n, out_is_device, budget, true, st, &ms, stats)) return rc;
+        if (cfg) {
+            cfg->mode = PT_BATCH_WAVEFRONT;
+            cfg->paths_in_flight = static_cast<int32_t>(budget);
+            cfg->tuned_ms = tuned_ms;
+        }
+        return PT_OK;
+    };
+    if (req_mode == PT_BATCH_WAVEFRONT) return run_wavefront(0.0f);
+
+    // ---- pick the mode and launch shape (autotuner) ----
     BatchTune tune{cfg && cfg->block_size ? cfg->block_size : 128,
                    cfg && cfg->blocks_per_sm ? cfg->blocks_per_sm : 0,
-                   cfg && cfg->chunk_spp ? cfg->chunk_spp : 8, 0.0};
+                   cfg && cfg->chunk_spp ? cfg->chunk_spp : 8, 0.0, PT_BATCH_PERSISTENT};
     const bool autotune = !cfg || cfg->autotune;
-    const std::string key = tune_key(device, in, n);
+    const std::string key = tune_key(device, in, n) + ":" + std::to_string(req_mode);
     bool cached = false;
     if (autotune) {
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -293,6 +490,15 @@ int render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batc
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
+        // the wavefront mode on the same calibration batch
+        if (req_mode == PT_BATCH_AUTO) {
+            std::vector<pt_batch_item> capped(in, in + n);
+            for (pt_batch_item& it : capped) it.spp = std::min(it.spp, 8);
+            float wms = 0.0f;
+            for (int rep = 0; rep < 2; ++rep)
+                if (int rc = batch_wavefront(capped.data(), n, 0, budget, false, st, &wms, nullptr)) return rc;
+            if (wms < best) { best = wms; tune.mode = PT_BATCH_WAVEFRONT; tune.ms = wms; }
+        }
         // chunk size: larger chunks amortise the per-unit setup; bounded by the partial buffer
         uint64_t pix = 0, spp_max = 0;
         for (uint32_t k = 0; k < n; ++k) {
@@ -303,6 +509,7 @@ int render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batc
         std::lock_guard<std::mutex> lk(g_tune_mu);
         g_tune_cache.emplace_back(key, tune);
     }
+    if (tune.mode == PT_BATCH_WAVEFRONT && req_mode == PT_BATCH_AUTO) return run_wavefront(static_cast<float>(tune.ms));
     if (tune.blocks_per_sm <= 0) tune.blocks_per_sm = max_blocks_per_sm(tune.block);
 
     // ---- the batch itself: one persistent launch + resolve, captured in a graph ----
@@ -379,8 +586,19 @@ int render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batc
         cfg->blocks_per_sm = tune.blocks_per_sm;
         cfg->chunk_spp = tune.chunk_spp;
         cfg->tuned_ms = static_cast<float>(tune.ms);
+        cfg->mode = PT_BATCH_PERSISTENT;
     }
     return PT_OK;
+}
+
+// Drops the cached wavefront slot of a scene that is being destroyed.
+void batch_forget_scene(const pt_scene* s) {
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    for (size_t i = 0; i < g_slots.size();) {
+        if (g_slots[i]->scene != s) { ++i; continue; }
+        slot_release(*g_slots[i]);
+        g_slots.erase(g_slots.begin() + static_cast<long>(i));
+    }
 }
 
 }  // namespace ptb

@@ -131,6 +131,7 @@ int pt_scene_create(const pt_vertex* vertices, uint32_t num_vertices, const pt_f
 int pt_scene_destroy(pt_scene* scene) {
     if (!scene) return PT_OK;
     drop_cache(scene);
+    batch_forget_scene(scene);
     free_scene_device(scene);
     unpin_host_arrays(scene);
     delete scene;
@@ -436,9 +437,18 @@ int pt_guide_set_learning_rate(pt_guide* guide, float lr) {
     guide_set_lr(guide, lr);
     return PT_OK;
 }
+int pt_guide_set_alpha(pt_guide* guide, float alpha) {
+    PT_REQUIRE(guide && alpha > 0.0f && alpha < 1.0f, "alpha must be in (0, 1)");
+    guide_set_alpha(guide, alpha);
+    return PT_OK;
+}
 int pt_guide_info(const pt_guide* guide, uint32_t* steps, uint32_t* last_samples) {
     PT_REQUIRE(guide, "null guide");
     return guide_info(guide, steps, last_samples);
+}
+int pt_guide_loss(const pt_guide* guide, float* loss) {
+    PT_REQUIRE(guide && loss, "null argument");
+    return guide_loss(guide, loss);
 }
 int pt_integrator_set_guide(pt_integrator* integ, pt_guide* guide, int32_t mode) {
     PT_REQUIRE(integ, "null integrator");

@@ -28,10 +28,13 @@ int  sampler_stream(int type, int w, int h, uint32_t frame, int spf, int sif, ui
                     int device, float* out_host);
 int  bsdf_eval(pt_scene* s, const float* in, uint32_t n, float* out_host);
 int  render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batch_config* cfg, pt_render_stats* stats);
+void batch_forget_scene(const pt_scene* s);
 int  guide_create(pt_scene* s, uint32_t seed, pt_guide** out);
 void guide_destroy(pt_guide* g);
 void guide_set_lr(pt_guide* g, float lr);
+void guide_set_alpha(pt_guide* g, float alpha);
 int  guide_info(const pt_guide* g, uint32_t* steps, uint32_t* samples);
+int  guide_loss(const pt_guide* g, float* loss);
 int  integrator_set_guide(pt_integrator* integ, pt_guide* g, int mode);
 int  guide_eval(pt_guide* g, const float* qd, uint32_t n, float* out);
 int  guide_get_params(const pt_guide* g, float* weights, float* grid, float* meta);

@@ -38,8 +38,14 @@ constexpr int kGLobes = 8;
 constexpr int kGOut = 40;                 // used outputs
 constexpr int kGOutPad = 48;              // 6 n-tiles of 8
 constexpr int kGMix = 40;                 // floats per mixture: 8 x (mu xyz, kappa) + 8 weights
-constexpr float kGuideAlpha = 0.5f;
-constexpr int kGuideMinibatches = 4;       // optimiser steps per wavefront pass
+constexpr float kGuideAlpha = 0.5f;        // default probability of sampling the mixture
+constexpr int kGuideMinibatchPaths = 1 << 17;
+
+// Optimiser steps per training pass of `paths` paths: one per 2^17 paths
+// (a few hundred thousand samples), 1 .. 32.
+inline int guide_minibatches(int64_t paths) {
+    return static_cast<int>(std::min<int64_t>(32, std::max<int64_t>(1, paths / kGuideMinibatchPaths)));
+}
 
 // layer l: out x in, row-major, rows padded to in + 8 bf16 in shared memory
 __host__ __device__ constexpr int g_in(int l) { return l == 0 ? kGIn : kGHid; }
@@ -70,6 +76,7 @@ struct GuideNet {
     float           inv_ext[3];
     float           scale[kGLevels];
     uint32_t        dense_limit; // levels with (res+1)^3 <= table use direct indexing
+    float*          loss;        // [0] sum of w (-log q), [1] samples, [2] mean of the last pass
 };
 
 // ---------------------------------------------------------------------------
@@ -304,7 +311,7 @@ namespace ptb {
 struct GuideSample { float4 pos_w; float4 dir; };
 
 // d(-w log q(dir)) / d(raw outputs) for one row (raw: 48 floats, out: 48 floats).
-__device__ void mixture_grad(const float* raw, f3 dir, float w, float* d) {
+__device__ float mixture_grad(const float* raw, f3 dir, float w, float* d) {
     float mix[kGMix];
     raw_to_mixture(raw, mix);
     float v[kGLobes];
@@ -334,6 +341,7 @@ __device__ void mixture_grad(const float* raw, f3 dir, float w, float* d) {
         d[5 * k] = dm.x; d[5 * k + 1] = dm.y; d[5 * k + 2] = dm.z;
     }
     for (int j = kGOut; j < kGOutPad; ++j) d[j] = 0.0f;
+    return q;
 }
 
 // Per-warp shared scratch for the backward pass (bf16):
@@ -527,12 +535,14 @@ __global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSa
         }
         __syncwarp();
         // loss gradient per row (lanes 0..15), scaled by 1/n
+        float row_loss = 0.0f;
         if (lane < 16) {
             const uint32_t r = tile * 16 + lane;
             float d[kGOutPad];
             if (r < n) {
                 const GuideSample s = samples[r];
-                mixture_grad(OUT + lane * kGOutPad, mk(s.dir.x, s.dir.y, s.dir.z), s.pos_w.w * inv_n, d);
+                const float q = mixture_grad(OUT + lane * kGOutPad, mk(s.dir.x, s.dir.y, s.dir.z), s.pos_w.w * inv_n, d);
+                row_loss = -s.pos_w.w * logf(q);
             } else {
                 for (int j = 0; j < kGOutPad; ++j) d[j] = 0.0f;
             }
@@ -541,6 +551,11 @@ __global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSa
                 DY[lane * (kGHid + 8) + j] = b;
                 DYT[j * 24 + lane] = b;
             }
+        }
+        for (int o = 16; o > 0; o >>= 1) row_loss += __shfl_xor_sync(0xffffffffu, row_loss, o);
+        if (lane == 0 && net.loss) {
+            atomicAdd(net.loss, row_loss);
+            atomicAdd(net.loss + 1, static_cast<float>(min(16u, n - tile * 16)));
         }
         __syncwarp();
         // layer 3 (48 x 64)
@@ -625,13 +640,17 @@ struct GuideState {
     uint32_t*    step = nullptr;      // optimiser steps taken (with the parameters: survives work resizes)
     int          mode = 0;            // 0 off, PT_GUIDE_USE, PT_GUIDE_TRAIN
     float        lr = 1e-2f;
+    float        alpha = kGuideAlpha;
 };
 
 // After a pass's minibatches: advance the step counter by the steps taken
 // and empty the sample buffer.
-__global__ void k_guide_step(uint32_t* sample_count, uint32_t* step, uint32_t cap, int nmb) {
+__global__ void k_guide_step(uint32_t* sample_count, uint32_t* step, float* loss, uint32_t cap, int nmb) {
     *step += steps_before(min(*sample_count, cap), nmb, nmb);
     *sample_count = 0u;
+    if (loss[1] > 0.0f) loss[2] = loss[0] / loss[1];
+    loss[0] = 0.0f;
+    loss[1] = 0.0f;
 }
 
 // Adam step for minibatch mb (skipped when it is empty); the step number is

@@ -70,6 +70,7 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     g.net.w_m = reinterpret_cast<float*>(base + off_wm + 2 * wf);
     g.net.w_v = reinterpret_cast<float*>(base + off_wm + 3 * wf);
     g.step = reinterpret_cast<uint32_t*>(base + off_step);
+    g.net.loss = reinterpret_cast<float*>(base + off_step + 16);
     // host-side initial values
     std::mt19937 rng(seed);
     std::vector<float> gm(2 * ng);

@@ -22,6 +22,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -80,6 +81,7 @@ struct WaveParams {
     float4*  f_new;
     // learned guiding (null when off)
     const float* gmix;   // queue-ordered mixtures, kGMix floats per entry
+    float    galpha;     // probability of sampling the mixture (one-sample MIS)
     float4*  grec;       // training records [depth][npath][4]
 };
 
@@ -172,10 +174,10 @@ __device__ __forceinline__ uint32_t sample_alias(const pt_alias_entry* t, uint32
 // At a guided vertex the directional strategy is the guide/BSDF mixture, so
 // its pdf (alpha q + (1 - alpha) p_bsdf) enters the power heuristic.
 __device__ __forceinline__ f3 direct_term(const MatEval& me, f3 wo, f3 wi, f3 n, f3 radiance, float light_pdf,
-                                          const float* gmix) {
+                                          const float* gmix, float galpha) {
     const BsdfEval b = PT_BSDF_EVAL(me, wo, wi, n, true);
     if (b.pdf <= 0.0f) return mk(0.0f);
-    const float dir_pdf = gmix ? kGuideAlpha * mix_pdf(gmix, wi) + (1.0f - kGuideAlpha) * b.pdf : b.pdf;
+    const float dir_pdf = gmix ? galpha * mix_pdf(gmix, wi) + (1.0f - galpha) * b.pdf : b.pdf;
     const float mis = power_heuristic(light_pdf, dir_pdf);
     return radiance * b.f * (mis / (light_pdf + 1e-7f));
 }
@@ -186,6 +188,7 @@ __device__ __forceinline__ f3 direct_term(const MatEval& me, f3 wo, f3 wi, f3 n,
 struct GuideVertex {
     const float* mix;
     float4* rec;
+    float alpha;
 };
 
 __device__ __forceinline__ void emit_shadow(const WaveParams& P, bool want, uint32_t path, uint32_t slot,
@@ -414,7 +417,7 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
             }
             if (ok) {
                 const f3 le = material_emission(s.materials[lf.material_id]);
-                contrib = T * direct_term(me, wo, wi, N, le, pdf, gmix);
+                contrib = T * direct_term(me, wo, wi, N, le, pdf, gmix, gv.alpha);
                 ok = !is_zero(contrib);
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
@@ -437,7 +440,7 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
             f3 contrib = mk(0.0f);
             if (ok) { pdf = env_pdf(s, wi); ok = pdf > 0.0f; }
             if (ok) {
-                contrib = T * direct_term(me, wo, wi, N, env_radiance(s, wi), pdf, gmix);
+                contrib = T * direct_term(me, wo, wi, N, env_radiance(s, wi), pdf, gmix, gv.alpha);
                 ok = !is_zero(contrib);
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
@@ -486,11 +489,11 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
     if (gmix) {
         // one-sample MIS between the learned mixture and the BSDF
         const float sel = rng_next(rng);
-        if (sel < kGuideAlpha) {
+        if (sel < gv.alpha) {
             const float u0 = rng_next(rng), u1 = rng_next(rng), u2 = rng_next(rng);
             bs.wi = mix_sample(gmix, u0, u1, u2);
             const BsdfEval ev = PT_BSDF_EVAL(me, wo, bs.wi, N, entering);
-            const float p = kGuideAlpha * mix_pdf(gmix, bs.wi) + (1.0f - kGuideAlpha) * ev.pdf;
+            const float p = gv.alpha * mix_pdf(gmix, bs.wi) + (1.0f - gv.alpha) * ev.pdf;
             bs.valid = p > 0.0f && !is_zero(ev.f);
             bs.pdf = p;
             bs.weight = bs.valid ? ev.f / p : mk(0.0f);
@@ -498,7 +501,7 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
         } else {
             bs = PT_BSDF_SAMPLE(me, wo, N, rng, arg_rtl, entering);
             if (bs.valid) {
-                const float p = kGuideAlpha * mix_pdf(gmix, bs.wi) + (1.0f - kGuideAlpha) * bs.pdf;
+                const float p = gv.alpha * mix_pdf(gmix, bs.wi) + (1.0f - gv.alpha) * bs.pdf;
                 bs.weight = bs.weight * ((bs.pdf + 1e-7f) / p);
                 bs.pdf = p;
             }
@@ -565,7 +568,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(WaveParams P, int q, int depth
         rng.s = P.rng[p];
         f3 no = mk(0.0f), nd = mk(0.0f);
         QueueSink sink{P, p};
-        GuideVertex gv{P.gmix ? P.gmix + static_cast<size_t>(i) * kGMix : nullptr, nullptr};
+        GuideVertex gv{P.gmix ? P.gmix + static_cast<size_t>(i) * kGMix : nullptr, nullptr, P.galpha};
         if (P.grec) {
             gv.rec = P.grec + (static_cast<size_t>(depth) * P.npath + p) * 4;
             gv.rec[1].w = 0.0f;
@@ -909,8 +912,10 @@ int wavefront_prepare(Wavefront& wf, int device, int npath, int n_slots) {
 // stage events are recorded (ev holds pairs per launch: kind, start, stop).
 struct StageEvent { int kind; cudaEvent_t a, b; };
 
-int enqueue_batch(Wavefront& wf, const WaveParams& P, int nframes, cudaStream_t st, std::vector<StageEvent>* ev,
-                  GuideState* gs = nullptr) {
+// Enqueues `total` samples per pixel, counted from the first sample of frame
+// P.pass->frame, as passes of the wavefront's lanes.
+int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cudaStream_t st,
+                  std::vector<StageEvent>* ev, GuideState* gs = nullptr) {
     const bool infer = gs && gs->mode != 0 && P.gmix;
     const bool train = infer && P.grec;
     auto timed = [&](int kind, auto&& launch) -> int {
@@ -928,7 +933,7 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int nframes, cudaStream_t 
         return PT_OK;
     };
     const int lanes = std::max(1, P.npath / std::max(P.npix, 1));
-    const int total = P.spf * nframes;
+    const int total = static_cast<int>(total_samples);
     for (int s0 = 0; s0 < total; s0 += lanes) {
         const int count = std::min(lanes, total - s0);
         if (int rc = timed(3, [&] { k_raygen<<<wf.grid_raygen, 256, 0, st>>>(P, s0, count); })) return rc;
@@ -950,15 +955,15 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int nframes, cudaStream_t 
             if (int rc = timed(4, [&] {
                     k_guide_collect<<<wf.grid_finalize, 256, 0, st>>>(P, P.npix * count, gs->net, gs->samples,
                                                                       gs->counters, gs->sample_cap);
-                    // kGuideMinibatches optimiser steps over this pass's samples
-                    for (int mb = 0; mb < kGuideMinibatches; ++mb) {
+                    // optimiser steps over this pass's samples in minibatches
+                    const int nmb = guide_minibatches(P.npix * count);
+                    for (int mb = 0; mb < nmb; ++mb) {
                         k_guide_train<<<wf.sms, 128, kGTrainSmem, st>>>(gs->net, gs->samples, gs->counters,
-                                                                         gs->sample_cap, mb, kGuideMinibatches);
-                        k_guide_adam<<<wf.sms * 8, 256, 0, st>>>(gs->net, gs->counters, gs->sample_cap, mb,
-                                                                 kGuideMinibatches, gs->step, gs->lr, gs->lr,
-                                                                 0.9f, 0.99f, 1e-10f);
+                                                                         gs->sample_cap, mb, nmb);
+                        k_guide_adam<<<wf.sms * 8, 256, 0, st>>>(gs->net, gs->counters, gs->sample_cap, mb, nmb,
+                                                                 gs->step, gs->lr, gs->lr, 0.9f, 0.99f, 1e-10f);
                     }
-                    k_guide_step<<<1, 1, 0, st>>>(gs->counters, gs->step, gs->sample_cap, kGuideMinibatches);
+                    k_guide_step<<<1, 1, 0, st>>>(gs->counters, gs->step, gs->net.loss, gs->sample_cap, nmb);
                 })) return rc;
         }
     }
@@ -1150,15 +1155,18 @@ void integrator_free(pt_integrator* integ) {
 }
 
 // Integrator::launch (Part_2/src/integrators/path.cu:244-255).
-int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scene_params* prm, int nframes,
-                      void* stream) {
+// Sizes the integrator's wavefront for `total` samples per pixel and fills the
+// launch parameters (P, built byte-wise with zeroed padding because its bytes
+// key the graph cache).  budget > 0 overrides the scene's paths-in-flight.
+int prepare_wave(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scene_params* prm, int64_t total,
+                 int64_t budget_override, WaveParams& P, int& lanes_out) {
     if (!s->dev.uploaded) { set_error("scene not uploaded: call pt_scene_upload first"); return PT_ERR_STATE; }
     if (film->width != prm->width || film->height != prm->height) { set_error("film size does not match params"); return PT_ERR_INVALID; }
     if (prm->width <= 0 || prm->height <= 0 || prm->sample_per_frame <= 0 || prm->max_depth < 0) {
         set_error("invalid scene params"); return PT_ERR_INVALID;
     }
     if (film->device != s->dev.device) { set_error("film and scene live on different devices"); return PT_ERR_INVALID; }
-    if (nframes < 1) { set_error("frame count must be positive"); return PT_ERR_INVALID; }
+    if (total < 1) { set_error("sample count must be positive"); return PT_ERR_INVALID; }
     if (!integ->wf) integ->wf = new Wavefront();
     Wavefront& wf = *integ->wf;
     const int npix = prm->width * prm->height;
@@ -1168,15 +1176,13 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     // budget holds (a guide's per-path records cap it lower)
     GuideState* gs = wf.guide;
     const bool guided = gs && gs->mode != 0;
-    int64_t budget = rs.paths_in_flight > 0 ? rs.paths_in_flight : kDefaultPathsInFlight;
+    int64_t budget = budget_override > 0 ? budget_override
+                   : (rs.paths_in_flight > 0 ? rs.paths_in_flight : kDefaultPathsInFlight);
     if (guided) budget = std::min<int64_t>(budget, gs->mode == PT_GUIDE_TRAIN ? kTrainingPathsInFlight
                                                                               : kGuidedPathsInFlight);
-    const int64_t total = static_cast<int64_t>(prm->sample_per_frame) * nframes;
     const int lanes = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(total, budget / npix)));
     const int npath = npix * lanes;
     if (int rc = wavefront_prepare(wf, s->dev.device, npath, n_slots)) return rc;
-    // Built byte-wise (padding zeroed) because the bytes key the graph cache.
-    WaveParams P;
     std::memset(&P, 0, sizeof(P));
     std::memcpy(&P, &wf.base, sizeof(P));
     const DeviceScene view = device_view(s);
@@ -1198,8 +1204,23 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
         if (gs->device != s->dev.device) { set_error("guide and scene live on different devices"); return PT_ERR_INVALID; }
         if (int rc = guide_prepare_work(*gs, npath, prm->max_depth)) return rc;
         P.gmix = gs->mix;
+        P.galpha = gs->alpha;
         P.grec = gs->mode == PT_GUIDE_TRAIN ? gs->rec : nullptr;
     }
+    lanes_out = lanes;
+    return PT_OK;
+}
+
+int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scene_params* prm, int nframes,
+                      void* stream) {
+    if (nframes < 1) { set_error("frame count must be positive"); return PT_ERR_INVALID; }
+    const int64_t total = static_cast<int64_t>(prm->sample_per_frame) * nframes;
+    WaveParams P;
+    int lanes = 1;
+    if (int rc = prepare_wave(integ, film, s, prm, total, 0, P, lanes)) return rc;
+    Wavefront& wf = *integ->wf;
+    GuideState* gs = wf.guide;
+    const pt_render_settings& rs = s->host.settings;
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : wf.own_stream;
     k_begin<<<1, 1, 0, st>>>(P.pass, s->frame_count);
     PT_CU(cudaGetLastError());
@@ -1211,7 +1232,7 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
         PT_CU(cudaEventCreate(&t0));
         PT_CU(cudaEventCreate(&t1));
         PT_CU(cudaEventRecord(t0, st));
-        int rc = enqueue_batch(wf, P, nframes, st, &ev, gs);
+        int rc = enqueue_batch(wf, P, total, st, &ev, gs);
         PT_CU(cudaEventRecord(t1, st));
         PT_CU(cudaEventSynchronize(t1));
         float ms = 0.0f;
@@ -1237,7 +1258,7 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
             if (wf.graph) { cudaGraphExecDestroy(wf.graph); wf.graph = nullptr; }
             cudaGraph_t g = nullptr;
             PT_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            const int rc = enqueue_batch(wf, P, nframes, st, nullptr, gs);
+            const int rc = enqueue_batch(wf, P, total, st, nullptr, gs);
             const cudaError_t ec = cudaStreamEndCapture(st, &g);
             if (rc) { if (g) cudaGraphDestroy(g); return rc; }
             if (ec != cudaSuccess) { set_error(std::string("graph capture failed: ") + cudaGetErrorString(ec)); return PT_ERR_CUDA; }
@@ -1248,13 +1269,14 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
         }
         PT_CU(cudaGraphLaunch(wf.graph, st));
     } else {
-        if (int rc = enqueue_batch(wf, P, nframes, st, nullptr, gs)) return rc;
+        if (int rc = enqueue_batch(wf, P, total, st, nullptr, gs)) return rc;
     }
     // k_begin + per pass (raygen, 3 per bounce, finalize)
     const uint64_t passes = static_cast<uint64_t>((total + lanes - 1) / lanes);
     if (!timing) wf.extend_launches += passes * static_cast<uint64_t>(P.max_depth);
     wf.kernel_launches += 1 + passes * (2 + 3 * static_cast<uint64_t>(P.max_depth));
-    if (P.gmix) wf.kernel_launches += passes * (P.max_depth + (P.grec ? 2 + 2 * kGuideMinibatches : 0));
+    if (P.gmix)
+        wf.kernel_launches += passes * (P.max_depth + (P.grec ? 2 + 2 * guide_minibatches(P.npix * lanes) : 0));
     return PT_OK;
 }
 
@@ -1463,6 +1485,7 @@ void guide_destroy(pt_guide* h) {
 }
 
 void guide_set_lr(pt_guide* h, float lr) { h->g.lr = lr; }
+void guide_set_alpha(pt_guide* h, float alpha) { h->g.alpha = alpha; }
 
 int guide_info(const pt_guide* h, uint32_t* steps, uint32_t* samples) {
     uint32_t c[2] = {0, 0};
@@ -1472,6 +1495,15 @@ int guide_info(const pt_guide* h, uint32_t* steps, uint32_t* samples) {
     if (h->g.counters) PT_CU(cudaMemcpy(&c[0], h->g.counters, 4, cudaMemcpyDeviceToHost));
     if (steps) *steps = c[1];
     if (samples) *samples = c[0];
+    return PT_OK;
+}
+
+int guide_loss(const pt_guide* h, float* loss) {
+    if (int rc = ensure_device(h->g.device)) return rc;
+    PT_CU(cudaDeviceSynchronize());
+    float l[3] = {0, 0, 0};
+    if (h->g.net.loss) PT_CU(cudaMemcpy(l, h->g.net.loss, sizeof(l), cudaMemcpyDeviceToHost));
+    *loss = l[2];
     return PT_OK;
 }
 
@@ -1519,7 +1551,9 @@ int guide_backward(pt_guide* h, const float* samples, uint32_t n, float* wgrad, 
     if (e == cudaSuccess) e = cudaMemset(h->g.net.w_grad, 0, kGWeights * sizeof(float));
     if (e == cudaSuccess) e = cudaMemset(h->g.net.grid_grad, 0, ng * sizeof(float2));
     if (e == cudaSuccess) {
-        k_guide_train<<<148, 128, kGTrainSmem>>>(h->g.net, ds, dn, n, 0, 1);
+        GuideNet net = h->g.net;
+        net.loss = nullptr;   // leave the training-loss record alone
+        k_guide_train<<<148, 128, kGTrainSmem>>>(net, ds, dn, n, 0, 1);
         e = cudaDeviceSynchronize();
     }
     if (e == cudaSuccess) e = cudaMemcpy(wgrad, h->g.net.w_grad, kGWeights * sizeof(float), cudaMemcpyDeviceToHost);

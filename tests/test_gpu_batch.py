@@ -54,7 +54,45 @@ def test_batch_autotuner_and_uneven_budgets():
         sa.spp = max(4, sa.spp // 32)
     ss = [_up(sa) for sa in batch]
     imgs, st, cfg = pt.render_batch([(s, sa.spp) for s, sa in zip(ss, batch)], autotune=True)
-    assert cfg["block_size"] in (64, 128, 256) and cfg["blocks_per_sm"] >= 1 and cfg["tuned_ms"] > 0
+    assert cfg["tuned_ms"] > 0
+    if cfg["mode"] == pt.BATCH_PERSISTENT:
+        assert cfg["block_size"] in (64, 128, 256) and cfg["blocks_per_sm"] >= 1
+    else:
+        assert cfg["mode"] == pt.BATCH_WAVEFRONT and cfg["paths_in_flight"] > 0
     assert st["paths"] == sum(64 * 48 * sa.spp for sa in batch)
     for img in imgs:
         assert np.isfinite(img).all() and img[..., :3].mean() > 0
+
+
+def test_batch_wavefront_mode_matches_single_scene_renders():
+    """Wavefront mode runs each item through the single-scene wavefront (as
+    parallel graph branches): with spp a multiple of the frame size the images
+    equal pt.render's bit for bit, whatever the share of path slots."""
+    sas = _batch_scenes()
+    ss = [_up(sa) for sa in sas]
+    items = [(s, sa.spp) for s, sa in zip(ss, sas)]
+    imgs, st, cfg = pt.render_batch(items, mode=pt.BATCH_WAVEFRONT)
+    assert cfg["mode"] == pt.BATCH_WAVEFRONT
+    small, _, _ = pt.render_batch(items, mode=pt.BATCH_WAVEFRONT, paths_in_flight=1 << 12)
+    for s, sa, img, img2 in zip(ss, sas, imgs, small):
+        ref = pt.render(s, sa.spp)
+        assert np.array_equal(img, ref), sa.name
+        assert np.array_equal(img2, ref), sa.name
+    assert st["paths"] == sum(int(sa.camera["width"]) * int(sa.camera["height"]) * sa.spp for sa in sas)
+
+
+def test_batch_modes_agree_and_autotuner_picks_one():
+    batch = scenes.uneven_batch(n_scenes=5, seed=3, env_size=(128, 64), tri_range=(1_000, 40_000))
+    for sa in batch:
+        sa.camera["width"], sa.camera["height"] = 48, 40
+        sa.spp = max(4, sa.spp // 64)
+    ss = [_up(sa) for sa in batch]
+    items = [(s, sa.spp, 3) for s, sa in zip(ss, batch)]
+    a, _, _ = pt.render_batch(items, mode=pt.BATCH_PERSISTENT, autotune=False, chunk_spp=4)
+    b, _, _ = pt.render_batch(items, mode=pt.BATCH_WAVEFRONT)
+    c, st, cfg = pt.render_batch(items, mode=pt.BATCH_AUTO, autotune=True)
+    assert cfg["mode"] in (pt.BATCH_PERSISTENT, pt.BATCH_WAVEFRONT)
+    for x, y, z in zip(a, b, c):
+        rel = np.abs(x[..., :3] - y[..., :3]) / np.maximum(np.abs(y[..., :3]), 1e-3)
+        assert np.median(rel) < 1e-5
+        assert np.isfinite(z).all()
