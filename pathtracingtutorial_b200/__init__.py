@@ -516,6 +516,18 @@ def trace_closest(scene: SceneManager, origins: np.ndarray, dirs: np.ndarray) ->
     return hits
 
 
+STATIC_TRACE_MAX_RAYS = 65536
+
+
+def trace_closest_static(scene: SceneManager, origins: np.ndarray, dirs: np.ndarray) -> np.ndarray:
+    """trace_closest through the allocation-free entry point (at most
+    STATIC_TRACE_MAX_RAYS rays per call)."""
+    rays = _pack_rays(origins, dirs, None)
+    hits = np.zeros(len(rays), HIT_DTYPE)
+    check(lib().pt_trace_closest_static(scene.handle, ptr(rays), len(rays), ptr(hits)))
+    return hits
+
+
 def trace_any(scene: SceneManager, origins: np.ndarray, dirs: np.ndarray, tmax: np.ndarray) -> np.ndarray:
     rays = _pack_rays(origins, dirs, tmax)
     occ = np.zeros(len(rays), np.uint8)

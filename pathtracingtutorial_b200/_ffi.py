@@ -163,6 +163,7 @@ _SIGS = [
     ("pt_guide_backward", C.c_int, [_P, _P, C.c_uint32, _P, _P]),
     ("pt_trace_closest", C.c_int, [_P, _P, C.c_uint32, _P, C.c_int32]),
     ("pt_trace_any", C.c_int, [_P, _P, C.c_uint32, _P, C.c_int32]),
+    ("pt_trace_closest_static", C.c_int, [_P, _P, C.c_uint32, _P]),
     ("pt_sampler_stream", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_uint32, C.c_int32, C.c_int32,
                                     C.c_uint32, C.c_uint32, C.c_int32, _P]),
     ("pt_bsdf_eval", C.c_int, [_P, _P, C.c_uint32, _P]),
