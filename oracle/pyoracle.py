@@ -1,5 +1,6 @@
-"""TEST INFRASTRUCTURE: Python access to the CPU oracle (liboracle.so) and to the
-reference's own host-compiled code (_ref/libptref.so).
+"""TEST INFRASTRUCTURE: Python access to the CPU oracle (liboracle.so), to the
+reference's own host-compiled code (_ref/libptref.so) and to the reference's
+own CUDA integrator built for sm_100a (_ref/libptref_gpu.so).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this module.  `Oracle` is the restatement (oracle/pt_oracle.cpp); `RefHarness`
@@ -18,6 +19,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libptref.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libptref_gpu.so")
 
 VERTEX = np.dtype([("position", "<f4", 3), ("_pad0", "<f4"), ("normal", "<f4", 3), ("_pad1", "<f4"),
                    ("uv", "<f4", 2), ("_pad2", "<f4", 2), ("tangent", "<f4", 4)])
@@ -63,7 +65,7 @@ def _p(a):
 
 def build(ref: bool = False) -> None:
     """Compile liboracle.so (and, when the reference tree is present, _ref/libptref.so)."""
-    targets = ["oracle", "ref"] if ref else ["oracle"]
+    targets = ["oracle", "ref", "ref-gpu"] if ref else ["oracle"]
     r = subprocess.run(["make", "-C", HERE, "-j8", *targets], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
@@ -301,3 +303,55 @@ class RefHarness:
                           C.c_uint32(num_frames), C.c_int(row0), C.c_int(row_step), C.c_int(threads), _p(acc),
                           _p(new), _p(stats))
         return acc, new, {"closest_rays": stats[0], "shadow_rays": stats[1], "paths": stats[2], "seconds": stats[3]}
+
+
+class RefGpu:
+    """The reference's own CUDA path tracer (kernelPathTrace through
+    PathIntegrator::launch, DeviceScene, Film), built unchanged for sm_100a
+    (requires oracle/_ref/libptref_gpu.so).  One instance = one scene."""
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REF_GPU_SO)
+
+    def __init__(self, sa, device: int = 0):
+        self.L = C.CDLL(REF_GPU_SO)
+        self.L.refgpu_frame_count.restype = C.c_uint32
+        v = np.ascontiguousarray(sa.vertices)
+        f = np.ascontiguousarray(sa.faces)
+        m = np.ascontiguousarray(sa.materials)
+        cam = np.ascontiguousarray(sa.camera)
+        self.width = int(np.frombuffer(cam.tobytes()[60:64], np.int32)[0])
+        self.height = int(np.frombuffer(cam.tobytes()[64:68], np.int32)[0])
+        env = None if sa.env is None else np.ascontiguousarray(sa.env, np.float32)
+        ew, eh = (env.shape[1], env.shape[0]) if env is not None else (0, 0)
+        st = np.array([sa.spp, sa.sample_per_frame, sa.max_depth, sa.sampler], np.int32)
+        h = C.c_void_p()
+        rc = self.L.refgpu_create(_p(v), C.c_uint32(len(v)), _p(f), C.c_uint32(len(f)), _p(m),
+                                  C.c_uint32(m.nbytes // 256), _p(env), C.c_int(ew), C.c_int(eh), _p(cam), _p(st),
+                                  C.c_int(device), C.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"reference GPU scene setup failed ({rc})")
+        self._h = h
+
+    def reset(self) -> None:
+        """Renderer::resetAccumulation: frame 0, cleared film."""
+        if self.L.refgpu_reset(self._h) != 0:
+            raise RuntimeError("reference GPU reset failed")
+
+    def render(self, frames: int) -> tuple[float, float]:
+        """`frames` renderBatch calls; returns (device ms, wall ms) of the loop."""
+        t = np.zeros(2, np.float64)
+        if self.L.refgpu_render(self._h, C.c_int(frames), _p(t)) != 0:
+            raise RuntimeError("reference GPU render failed")
+        return float(t[0]), float(t[1])
+
+    def image(self) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        self.L.refgpu_download(self._h, _p(out))
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            self.L.refgpu_destroy(self._h)
+            self._h = None
