@@ -83,6 +83,28 @@ def test_hit_ids_bit_exact(oracle, name):
     assert np.array_equal(occ, ref_occ)
 
 
+def test_hit_ids_bit_exact_large_scene(oracle):
+    """Seeded rays through a 51,202-triangle displaced-sphere field (BVH depth
+    19): origins inside and outside the spheres, directions of every octant,
+    plus rays whose origin lies on a bounding-box plane."""
+    sa = scenes.icosphere_field(n_spheres=40, subdiv=3, width=64, height=36, env_size=(64, 32))
+    s = _scene(sa)
+    prep = oracle.prepare(sa)
+    lo, hi = sa.vertices["position"].min(0), sa.vertices["position"].max(0)
+    o, d, t = _rays(200000, lo - 1.0, hi + 1.0, 11)
+    o[:2000] = sa.vertices["position"][np.random.default_rng(5).integers(0, len(sa.vertices), 2000)]
+    hits = pt.trace_closest(s, o, d)
+    rays = np.zeros((len(o), 8), np.float32)
+    rays[:, :3], rays[:, 4:7], rays[:, 7] = o, d, t
+    ref, _ = oracle.trace(prep.nodes, prep.vertices, prep.faces, rays)
+    gpu = np.stack([hits["t"], hits["prim"].view(np.float32), hits["u"], hits["v"]], 1)
+    assert (hits["prim"] >= 0).mean() > 0.2
+    assert np.array_equal(gpu.view(np.uint32), ref.view(np.uint32))
+    occ = pt.trace_any(s, o, d, t)
+    ref_occ, _ = oracle.trace(prep.nodes, prep.vertices, prep.faces, rays, any_hit=True)
+    assert np.array_equal(occ, ref_occ)
+
+
 def test_camera_rays_hit_ids(oracle):
     """Primary rays generated on the host in the reference's arithmetic."""
     sa = scenes.icosphere_field(n_spheres=60, subdiv=3, width=96, height=54, env_size=(64, 32))
