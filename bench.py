@@ -4,9 +4,15 @@
 ground quad, Disney materials, 2048x1024 synthetic sky with a 5e4 sun lobe),
 1920x1080, 256 spp, max depth 16, Sobol.
 
-One step = one full render of that workload: 64 launches of 4 samples per pixel
-(the reference's Renderer::renderAll over PathIntegrator::launch), scene
-resident in HBM.  Rays = camera + extension + shadow rays traced.
+One step = one full render of that workload (the reference's
+Renderer::renderAll: 64 frames of 4 samples per pixel), issued as one
+graph-captured launch of 16 wavefront passes of 16 spp; scene resident in HBM.
+Rays = camera + extension + shadow rays traced.
+
+The line also carries the second half of the metric, measured on the
+hidden-light room (1024x1024, depth 16): relMSE of the plain and the guided
+integrator against a 4096-spp plain reference, and their extrapolated time to
+relMSE 1e-3 (key "convergence").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -45,6 +51,8 @@ def parse_args():
     p.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true",
                    help="skip the CPU baseline leg (profiling runs; the line then carries cpu_baseline null)")
+    p.add_argument("--no-convergence", action="store_true",
+                   help="skip the guided-vs-plain convergence leg (the line then carries convergence null)")
     return p.parse_args()
 
 
@@ -216,6 +224,73 @@ def cpu_baseline(sa, spp, seconds):
                       f"{s['seconds']:.1f} s"}
 
 
+def convergence(local: int, stream, small: bool):
+    """Guided vs plain on the hidden-light room (202,002 triangles, 1024x1024,
+    depth 16, Sobol): relMSE against a 4096-spp plain render on independent
+    sample indices, each arm timed with CUDA events; the guide trains online
+    for 64 spp (timed) before it renders.  Time to relMSE 1e-3 is extrapolated
+    with relMSE ~ 1/time (both estimators are unbiased), after subtracting the
+    reference's own noise (estimated from the plain arm: relMSE x spp / 4096)."""
+    import numpy as np
+    import torch
+    import pathtracingtutorial_b200 as pt
+    from pathtracingtutorial_b200 import scenes
+    w = 256 if small else 1024
+    n_ref, n_plain, n_train, n_guided = (256, 64, 16, 64) if small else (4096, 256, 64, 256)
+    sa = scenes.hidden_light_room(width=w, height=w)
+    scene = sa.scene()
+    scene.build_accel()
+    scene.upload_to_device(local)
+    spf = sa.sample_per_frame
+    handle = stream.cuda_stream
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    r = pt.Renderer(scene, device=local, stream=handle)
+    r.reset_accumulation()
+    scene.set_frame_count(1_000_000)
+    ref_ms = timed(lambda: r.render_frames(n_ref // spf))
+    ref = r.download_current_image()[..., :3].astype(np.float64)
+
+    def relmse(img):
+        return float(np.mean((img[..., :3].astype(np.float64) - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    r.reset_accumulation()
+    scene.set_frame_count(0)
+    t_plain = timed(lambda: r.render_frames(n_plain // spf))
+    e_plain = relmse(r.download_current_image())
+    g = pt.Guide(scene, seed=1)
+    rg = pt.Renderer(scene, device=local, stream=handle)
+    g.attach(rg.integrator, pt.Guide.TRAIN)
+    rg.reset_accumulation()
+    scene.set_frame_count(100_000)
+    t_train = timed(lambda: rg.render_frames(n_train // spf))
+    g.attach(rg.integrator, pt.Guide.USE)
+    rg.reset_accumulation()
+    scene.set_frame_count(0)
+    t_guided = timed(lambda: rg.render_frames(n_guided // spf))
+    e_guided = relmse(rg.download_current_image())
+    g.close()
+    e_ref = e_plain * n_plain / n_ref
+    tp = t_plain * max(e_plain - e_ref, 1e-12) / 1e-3
+    tg = t_train + t_guided * max(e_guided - e_ref, 1e-12) / 1e-3
+    return {"scene": f"hidden_light_room {len(sa.faces)} tri, {w}x{w}, depth {sa.max_depth}, sobol",
+            "reference": f"plain, {n_ref} spp, independent samples ({ref_ms:.0f} ms)",
+            "plain": {"spp": n_plain, "ms": round(t_plain, 1), "relmse": round(e_plain, 6)},
+            "guided": {"train_spp": n_train, "train_ms": round(t_train, 1), "spp": n_guided,
+                       "ms": round(t_guided, 1), "relmse": round(e_guided, 6)},
+            "reference_noise_relmse": round(e_ref, 6),
+            "time_to_relmse_1e-3_ms": {"plain": round(tp, 1), "guided": round(tg, 1)},
+            "guided_speedup": round(tp / tg, 3)}
+
+
 def ours(args):
     import numpy as np
     import torch
@@ -323,6 +398,10 @@ def ours(args):
         if dist is not None:
             dist.destroy_process_group()
         return
+    conv = None
+    if world == 1 and not args.no_convergence:
+        with torch.cuda.stream(stream):
+            conv = convergence(local, stream, args.small)
     cpu = cpu_baseline(sa, spp, args.cpu_sample_seconds) if world == 1 and not args.no_cpu_baseline else None
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -348,6 +427,7 @@ def ours(args):
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
         "gpu_launches": int(st["kernel_launches"]),
+        "convergence": conv,
     }
     print(json.dumps(line))
     if dist is not None:

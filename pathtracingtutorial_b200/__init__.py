@@ -463,14 +463,13 @@ def render_guided(scene: SceneManager, train_spp: int, spp: int, guide: Guide | 
     g.attach(r.integrator, Guide.TRAIN)
     r.reset_accumulation()
     scene.set_frame_count(first_frame + 100000)   # training samples are independent of the image's
-    for _ in range((train_spp + spf - 1) // spf):
-        r.render_batch()
+    if train_spp > 0:
+        r.render_frames((train_spp + spf - 1) // spf)
     g.attach(r.integrator, Guide.USE)
     r.reset_accumulation()
     scene.set_frame_count(first_frame)
     r.integrator.reset_stats()
-    for _ in range((spp + spf - 1) // spf):
-        r.render_batch()
+    r.render_frames((spp + spf - 1) // spf)
     r.synchronize()
     img = r.download_current_image()
     return img, g, r.integrator.stats()

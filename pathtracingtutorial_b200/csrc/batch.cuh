@@ -55,7 +55,7 @@ __device__ f3 trace_path_inline(const BatchItemDev& it, int x, int y, PathRng& r
         if (depth == 0) ++bc.camera; else ++bc.ext;
         const bool last = depth == it.max_depth - 1;
         f3 no, nd;
-        const bool cont = shade_path(it.scene, it.arg_rtl, depth, last, o, d, make_float4(t, __int_as_float(prim), u, v),
+        const bool cont = shade_path<false>(it.scene, it.arg_rtl, depth, last, o, d, make_float4(t, __int_as_float(prim), u, v),
                                      T, last_pdf, last_delta, L, rng, no, nd, sink);
         if (!cont || last) break;
         o = no;

@@ -17,9 +17,11 @@
 // layers in registers (an accumulator fragment pair is the next layer's A
 // fragment), weights sit in shared memory with padded rows.
 //
-// Training minimises the KL divergence from the normalised incident radiance
-// to q with the one-sample estimate  -L_in(w) / p(w) * log q(w | x)  per
-// recorded path vertex; the backward pass runs on the tensor cores too
+// Training minimises the KL divergence from the normalised cosine-weighted
+// incident radiance to q with the one-sample estimate
+// -L_in(w) |cos| / p(w) * log q(w | x)  per recorded path vertex, in
+// minibatches interleaved over the whole image; the backward pass runs on the
+// tensor cores too
 // (dX = dY W and dW = dY^T X per CTA tile), the hash-grid gradient is scattered
 // with FP32 atomics, and Adam updates FP32 master copies.
 
@@ -39,10 +41,10 @@ constexpr int kGOut = 40;                 // used outputs
 constexpr int kGOutPad = 48;              // 6 n-tiles of 8
 constexpr int kGMix = 40;                 // floats per mixture: 8 x (mu xyz, kappa) + 8 weights
 constexpr float kGuideAlpha = 0.5f;        // default probability of sampling the mixture
-constexpr int kGuideMinibatchPaths = 1 << 17;
+constexpr int kGuideMinibatchPaths = 1 << 15;
 
-// Optimiser steps per training pass of `paths` paths: one per 2^17 paths
-// (a few hundred thousand samples), 1 .. 32.
+// Optimiser steps per training pass of `paths` paths: one per 2^15 paths
+// (about 10^5 samples), 1 .. 32.
 inline int guide_minibatches(int64_t paths) {
     return static_cast<int>(std::min<int64_t>(32, std::max<int64_t>(1, paths / kGuideMinibatchPaths)));
 }
@@ -446,31 +448,31 @@ __device__ __forceinline__ void store_dy(const float (&acc)[N / 8][4], const __n
     }
 }
 
-// Sample range of minibatch mb of nmb over the first n samples.
-__host__ __device__ __forceinline__ void minibatch_range(uint32_t n, int mb, int nmb, uint32_t& lo, uint32_t& hi) {
-    lo = static_cast<uint32_t>(static_cast<uint64_t>(n) * mb / nmb);
-    hi = static_cast<uint32_t>(static_cast<uint64_t>(n) * (mb + 1) / nmb);
+// Minibatch mb of nmb over the first n samples takes samples mb, mb + nmb,
+// mb + 2 nmb, ...: the samples are collected in path (pixel) order, so
+// interleaving gives every optimiser step samples from the whole image
+// instead of one band of rows.
+__host__ __device__ __forceinline__ uint32_t minibatch_size(uint32_t n, int mb, int nmb) {
+    return n > static_cast<uint32_t>(mb) ? (n - static_cast<uint32_t>(mb) + static_cast<uint32_t>(nmb) - 1u) /
+                                               static_cast<uint32_t>(nmb)
+                                         : 0u;
 }
 
 // Optimiser steps taken for the first mb minibatches (the empty ones take none).
 __host__ __device__ __forceinline__ uint32_t steps_before(uint32_t n, int mb, int nmb) {
     uint32_t k = 0;
-    for (int i = 0; i < mb; ++i) {
-        uint32_t lo, hi;
-        minibatch_range(n, i, nmb, lo, hi);
-        k += hi > lo ? 1u : 0u;
-    }
+    for (int i = 0; i < mb; ++i) k += minibatch_size(n, i, nmb) > 0u ? 1u : 0u;
     return k;
 }
 
 // Gradient of the mean loss over minibatch mb (of nmb) of the collected samples.
 __global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSample* __restrict__ samples_all,
                                                      const uint32_t* count, uint32_t cap, int mb, int nmb) {
-    uint32_t b0, b1;
-    minibatch_range(min(*count, cap), mb, nmb, b0, b1);
-    if (b1 <= b0) return;
-    const GuideSample* __restrict__ samples = samples_all + b0;
-    const uint32_t n = b1 - b0;
+    const uint32_t n = minibatch_size(min(*count, cap), mb, nmb);
+    if (n == 0u) return;
+    // row r of this minibatch is sample mb + r * nmb
+    const GuideSample* __restrict__ samples = samples_all + mb;
+    const uint32_t sstride = static_cast<uint32_t>(nmb);
     const float inv_n = 1.0f / static_cast<float>(n);
     extern __shared__ __align__(16) unsigned char g_smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(g_smem);                       // W  [out][in+8]
@@ -506,8 +508,10 @@ __global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSa
     const uint32_t tiles = (n + 15) / 16;
     for (uint32_t tile = blockIdx.x * 4 + warp; tile < tiles; tile += gridDim.x * 4) {
         const uint32_t r0 = tile * 16 + g, r1 = r0 + 8;
-        const GuideSample s0 = r0 < n ? samples[r0] : GuideSample{make_float4(0.5f, 0.5f, 0.5f, 0.0f), make_float4(0, 0, 1, 0)};
-        const GuideSample s1 = r1 < n ? samples[r1] : GuideSample{make_float4(0.5f, 0.5f, 0.5f, 0.0f), make_float4(0, 0, 1, 0)};
+        const GuideSample s0 = r0 < n ? samples[static_cast<size_t>(r0) * sstride]
+                                      : GuideSample{make_float4(0.5f, 0.5f, 0.5f, 0.0f), make_float4(0, 0, 1, 0)};
+        const GuideSample s1 = r1 < n ? samples[static_cast<size_t>(r1) * sstride]
+                                      : GuideSample{make_float4(0.5f, 0.5f, 0.5f, 0.0f), make_float4(0, 0, 1, 0)};
         const f3 p0 = mk(s0.pos_w.x, s0.pos_w.y, s0.pos_w.z), p1 = mk(s1.pos_w.x, s1.pos_w.y, s1.pos_w.z);
         // forward, keeping every layer's input
         uint32_t a0[2][4];
@@ -540,7 +544,7 @@ __global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSa
             const uint32_t r = tile * 16 + lane;
             float d[kGOutPad];
             if (r < n) {
-                const GuideSample s = samples[r];
+                const GuideSample s = samples[static_cast<size_t>(r) * sstride];
                 const float q = mixture_grad(OUT + lane * kGOutPad, mk(s.dir.x, s.dir.y, s.dir.z), s.pos_w.w * inv_n, d);
                 row_loss = -s.pos_w.w * logf(q);
             } else {
@@ -658,9 +662,7 @@ __global__ void k_guide_step(uint32_t* sample_count, uint32_t* step, float* loss
 __global__ void k_guide_adam(GuideNet net, const uint32_t* count, uint32_t cap, int mb, int nmb, const uint32_t* step,
                              float lr_w, float lr_g, float b1, float b2, float eps) {
     const uint32_t n = min(*count, cap);
-    uint32_t lo, hi;
-    minibatch_range(n, mb, nmb, lo, hi);
-    if (hi <= lo) return;
+    if (minibatch_size(n, mb, nmb) == 0u) return;
     const float t = static_cast<float>(*step + steps_before(n, mb, nmb) + 1u);
     const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
     const size_t nw = kGWeights;

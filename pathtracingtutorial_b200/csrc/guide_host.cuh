@@ -104,28 +104,31 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
 
 // Mixture buffer (one per queue entry), training records (depth x npix x 64 B),
 // training samples and counters, sized for npix paths and max_depth bounces.
-inline int guide_prepare_work(GuideState& g, int npix, int depth) {
-    if (g.work && g.npix == npix && g.depth == depth) return PT_OK;
+// Work buffers for passes of `npix` paths: the mixtures always, the training
+// records and samples only when `records` (training) -- a guide that only
+// samples can then run passes as large as the plain integrator's.
+inline int guide_prepare_work(GuideState& g, int npix, int depth, bool records) {
+    if (g.work && g.npix == npix && g.depth == depth && (g.rec != nullptr || !records)) return PT_OK;
     if (!guide_cuda_ok(cudaSetDevice(g.device), "cudaSetDevice")) return PT_ERR_CUDA;
     if (g.work) { cudaFree(g.work); g.work = nullptr; }
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t P = static_cast<size_t>(npix), D = static_cast<size_t>(std::max(depth, 1));
-    const size_t cap = std::min<size_t>(P * D, size_t(1) << 24);
+    const size_t cap = records ? std::min<size_t>(P * D, size_t(1) << 24) : 0;
     const size_t b_mix = al(P * kGMix * sizeof(float));
-    const size_t b_rec = al(D * P * 4 * sizeof(float4));
+    const size_t b_rec = records ? al(D * P * 4 * sizeof(float4)) : 0;
     const size_t b_smp = al(cap * sizeof(GuideSample));
     const size_t total = b_mix + b_rec + b_smp + 256;
     if (!guide_cuda_ok(cudaMalloc(&g.work, total), "work allocation")) return PT_ERR_NOMEM;
     g.work_bytes = total;
     char* base = static_cast<char*>(g.work);
     g.mix = reinterpret_cast<float*>(base);
-    g.rec = reinterpret_cast<float4*>(base + b_mix);
-    g.samples = reinterpret_cast<GuideSample*>(base + b_mix + b_rec);
+    g.rec = records ? reinterpret_cast<float4*>(base + b_mix) : nullptr;
+    g.samples = records ? reinterpret_cast<GuideSample*>(base + b_mix + b_rec) : nullptr;
     g.counters = reinterpret_cast<uint32_t*>(base + b_mix + b_rec + b_smp);
     g.sample_cap = static_cast<uint32_t>(cap);
     g.npix = npix;
     g.depth = depth;
-    const bool ok = guide_cuda_ok(cudaMemset(g.rec, 0, b_rec), "clear") &&
+    const bool ok = (b_rec == 0 || guide_cuda_ok(cudaMemset(g.rec, 0, b_rec), "clear")) &&
                     guide_cuda_ok(cudaMemset(g.counters, 0, 256), "clear");
     return ok ? PT_OK : PT_ERR_CUDA;
 }

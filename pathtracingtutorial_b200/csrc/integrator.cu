@@ -173,11 +173,15 @@ __device__ __forceinline__ uint32_t sample_alias(const pt_alias_entry* t, uint32
 // evaluateDirectLight (direct_lighting.cuh:204-218) without the visibility term.
 // At a guided vertex the directional strategy is the guide/BSDF mixture, so
 // its pdf (alpha q + (1 - alpha) p_bsdf) enters the power heuristic.
+template <bool Guided>
 __device__ __forceinline__ f3 direct_term(const MatEval& me, f3 wo, f3 wi, f3 n, f3 radiance, float light_pdf,
                                           const float* gmix, float galpha) {
     const BsdfEval b = PT_BSDF_EVAL(me, wo, wi, n, true);
     if (b.pdf <= 0.0f) return mk(0.0f);
-    const float dir_pdf = gmix ? galpha * mix_pdf(gmix, wi) + (1.0f - galpha) * b.pdf : b.pdf;
+    float dir_pdf = b.pdf;
+    if constexpr (Guided) {
+        if (gmix) dir_pdf = galpha * mix_pdf(gmix, wi) + (1.0f - galpha) * b.pdf;
+    }
     const float mis = power_heuristic(light_pdf, dir_pdf);
     return radiance * b.f * (mis / (light_pdf + 1e-7f));
 }
@@ -261,7 +265,7 @@ __global__ void __launch_bounds__(256) k_raygen(WaveParams P, int s0, int count)
         f3 pos, dir;
         camera_ray(P.cam, P.width, P.height, x, y, rng, pos, dir);
         P.queue[0][p] = static_cast<uint32_t>(p);
-        P.ray_o[0][p] = f4of(pos, 0.0f);
+        P.ray_o[0][p] = f4of(pos, 1.0f);   // w: roulette throughput of the guided integrator
         P.ray_d[0][p] = f4of(dir, 0.0f);
         P.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
         P.lo[p] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
@@ -333,11 +337,12 @@ struct InlineSink {
 };
 
 // One bounce of pathTrace (path.cu:69-199).  Returns true when the path
-// continues with ray (no, nd).  Shadow rays go to `sink`.
-template <class Sink>
+// continues with ray (no, nd).  Shadow rays go to `sink`.  Guided = false
+// compiles the plain integrator without any of the guiding code.
+template <bool Guided, class Sink>
 __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool last, f3 ro, f3 rd, float4 h,
                            f3& T, float& last_pdf, bool& last_delta, f3& L, PathRng& rng, f3& no, f3& nd,
-                           Sink& sink, GuideVertex gv = GuideVertex{nullptr, nullptr}) {
+                           Sink& sink, GuideVertex gv = GuideVertex{nullptr, nullptr}, float* rr_w = nullptr) {
     const int prim = __float_as_int(h.y);
     if (prim < 0) {
         const f3 env = env_radiance(s, rd);
@@ -376,7 +381,7 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
     const bool delta_surface = (me.metallic >= 1.0f && me.roughness < 0.01f) ||
                                (me.spec_trans >= 1.0f && me.roughness < 0.01f);
     // guided vertex: a mixture is available and no lobe can be a delta
-    const float* gmix = (gv.mix != nullptr && me.roughness >= 0.01f) ? gv.mix : nullptr;
+    const float* gmix = (Guided && gv.mix != nullptr && me.roughness >= 0.01f) ? gv.mix : nullptr;
     if (!delta_surface) {
         const bool has_area = s.num_emissive > 0 && s.emissive != nullptr;
         const bool has_env = has_env_light(s);
@@ -417,7 +422,7 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
             }
             if (ok) {
                 const f3 le = material_emission(s.materials[lf.material_id]);
-                contrib = T * direct_term(me, wo, wi, N, le, pdf, gmix, gv.alpha);
+                contrib = T * direct_term<Guided>(me, wo, wi, N, le, pdf, gmix, gv.alpha);
                 ok = !is_zero(contrib);
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
@@ -440,7 +445,7 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
             f3 contrib = mk(0.0f);
             if (ok) { pdf = env_pdf(s, wi); ok = pdf > 0.0f; }
             if (ok) {
-                contrib = T * direct_term(me, wo, wi, N, env_radiance(s, wi), pdf, gmix, gv.alpha);
+                contrib = T * direct_term<Guided>(me, wo, wi, N, env_radiance(s, wi), pdf, gmix, gv.alpha);
                 ok = !is_zero(contrib);
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
@@ -486,7 +491,8 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
     }
     if (last) return false;   // the sampled continuation would never be traced
     BsdfSample bs;
-    if (gmix) {
+    float plain_w = 0.0f;   // guided: max3(f cos / p_bsdf) of this vertex, for the roulette
+    if (Guided && gmix) {
         // one-sample MIS between the learned mixture and the BSDF
         const float sel = rng_next(rng);
         if (sel < gv.alpha) {
@@ -498,8 +504,10 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
             bs.pdf = p;
             bs.weight = bs.valid ? ev.f / p : mk(0.0f);
             bs.delta = false;
+            plain_w = ev.pdf > 0.0f ? max3(ev.f) / ev.pdf : max3(bs.weight);
         } else {
             bs = PT_BSDF_SAMPLE(me, wo, N, rng, arg_rtl, entering);
+            plain_w = max3(bs.weight);
             if (bs.valid) {
                 const float p = gv.alpha * mix_pdf(gmix, bs.wi) + (1.0f - gv.alpha) * bs.pdf;
                 bs.weight = bs.weight * ((bs.pdf + 1e-7f) / p);
@@ -508,9 +516,11 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
         }
     } else {
         bs = PT_BSDF_SAMPLE(me, wo, N, rng, arg_rtl, entering);
+        plain_w = max3(bs.weight);
     }
     if (!bs.valid) return false;
     T *= bs.weight;
+    if (Guided && rr_w) *rr_w *= plain_w;
     const bool transmitted = dot(bs.wi, gn) < 0.0f;
     const f3 off = transmitted ? -gn : gn;
     no = hp + off * 1e-4f;
@@ -518,29 +528,37 @@ __device__ bool shade_path(const DeviceScene& s, int arg_rtl, int depth, bool la
     if (transmitted && me.thickness > 0.0f && me.att_distance < 1e20f) {
         const float th = me.thickness, ad = me.att_distance;
         const f3 ac = me.att_color;
-        T *= mk(expf(-th * fmaxf(-logf(fmaxf(ac.x, 1e-6f)), 0.0f) / ad),
-                expf(-th * fmaxf(-logf(fmaxf(ac.y, 1e-6f)), 0.0f) / ad),
-                expf(-th * fmaxf(-logf(fmaxf(ac.z, 1e-6f)), 0.0f) / ad));
+        const f3 tr = mk(expf(-th * fmaxf(-logf(fmaxf(ac.x, 1e-6f)), 0.0f) / ad),
+                         expf(-th * fmaxf(-logf(fmaxf(ac.y, 1e-6f)), 0.0f) / ad),
+                         expf(-th * fmaxf(-logf(fmaxf(ac.z, 1e-6f)), 0.0f) / ad));
+        T *= tr;
+        if (Guided && rr_w) *rr_w *= max3(tr);
     }
     last_pdf = bs.pdf;
     last_delta = bs.delta;
     if (depth > 2) {
-        const float surv = fminf(max3(T), 0.95f);
+        // Russian roulette (path.cu:193-196).  A guided path decides on the
+        // throughput it would have had under BSDF sampling: its own throughput
+        // is small exactly where the guide sent it towards bright light, and
+        // rouletting on it would end the paths the guide is there to find.
+        const float surv = fminf((Guided && rr_w) ? *rr_w : max3(T), 0.95f);
         if (rng_next(rng) >= surv) return false;
         T = T / surv;
+        if (Guided && rr_w) *rr_w /= surv;
     }
-    if (gv.rec && !bs.delta) {
-        // training record: where, which way, with which pdf, and the throughput
-        // that scales everything found along this direction
+    if (Guided && gv.rec && !bs.delta) {
+        // training record: where, which way, with which pdf, the throughput
+        // that scales everything found along this direction, |cos| to the normal
         gv.rec[0] = make_float4(hp.x, hp.y, hp.z, bs.pdf);
         gv.rec[1] = make_float4(nd.x, nd.y, nd.z, 1.0f);
-        gv.rec[2] = make_float4(T.x, T.y, T.z, 0.0f);
+        gv.rec[2] = make_float4(T.x, T.y, T.z, fabsf(dot(N, nd)));
     }
     return true;
 }
 
 // 5 blocks of 128 per SM (96 registers): the register-limited occupancy of 4
 // left too few warps to cover the material and vertex fetches.
+template <bool Guided>
 __global__ void __launch_bounds__(128, 5) k_shade(WaveParams P, int q, int depth, int s0) {
     const uint32_t cap = static_cast<uint32_t>(P.npath);
     const uint32_t n = min(P.counts[q], cap);
@@ -551,6 +569,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(WaveParams P, int q, int depth
         const uint32_t p = P.queue[q][i];
         if (p >= cap) { atomicOr(P.err, kErrQueueOverflow); continue; }
         const float4 o4 = P.ray_o[q][i];
+        float rr_w = o4.w;
         const float4 d4 = P.ray_d[q][i];
         const float4 h = P.hit[i];
         const float4 thr = P.thr[p];
@@ -568,8 +587,8 @@ __global__ void __launch_bounds__(128, 5) k_shade(WaveParams P, int q, int depth
         rng.s = P.rng[p];
         f3 no = mk(0.0f), nd = mk(0.0f);
         QueueSink sink{P, p};
-        GuideVertex gv{P.gmix ? P.gmix + static_cast<size_t>(i) * kGMix : nullptr, nullptr, P.galpha};
-        if (P.grec) {
+        GuideVertex gv{Guided && P.gmix ? P.gmix + static_cast<size_t>(i) * kGMix : nullptr, nullptr, P.galpha};
+        if (Guided && P.grec) {
             gv.rec = P.grec + (static_cast<size_t>(depth) * P.npath + p) * 4;
             gv.rec[1].w = 0.0f;
             if (depth > 0) {
@@ -583,8 +602,8 @@ __global__ void __launch_bounds__(128, 5) k_shade(WaveParams P, int q, int depth
                 }
             }
         }
-        const bool cont = shade_path(P.scene, P.arg_rtl, depth, last, f3of(o4), f3of(d4), h, T, last_pdf,
-                                     last_delta, L, rng, no, nd, sink, gv) && !last;
+        const bool cont = shade_path<Guided>(P.scene, P.arg_rtl, depth, last, f3of(o4), f3of(d4), h, T, last_pdf,
+                                             last_delta, L, rng, no, nd, sink, gv, &rr_w) && !last;
         P.thr[p] = f4of(T, last_pdf);
         P.lo[p] = f4of(L, last_delta ? 1.0f : 0.0f);
         P.rng[p] = rng.s;
@@ -592,7 +611,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(WaveParams P, int q, int depth
         if (cont) {
             if (j < cap) {
                 P.queue[q ^ 1][j] = p;
-                P.ray_o[q ^ 1][j] = f4of(no, 0.0f);
+                P.ray_o[q ^ 1][j] = f4of(no, rr_w);
                 P.ray_d[q ^ 1][j] = f4of(nd, 0.0f);
             } else {
                 atomicOr(P.err, kErrQueueOverflow);
@@ -677,7 +696,8 @@ __global__ void __launch_bounds__(256) k_finalize(WaveParams P, int s0, int coun
 // Turn this pass's guide records into training samples: for each recorded
 // vertex, the incident radiance along its sampled direction is the part of the
 // path's final estimate gathered after it, divided by the throughput after it
-// (luminance, clamped like a sample); weight = L_in / p.  Records are cleared.
+// (luminance, clamped like a sample); weight = L_in |cos| / p, so the guide
+// learns the cosine-weighted incident radiance.  Records are cleared.
 __global__ void __launch_bounds__(256) k_guide_collect(WaveParams P, int npaths, GuideNet net, GuideSample* out,
                                                        uint32_t* count, uint32_t cap) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npaths; p += gridDim.x * blockDim.x) {
@@ -695,7 +715,7 @@ __global__ void __launch_bounds__(256) k_guide_collect(WaveParams P, int npaths,
                 const f3 S = f3of(r[3]);
                 const f3 Lin = mk(Ta.x > 0.0f ? (Lf.x - S.x) / Ta.x : 0.0f, Ta.y > 0.0f ? (Lf.y - S.y) / Ta.y : 0.0f,
                                   Ta.z > 0.0f ? (Lf.z - S.z) / Ta.z : 0.0f);
-                const float lum = fminf(fmaxf(luminance(Lin), 0.0f), 100.0f);
+                const float lum = fminf(fmaxf(luminance(Lin), 0.0f), 100.0f) * r[2].w;
                 w = r0.w > 0.0f ? lum / r0.w : 0.0f;
                 if (!(w < 1e30f)) w = 0.0f;
             }
@@ -856,7 +876,7 @@ int wavefront_prepare(Wavefront& wf, int device, int npath, int n_slots) {
         wf.sms = sms;
         wf.grid_raygen = grid_for(reinterpret_cast<const void*>(k_raygen), 256, sms);
         wf.grid_extend = grid_for(reinterpret_cast<const void*>(k_extend), 128, sms);
-        wf.grid_shade = grid_for(reinterpret_cast<const void*>(k_shade), 128, sms);
+        wf.grid_shade = grid_for(reinterpret_cast<const void*>(k_shade<false>), 128, sms);
         wf.grid_shadow = grid_for(reinterpret_cast<const void*>(k_shadow), 128, sms);
         wf.grid_finalize = grid_for(reinterpret_cast<const void*>(k_finalize), 256, sms);
         wf.device = device;
@@ -947,7 +967,10 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
                                                                             P.ray_d[q], P.hit, gs->mix);
                     })) return rc;
             }
-            if (int rc = timed(1, [&] { k_shade<<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0); })) return rc;
+            if (int rc = timed(1, [&] {
+                    if (P.gmix) k_shade<true><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                    else k_shade<false><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                })) return rc;
             if (int rc = timed(2, [&] { k_shadow<<<wf.grid_shadow, 128, 0, st>>>(P); })) return rc;
         }
         if (int rc = timed(3, [&] { k_finalize<<<wf.grid_finalize, 256, 0, st>>>(P, s0, count); })) return rc;
@@ -1202,7 +1225,7 @@ int prepare_wave(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scen
     P.f_new = static_cast<float4*>(film->fresh);
     if (guided) {
         if (gs->device != s->dev.device) { set_error("guide and scene live on different devices"); return PT_ERR_INVALID; }
-        if (int rc = guide_prepare_work(*gs, npath, prm->max_depth)) return rc;
+        if (int rc = guide_prepare_work(*gs, npath, prm->max_depth, gs->mode == PT_GUIDE_TRAIN)) return rc;
         P.gmix = gs->mix;
         P.galpha = gs->alpha;
         P.grec = gs->mode == PT_GUIDE_TRAIN ? gs->rec : nullptr;

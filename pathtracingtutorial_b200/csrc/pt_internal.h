@@ -37,10 +37,10 @@ constexpr float kTwoPi  = 6.28318530717958647692f;
 // deeper than this are rejected at build time, and the kernels still guard.
 constexpr int kStackDepth = 64;
 // Default path slots of the wavefront (pt_render_settings.paths_in_flight = 0):
-// about 260 B of path state each with two light slots (8.7 GB).  With a
-// guide attached the training records (64 B per path and bounce) cap it.
+// about 260 B of path state each with two light slots (8.7 GB).  A guide
+// that samples adds its mixture per path (160 B; 2.7 GB at 2^24 paths).
 constexpr int64_t kDefaultPathsInFlight = int64_t(1) << 25;
-constexpr int64_t kGuidedPathsInFlight = int64_t(1) << 22;
+constexpr int64_t kGuidedPathsInFlight = int64_t(1) << 24;
 // While a guide trains, passes stay small: every pass ends with optimiser
 // steps, so smaller passes mean more steps per sample.
 constexpr int64_t kTrainingPathsInFlight = int64_t(1) << 20;
