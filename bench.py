@@ -192,23 +192,31 @@ def reference_arm(args):
 
 
 def cpu_baseline(sa, spp, seconds):
-    """Reference CPU path timed on this host (rank 0, N=1): bounded row sample."""
+    """Reference CPU path timed on this host (rank 0, N=1): a bounded sample of
+    the workload -- every k-th row, k chosen so one frame takes a fraction of
+    `seconds`, then consecutive frames (sample indices as in the full render)
+    until `seconds` of CPU time have been spent."""
     import numpy as np
     from oracle.pyoracle import Oracle, RefHarness
     cores = os.cpu_count() or 1
     st = np.array([spp, sa.sample_per_frame, sa.max_depth, sa.sampler], np.int32)
     h = int(sa.camera["height"])
-    frames = 1
+    max_frames = max(1, spp // sa.sample_per_frame)
+    rays = secs = paths = 0.0
+    frames = 0
     if RefHarness.available():
         R = RefHarness()
         _, _, cal = R.render(sa.vertices, sa.faces, sa.materials, sa.camera, st, sa.env, num_frames=1, row0=0,
                              row_step=max(1, h // 8), threads=cores)
         per_row = cal["seconds"] / len(range(0, h, max(1, h // 8)))
-        stride = max(1, int(h / max(1.0, seconds / max(per_row, 1e-6))))
-        # a whole image of one frame is shorter than the sample: render more frames
-        frames = max(1, min(spp // sa.sample_per_frame, int(seconds / max(per_row * h / stride, 1e-6))))
-        _, _, s = R.render(sa.vertices, sa.faces, sa.materials, sa.camera, st, sa.env, num_frames=frames, row0=1,
-                           row_step=stride, threads=cores)
+        stride = max(1, int(h / max(1.0, 0.25 * seconds / max(per_row, 1e-6))))
+        while secs < seconds and frames < max_frames:
+            _, _, s = R.render(sa.vertices, sa.faces, sa.materials, sa.camera, st, sa.env, first_frame=frames,
+                               num_frames=1, row0=1, row_step=stride, threads=cores)
+            rays += s["closest_rays"] + s["shadow_rays"]
+            secs += s["seconds"]
+            paths += s["paths"]
+            frames += 1
         kind = "reference"
     else:
         O = Oracle()
@@ -216,12 +224,12 @@ def cpu_baseline(sa, spp, seconds):
         stride = max(1, h // 16)
         _, s = O.render(prep, sa.sample_per_frame, sa.max_depth, sa.sampler, frames=1, precision=32, rtl=1,
                         row0=1, row_step=stride, threads=cores)
+        rays, secs, paths, frames = s["closest_rays"] + s["shadow_rays"], s["seconds"], s["paths"], 1
         kind = "port"
-    rays = s["closest_rays"] + s["shadow_rays"]
-    return {"value": round(rays / s["seconds"] / 1e6, 3), "unit": METRIC, "cores": cores, "kind": kind,
+    return {"value": round(float(rays / secs / 1e6), 3), "unit": METRIC, "cores": cores, "kind": kind,
             "sample": f"every {stride}th row of {int(sa.camera['width'])}x{h}, {frames * sa.sample_per_frame} spp "
-                      f"({frames} frames of {sa.sample_per_frame}), {int(s['paths'])} paths, {int(rays)} rays, "
-                      f"{s['seconds']:.1f} s"}
+                      f"({frames} frames of {sa.sample_per_frame}), {int(paths)} paths, {int(rays)} rays, "
+                      f"{secs:.1f} s"}
 
 
 def convergence(local: int, stream, small: bool):
@@ -230,7 +238,8 @@ def convergence(local: int, stream, small: bool):
     sample indices, each arm timed with CUDA events; the guide trains online
     for 64 spp (timed) before it renders.  Time to relMSE 1e-3 is extrapolated
     with relMSE ~ 1/time (both estimators are unbiased), after subtracting the
-    reference's own noise (estimated from the plain arm: relMSE x spp / 4096)."""
+    reference's own noise (estimated from the plain arm, whose relMSE is its
+    own noise c / spp plus the reference's c / 4096)."""
     import numpy as np
     import torch
     import pathtracingtutorial_b200 as pt
@@ -278,7 +287,8 @@ def convergence(local: int, stream, small: bool):
     t_guided = timed(lambda: rg.render_frames(n_guided // spf))
     e_guided = relmse(rg.download_current_image())
     g.close()
-    e_ref = e_plain * n_plain / n_ref
+    # plain: e_plain = c / n_plain + c / n_ref (its own noise plus the reference's)
+    e_ref = e_plain * n_plain / (n_plain + n_ref)
     tp = t_plain * max(e_plain - e_ref, 1e-12) / 1e-3
     tg = t_train + t_guided * max(e_guided - e_ref, 1e-12) / 1e-3
     return {"scene": f"hidden_light_room {len(sa.faces)} tri, {w}x{w}, depth {sa.max_depth}, sobol",

@@ -259,7 +259,15 @@ __device__ __forceinline__ f3 mix_sample(const float* mix, float u0, float u1, f
 // ---------------------------------------------------------------------------
 // Inference over a ray queue: position = hit point of queue entry i.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_guide_infer(GuideNet net, const uint32_t* counts, int q, uint32_t cap,
+// 4 warps share one copy of the weights in shared memory; 4 blocks per SM
+// (up to 128 registers a thread).  8-warp blocks at 4 per SM left too little
+// of the SM's unified L1/shared storage for the L1 cache that serves the
+// hash-grid gathers and ran 15 % slower; 5 blocks at 69 registers ran 10 %
+// slower.
+constexpr int kGInferWarps = 4;
+constexpr int kGInferBlocksPerSm = 4;
+__global__ void __launch_bounds__(32 * kGInferWarps, kGInferBlocksPerSm)
+k_guide_infer(GuideNet net, const uint32_t* counts, int q, uint32_t cap,
                                                      const float4* ray_o, const float4* ray_d, const float4* hit,
                                                      float* mix_out) {
     extern __shared__ __align__(16) unsigned char g_smem[];
@@ -619,7 +627,7 @@ __global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSa
 // Adam on the MLP weights (FP32 master -> BF16 copy) and the hash grid
 // (FP32 master -> FP16 copy); gradients are cleared.
 // dynamic shared memory of the two network kernels (4 warps per CTA)
-constexpr int kGInferSmem = kGSmemW * 2 + 4 * 16 * kGOutPad * 4;
+constexpr int kGInferSmem = kGSmemW * 2 + kGInferWarps * 16 * kGOutPad * 4;
 constexpr int kGTrainSmem = (2 * kGSmemW + 64) * 2 + kGWeights * 4 + 4 * kGWarpScratch;
 static_assert(kGTrainSmem <= 227 * 1024, "training kernel shared memory");
 static_assert(((2 * kGSmemW + 64) * 2) % 16 == 0 && (kGWeights * 4) % 16 == 0 && kGWarpScratch % 16 == 0,

@@ -569,7 +569,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(WaveParams P, int q, int depth
         const uint32_t p = P.queue[q][i];
         if (p >= cap) { atomicOr(P.err, kErrQueueOverflow); continue; }
         const float4 o4 = P.ray_o[q][i];
-        float rr_w = o4.w;
+        float rr_w = Guided ? o4.w : 1.0f;
         const float4 d4 = P.ray_d[q][i];
         const float4 h = P.hit[i];
         const float4 thr = P.thr[p];
@@ -611,7 +611,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(WaveParams P, int q, int depth
         if (cont) {
             if (j < cap) {
                 P.queue[q ^ 1][j] = p;
-                P.ray_o[q ^ 1][j] = f4of(no, rr_w);
+                P.ray_o[q ^ 1][j] = f4of(no, Guided ? rr_w : 1.0f);
                 P.ray_d[q ^ 1][j] = f4of(nd, 0.0f);
             } else {
                 atomicOr(P.err, kErrQueueOverflow);
@@ -962,7 +962,8 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
             if (int rc = timed(0, [&] { k_extend<<<wf.grid_extend, 128, 0, st>>>(P, q, d); })) return rc;
             if (infer) {
                 if (int rc = timed(4, [&] {
-                        k_guide_infer<<<wf.sms * 4, 128, kGInferSmem, st>>>(gs->net, P.counts, q,
+                        k_guide_infer<<<wf.sms * kGInferBlocksPerSm, 32 * kGInferWarps, kGInferSmem, st>>>(
+                                                                            gs->net, P.counts, q,
                                                                             static_cast<uint32_t>(P.npath), P.ray_o[q],
                                                                             P.ray_d[q], P.hit, gs->mix);
                     })) return rc;
@@ -1461,6 +1462,10 @@ struct pt_guide {
 
 namespace ptb {
 
+// 4 warps; its dynamic shared memory (weights + 4 output tiles) stays under
+// the 48 KB that needs no opt-in.
+constexpr int kGEvalSmem = kGSmemW * 2 + 4 * 16 * kGOutPad * 4;
+static_assert(kGEvalSmem <= 48 * 1024, "guide eval shared memory");
 __global__ void __launch_bounds__(128) k_guide_eval(GuideNet net, const float* qd, uint32_t n, float* out) {
     extern __shared__ __align__(16) unsigned char g_smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(g_smem);
@@ -1577,7 +1582,8 @@ int guide_backward(pt_guide* h, const float* samples, uint32_t n, float* wgrad, 
         GuideNet net = h->g.net;
         net.loss = nullptr;   // leave the training-loss record alone
         k_guide_train<<<148, 128, kGTrainSmem>>>(net, ds, dn, n, 0, 1);
-        e = cudaDeviceSynchronize();
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
     }
     if (e == cudaSuccess) e = cudaMemcpy(wgrad, h->g.net.w_grad, kGWeights * sizeof(float), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && ggrad) e = cudaMemcpy(ggrad, h->g.net.grid_grad, ng * sizeof(float2), cudaMemcpyDeviceToHost);
@@ -1598,8 +1604,9 @@ int guide_eval(pt_guide* h, const float* qd, uint32_t n, float* out) {
     if (cudaMalloc(&dout, static_cast<size_t>(n) * 4) != cudaSuccess) { cudaFree(dq); cudaGetLastError(); set_error("alloc"); return PT_ERR_NOMEM; }
     cudaError_t e = cudaMemcpy(dq, qd, static_cast<size_t>(n) * 24, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
-        k_guide_eval<<<148, 128, kGInferSmem>>>(h->g.net, dq, n, dout);
-        e = cudaMemcpy(out, dout, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost);
+        k_guide_eval<<<148, 128, kGEvalSmem>>>(h->g.net, dq, n, dout);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(out, dout, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost);
     }
     cudaFree(dq);
     cudaFree(dout);
