@@ -51,6 +51,8 @@ def parse_args():
     p.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true",
                    help="skip the CPU baseline leg (profiling runs; the line then carries cpu_baseline null)")
+    p.add_argument("--workload", choices=["render", "batch"], default="render",
+                   help="render: the bench line; batch: the 64-scene uneven batch in one launch (a separate line)")
     p.add_argument("--no-convergence", action="store_true",
                    help="skip the guided-vs-plain convergence leg (the line then carries convergence null)")
     return p.parse_args()
@@ -444,9 +446,58 @@ def ours(args):
         dist.destroy_process_group()
 
 
+def batch_workload(args):
+    """--workload batch: the uneven batch (64 scenes like the icosphere field,
+    triangles log-uniform in 1k..2M, resolutions from {256^2, 512^2, 1024^2,
+    1280x720}, 16..512 spp, depth 12, one shared sky) rendered by one
+    pt.render_batch call (the autotuner picks persistent or wavefront mode on
+    a first call), against rendering the 64 scenes one after another with
+    pt.render.  Wall time of each call (it returns host images), rays counted
+    by the kernels."""
+    import torch
+    import pathtracingtutorial_b200 as pt
+    from pathtracingtutorial_b200 import scenes
+    torch.cuda.set_device(0)
+    batch = scenes.uneven_batch(n_scenes=64)
+    ss = []
+    for sa in batch:
+        sc = sa.scene()
+        sc.build_accel()
+        sc.upload_to_device(0)
+        ss.append(sc)
+    items = [(sc, sa.spp) for sc, sa in zip(ss, batch)]
+    _, _, cfg = pt.render_batch(items, autotune=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, st, _ = pt.render_batch(items, block_size=cfg["block_size"], blocks_per_sm=cfg["blocks_per_sm"],
+                               chunk_spp=cfg["chunk_spp"], autotune=False, mode=cfg["mode"],
+                               paths_in_flight=cfg["paths_in_flight"])
+    t_batch = time.perf_counter() - t0
+    rays = st["camera_rays"] + st["extension_rays"] + st["shadow_rays"]
+    t0 = time.perf_counter()
+    rays_seq = 0
+    for sc, sa in zip(ss, batch):
+        _, s1 = pt.render(sc, sa.spp, stats=True)
+        rays_seq += s1["camera_rays"] + s1["extension_rays"] + s1["shadow_rays"]
+    t_seq = time.perf_counter() - t0
+    mode = {pt.BATCH_PERSISTENT: "persistent", pt.BATCH_WAVEFRONT: "wavefront"}.get(cfg["mode"], str(cfg["mode"]))
+    print(json.dumps({
+        "metric": METRIC, "workload": "uneven batch: 64 scenes, %d triangles, %d pixels x spp, depth 12"
+        % (sum(len(sa.faces) for sa in batch), st["paths"]),
+        "value": round(rays / t_batch / 1e6, 2), "unit": METRIC, "seconds": round(t_batch, 3),
+        "paths": int(st["paths"]), "rays": int(rays),
+        "sequential": {"value": round(rays_seq / t_seq / 1e6, 2), "seconds": round(t_seq, 3)},
+        "batch_speedup": round(t_seq / t_batch, 3),
+        "autotuned": {"mode": mode, "block_size": cfg["block_size"], "blocks_per_sm": cfg["blocks_per_sm"],
+                      "chunk_spp": cfg["chunk_spp"], "paths_in_flight": cfg["paths_in_flight"],
+                      "tuned_ms": round(cfg["tuned_ms"], 2)}}))
+
+
 def main():
     args = parse_args()
-    if args.impl == "reference":
+    if args.workload == "batch":
+        batch_workload(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         ours(args)

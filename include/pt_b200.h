@@ -257,7 +257,9 @@ int pt_renderer_reset_accumulation(pt_film* film, pt_scene* scene);             
 /* Frame counter that drives sample indices (DeviceScene::frameCount, device_scene.h:97). */
 int pt_scene_set_frame_count(pt_scene* scene, uint32_t frame_count);
 /* render(scene, spp) -> HDR image: build (if needed), upload (if needed), render
- * spp samples per pixel, write width*height*4 floats (RGBA, row y at y*width*4). */
+ * spp samples per pixel, write width*height*4 floats (RGBA, row y at y*width*4).
+ * Keeps a film per scene and one integrator per device shared by all scenes;
+ * concurrent pt_render calls are serialised. */
 int pt_render(pt_scene* scene, int32_t spp, float* out_rgba, int32_t out_is_device,
               pt_render_stats* stats);
 

@@ -36,14 +36,23 @@ using namespace ptb;
 namespace {
 
 // Per-scene render state reused by pt_render (film + integrator).
+// pt_render keeps a film per scene and ONE integrator per device for all
+// scenes: the integrator's wavefront state is sized for the largest pass
+// (up to 2^25 paths, several GB), so one per scene would run a process that
+// renders many scenes out of device memory.  pt_render calls are serialised
+// by g_render_mu (each is synchronous anyway).
 struct RenderCache {
-    pt_film*       film = nullptr;
-    pt_integrator* integ = nullptr;
+    pt_film* film = nullptr;
 };
 
 std::mutex g_cache_mu;
+std::mutex g_render_mu;
 std::unordered_map<pt_scene*, RenderCache>& caches() {
     static std::unordered_map<pt_scene*, RenderCache> m;
+    return m;
+}
+std::unordered_map<int, pt_integrator*>& device_integrators() {
+    static std::unordered_map<int, pt_integrator*> m;
     return m;
 }
 
@@ -52,7 +61,6 @@ void drop_cache(pt_scene* s) {
     auto it = caches().find(s);
     if (it == caches().end()) return;
     if (it->second.film) { film_free(it->second.film); delete it->second.film; }
-    if (it->second.integ) { integrator_free(it->second.integ); delete it->second.integ; }
     caches().erase(it);
 }
 
@@ -381,6 +389,7 @@ int pt_render(pt_scene* s, int32_t spp, float* out_rgba, int32_t out_is_device, 
     const int dev = s->dev.device;
     const int w = s->host.camera.width, h = s->host.camera.height;
     PT_REQUIRE(w > 0 && h > 0, "camera resolution must be positive");
+    std::lock_guard<std::mutex> render_lock(g_render_mu);
     RenderCache rcache;
     {
         std::lock_guard<std::mutex> lk(g_cache_mu);
@@ -392,23 +401,24 @@ int pt_render(pt_scene* s, int32_t spp, float* out_rgba, int32_t out_is_device, 
     if (!rcache.film) {
         if (int rc = pt_film_create(w, h, dev, &rcache.film)) return rc;
     }
-    if (!rcache.integ) {
-        if (int rc = pt_integrator_create("path", &rcache.integ)) return rc;
-    }
     {
         std::lock_guard<std::mutex> lk(g_cache_mu);
         caches()[s] = rcache;
     }
+    pt_integrator*& integ = device_integrators()[dev];
+    if (!integ) {
+        if (int rc = pt_integrator_create("path", &integ)) return rc;
+    }
     if (int rc = pt_renderer_reset_accumulation(rcache.film, s)) return rc;
-    pt_integrator_reset_stats(rcache.integ);
+    pt_integrator_reset_stats(integ);
     const int spf = s->host.settings.sample_per_frame;
     // Renderer::renderAll: whole batches until frameCount * spf >= spp, here
     // all of them in one launch (the same samples, in the same order)
     const int64_t frames = (static_cast<int64_t>(spp) + spf - 1) / spf;
-    if (int rc = pt_renderer_render_frames(rcache.integ, rcache.film, s, static_cast<uint32_t>(frames), nullptr)) return rc;
-    if (int rc = integrator_check(rcache.integ, true)) return rc;
+    if (int rc = pt_renderer_render_frames(integ, rcache.film, s, static_cast<uint32_t>(frames), nullptr)) return rc;
+    if (int rc = integrator_check(integ, true)) return rc;
     if (int rc = film_download(rcache.film, out_rgba, false, out_is_device == 0)) return rc;
-    if (stats) integrator_stats(rcache.integ, stats);
+    if (stats) integrator_stats(integ, stats);
     return device_sync(dev);
     PT_GUARD_END
 }
