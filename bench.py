@@ -51,8 +51,13 @@ def parse_args():
     p.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true",
                    help="skip the CPU baseline leg (profiling runs; the line then carries cpu_baseline null)")
-    p.add_argument("--workload", choices=["render", "batch"], default="render",
-                   help="render: the bench line; batch: the 64-scene uneven batch in one launch (a separate line)")
+    p.add_argument("--paths-in-flight", type=int, default=0,
+                   help="wavefront path slots of the render (0: the library default)")
+    p.add_argument("--workload", choices=["render", "batch", "large"], default="render",
+                   help="render: the bench line; batch: the 64-scene uneven batch in one launch; large: the "
+                        "20M-triangle 16-camera case (separate lines)")
+    p.add_argument("--large-spp", type=int, default=32, help="samples per pixel per camera of --workload large")
+    p.add_argument("--large-train-spp", type=int, default=16, help="guide training spp of --workload large")
     p.add_argument("--no-convergence", action="store_true",
                    help="skip the guided-vs-plain convergence leg (the line then carries convergence null)")
     return p.parse_args()
@@ -326,6 +331,8 @@ def ours(args):
     sa = workload(args.small)
     spp = args.spp
     scene = sa.scene()
+    if args.paths_in_flight > 0:
+        scene.update_settings(paths_in_flight=args.paths_in_flight)
     scene.build_accel()
     scene.upload_to_device(local)
     spf = sa.sample_per_frame
@@ -410,6 +417,10 @@ def ours(args):
         if dist is not None:
             dist.destroy_process_group()
         return
+    # release this render's wavefront state (tens of GB) before the next legs
+    renderer.integrator.close()
+    renderer.film.close()
+    del renderer
     conv = None
     if world == 1 and not args.no_convergence:
         with torch.cuda.stream(stream):
@@ -493,10 +504,69 @@ def batch_workload(args):
                       "tuned_ms": round(cfg["tuned_ms"], 2)}}))
 
 
+def large_workload(args):
+    """--workload large: the combined large case -- about 20M triangles
+    (displaced icospheres and tetrahedral clutter, flattened), Disney
+    materials, the synthetic sky and 32 small area lights, 16 cameras at
+    1920x1080, depth 16 -- rendered as ONE batch of 16 camera items of the one
+    uploaded scene, plain and guided (the guide trained online on the first
+    camera first).  --large-spp samples per pixel per camera (the full case
+    is 512)."""
+    import torch
+    import pathtracingtutorial_b200 as pt
+    from pathtracingtutorial_b200 import scenes
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    sa, cams = scenes.large_scene()
+    t_gen = time.perf_counter() - t0
+    scene = sa.scene()
+    t0 = time.perf_counter()
+    scene.build_accel()
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    scene.upload_to_device(0)
+    t_upload = time.perf_counter() - t0
+    info = scene.info()
+    spp = args.large_spp
+    items = [(scene, spp, 0, c) for c in cams]
+    pt.render_batch([(scene, 4, 0, c) for c in cams[:2]], mode=pt.BATCH_WAVEFRONT)   # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, st, cfg = pt.render_batch(items, mode=pt.BATCH_WAVEFRONT)
+    t_plain = time.perf_counter() - t0
+    rays = st["camera_rays"] + st["extension_rays"] + st["shadow_rays"]
+    g = pt.Guide(scene, seed=1)
+    r = pt.Renderer(scene)
+    g.attach(r.integrator, pt.Guide.TRAIN)
+    r.reset_accumulation()
+    scene.set_frame_count(100_000)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r.render_frames(max(1, args.large_train_spp // sa.sample_per_frame))
+    r.synchronize()
+    t_train = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    _, stg, _ = pt.render_batch([(scene, spp, 0, c, g) for c in cams])
+    t_guided = time.perf_counter() - t0
+    rays_g = stg["camera_rays"] + stg["extension_rays"] + stg["shadow_rays"]
+    g.close()
+    print(json.dumps({
+        "metric": METRIC, "workload": f"large scene {info['num_faces']} tri (BVH {info['num_bvh_nodes']} nodes, depth "
+                                      f"{info['bvh_max_depth']}), 16 cameras 1920x1080, {spp} spp each, depth 16",
+        "host_seconds": {"generate": round(t_gen, 1), "bvh_build": round(t_build, 1), "upload": round(t_upload, 2)},
+        "device_bytes": int(info["device_bytes"]),
+        "plain": {"value": round(rays / t_plain / 1e6, 2), "unit": METRIC, "seconds": round(t_plain, 3),
+                  "paths": int(st["paths"]), "rays": int(rays)},
+        "guided": {"value": round(rays_g / t_guided / 1e6, 2), "unit": METRIC, "seconds": round(t_guided, 3),
+                   "train_spp": args.large_train_spp, "train_seconds": round(t_train, 3), "rays": int(rays_g)}}))
+
+
 def main():
     args = parse_args()
     if args.workload == "batch":
         batch_workload(args)
+    elif args.workload == "large":
+        large_workload(args)
     elif args.impl == "reference":
         reference_arm(args)
     else:

@@ -150,7 +150,7 @@ typedef struct pt_render_settings {
     uint32_t pcg_seed;          /* added knob; 0 reproduces the reference seeding */
     int32_t  arg_order;         /* PT_ARGS_*                                      */
     int32_t  flags;             /* PT_FLAG_*                                      */
-    int32_t  paths_in_flight;   /* added: wavefront path slots (0 = 2^23); samples of a
+    int32_t  paths_in_flight;   /* added: wavefront path slots (0 = 2^27); samples of a
                                    frame run concurrently while they fit.  Results do
                                    not depend on it. */
 } pt_render_settings;
@@ -267,6 +267,7 @@ int pt_render(pt_scene* scene, int32_t spp, float* out_rgba, int32_t out_is_devi
  *      scene per process).  Many scenes of uneven size and sample budget are
  *      rendered by ONE persistent kernel launch captured in a CUDA graph; launch
  *      shape and chunking come from the built-in autotuner unless fixed in cfg. */
+typedef struct pt_guide pt_guide;
 typedef struct pt_batch_item {
     pt_scene* scene;        /* built and uploaded; all items on one device          */
     int32_t   spp;          /* samples per pixel for this item                       */
@@ -274,6 +275,10 @@ typedef struct pt_batch_item {
     uint32_t  first_frame;  /* frame index of the first sample (sample offset)       */
     int32_t   _pad;
     float*    out_rgba;     /* width*height*4 floats (host, or device, 16 B aligned) */
+    const pt_camera* camera;/* NULL: the scene's camera; else this item's camera and
+                               resolution (many cameras of one scene in one batch)   */
+    pt_guide* guide;        /* NULL: BSDF sampling; else sample with this trained
+                               guide (wavefront mode only; the guide is only read)  */
 } pt_batch_item;
 
 typedef struct pt_batch_config {
@@ -283,7 +288,7 @@ typedef struct pt_batch_config {
     int32_t autotune;       /* 1: time candidate shapes (cached per batch class) */
     float   tuned_ms;       /* out: calibration time of the chosen shape */
     int32_t mode;           /* PT_BATCH_AUTO / _PERSISTENT / _WAVEFRONT; out: the mode used */
-    int32_t paths_in_flight;/* wavefront mode: path slots shared by all items (0: 2^25) */
+    int32_t paths_in_flight;/* wavefront mode: path slots shared by all items (0: 2^27) */
     int32_t _pad;
 } pt_batch_config;
 /* Batch modes.  PERSISTENT: one persistent kernel traces whole paths of all
@@ -306,7 +311,6 @@ int pt_render_batch(const pt_batch_item* items, uint32_t n, int32_t out_is_devic
 #define PT_GUIDE_OFF   0
 #define PT_GUIDE_USE   1   /* sample with the network, do not train      */
 #define PT_GUIDE_TRAIN 2   /* sample with it and train after every pass  */
-typedef struct pt_guide pt_guide;
 int pt_guide_create(pt_scene* scene, uint32_t seed, pt_guide** out);   /* scene must be uploaded */
 int pt_guide_destroy(pt_guide* guide);
 int pt_guide_set_learning_rate(pt_guide* guide, float lr);

@@ -480,17 +480,23 @@ BATCH_AUTO, BATCH_PERSISTENT, BATCH_WAVEFRONT = _ffi.BATCH_AUTO, _ffi.BATCH_PERS
 
 def render_batch(items, block_size: int = 0, blocks_per_sm: int = 0, chunk_spp: int = 0, autotune: bool = True,
                  mode: int = BATCH_AUTO, paths_in_flight: int = 0):
-    """Render [(scene, spp[, first_frame])...] in one graph launch: one
-    persistent kernel over all items, or every item's wavefront as a parallel
-    graph branch (mode; AUTO lets the autotuner time both).
+    """Render [(scene, spp[, first_frame[, camera[, guide]]])...] in one graph
+    launch: one persistent kernel over all items, or every item's wavefront as
+    a parallel graph branch (mode; AUTO lets the autotuner time both).  An
+    item's camera (a make_camera array; None: the scene's) sets its view and
+    resolution, so many cameras of one scene share its device data; an item
+    with a trained Guide samples with it (wavefront mode).
     Returns (list of (H, W, 4) images, stats dict, config dict)."""
     n = len(items)
     arr = (_ffi.BatchItem * n)()
     outs = []
+    keep = []
     for k, it in enumerate(items):
         scene, spp = it[0], it[1]
         first = it[2] if len(it) > 2 else 0
-        cam = scene.camera
+        icam = it[3] if len(it) > 3 else None
+        guide = it[4] if len(it) > 4 else None
+        cam = scene.camera if icam is None else icam
         img = np.zeros((int(cam["height"]), int(cam["width"]), 4), np.float32)
         outs.append(img)
         arr[k].scene = scene.handle
@@ -498,6 +504,12 @@ def render_batch(items, block_size: int = 0, blocks_per_sm: int = 0, chunk_spp: 
         arr[k].max_depth = -1
         arr[k].first_frame = int(first)
         arr[k].out_rgba = img.ctypes.data
+        if icam is not None:
+            c = np.ascontiguousarray(icam, CAMERA_DTYPE)
+            keep.append(c)
+            arr[k].camera = c.ctypes.data
+        if guide is not None:
+            arr[k].guide = guide._h
     cfg = _ffi.BatchConfig(block_size, blocks_per_sm, chunk_spp, 1 if autotune else 0, 0.0, int(mode),
                            int(paths_in_flight), 0)
     st = _ffi.RenderStats()

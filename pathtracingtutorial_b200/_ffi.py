@@ -95,7 +95,7 @@ class RenderStats(C.Structure):
 
 class BatchItem(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("spp", C.c_int32), ("max_depth", C.c_int32), ("first_frame", C.c_uint32),
-                ("_pad", C.c_int32), ("out_rgba", C.c_void_p)]
+                ("_pad", C.c_int32), ("out_rgba", C.c_void_p), ("camera", C.c_void_p), ("guide", C.c_void_p)]
 
 
 class BatchConfig(C.Structure):
@@ -107,7 +107,7 @@ class BatchConfig(C.Structure):
 BATCH_AUTO, BATCH_PERSISTENT, BATCH_WAVEFRONT = 0, 1, 2
 
 
-assert C.sizeof(SceneParams) == 88 and C.sizeof(CameraFrame) == 64 and C.sizeof(BatchItem) == 32
+assert C.sizeof(SceneParams) == 88 and C.sizeof(CameraFrame) == 64 and C.sizeof(BatchItem) == 48
 
 # (name, restype, argtypes) for every entry point declared in include/pt_b200.h
 _P = C.c_void_p

@@ -167,17 +167,21 @@ int max_blocks_per_sm(int block) {
     return v;
 }
 
+// The camera an item renders: its own, else its scene's.
+const pt_camera& item_camera(const pt_batch_item& it) { return it.camera ? *it.camera : it.scene->host.camera; }
+
 BatchPlan make_plan(const pt_batch_item* in, uint32_t n, uint32_t chunk_spp, int cap_spp) {
     BatchPlan plan;
     plan.items.resize(n);
     for (uint32_t k = 0; k < n; ++k) {
         const pt_scene* s = in[k].scene;
+        const pt_camera& cam = item_camera(in[k]);
         BatchItemDev& it = plan.items[k];
         std::memset(&it, 0, sizeof(it));
         it.scene = device_view(s);
-        it.cam = camera_frame(s->host.camera);
-        it.width = s->host.camera.width;
-        it.height = s->host.camera.height;
+        it.cam = camera_frame(cam);
+        it.width = cam.width;
+        it.height = cam.height;
         it.spp = cap_spp > 0 ? std::min(cap_spp, in[k].spp) : in[k].spp;
         it.spf = s->host.settings.sample_per_frame;
         it.max_depth = in[k].max_depth >= 0 ? in[k].max_depth : s->host.settings.max_depth;
@@ -206,6 +210,10 @@ struct BatchSlot {
     int             dup = 0;          // k-th item of the batch with this scene
     pt_integrator*  integ = nullptr;
     pt_film*        film = nullptr;
+    // a guided item samples through a view of its guide: the guide's network
+    // (read only), this slot's own mixture buffer -- items that share one
+    // guide run concurrently in the batch graph
+    GuideState      gview{};
 };
 std::mutex g_slot_mu;
 // one integrator + film per scene, reused across batches (heap cells: the
@@ -217,13 +225,15 @@ constexpr int kBatchBranches = 16;
 void slot_release(BatchSlot& sl) {
     if (sl.integ) { integrator_free(sl.integ); delete sl.integ; }
     if (sl.film) { film_free(sl.film); delete sl.film; }
+    sl.gview.params = nullptr;   // owned by the guide
+    guide_free(sl.gview);
     sl = BatchSlot{};
 }
 
-// Integrator and film for the dup-th batch item rendering scene s (its camera
-// size, its device); caller holds g_slot_mu.
-int batch_slot(const pt_scene* s, int dup, BatchSlot*& out) {
-    const int w = s->host.camera.width, h = s->host.camera.height, dev = s->dev.device;
+// Integrator and film for the dup-th batch item rendering scene s at w x h
+// on its device; caller holds g_slot_mu.
+int batch_slot(const pt_scene* s, int dup, int w, int h, BatchSlot*& out) {
+    const int dev = s->dev.device;
     out = nullptr;
     for (auto& cell : g_slots) {
         BatchSlot& sl = *cell;
@@ -274,7 +284,7 @@ int batch_wavefront(const pt_batch_item* in, uint32_t n, int out_is_device, int6
     if (int rc = side_streams(device, side)) return rc;
     double work_total = 0.0;
     for (uint32_t k = 0; k < n; ++k)
-        work_total += static_cast<double>(in[k].scene->host.camera.width) * in[k].scene->host.camera.height * in[k].spp;
+        work_total += static_cast<double>(item_camera(in[k]).width) * item_camera(in[k]).height * in[k].spp;
     std::vector<BatchSlot*> slots(n, nullptr);
     std::vector<WaveParams> P(n);
     std::vector<int64_t> total(n);
@@ -282,9 +292,39 @@ int batch_wavefront(const pt_batch_item* in, uint32_t n, int out_is_device, int6
         pt_scene* s = in[k].scene;
         int dup = 0;   // items sharing a scene need their own wavefront and film
         for (uint32_t j = 0; j < k; ++j) dup += in[j].scene == s ? 1 : 0;
-        if (int rc = batch_slot(s, dup, slots[k])) return rc;
+        const pt_camera& cam = item_camera(in[k]);
+        if (int rc = batch_slot(s, dup, cam.width, cam.height, slots[k])) return rc;
         pt_scene_params prm;
         if (int rc = pt_scene_build_params(s, &prm)) return rc;
+        if (in[k].camera) {
+            prm.camera = camera_frame(cam);
+            prm.width = cam.width;
+            prm.height = cam.height;
+        }
+        // guide view (or none) for this item's wavefront
+        if (!slots[k]->integ->wf) slots[k]->integ->wf = new Wavefront();
+        GuideState* gs_k = nullptr;
+        if (in[k].guide) {
+            const GuideState& g = guide_state(in[k].guide);
+            GuideState& v = slots[k]->gview;
+            if (v.device != g.device || v.net.w != g.net.w) {
+                v.params = nullptr;
+                guide_free(v);
+                v = GuideState{};
+                v.device = g.device;
+            }
+            v.net = g.net;
+            v.step = g.step;
+            v.alpha = g.alpha;
+            v.lr = g.lr;
+            v.mode = PT_GUIDE_USE;
+            gs_k = &v;
+        }
+        if (slots[k]->integ->wf->guide != gs_k) {
+            slots[k]->integ->wf->guide = gs_k;
+            Wavefront& wfk = *slots[k]->integ->wf;
+            if (wfk.graph) { cudaGraphExecDestroy(wfk.graph); wfk.graph = nullptr; wfk.graph_key.clear(); }
+        }
         if (in[k].max_depth >= 0) prm.max_depth = in[k].max_depth;
         const int64_t npix = static_cast<int64_t>(prm.width) * prm.height;
         total[k] = in[k].spp;
@@ -314,7 +354,7 @@ int batch_wavefront(const pt_batch_item* in, uint32_t n, int out_is_device, int6
         cudaStream_t bs = (*side)[k % branches];
         Wavefront& wf = *slots[k]->integ->wf;
         k_begin<<<1, 1, 0, bs>>>(P[k].pass, in[k].first_frame);
-        rc = enqueue_batch(wf, P[k], total[k], bs, nullptr, nullptr);
+        rc = enqueue_batch(wf, P[k], total[k], bs, nullptr, wf.guide);
         if (rc == PT_OK && write_out) {
             const int np = P[k].npix;
             float4* out = out_is_device ? reinterpret_cast<float4*>(in[k].out_rgba)
@@ -386,7 +426,7 @@ std::string tune_key(int device, const pt_batch_item* items, uint32_t n) {
     uint64_t tris = 0, pix = 0, spp = 0;
     for (uint32_t k = 0; k < n; ++k) {
         tris += items[k].scene->host.faces.size();
-        pix += static_cast<uint64_t>(items[k].scene->host.camera.width) * items[k].scene->host.camera.height;
+        pix += static_cast<uint64_t>(item_camera(items[k]).width) * item_camera(items[k]).height;
         spp += static_cast<uint64_t>(items[k].spp);
     }
     auto lg = [](uint64_t v) { int b = 0; while (v > 1) { v >>= 1; ++b; } return b; };
@@ -404,6 +444,14 @@ int render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batc
         if (!in[k].scene || !in[k].scene->dev.uploaded) { set_error("batch item " + std::to_string(k) + ": scene not uploaded"); return PT_ERR_STATE; }
         if (in[k].scene->dev.device != device) { set_error("batch items must live on one device"); return PT_ERR_INVALID; }
         if (in[k].spp <= 0 || !in[k].out_rgba) { set_error("batch item " + std::to_string(k) + ": invalid spp or output"); return PT_ERR_INVALID; }
+        if (in[k].camera && (in[k].camera->width <= 0 || in[k].camera->height <= 0)) {
+            set_error("batch item " + std::to_string(k) + ": camera resolution must be positive");
+            return PT_ERR_INVALID;
+        }
+        if (in[k].guide && guide_state(in[k].guide).device != device) {
+            set_error("batch item " + std::to_string(k) + ": guide lives on another device");
+            return PT_ERR_INVALID;
+        }
     }
     if (int rc = ensure_device(device)) return rc;
     int sms = 0;
@@ -423,10 +471,18 @@ int render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batc
     unsigned long long* d_stats = d_misc + 8;
     uint32_t* d_err = reinterpret_cast<uint32_t*>(d_misc + 32);
 
-    const int req_mode = cfg ? cfg->mode : PT_BATCH_AUTO;
+    int req_mode = cfg ? cfg->mode : PT_BATCH_AUTO;
     if (req_mode != PT_BATCH_AUTO && req_mode != PT_BATCH_PERSISTENT && req_mode != PT_BATCH_WAVEFRONT) {
         set_error("unknown batch mode");
         return PT_ERR_INVALID;
+    }
+    bool guided = false;
+    for (uint32_t k = 0; k < n; ++k) guided = guided || in[k].guide != nullptr;
+    if (guided) {
+        // the persistent kernel traces whole paths per thread and has no
+        // warp-wide network evaluation: guided items run in wavefront mode
+        if (req_mode == PT_BATCH_PERSISTENT) { set_error("guided batch items need wavefront mode"); return PT_ERR_INVALID; }
+        req_mode = PT_BATCH_WAVEFRONT;
     }
     const int64_t budget = cfg && cfg->paths_in_flight > 0 ? cfg->paths_in_flight : kDefaultPathsInFlight;
     auto run_wavefront = [&](float tuned_ms) -> int {

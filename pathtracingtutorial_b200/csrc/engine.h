@@ -63,6 +63,8 @@ struct DeviceSceneBuffers {
     void*    env_array = nullptr;          // cudaArray_t
     unsigned long long env_tex = 0;        // cudaTextureObject_t
     uint64_t bytes = 0;
+    size_t   sizes[11] = {};               // bytes of the buffers above, in declaration order
+    int      env_w = 0, env_h = 0;
 };
 
 // Default render settings (RenderSettings defaults, scene.h:16-22).

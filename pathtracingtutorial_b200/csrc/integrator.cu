@@ -1063,11 +1063,43 @@ static void pin_host_arrays(pt_scene* s) {
 
 int upload_scene(pt_scene* s, int device) {
     if (!s->tables.built) { set_error("scene not built: call pt_scene_build_accel first"); return PT_ERR_STATE; }
+    const HostScene& hs = s->host;
+    const SceneTables& ts = s->tables;
+    DeviceSceneBuffers& d = s->dev;
+    void** bufs[11] = {&d.inner, &d.tris, &d.vertices, &d.faces, &d.materials, &d.emissive, &d.tri_pmf,
+                       &d.tri_alias, &d.env_pmf, &d.env_alias, &d.punctual};
+    const void* srcs[11] = {ts.inner.data(), ts.tris.data(), hs.vertices.data(), hs.faces.data(),
+                            hs.materials.data(), ts.emissive.data(), ts.tri_pmf.data(), ts.tri_alias.data(),
+                            ts.env_pmf.data(), ts.env_alias.data(), hs.punctual.data()};
+    const size_t sizes[11] = {ts.inner.size() * sizeof(InnerNode), ts.tris.size() * sizeof(TriRecord),
+                              hs.vertices.size() * sizeof(pt_vertex), hs.faces.size() * sizeof(pt_face),
+                              hs.materials.size() * sizeof(pt_material), ts.emissive.size() * sizeof(pt_emissive_ref),
+                              ts.tri_pmf.size() * sizeof(float), ts.tri_alias.size() * sizeof(pt_alias_entry),
+                              ts.env_pmf.size() * sizeof(float), ts.env_alias.size() * sizeof(pt_alias_entry),
+                              hs.punctual.size() * sizeof(pt_punctual_light)};
+    // Same device and the same buffer sizes: copy into the existing buffers.
+    // The device addresses stay, so a render graph captured for them stays valid.
+    bool same = d.uploaded && d.device == device && d.env_w == hs.env_w && d.env_h == hs.env_h;
+    for (int i = 0; i < 11 && same; ++i) same = d.sizes[i] == sizes[i];
+    if (same) {
+        if (int rc = ensure_device(device)) return rc;
+        pin_host_arrays(s);
+        for (int i = 0; i < 11; ++i)
+            if (sizes[i]) PT_CU(cudaMemcpy(*bufs[i], srcs[i], sizes[i], cudaMemcpyHostToDevice));
+        if (hs.env_w > 0 && hs.env_h > 0) {
+            const size_t pitch = static_cast<size_t>(hs.env_w) * 4 * sizeof(float);
+            PT_CU(cudaMemcpy2DToArray(static_cast<cudaArray_t>(d.env_array), 0, 0, hs.env_rgba.data(), pitch, pitch,
+                                      hs.env_h, cudaMemcpyHostToDevice));
+        }
+        return PT_OK;
+    }
     free_scene_device(s);
     if (int rc = ensure_device(device)) return rc;
     pin_host_arrays(s);
-    DeviceSceneBuffers& d = s->dev;
     d.device = device;
+    for (int i = 0; i < 11; ++i) d.sizes[i] = sizes[i];
+    d.env_w = hs.env_w;
+    d.env_h = hs.env_h;
     auto up = [&](void** dst, const void* src, size_t bytes) -> int {
         if (bytes == 0) { *dst = nullptr; return PT_OK; }
         if (cudaMalloc(dst, bytes) != cudaSuccess) {
@@ -1204,9 +1236,16 @@ int prepare_wave(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scen
                    : (rs.paths_in_flight > 0 ? rs.paths_in_flight : kDefaultPathsInFlight);
     if (guided) budget = std::min<int64_t>(budget, gs->mode == PT_GUIDE_TRAIN ? kTrainingPathsInFlight
                                                                               : kGuidedPathsInFlight);
-    const int lanes = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(total, budget / npix)));
+    int lanes = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(total, budget / npix)));
+    // fewer samples in flight when the device cannot hold the path slots
+    // (results do not depend on the pass size)
+    int rc_alloc = wavefront_prepare(wf, s->dev.device, npix * lanes, n_slots);
+    while (rc_alloc == PT_ERR_NOMEM && lanes > 1) {
+        lanes /= 2;
+        rc_alloc = wavefront_prepare(wf, s->dev.device, npix * lanes, n_slots);
+    }
+    if (rc_alloc) return rc_alloc;
     const int npath = npix * lanes;
-    if (int rc = wavefront_prepare(wf, s->dev.device, npath, n_slots)) return rc;
     std::memset(&P, 0, sizeof(P));
     std::memcpy(&P, &wf.base, sizeof(P));
     const DeviceScene view = device_view(s);
@@ -1451,14 +1490,18 @@ int device_sync(int device) {
 
 }  // namespace ptb
 
-#include "batch.cuh"
-
 // ---------------------------------------------------------------------------
 // Guide handles
 // ---------------------------------------------------------------------------
 struct pt_guide {
     ptb::GuideState g;
 };
+
+namespace ptb {
+inline const GuideState& guide_state(const pt_guide* h) { return h->g; }
+}  // namespace ptb
+
+#include "batch.cuh"
 
 namespace ptb {
 

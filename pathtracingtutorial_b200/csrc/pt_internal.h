@@ -37,9 +37,13 @@ constexpr float kTwoPi  = 6.28318530717958647692f;
 // deeper than this are rejected at build time, and the kernels still guard.
 constexpr int kStackDepth = 64;
 // Default path slots of the wavefront (pt_render_settings.paths_in_flight = 0):
-// about 260 B of path state each with two light slots (8.7 GB).  A guide
-// that samples adds its mixture per path (160 B; 2.7 GB at 2^24 paths).
-constexpr int64_t kDefaultPathsInFlight = int64_t(1) << 25;
+// about 260 B of path state each with two light slots (35 GB of the B200's
+// 180 GB; a pass allocates only what its pixels x samples need, and halves
+// itself when the device cannot hold it).  Larger passes amortise the short
+// launches of the deep bounces: on the 1080p 256-spp workload 2^25 / 2^26 /
+// 2^27 slots render at 1621 / 1684 / 1719 Mrays/s.  A guide that samples
+// adds its mixture per path (160 B; 2.7 GB at 2^24 paths).
+constexpr int64_t kDefaultPathsInFlight = int64_t(1) << 27;
 constexpr int64_t kGuidedPathsInFlight = int64_t(1) << 24;
 // While a guide trains, passes stay small: every pass ends with optimiser
 // steps, so smaller passes mean more steps per sample.

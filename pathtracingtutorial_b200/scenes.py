@@ -354,3 +354,60 @@ def hidden_light_room(n_boxes: int = 300, box_subdiv: int = 7, width: int = 1024
     cam = make_camera(position=(-4.6, 1.7, 4.6), look_at=(1.0, 1.2, -1.0), fov=70.0, width=width, height=height)
     return SceneArrays(f"hidden_light_room_{len(f)}tri", v, f, mats, cam, None, spp=spp, sample_per_frame=4,
                        max_depth=max_depth, sampler=SAMPLER_SOBOL, meta={"triangles": int(len(f))})
+
+
+# ---------------------------------------------------------------------------
+# Combined large case
+# ---------------------------------------------------------------------------
+def large_scene(n_spheres: int = 3500, subdiv: int = 4, n_tets: int = 500_000, n_lights: int = 32,
+                n_cameras: int = 16, width: int = 1920, height: int = 1080, spp: int = 512, max_depth: int = 16,
+                seed: int = 13, env_size=(2048, 1024)):
+    """About 20M triangles flattened from displaced icospheres (as in
+    icosphere_field, spread over a larger field) and random tetrahedral
+    clutter, Disney materials as in icosphere_field, the synthetic sky, and
+    n_lights small emissive quads; n_cameras views on a ring around the field.
+    Returns (SceneArrays, list of cameras)."""
+    rng = np.random.default_rng(seed)
+    field = icosphere_field(n_spheres=n_spheres, subdiv=subdiv, width=width, height=height, spp=spp,
+                            max_depth=max_depth, seed=seed, env_size=env_size)
+    # spread the spheres: the field generator places them in a 44 x 35 area
+    v = field.vertices.copy()
+    f = field.faces.copy()
+    mats = list(field.materials)
+    # tetrahedral clutter: 4 triangles each, edge 0.05 .. 0.6, on the ground
+    c = np.stack([rng.uniform(-60, 60, n_tets), np.zeros(n_tets), rng.uniform(-60, 60, n_tets)], 1)
+    size = np.exp(rng.uniform(np.log(0.05), np.log(0.6), n_tets))[:, None]
+    corners = rng.normal(size=(n_tets, 4, 3))
+    corners /= np.linalg.norm(corners, axis=2, keepdims=True)
+    corners[..., 1] = np.abs(corners[..., 1])
+    tv = (c[:, None, :] + corners * size[:, :, None]).reshape(-1, 3)
+    tt = np.array([[0, 1, 2], [0, 3, 1], [0, 2, 3], [1, 3, 2]])
+    ttri = (tt[None] + (np.arange(n_tets) * 4)[:, None, None]).reshape(-1, 3)
+    tn = _vertex_normals(tv, ttri)
+    n_tm = 64
+    for _ in range(n_tm):
+        mats.append(default_material(base_color=tuple(rng.uniform(0, 1, 3)), metallic=rng.uniform(0, 1),
+                                     roughness=rng.uniform(0.05, 1.0), clearcoat=rng.uniform(0, 1)))
+    tmat = np.repeat(len(field.materials) + rng.integers(0, n_tm, n_tets).astype(np.int32), 4)
+    # small area lights above the field
+    light_mat = len(mats)
+    mats.append(default_material(base_color=(1, 1, 1), emissive=(40.0, 36.0, 30.0)))
+    b = _Builder()
+    b.add((tv.astype(np.float32), tn.astype(np.float32), np.zeros((len(tv), 2), np.float32),
+           np.zeros((len(tv), 4), np.float32), ttri, tmat))
+    for _ in range(n_lights):
+        x, z, y, s = rng.uniform(-40, 40), rng.uniform(-40, 40), rng.uniform(6, 12), rng.uniform(0.2, 0.5)
+        b.add(quad((x - s, y, z + s), (x + s, y, z + s), (x + s, y, z - s), (x - s, y, z - s), light_mat))
+    cv, cf = b.arrays()
+    cf["v0"] += len(v); cf["v1"] += len(v); cf["v2"] += len(v)
+    v = np.concatenate([v, cv])
+    f = np.concatenate([f, cf])
+    mats = np.concatenate([np.atleast_1d(m) for m in mats])
+    cams = []
+    for k in range(n_cameras):
+        a = 2 * np.pi * k / n_cameras
+        cams.append(make_camera(position=(48 * np.cos(a), 6.0 + 4.0 * (k % 3), 48 * np.sin(a)),
+                                look_at=(0.0, 1.0, 0.0), fov=45.0, width=width, height=height))
+    sa = SceneArrays(f"large_scene_{len(f)}tri", v, f, mats, cams[0], field.env, spp=spp, sample_per_frame=4,
+                     max_depth=max_depth, sampler=SAMPLER_SOBOL, meta={"triangles": int(len(f))})
+    return sa, cams

@@ -96,3 +96,55 @@ def test_batch_modes_agree_and_autotuner_picks_one():
         rel = np.abs(x[..., :3] - y[..., :3]) / np.maximum(np.abs(y[..., :3]), 1e-3)
         assert np.median(rel) < 1e-5
         assert np.isfinite(z).all()
+
+
+def test_batch_item_cameras_share_one_scene():
+    """Three cameras of one uploaded scene in one batch: each image equals the
+    single-scene render with that camera (wavefront mode: bit for bit)."""
+    sa = scenes.icosphere_field(n_spheres=30, subdiv=2, width=64, height=36, spp=8, max_depth=10, env_size=(128, 64))
+    s = _up(sa)
+    cams = [pt.make_camera(position=(0, 2, 14), look_at=(0, 0, 0), fov=50.0, width=64, height=36),
+            pt.make_camera(position=(9, 4, 6), look_at=(0, 0.5, 0), fov=60.0, width=48, height=48),
+            pt.make_camera(position=(-8, 1, -8), look_at=(0, 0, 0), fov=40.0, width=80, height=24)]
+    items = [(s, 8, 0, c) for c in cams]
+    imgs, st, cfg = pt.render_batch(items, mode=pt.BATCH_WAVEFRONT)
+    pers, _, _ = pt.render_batch(items, mode=pt.BATCH_PERSISTENT, autotune=False, chunk_spp=4)
+    assert st["paths"] == sum(int(c["width"]) * int(c["height"]) * 8 for c in cams)
+    for c, img, img2 in zip(cams, imgs, pers):
+        assert img.shape == (int(c["height"]), int(c["width"]), 4)
+        s.update_camera(c)
+        ref = pt.render(s, 8)
+        assert np.array_equal(img, ref)
+        rel = np.abs(img2[..., :3] - ref[..., :3]) / np.maximum(np.abs(ref[..., :3]), 1e-3)
+        assert np.median(rel) < 1e-5
+
+
+def test_batch_guided_items_match_single_guided_renders():
+    """Guided items (two cameras sharing one trained guide, wavefront mode)
+    render exactly what a single-scene guided render of the same frames does;
+    asking for persistent mode with a guide is an error."""
+    sa = scenes.hidden_light_room(width=40, height=40, n_boxes=40, box_subdiv=2, spp=8, max_depth=10)
+    s = _up(sa)
+    g = pt.Guide(s, seed=3)
+    r = pt.Renderer(s)
+    g.attach(r.integrator, pt.Guide.TRAIN)
+    r.reset_accumulation()
+    s.set_frame_count(1000)
+    r.render_frames(8)
+    r.synchronize()
+    cams = [sa.camera, pt.make_camera(position=(2.0, 2.5, 3.0), look_at=(-1.0, 1.0, -1.0), fov=70.0,
+                                      width=32, height=24)]
+    imgs, st, cfg = pt.render_batch([(s, 8, 0, c, g) for c in cams])
+    assert cfg["mode"] == pt.BATCH_WAVEFRONT
+    for c, img in zip(cams, imgs):
+        s.update_camera(c)
+        rg = pt.Renderer(s)
+        g.attach(rg.integrator, pt.Guide.USE)
+        rg.reset_accumulation()
+        s.set_frame_count(0)
+        rg.render_frames(2)
+        rg.synchronize()
+        assert np.array_equal(img, rg.download_current_image())
+    with pytest.raises(pt.PTError):
+        pt.render_batch([(s, 8, 0, None, g)], mode=pt.BATCH_PERSISTENT, autotune=False)
+    g.close()
