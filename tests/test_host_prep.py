@@ -228,3 +228,19 @@ def test_hdr_roundtrip(tmp_path):
     (tmp_path / "s.json").write_text(json.dumps(obj))
     s = pt.SceneManager.load(str(tmp_path / "s.json"))
     assert s.info()["env_width"] == 12 and s.info()["env_height"] == 8
+
+
+def test_large_scene_generator_small():
+    """The combined large case generator at small counts: spheres + clutter +
+    light quads flattened into one scene, one camera per view, emissive
+    tables hold exactly the light quads' triangles."""
+    sa, cams = scenes.large_scene(n_spheres=20, subdiv=2, n_tets=500, n_lights=5, n_cameras=3, width=64,
+                                  height=32, env_size=(64, 32))
+    assert len(sa.faces) == 20 * 320 + 2 + 500 * 4 + 5 * 2
+    assert len(cams) == 3 and all(int(c["width"]) == 64 for c in cams)
+    assert int(sa.faces["v0"].max()) < len(sa.vertices) and int(sa.faces["material_id"].max()) < len(sa.materials)
+    s = sa.scene()
+    s.build_accel()
+    info = s.info()
+    assert info["num_faces"] == len(sa.faces)
+    assert info["num_emissive_triangles"] == 10
