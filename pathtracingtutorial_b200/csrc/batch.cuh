@@ -411,7 +411,7 @@ int batch_wavefront(const pt_batch_item* in, uint32_t n, int out_is_device, int6
         for (uint32_t k = 0; k < n; ++k) {
             const int lanes = std::max(1, P[k].npath / std::max(P[k].npix, 1));
             const uint64_t passes = static_cast<uint64_t>((total[k] + lanes - 1) / lanes);
-            launches += 1 + passes * (2 + 3 * static_cast<uint64_t>(P[k].max_depth)) + (write_out ? 1 : 0);
+            launches += 1 + passes * (1 + 4 * static_cast<uint64_t>(P[k].max_depth)) + (write_out ? 1 : 0);
         }
         stats->kernel_launches = launches;
     }
