@@ -474,7 +474,11 @@ __host__ __device__ __forceinline__ uint32_t steps_before(uint32_t n, int mb, in
 }
 
 // Gradient of the mean loss over minibatch mb (of nmb) of the collected samples.
-__global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSample* __restrict__ samples_all,
+// Training CTAs hold one copy of both weight layouts and the FP32 weight
+// gradient in shared memory for kGTrainWarps warps (one CTA per SM fits):
+// 6 warps instead of 4 hide more of the gradient scatter's latency.
+constexpr int kGTrainWarps = 6;
+__global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net, const GuideSample* __restrict__ samples_all,
                                                      const uint32_t* count, uint32_t cap, int mb, int nmb) {
     const uint32_t n = minibatch_size(min(*count, cap), mb, nmb);
     if (n == 0u) return;
@@ -514,7 +518,7 @@ __global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSa
     const __nv_bfloat16* WT2 = WT1 + kGHid * (kGHid + 8);
     const __nv_bfloat16* WT3 = WT2 + kGHid * (kGHid + 8);
     const uint32_t tiles = (n + 15) / 16;
-    for (uint32_t tile = blockIdx.x * 4 + warp; tile < tiles; tile += gridDim.x * 4) {
+    for (uint32_t tile = blockIdx.x * kGTrainWarps + warp; tile < tiles; tile += gridDim.x * kGTrainWarps) {
         const uint32_t r0 = tile * 16 + g, r1 = r0 + 8;
         const GuideSample s0 = r0 < n ? samples[static_cast<size_t>(r0) * sstride]
                                       : GuideSample{make_float4(0.5f, 0.5f, 0.5f, 0.0f), make_float4(0, 0, 1, 0)};
@@ -628,7 +632,7 @@ __global__ void __launch_bounds__(128) k_guide_train(GuideNet net, const GuideSa
 // (FP32 master -> FP16 copy); gradients are cleared.
 // dynamic shared memory of the two network kernels (4 warps per CTA)
 constexpr int kGInferSmem = kGSmemW * 2 + kGInferWarps * 16 * kGOutPad * 4;
-constexpr int kGTrainSmem = (2 * kGSmemW + 64) * 2 + kGWeights * 4 + 4 * kGWarpScratch;
+constexpr int kGTrainSmem = (2 * kGSmemW + 64) * 2 + kGWeights * 4 + kGTrainWarps * kGWarpScratch;
 static_assert(kGTrainSmem <= 227 * 1024, "training kernel shared memory");
 static_assert(((2 * kGSmemW + 64) * 2) % 16 == 0 && (kGWeights * 4) % 16 == 0 && kGWarpScratch % 16 == 0,
               "shared memory carve alignment");

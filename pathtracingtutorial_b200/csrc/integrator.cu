@@ -1095,7 +1095,7 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
                     // optimiser steps over this pass's samples in minibatches
                     const int nmb = guide_minibatches(P.npix * count);
                     for (int mb = 0; mb < nmb; ++mb) {
-                        k_guide_train<<<wf.sms, 128, kGTrainSmem, st>>>(gs->net, gs->samples, gs->counters,
+                        k_guide_train<<<wf.sms, 32 * kGTrainWarps, kGTrainSmem, st>>>(gs->net, gs->samples, gs->counters,
                                                                          gs->sample_cap, mb, nmb);
                         k_guide_adam<<<wf.sms * 8, 256, 0, st>>>(gs->net, gs->counters, gs->sample_cap, mb, nmb,
                                                                  gs->step, gs->lr, gs->lr, 0.9f, 0.99f, 1e-10f);
@@ -1737,7 +1737,7 @@ int guide_backward(pt_guide* h, const float* samples, uint32_t n, float* wgrad, 
     if (e == cudaSuccess) {
         GuideNet net = h->g.net;
         net.loss = nullptr;   // leave the training-loss record alone
-        k_guide_train<<<148, 128, kGTrainSmem>>>(net, ds, dn, n, 0, 1);
+        k_guide_train<<<148, 32 * kGTrainWarps, kGTrainSmem>>>(net, ds, dn, n, 0, 1);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
     }
