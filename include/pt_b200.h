@@ -211,6 +211,30 @@ int pt_scene_get_camera(const pt_scene* scene, pt_camera* cam);
  * SAH BVH (reorders faces: triangle ids are BVH-ordered face indices), emissive
  * triangle and environment alias tables, and the device node layout.  Host only. */
 int pt_scene_build_accel(pt_scene* scene);
+
+/* The same prep with the BVH built on `device` instead of by the reference's
+ * host builder (BVHBuilder::build, Part_2/src/accel/bvh_builder.cpp:56-221):
+ * a linear BVH over 63-bit Morton codes (Karras radix tree) whose subtrees
+ * become leaves by the reference's two rules: at most 3 faces (fewer than its
+ * LeafThreshold of 4), or at most `max_leaf` faces (0 = 8) where its SAH cost
+ * model (traversal 0.5, intersection 1) prefers a leaf; max_leaf below 3 also
+ * caps the first rule.  Faces are reordered
+ * into leaf order as by pt_scene_build_accel; light and environment tables are
+ * then built on the host.  Closest-hit distances equal those of the host-built
+ * tree; triangle ids, the light table order and hence the images' sample
+ * streams differ from the reference's.  Deterministic: the same scene gives
+ * the same tree.  Fails with PT_ERR_INVALID when a face indexes a missing
+ * vertex or material or the tree is deeper than the traversal stack (64).
+ * `stats` may be null. */
+typedef struct pt_build_stats {
+    double   total_ms;      /* the whole call, host wall time                 */
+    double   upload_ms;     /* vertices and faces to the device (CUDA events)  */
+    double   device_ms;     /* boxes, codes, sort, tree, collapse, emission    */
+    double   download_ms;   /* nodes, triangle records, reordered faces back   */
+    double   tables_ms;     /* emissive and environment tables on the host     */
+    uint32_t inner_nodes, leaves, depth, max_leaf;
+} pt_build_stats;
+int pt_scene_build_accel_device(pt_scene* scene, int32_t device, uint32_t max_leaf, pt_build_stats* stats);
 /* ---- scene: upload (SceneManager::uploadToDevice / DeviceScene::uploadFrom,
  *      Part_2/src/scene/device_scene.cu:8-57) ---- */
 int pt_scene_upload(pt_scene* scene, int32_t device);
@@ -225,6 +249,15 @@ int pt_scene_get_emissive(const pt_scene* scene, pt_emissive_ref* refs, uint32_t
                           float* face_pmf, uint32_t cap_pmf,
                           pt_alias_entry* alias, uint32_t cap_alias);
 int pt_scene_get_env_tables(const pt_scene* scene, float* pmf, pt_alias_entry* alias, uint32_t cap);
+/* The device node layout as built (either builder): `inner` receives
+ * num_inner_nodes records of 64 bytes (child 0 box lo xyz, hi xyz, child 1 box
+ * lo xyz, hi xyz, ref0, ref1, meta, pad; ref bit 31 = leaf starting at that
+ * triangle record, meta bits 0-1 = split axis, bit 2 = child 0's centre below
+ * child 1's), `tris` num_faces records of 48 bytes (v0, v1 - v0, v2 - v0,
+ * flags: bit 0 = last of its leaf, 2 pad words); root_ref = kLeafBit|first for
+ * a one-leaf tree, else 0.  For tests and tools; either pointer may be null. */
+int pt_scene_get_traversal(const pt_scene* scene, void* inner, uint32_t cap_inner, void* tris, uint32_t cap_tris,
+                           uint32_t* root_ref);
 
 /* ---- film (Film, Part_2/src/film/film.h:9-40) ----
  * Per pixel: compensated FP32 sum (Neumaier), compensation, sample count, and
@@ -357,6 +390,14 @@ int pt_sampler_stream(int32_t sampler_type, int32_t width, int32_t height,
 /* BSDF table: for n (material index, wo, wi, n, t) records evaluate the device
  * Disney BSDF.  in: n x 13 floats (mat, wo[3], wi[3], N[3], T[3]); out: n x 4 (f.rgb, pdf). */
 int pt_bsdf_eval(pt_scene* scene, const float* in, uint32_t n, float* out_host);
+/* Display tone mapping of the reference's preview shader
+ * (Part_2/preview/tone_mapping.frag:12-29, drawn there through OpenGL; here a
+ * headless buffer): c' = 1 - exp(-c * 2^exposure) per channel, sRGB transfer
+ * curve, 8-bit unorm.  rgba: width*height*4 floats (A ignored); out_rgba8:
+ * width*height*4 bytes (A = 255); host or device pointers.  The preview's
+ * default exposure is -2.8. */
+int pt_tonemap(const float* rgba, int32_t width, int32_t height, float exposure, uint8_t* out_rgba8,
+               int32_t ptrs_are_device, int32_t device);
 
 #ifdef __cplusplus
 }

@@ -355,3 +355,15 @@ class RefGpu:
         if self._h:
             self.L.refgpu_destroy(self._h)
             self._h = None
+
+
+def tonemap_ref(img, exposure=-2.8):
+    """The reference preview's display mapping (Part_2/preview/tone_mapping.frag:12-29)
+    in float64: 1 - exp(-c * 2^exposure), linear_to_srgb per channel (:12-19),
+    then 8-bit unorm with round to nearest.  Returns (H, W, 4) uint8, alpha 255."""
+    c = np.asarray(img, np.float64)[..., :3]
+    t = 1.0 - np.exp(-c * 2.0 ** exposure)
+    e = np.where(t <= 0.0031308, 12.92 * t, 1.055 * np.power(np.maximum(t, 0.0), 1.0 / 2.4) - 0.055)
+    out = np.full(c.shape[:2] + (4,), 255, np.uint8)
+    out[..., :3] = np.rint(np.clip(e, 0.0, 1.0) * 255.0).astype(np.uint8)
+    return out

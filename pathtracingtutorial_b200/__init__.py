@@ -32,7 +32,7 @@ from ._ffi import SAMPLER_PCG, SAMPLER_SOBOL, FLAG_WATERTIGHT, FLAG_STAGE_TIMING
     FLAG_COUNT_TRAVERSAL, ARGS_LTR, ARGS_RTL
 
 __all__ = ["SceneManager", "PathIntegrator", "Film", "Renderer", "render", "default_material", "make_camera",
-           "trace_closest", "trace_any", "sampler_stream", "bsdf_eval", "write_hdr", "read_hdr",
+           "trace_closest", "trace_any", "sampler_stream", "bsdf_eval", "write_hdr", "read_hdr", "tonemap",
            "compute_rmse", "rmse_to_db", "PTError", "VERTEX_DTYPE", "FACE_DTYPE", "MATERIAL_DTYPE",
            "CAMERA_DTYPE", "PUNCTUAL_DTYPE", "BVH_NODE_DTYPE", "SAMPLER_PCG", "SAMPLER_SOBOL",
            "FLAG_WATERTIGHT", "FLAG_STAGE_TIMING", "FLAG_NO_GRAPH", "FLAG_COUNT_TRAVERSAL",
@@ -170,8 +170,18 @@ class SceneManager:
         check(lib().pt_scene_set_punctual_lights(self._h, ptr(L), len(L)))
 
     # -- prep / upload --
-    def build_accel(self) -> None:
-        check(lib().pt_scene_build_accel(self._h))
+    def build_accel(self, builder: str = "host", device: int = 0, max_leaf: int = 0) -> dict | None:
+        """SceneManager::buildAccel.  builder="host" is the reference's SAH
+        build (node for node); builder="device" builds a linear BVH with SAH
+        leaf collapse on `device` and returns its timings and sizes."""
+        if builder == "host":
+            check(lib().pt_scene_build_accel(self._h))
+            return None
+        if builder != "device":
+            raise ValueError(f"unknown builder {builder!r} (host or device)")
+        st = _ffi.BuildStats()
+        check(lib().pt_scene_build_accel_device(self._h, device, max_leaf, C.byref(st)))
+        return st.as_dict()
 
     def upload_to_device(self, device: int = 0) -> None:
         check(lib().pt_scene_upload(self._h, device))
@@ -206,6 +216,16 @@ class SceneManager:
         out = np.zeros(self.info()["num_bvh_nodes"], BVH_NODE_DTYPE)
         check(lib().pt_scene_get_bvh(self._h, ptr(out), len(out)))
         return out
+
+    def traversal_layout(self) -> tuple[np.ndarray, np.ndarray, int]:
+        """(inner nodes as uint32[n, 16], triangle records as uint32[m, 12],
+        root_ref): the device node layout, bit for bit."""
+        info = self.info()
+        inner = np.zeros((info["num_inner_nodes"], 16), np.uint32)
+        tris = np.zeros((info["num_faces"], 12), np.uint32)
+        root = C.c_uint32(0)
+        check(lib().pt_scene_get_traversal(self._h, ptr(inner), len(inner), ptr(tris), len(tris), C.byref(root)))
+        return inner, tris, int(root.value)
 
     def emissive_tables(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
         info = self.info()
@@ -569,6 +589,19 @@ def bsdf_eval(scene: SceneManager, records: np.ndarray) -> np.ndarray:
     rec = np.ascontiguousarray(records, np.float32)
     out = np.zeros((len(rec), 4), np.float32)
     check(lib().pt_bsdf_eval(scene.handle, ptr(rec), len(rec), ptr(out)))
+    return out
+
+
+def tonemap(img: np.ndarray, exposure: float = -2.8, device: int = 0) -> np.ndarray:
+    """Display image of the reference's preview tone mapping
+    (Part_2/preview/tone_mapping.frag:12-29) computed on the GPU:
+    (H, W, 4) float radiance -> (H, W, 4) uint8 sRGB, alpha 255."""
+    a = np.ascontiguousarray(img, np.float32)
+    h, w = a.shape[0], a.shape[1]
+    if a.shape[2] == 3:
+        a = np.ascontiguousarray(np.concatenate([a, np.ones((h, w, 1), np.float32)], 2))
+    out = np.zeros((h, w, 4), np.uint8)
+    check(lib().pt_tonemap(ptr(a), w, h, float(exposure), ptr(out), 0, device))
     return out
 
 

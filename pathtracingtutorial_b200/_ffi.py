@@ -73,6 +73,18 @@ class RenderSettings(C.Structure):
                 ("flags", C.c_int32), ("paths_in_flight", C.c_int32)]
 
 
+class BuildStats(C.Structure):
+    _fields_ = [("total_ms", C.c_double), ("upload_ms", C.c_double), ("device_ms", C.c_double),
+                ("download_ms", C.c_double), ("tables_ms", C.c_double), ("inner_nodes", C.c_uint32),
+                ("leaves", C.c_uint32), ("depth", C.c_uint32), ("max_leaf", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+assert C.sizeof(BuildStats) == 56
+
+
 class SceneInfo(C.Structure):
     _fields_ = [("num_vertices", C.c_uint32), ("num_faces", C.c_uint32), ("num_materials", C.c_uint32),
                 ("num_bvh_nodes", C.c_uint32), ("num_emissive_triangles", C.c_uint32),
@@ -125,6 +137,8 @@ _SIGS = [
     ("pt_scene_set_camera", C.c_int, [_P, _P]),
     ("pt_scene_get_camera", C.c_int, [_P, _P]),
     ("pt_scene_build_accel", C.c_int, [_P]),
+    ("pt_scene_build_accel_device", C.c_int, [_P, C.c_int32, C.c_uint32, C.POINTER(BuildStats)]),
+    ("pt_scene_get_traversal", C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
     ("pt_scene_upload", C.c_int, [_P, C.c_int32]),
     ("pt_scene_info_get", C.c_int, [_P, C.POINTER(SceneInfo)]),
     ("pt_scene_build_params", C.c_int, [_P, C.POINTER(SceneParams)]),
@@ -167,6 +181,7 @@ _SIGS = [
     ("pt_sampler_stream", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_uint32, C.c_int32, C.c_int32,
                                     C.c_uint32, C.c_uint32, C.c_int32, _P]),
     ("pt_bsdf_eval", C.c_int, [_P, _P, C.c_uint32, _P]),
+    ("pt_tonemap", C.c_int, [_P, C.c_int32, C.c_int32, C.c_float, _P, C.c_int32, C.c_int32]),
 ]
 EXPORTED = [name for name, _, _ in _SIGS]
 

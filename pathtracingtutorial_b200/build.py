@@ -22,7 +22,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 CXX_SOURCES = ["host_prep.cpp", "scene_io.cpp", "capi.cpp"]
-CU_SOURCES = ["integrator.cu", "static_trace.cu"]
+CU_SOURCES = ["integrator.cu", "static_trace.cu", "lbvh.cu"]
 HEADERS = ["pt_internal.h", "sampler.h", "bsdf.h", "traverse.h", "engine.h", "device_api.h", "batch.cuh", "guide.cuh", "guide_host.cuh"]
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]

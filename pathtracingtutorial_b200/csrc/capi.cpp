@@ -4,6 +4,7 @@
 // uploadToDevice -> Renderer::renderAll -> download
 // (Part_2/src/main.cpp:69-78,148-149), but every entry point returns a status
 // code instead of exiting, and the library owns all device memory.
+#include <cmath>
 #include <algorithm>
 #include <cctype>
 #include <cstring>
@@ -212,6 +213,20 @@ int pt_scene_build_accel(pt_scene* s) {
     PT_GUARD_END
 }
 
+int pt_scene_build_accel_device(pt_scene* s, int32_t device, uint32_t max_leaf, pt_build_stats* stats) {
+    PT_REQUIRE(s, "null scene");
+    PT_REQUIRE(device >= 0, "device must be >= 0");
+    PT_REQUIRE(max_leaf <= 64, "max_leaf must be at most 64");
+    PT_GUARD_BEGIN
+    invalidate_build(s);
+    const uint32_t leaf = max_leaf ? max_leaf : 8u;
+    const int rc = build_accel_device(s, device, leaf, stats);
+    if (rc != PT_OK) s->tables = SceneTables{};
+    else if (stats) stats->max_leaf = leaf;
+    return rc;
+    PT_GUARD_END
+}
+
 int pt_scene_upload(pt_scene* s, int32_t device) {
     PT_REQUIRE(s, "null scene");
     PT_REQUIRE(device >= 0, "device must be >= 0");
@@ -226,7 +241,8 @@ int pt_scene_info_get(const pt_scene* s, pt_scene_info* info) {
     info->num_vertices = static_cast<uint32_t>(s->host.vertices.size());
     info->num_faces = static_cast<uint32_t>(s->host.faces.size());
     info->num_materials = static_cast<uint32_t>(s->host.materials.size());
-    info->num_bvh_nodes = static_cast<uint32_t>(s->tables.bvh.size());
+    info->num_bvh_nodes = static_cast<uint32_t>(
+        s->tables.bvh.empty() && s->tables.built ? s->tables.inner.size() + s->tables.num_leaves : s->tables.bvh.size());
     info->num_emissive_triangles = static_cast<uint32_t>(s->tables.emissive.size());
     info->num_punctual_lights = static_cast<uint32_t>(s->host.punctual.size());
     info->env_width = s->host.env_w;
@@ -266,7 +282,30 @@ int pt_scene_get_materials(const pt_scene* s, pt_material* out, uint32_t cap) {
 }
 int pt_scene_get_bvh(const pt_scene* s, pt_bvh_node* out, uint32_t cap) {
     PT_REQUIRE(s, "null scene");
+    PT_GUARD_BEGIN
+    if (s->tables.bvh.empty() && s->tables.built) {   // built on the device: derive from the traversal layout
+        std::vector<pt_bvh_node> nodes;
+        if (!nodes_from_traversal_layout(s->tables, nodes)) return PT_ERR_INVALID;
+        return copy_out(nodes, out, cap);
+    }
     return copy_out(s->tables.bvh, out, cap);
+    PT_GUARD_END
+}
+int pt_scene_get_traversal(const pt_scene* s, void* inner, uint32_t cap_inner, void* tris, uint32_t cap_tris,
+                           uint32_t* root_ref) {
+    PT_REQUIRE(s, "null scene");
+    PT_REQUIRE(s->tables.built, "scene not built");
+    if (inner) {
+        PT_REQUIRE(cap_inner >= s->tables.inner.size(), "inner capacity too small");
+        if (!s->tables.inner.empty())
+            std::memcpy(inner, s->tables.inner.data(), s->tables.inner.size() * sizeof(InnerNode));
+    }
+    if (tris) {
+        PT_REQUIRE(cap_tris >= s->tables.tris.size(), "triangle capacity too small");
+        if (!s->tables.tris.empty()) std::memcpy(tris, s->tables.tris.data(), s->tables.tris.size() * sizeof(TriRecord));
+    }
+    if (root_ref) *root_ref = s->tables.root_ref;
+    return PT_OK;
 }
 int pt_scene_get_emissive(const pt_scene* s, pt_emissive_ref* refs, uint32_t cap_refs, float* face_pmf,
                           uint32_t cap_pmf, pt_alias_entry* alias, uint32_t cap_alias) {
@@ -501,6 +540,13 @@ int pt_sampler_stream(int32_t sampler_type, int32_t width, int32_t height, uint3
 int pt_bsdf_eval(pt_scene* s, const float* in, uint32_t n, float* out_host) {
     PT_REQUIRE(s && (n == 0 || (in && out_host)), "null argument");
     return bsdf_eval(s, in, n, out_host);
+}
+int pt_tonemap(const float* rgba, int32_t width, int32_t height, float exposure, uint8_t* out_rgba8,
+               int32_t ptrs_are_device, int32_t device) {
+    PT_REQUIRE(width >= 0 && height >= 0, "invalid sizes");
+    PT_REQUIRE((width == 0 || height == 0) || (rgba && out_rgba8), "null argument");
+    PT_REQUIRE(std::isfinite(exposure), "exposure must be finite");
+    return tonemap(rgba, width, height, exposure, out_rgba8, ptrs_are_device != 0, device);
 }
 
 }  // extern "C"

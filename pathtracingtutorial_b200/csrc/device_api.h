@@ -10,6 +10,7 @@ DeviceScene device_view(const pt_scene* s);
 void free_scene_device(pt_scene* s);
 void unpin_host_arrays(pt_scene* s);
 int  upload_scene(pt_scene* s, int device);
+int  build_accel_device(pt_scene* s, int device, uint32_t max_leaf, pt_build_stats* stats);
 
 int  film_alloc(pt_film* f);
 void film_free(pt_film* f);
@@ -27,6 +28,7 @@ int  trace_rays(pt_scene* s, const float* rays, uint32_t n, pt_hit* hits, uint8_
 int  sampler_stream(int type, int w, int h, uint32_t frame, int spf, int sif, uint32_t ndims, uint32_t seed,
                     int device, float* out_host);
 int  bsdf_eval(pt_scene* s, const float* in, uint32_t n, float* out_host);
+int  tonemap(const float* rgba, int w, int h, float exposure, uint8_t* out, bool device_ptrs, int device);
 int  render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batch_config* cfg, pt_render_stats* stats);
 void batch_forget_scene(const pt_scene* s);
 int  guide_create(pt_scene* s, uint32_t seed, pt_guide** out);

@@ -83,6 +83,7 @@ std::vector<pt_alias_entry> build_alias_table(const std::vector<float>& weights)
 void build_emissive_tables(const HostScene& hs, SceneTables& t);
 void build_env_tables(const HostScene& hs, SceneTables& t);
 bool build_traversal_layout(const HostScene& hs, SceneTables& t);
+bool nodes_from_traversal_layout(const SceneTables& t, std::vector<pt_bvh_node>& nodes);
 // Quad -> 2 triangles (shapes::buildQuad, Part_2/src/geometry/shapes.cpp:5-22).
 void add_quad(const float a[3], const float b[3], const float c[3], const float d[3], int mat,
               std::vector<pt_vertex>& verts, std::vector<pt_face>& faces);

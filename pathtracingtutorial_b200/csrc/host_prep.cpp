@@ -456,6 +456,67 @@ bool build_traversal_layout(const HostScene& hs, SceneTables& t) {
     return true;
 }
 
+// The reference's node layout (BVHNode, Part_2/src/accel/bvh.h) recovered from
+// the traversal layout, for trees that exist only in that layout (built on the
+// device): inner node k keeps index k, leaves follow in the order their parents
+// list them; a node's box is the one its parent carries (the root's is
+// root_lo/hi), a leaf's count runs to its flagged last triangle record.
+bool nodes_from_traversal_layout(const SceneTables& t, std::vector<pt_bvh_node>& nodes) {
+    nodes.clear();
+    if (!t.built || t.tris.empty()) return true;
+    const uint32_t ni = static_cast<uint32_t>(t.inner.size());
+    const uint32_t nt = static_cast<uint32_t>(t.tris.size());
+    auto leaf_count = [&](uint32_t first, uint32_t& cnt) {
+        uint32_t i = first;
+        while (i < nt && !(t.tris[i].flags & 1u)) ++i;
+        if (i >= nt) return false;
+        cnt = i - first + 1;
+        return true;
+    };
+    auto set_box = [](pt_bvh_node& n, const float* lo, const float* hi) {
+        for (int a = 0; a < 3; ++a) { n.bmin[a] = lo[a]; n.bmax[a] = hi[a]; }
+    };
+    if (t.root_ref & kLeafBit) {
+        nodes.resize(1);
+        uint32_t cnt = 0;
+        if (!leaf_count(t.root_ref & ~kLeafBit, cnt)) { set_error("malformed leaf"); return false; }
+        set_box(nodes[0], t.root_lo, t.root_hi);
+        nodes[0].data0 = t.root_ref;
+        nodes[0].data1 = cnt;
+        return true;
+    }
+    nodes.resize(ni);
+    set_box(nodes[0], t.root_lo, t.root_hi);
+    for (uint32_t k = 0; k < ni; ++k) {
+        const InnerNode& o = t.inner[k];
+        const float lo0[3] = {o.c0lo[0], o.c0lo[1], o.c0lo[2]}, hi0[3] = {o.c0hi_x, o.c0hi_yz[0], o.c0hi_yz[1]};
+        const float lo1[3] = {o.c1lo_xy[0], o.c1lo_xy[1], o.c1lo_z}, hi1[3] = {o.c1hi[0], o.c1hi[1], o.c1hi[2]};
+        uint32_t idx[2];
+        const uint32_t refs[2] = {o.ref0, o.ref1};
+        const float* los[2] = {lo0, lo1};
+        const float* his[2] = {hi0, hi1};
+        for (int c = 0; c < 2; ++c) {
+            pt_bvh_node n{};
+            set_box(n, los[c], his[c]);
+            if (refs[c] & kLeafBit) {
+                uint32_t cnt = 0;
+                if (!leaf_count(refs[c] & ~kLeafBit, cnt)) { set_error("malformed leaf"); return false; }
+                n.data0 = refs[c];
+                n.data1 = cnt;
+                idx[c] = static_cast<uint32_t>(nodes.size());
+                nodes.push_back(n);
+            } else {
+                if (refs[c] >= ni || refs[c] == 0) { set_error("malformed inner node reference"); return false; }
+                idx[c] = refs[c];
+                set_box(nodes[refs[c]], los[c], his[c]);
+            }
+        }
+        nodes[k].data0 = idx[0];
+        nodes[k].data1 = idx[1];
+    }
+    return true;
+}
+
 // ---------------------------------------------------------------------------
 // Camera basis (Part_2/src/camera/camera.h:36-51).
 // ---------------------------------------------------------------------------

@@ -1553,6 +1553,53 @@ int trace_rays(pt_scene* s, const float* rays, uint32_t n, pt_hit* hits, uint8_t
     return PT_OK;
 }
 
+// Display tone mapping of the reference's preview (Part_2/preview/
+// tone_mapping.frag:12-29): 1 - exp(-c * 2^exposure) per channel, then the
+// sRGB transfer curve, written as 8-bit unorm (round to nearest, as the
+// display framebuffer stores it), alpha 255.
+__global__ void k_tonemap(const float4* __restrict__ in, uchar4* __restrict__ out, uint32_t n, float scale) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 c = in[i];
+        auto enc = [&](float v) -> unsigned char {
+            const float t = 1.0f - expf(-v * scale);
+            const float e = t <= 0.0031308f ? 12.92f * t : 1.055f * powf(t, 1.0f / 2.4f) - 0.055f;
+            return static_cast<unsigned char>(__float2int_rn(fminf(fmaxf(e, 0.0f), 1.0f) * 255.0f));
+        };
+        out[i] = make_uchar4(enc(c.x), enc(c.y), enc(c.z), 255);
+    }
+}
+
+int tonemap(const float* rgba, int w, int h, float exposure, uint8_t* out, bool device_ptrs, int device) {
+    if (int rc = ensure_device(device)) return rc;
+    const size_t n = static_cast<size_t>(w) * h;
+    if (n == 0) return PT_OK;
+    const float scale = std::exp2(exposure);
+    const int grid = static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 16));
+    if (device_ptrs) {
+        k_tonemap<<<grid, 256>>>(reinterpret_cast<const float4*>(rgba), reinterpret_cast<uchar4*>(out),
+                                 static_cast<uint32_t>(n), scale);
+        PT_CU(cudaGetLastError());
+        PT_CU(cudaDeviceSynchronize());
+        return PT_OK;
+    }
+    float4* din = nullptr;
+    uchar4* dout = nullptr;
+    PT_CU(cudaMalloc(&din, n * sizeof(float4)));
+    if (cudaMalloc(&dout, n * sizeof(uchar4)) != cudaSuccess) {
+        cudaFree(din); cudaGetLastError(); set_error("tone map: allocation failed"); return PT_ERR_NOMEM;
+    }
+    cudaError_t e = cudaMemcpy(din, rgba, n * sizeof(float4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_tonemap<<<grid, 256>>>(din, dout, static_cast<uint32_t>(n), scale);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, n * sizeof(uchar4), cudaMemcpyDeviceToHost);
+    cudaFree(din);
+    cudaFree(dout);
+    if (e != cudaSuccess) { set_error(std::string("tone map: ") + cudaGetErrorString(e)); return PT_ERR_CUDA; }
+    return PT_OK;
+}
+
 int sampler_stream(int type, int w, int h, uint32_t frame, int spf, int sif, uint32_t ndims, uint32_t seed,
                    int device, float* out_host) {
     if (int rc = ensure_device(device)) return rc;

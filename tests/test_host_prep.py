@@ -244,3 +244,17 @@ def test_large_scene_generator_small():
     info = s.info()
     assert info["num_faces"] == len(sa.faces)
     assert info["num_emissive_triangles"] == 10
+
+
+def test_tonemap_oracle_known_values():
+    """The tone-map restatement at points worked by hand from the preview
+    shader (tone_mapping.frag:12-29): black, the linear sRGB segment, c = 1 at
+    exposure 0 (1 - 1/e -> sRGB 0.8165 -> 208), saturation."""
+    import math
+    from oracle.pyoracle import tonemap_ref
+    img = np.array([[[0.0, 1e-4, 1.0, 1], [1e9, 1e9, 1e9, 1]]], np.float32)
+    out = tonemap_ref(img, 0.0)
+    t = 1 - math.exp(-1e-4)
+    assert out[0, 0, 0] == 0 and out[0, 0, 1] == round(12.92 * t * 255)
+    assert out[0, 0, 2] == round((1.055 * (1 - math.exp(-1.0)) ** (1 / 2.4) - 0.055) * 255) == 208
+    assert (out[0, 1, :3] == 255).all() and (out[..., 3] == 255).all()
