@@ -218,7 +218,11 @@ int pt_scene_build_accel(pt_scene* scene);
  * become leaves by the reference's two rules: at most 3 faces (fewer than its
  * LeafThreshold of 4), or at most `max_leaf` faces (0 = 8) where its SAH cost
  * model (traversal 0.5, intersection 1) prefers a leaf; max_leaf below 3 also
- * caps the first rule.  Faces are reordered
+ * caps the first rule.  Before the leaf decisions every inner node's treelet
+ * of `treelet_leaves` leaves (0 = 7, 1-2 = off) is re-topologised to its least
+ * SAH cost (Karras and Aila's treelet restructuring, one bottom-up pass), and
+ * faces are laid out in the final tree's depth-first order.  The tree is
+ * walked on the host before it is accepted (PT_ERR_DEVICE if malformed).  Faces are reordered
  * into leaf order as by pt_scene_build_accel; light and environment tables are
  * then built on the host.  Closest-hit distances equal those of the host-built
  * tree; triangle ids, the light table order and hence the images' sample
@@ -231,10 +235,11 @@ typedef struct pt_build_stats {
     double   upload_ms;     /* vertices and faces to the device (CUDA events)  */
     double   device_ms;     /* boxes, codes, sort, tree, collapse, emission    */
     double   download_ms;   /* nodes, triangle records, reordered faces back   */
-    double   tables_ms;     /* emissive and environment tables on the host     */
+    double   tables_ms;     /* tree check, emissive and environment tables    */
     uint32_t inner_nodes, leaves, depth, max_leaf;
 } pt_build_stats;
-int pt_scene_build_accel_device(pt_scene* scene, int32_t device, uint32_t max_leaf, pt_build_stats* stats);
+int pt_scene_build_accel_device(pt_scene* scene, int32_t device, uint32_t max_leaf, uint32_t treelet_leaves,
+                                pt_build_stats* stats);
 /* ---- scene: upload (SceneManager::uploadToDevice / DeviceScene::uploadFrom,
  *      Part_2/src/scene/device_scene.cu:8-57) ---- */
 int pt_scene_upload(pt_scene* scene, int32_t device);

@@ -18,13 +18,20 @@ for bit:
       the highest bit where keys f and l differ; its children are the leaf
       gamma (if gamma == f) or inner node gamma, and the leaf gamma + 1 (if
       gamma + 1 == l) or inner node gamma + 1; the root is inner node 0;
-  post-order: box = union of the children; A = dx dy + dy dz + dz dx;
-      tree cost = (0.5 A + cost_left) + cost_right (a single face costs its A),
+  every inner node after its subtree (the device's bottom-up order): with
+      treelet >= 3 its treelet is re-topologised first (see restructure:
+      open the largest-area inner leaf until `treelet` leaves, dynamic
+      programming over the leaf subsets, the first strict minimum in
+      descending-submask order of the splits holding the lowest leaf, inner
+      nodes reused depth first from a LIFO stack); then box = union of the
+      children; A = dx dy + dy dz + dz dx;
+      tree cost = 0.5 A + (cost_left + cost_right) (a single face costs its A),
       leaf cost = count * A, the node becomes a leaf when count <= min(3,
       max_leaf) (the reference's LeafThreshold rule, bvh_builder.cpp:10,99) or
       when count <= max_leaf and leaf cost <= tree cost;
   surviving inner nodes (no collapsed ancestor, not collapsed) are numbered
-      in increasing inner-node index; each becomes one 16-word record.
+      in increasing inner-node index; each becomes one 16-word record; faces
+      take their depth-first position in the final tree.
 All float arithmetic is numpy float32, one rounding per operation, in the
 device's order.
 """
@@ -69,11 +76,23 @@ def _half_area(lo, hi) -> np.float32:
     return F(F(F(dx * dy) + F(dy * dz)) + F(dz * dx))
 
 
-def build(positions: np.ndarray, faces: np.ndarray, max_leaf: int = 8) -> dict:
-    """The device builder's outputs: order (sorted face index per position),
+def _node_cost(area, children, cnt, min_leaf, max_leaf):
+    tree = F(F(F(0.5) * area) + children)
+    leaf = F(F(cnt) * area)
+    col = cnt <= min_leaf or (cnt <= max_leaf and leaf <= tree)
+    return (leaf if col else tree), col
+
+
+def _low_index(x: int) -> int:
+    return (x & -x).bit_length() - 1
+
+
+def build(positions: np.ndarray, faces: np.ndarray, max_leaf: int = 8, treelet: int = 7) -> dict:
+    """The device builder's outputs: order (face index per final position),
     inner (uint32[k, 16]), leaf_last (positions whose record ends a leaf),
-    root_ref, root box, depth, leaves."""
+    root_ref, root box, depth, leaves.  treelet < 3: no restructuring."""
     n = len(faces)
+    min_leaf = min(max_leaf, 3)
     lo, hi = face_boxes(positions, faces)
     codes = morton_codes(lo, hi)
     order = np.argsort(codes, kind="stable")
@@ -82,63 +101,150 @@ def build(positions: np.ndarray, faces: np.ndarray, max_leaf: int = 8) -> dict:
     m = n - 1
 
     # top-down radix tree (inner node index = the split rule's numbering)
-    child = np.zeros((max(m, 0), 2), np.uint64)
-    rng = np.zeros((max(m, 0), 2), np.int64)
-    parent = np.full(max(m, 0), -1, np.int64)
-    post = []
+    child = [[0, 0] for _ in range(max(m, 0))]
+    parent = [-1] * max(m, 0)
+    parent_leaf = [-1] * n
+    pre = []
     if m > 0:
         stack = [(0, 0, n - 1)]
         while stack:
             node, f, l = stack.pop()
-            rng[node] = (f, l)
             p = (keys[f] ^ keys[l]).bit_length() - 1
             thr = (keys[l] >> p) << p
             gamma = bisect.bisect_left(keys, thr, f, l + 1) - 1
-            post.append(node)
+            pre.append(node)
             kids = []
             for c, (cf, cl) in ((gamma, (f, gamma)), (gamma + 1, (gamma + 1, l))):
                 if cf == cl:
                     kids.append(LEAF | c)
+                    parent_leaf[c] = node
                 else:
                     kids.append(c)
                     parent[c] = node
                     stack.append((c, cf, cl))
             child[node] = kids
-    post.reverse()   # children before parents
 
     nlo = np.zeros((max(m, 0), 3), np.float32)
     nhi = np.zeros((max(m, 0), 3), np.float32)
-    cost = np.zeros(max(m, 0), np.float32)
-    cnt = np.zeros(max(m, 0), np.int64)
-    col = np.zeros(max(m, 0), bool)
+    cost = [F(0)] * max(m, 0)
+    cnt = [0] * max(m, 0)
+    col = [False] * max(m, 0)
 
     def info(c):
-        c = int(c)
         if c & LEAF:
             p = c & ~LEAF
             return slo[p], shi[p], _half_area(slo[p], shi[p]), 1
-        return nlo[c], nhi[c], cost[c], int(cnt[c])
+        return nlo[c], nhi[c], cost[c], cnt[c]
 
-    for node in post:
-        la, ha, ca, na = info(child[node, 0])
-        lb, hb, cbb, nb = info(child[node, 1])
+    def set_parent(c, p):
+        if c & LEAF:
+            parent_leaf[c & ~LEAF] = p
+        else:
+            parent[c] = p
+
+    def restructure(node):
+        leaf = list(child[node])
+        larea = [_half_area(*info(c)[:2]) for c in leaf]
+        inner_pool = [node]
+        while len(leaf) < treelet:
+            best, ba = -1, F(0)
+            for i, c in enumerate(leaf):
+                if not (c & LEAF) and (best < 0 or larea[i] > ba):
+                    best, ba = i, larea[i]
+            if best < 0:
+                break
+            x = leaf[best]
+            a, b = child[x]
+            inner_pool.append(x)
+            leaf[best], larea[best] = a, _half_area(*info(a)[:2])
+            leaf.append(b)
+            larea.append(_half_area(*info(b)[:2]))
+        nl = len(leaf)
+        if nl < 3:
+            return
+        li = [info(c) for c in leaf]
+        full = (1 << nl) - 1
+        dp = [F(0)] * (full + 1)
+        split = [0] * (full + 1)
+
+        def members(S):
+            idx = [i for i in range(nl) if (S >> i) & 1]
+            blo = np.min(np.stack([li[i][0] for i in idx]), 0)
+            bhi = np.max(np.stack([li[i][1] for i in idx]), 0)
+            return blo, bhi, sum(li[i][3] for i in idx)
+
+        for S in range(1, full + 1):
+            if S & (S - 1) == 0:
+                dp[S] = li[_low_index(S)][2]
+                continue
+            blo, bhi, k = members(S)
+            low = S & -S
+            best, bp = None, low
+            P = (S - 1) & S
+            while P:
+                if P & low:
+                    c = F(dp[P] + dp[S ^ P])
+                    if best is None or c < best:
+                        best, bp = c, P
+                P = (P - 1) & S
+            dp[S] = _node_cost(_half_area(blo, bhi), best, k, min_leaf, max_leaf)[0]
+            split[S] = bp
+        stack = [(full, node)]
+        nxt = 1
+        made = []
+        while stack:
+            S, me = stack.pop()
+            made.append((S, me))
+            refs = []
+            for part in (split[S], S ^ split[S]):
+                if part & (part - 1) == 0:
+                    r = leaf[_low_index(part)]
+                else:
+                    r = inner_pool[nxt]
+                    nxt += 1
+                    stack.append((part, r))
+                set_parent(r, me)
+                refs.append(r)
+            child[me] = refs
+        for S, me in reversed(made[1:]):
+            blo, bhi, k = members(S)
+            nlo[me], nhi[me], cnt[me] = blo, bhi, k
+            cost[me] = dp[S]
+            col[me] = _node_cost(_half_area(blo, bhi), F(dp[split[S]] + dp[S ^ split[S]]), k, min_leaf, max_leaf)[1]
+
+    for node in reversed(pre):                   # every node after its subtree
+        if treelet >= 3:
+            restructure(node)
+        la, ha, ca, na = info(child[node][0])
+        lb, hb, cbb, nb = info(child[node][1])
         blo, bhi = np.minimum(la, lb), np.maximum(ha, hb)
-        area = _half_area(blo, bhi)
-        tree = F(F(F(F(0.5) * area) + ca) + cbb)
-        k = na + nb
-        leaf = F(F(k) * area)
-        c_ = k <= min(max_leaf, 3) or (k <= max_leaf and leaf <= tree)
-        nlo[node], nhi[node], cnt[node], col[node] = blo, bhi, k, c_
-        cost[node] = leaf if c_ else tree
+        nlo[node], nhi[node], cnt[node] = blo, bhi, na + nb
+        cost[node], col[node] = _node_cost(_half_area(blo, bhi), F(ca + cbb), na + nb, min_leaf, max_leaf)
+
+    def count_of(c):
+        return 1 if c & LEAF else cnt[c]
 
     keep = np.zeros(max(m, 0), bool)
     depth = np.zeros(max(m, 0), np.int64)
-    for node in reversed(post):                  # parents before children
-        par = parent[node]
-        if col[node] or (par >= 0 and not keep[par]):
-            continue
-        keep[node] = True
-        depth[node] = 0 if par < 0 else depth[par] + 1
+    offset = [0] * max(m, 0)
+    for i in range(max(m, 0)):
+        kp, off, d = not col[i], 0, 0
+        c, a = i, parent[i]
+        while a >= 0:
+            if col[a]:
+                kp = False
+            if child[a][1] == c:
+                off += count_of(child[a][0])
+            d += 1
+            c, a = a, parent[a]
+        keep[i], offset[i], depth[i] = kp, off, d
+    pos = np.zeros(n, np.int64)
+    for p in range(n):
+        a = parent_leaf[p]
+        if a >= 0:
+            pos[p] = offset[a] + (count_of(child[a][0]) if child[a][1] == (LEAF | p) else 0)
+    final = np.empty(n, np.int64)
+    final[pos] = order
     scan = np.cumsum(keep) - keep
     kept = int(keep.sum())
 
@@ -146,21 +252,20 @@ def build(positions: np.ndarray, faces: np.ndarray, max_leaf: int = 8) -> dict:
     leaf_last = []
 
     def ref(c):
-        c = int(c)
         if c & LEAF:
             p = c & ~LEAF
-            leaf_last.append(p)
-            return slo[p], shi[p], c
+            leaf_last.append(int(pos[p]))
+            return slo[p], shi[p], LEAF | int(pos[p])
         if col[c]:
-            leaf_last.append(int(rng[c, 1]))
-            return nlo[c], nhi[c], LEAF | int(rng[c, 0])
+            leaf_last.append(offset[c] + cnt[c] - 1)
+            return nlo[c], nhi[c], LEAF | offset[c]
         return nlo[c], nhi[c], int(scan[c])
 
     for i in range(max(m, 0)):
         if not keep[i]:
             continue
-        l0, h0, r0 = ref(child[i, 0])
-        l1, h1, r1 = ref(child[i, 1])
+        l0, h0, r0 = ref(child[i][0])
+        l1, h1, r1 = ref(child[i][1])
         d = nhi[i] - nlo[i]
         axis = 0 if (d[0] > d[1] and d[0] > d[2]) else (1 if d[1] > d[2] else 2)
         c0 = F(F(l0[axis] + h0[axis]) * F(0.5))
@@ -177,9 +282,10 @@ def build(positions: np.ndarray, faces: np.ndarray, max_leaf: int = 8) -> dict:
     else:
         root_ref = 0
         rlo, rhi = nlo[0], nhi[0]
-    return {"order": order, "inner": inner, "leaf_last": np.array(sorted(leaf_last), np.int64),
+    return {"order": final, "inner": inner, "leaf_last": np.array(sorted(leaf_last), np.int64),
             "root_ref": root_ref, "root_lo": rlo, "root_hi": rhi,
-            "depth": int(depth[keep].max() + 1) if kept else 0, "leaves": len(leaf_last)}
+            "depth": int(depth[keep].max() + 1) if kept else 0, "leaves": len(leaf_last),
+            "sah_cost": float(cost[0] / _half_area(rlo, rhi)) if m > 0 else 1.0}
 
 
 def tri_records(positions: np.ndarray, faces_sorted: np.ndarray, leaf_last: np.ndarray) -> np.ndarray:

@@ -170,17 +170,19 @@ class SceneManager:
         check(lib().pt_scene_set_punctual_lights(self._h, ptr(L), len(L)))
 
     # -- prep / upload --
-    def build_accel(self, builder: str = "host", device: int = 0, max_leaf: int = 0) -> dict | None:
+    def build_accel(self, builder: str = "host", device: int = 0, max_leaf: int = 0,
+                    treelet: int = 0) -> dict | None:
         """SceneManager::buildAccel.  builder="host" is the reference's SAH
-        build (node for node); builder="device" builds a linear BVH with SAH
-        leaf collapse on `device` and returns its timings and sizes."""
+        build (node for node); builder="device" builds a linear BVH on
+        `device`, re-topologises its treelets of `treelet` leaves (0 = 7, 1 =
+        off) and collapses leaves by the SAH, and returns its timings and sizes."""
         if builder == "host":
             check(lib().pt_scene_build_accel(self._h))
             return None
         if builder != "device":
             raise ValueError(f"unknown builder {builder!r} (host or device)")
         st = _ffi.BuildStats()
-        check(lib().pt_scene_build_accel_device(self._h, device, max_leaf, C.byref(st)))
+        check(lib().pt_scene_build_accel_device(self._h, device, max_leaf, treelet, C.byref(st)))
         return st.as_dict()
 
     def upload_to_device(self, device: int = 0) -> None:

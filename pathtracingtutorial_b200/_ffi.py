@@ -137,7 +137,7 @@ _SIGS = [
     ("pt_scene_set_camera", C.c_int, [_P, _P]),
     ("pt_scene_get_camera", C.c_int, [_P, _P]),
     ("pt_scene_build_accel", C.c_int, [_P]),
-    ("pt_scene_build_accel_device", C.c_int, [_P, C.c_int32, C.c_uint32, C.POINTER(BuildStats)]),
+    ("pt_scene_build_accel_device", C.c_int, [_P, C.c_int32, C.c_uint32, C.c_uint32, C.POINTER(BuildStats)]),
     ("pt_scene_get_traversal", C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
     ("pt_scene_upload", C.c_int, [_P, C.c_int32]),
     ("pt_scene_info_get", C.c_int, [_P, C.POINTER(SceneInfo)]),

@@ -213,14 +213,17 @@ int pt_scene_build_accel(pt_scene* s) {
     PT_GUARD_END
 }
 
-int pt_scene_build_accel_device(pt_scene* s, int32_t device, uint32_t max_leaf, pt_build_stats* stats) {
+int pt_scene_build_accel_device(pt_scene* s, int32_t device, uint32_t max_leaf, uint32_t treelet_leaves,
+                                pt_build_stats* stats) {
     PT_REQUIRE(s, "null scene");
     PT_REQUIRE(device >= 0, "device must be >= 0");
     PT_REQUIRE(max_leaf <= 64, "max_leaf must be at most 64");
+    PT_REQUIRE(treelet_leaves <= 7, "treelet_leaves must be at most 7");
     PT_GUARD_BEGIN
     invalidate_build(s);
     const uint32_t leaf = max_leaf ? max_leaf : 8u;
-    const int rc = build_accel_device(s, device, leaf, stats);
+    const int treelet = treelet_leaves == 0 ? 7 : (treelet_leaves < 3 ? 0 : static_cast<int>(treelet_leaves));
+    const int rc = build_accel_device(s, device, leaf, treelet, stats);
     if (rc != PT_OK) s->tables = SceneTables{};
     else if (stats) stats->max_leaf = leaf;
     return rc;

@@ -53,6 +53,8 @@ namespace {
 
 constexpr uint32_t kNone = 0xffffffffu;
 constexpr int kLbThreads = 256;
+constexpr int kMaxTreelet = 7;   // leaves of a restructured treelet (2^7 subsets)
+constexpr uint32_t kMaxWalk = 1u << 12;   // bound on any climb to the root (a tree is far shallower)
 
 __device__ __forceinline__ uint32_t ord_of(float f) {
     const uint32_t u = __float_as_uint(f);
@@ -171,7 +173,7 @@ __device__ __forceinline__ int lb_delta(const uint64_t* __restrict__ k, int64_t 
 // Inner node i of the radix tree over n sorted codes (i < n - 1): the range
 // it covers, the split, and its children (kLeafBit | position for a leaf).
 __global__ void __launch_bounds__(kLbThreads) k_lbvh_tree(const uint64_t* __restrict__ k, uint32_t n,
-                                                         uint2* __restrict__ child, uint2* __restrict__ range,
+                                                         uint2* __restrict__ child,
                                                          uint32_t* __restrict__ parent_inner,
                                                          uint32_t* __restrict__ parent_leaf) {
     const int64_t nn = n;
@@ -200,7 +202,6 @@ __global__ void __launch_bounds__(kLbThreads) k_lbvh_tree(const uint64_t* __rest
         if (last == gamma + 1) { c1 = kLeafBit | static_cast<uint32_t>(gamma + 1); parent_leaf[gamma + 1] = ii; }
         else { c1 = static_cast<uint32_t>(gamma + 1); parent_inner[gamma + 1] = ii; }
         child[ii] = make_uint2(c0, c1);
-        range[ii] = make_uint2(static_cast<uint32_t>(first), static_cast<uint32_t>(last));
         if (ii == 0) parent_inner[0] = kNone;
     }
 }
@@ -210,6 +211,7 @@ struct ChildInfo {
     uint32_t count;
 };
 
+// Children written by other threads of the same launch are read through L2.
 __device__ __forceinline__ ChildInfo child_info(uint32_t c, const uint32_t* __restrict__ sorted,
                                                 const float4* __restrict__ blo, const float4* __restrict__ bhi,
                                                 const float4* nlo, const float4* nhi, const uint32_t* ncount) {
@@ -220,7 +222,7 @@ __device__ __forceinline__ ChildInfo child_info(uint32_t c, const uint32_t* __re
         r.hi = bhi[f];
         r.hi.w = half_area(r.lo, r.hi);   // one triangle
         r.count = 1;
-    } else {                              // written by another thread: read through L2
+    } else {
         r.lo = __ldcg(nlo + c);
         r.hi = __ldcg(nhi + c);
         r.count = __ldcg(ncount + c);
@@ -228,65 +230,243 @@ __device__ __forceinline__ ChildInfo child_info(uint32_t c, const uint32_t* __re
     return r;
 }
 
+// SAH cost of a node of `cnt` faces and half area `area` whose children cost
+// `children` together: tree = 0.5 A + children, leaf = cnt A.  It becomes a
+// leaf when it holds at most min_leaf faces (the reference's rule: fewer than
+// LeafThreshold = 4, bvh_builder.cpp:10,99) or at most max_leaf faces at a
+// leaf cost not above its tree cost.
+__device__ __forceinline__ float node_cost(float area, float children, uint32_t cnt, uint32_t min_leaf,
+                                           uint32_t max_leaf, bool& col) {
+    const float tree = __fadd_rn(__fmul_rn(0.5f, area), children);
+    const float leaf = __fmul_rn(__uint2float_rn(cnt), area);
+    col = cnt <= min_leaf || (cnt <= max_leaf && leaf <= tree);
+    return col ? leaf : tree;
+}
+
+__device__ __forceinline__ float ref_area(uint32_t c, const uint32_t* __restrict__ sorted,
+                                          const float4* __restrict__ blo, const float4* __restrict__ bhi,
+                                          const float4* nlo, const float4* nhi) {
+    if (c & kLeafBit) {
+        const uint32_t f = sorted[c & ~kLeafBit];
+        return half_area(blo[f], bhi[f]);
+    }
+    return half_area(__ldcg(nlo + c), __ldcg(nhi + c));
+}
+
+__device__ __forceinline__ void set_parent(uint32_t c, uint32_t p, uint32_t* parent_inner, uint32_t* parent_leaf) {
+    if (c & kLeafBit) __stcg(parent_leaf + (c & ~kLeafBit), p);
+    else __stcg(parent_inner + c, p);
+}
+
+// Treelet restructuring (Karras and Aila, "Fast parallel construction of
+// high-quality bounding volume hierarchies", HPG 2013), one pass.  The treelet
+// of `node`: start from its two children and repeatedly open the inner-node
+// leaf of largest area (first on ties) until `max_leaves` leaves; the treelet's
+// inner nodes (node first, then in opening order) are reused.  Dynamic
+// programming over the 2^k leaf subsets finds the topology of least SAH cost
+// (subsets in increasing order; for subset S the splits P containing S's
+// lowest leaf, in descending submask order, the first strict minimum wins;
+// P becomes the left child).  The new topology is written with the inner
+// nodes handed out depth first, right part first (a LIFO stack), and the
+// moved nodes' summaries are recomputed children first.
+__device__ void restructure(uint32_t node, int max_leaves, uint2* child, uint32_t* parent_inner,
+                            uint32_t* parent_leaf, const uint32_t* __restrict__ sorted,
+                            const float4* __restrict__ blo, const float4* __restrict__ bhi, float4* nlo,
+                            float4* nhi, uint32_t* ncount, uint8_t* __restrict__ collapse, uint32_t min_leaf,
+                            uint32_t max_leaf) {
+    uint32_t leaf[kMaxTreelet];
+    float larea[kMaxTreelet];
+    uint32_t inner[kMaxTreelet - 1];
+    const uint2 ch = __ldcg(child + node);
+    leaf[0] = ch.x;
+    leaf[1] = ch.y;
+    larea[0] = ref_area(ch.x, sorted, blo, bhi, nlo, nhi);
+    larea[1] = ref_area(ch.y, sorted, blo, bhi, nlo, nhi);
+    inner[0] = node;
+    int nl = 2, ni = 1;
+    while (nl < max_leaves) {
+        int best = -1;
+        float ba = 0.0f;
+        for (int i = 0; i < nl; ++i)
+            if (!(leaf[i] & kLeafBit) && (best < 0 || larea[i] > ba)) { ba = larea[i]; best = i; }
+        if (best < 0) break;
+        const uint32_t x = leaf[best];
+        const uint2 cc = __ldcg(child + x);
+        inner[ni++] = x;
+        leaf[best] = cc.x;
+        larea[best] = ref_area(cc.x, sorted, blo, bhi, nlo, nhi);
+        leaf[nl] = cc.y;
+        larea[nl] = ref_area(cc.y, sorted, blo, bhi, nlo, nhi);
+        ++nl;
+    }
+    if (nl < 3) return;
+    float4 llo[kMaxTreelet], lhi[kMaxTreelet];
+    uint32_t lcnt[kMaxTreelet];
+    for (int i = 0; i < nl; ++i) {
+        const ChildInfo ci = child_info(leaf[i], sorted, blo, bhi, nlo, nhi, ncount);
+        llo[i] = ci.lo;
+        lhi[i] = ci.hi;
+        lcnt[i] = ci.count;
+    }
+    float cost[1 << kMaxTreelet];
+    uint8_t split[1 << kMaxTreelet];
+    const uint32_t full = (1u << nl) - 1u;
+    for (uint32_t S = 1; S <= full; ++S) {
+        if ((S & (S - 1)) == 0) { cost[S] = lhi[__ffs(S) - 1].w; continue; }
+        float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+        uint32_t cnt = 0;
+        for (int i = 0; i < nl; ++i) {
+            if (!((S >> i) & 1u)) continue;
+            lo.x = fminf(lo.x, llo[i].x); lo.y = fminf(lo.y, llo[i].y); lo.z = fminf(lo.z, llo[i].z);
+            hi.x = fmaxf(hi.x, lhi[i].x); hi.y = fmaxf(hi.y, lhi[i].y); hi.z = fmaxf(hi.z, lhi[i].z);
+            cnt += lcnt[i];
+        }
+        const uint32_t low = S & (0u - S);
+        float best = INFINITY;
+        uint32_t bp = low;
+        for (uint32_t P = (S - 1u) & S; P; P = (P - 1u) & S) {
+            if (!(P & low)) continue;
+            const float c = __fadd_rn(cost[P], cost[S ^ P]);
+            if (c < best) { best = c; bp = P; }
+        }
+        bool col;
+        cost[S] = node_cost(half_area(lo, hi), best, cnt, min_leaf, max_leaf, col);
+        split[S] = static_cast<uint8_t>(bp);
+    }
+    // write the topology: (subset, inner node) on a LIFO stack
+    uint8_t st_s[kMaxTreelet];
+    uint32_t st_n[kMaxTreelet];
+    uint8_t made_s[kMaxTreelet - 1];
+    uint32_t made_n[kMaxTreelet - 1];
+    int sp = 0, next = 1, nm = 0;
+    st_s[sp] = static_cast<uint8_t>(full);
+    st_n[sp++] = node;
+    while (sp) {
+        --sp;
+        const uint32_t S = st_s[sp], me = st_n[sp];
+        made_s[nm] = static_cast<uint8_t>(S);
+        made_n[nm++] = me;
+        const uint32_t parts[2] = {split[S], S ^ split[S]};
+        uint32_t ref[2];
+        for (int k = 0; k < 2; ++k) {
+            if ((parts[k] & (parts[k] - 1u)) == 0) {
+                ref[k] = leaf[__ffs(parts[k]) - 1];
+            } else {
+                ref[k] = inner[next++];
+                st_s[sp] = static_cast<uint8_t>(parts[k]);
+                st_n[sp++] = ref[k];
+            }
+            set_parent(ref[k], me, parent_inner, parent_leaf);
+        }
+        __stcg(child + me, make_uint2(ref[0], ref[1]));
+    }
+    // summaries of the moved inner nodes, children first (the root's is
+    // written by the caller)
+    for (int j = nm - 1; j >= 1; --j) {
+        const uint32_t S = made_s[j], me = made_n[j];
+        float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+        uint32_t cnt = 0;
+        for (int i = 0; i < nl; ++i) {
+            if (!((S >> i) & 1u)) continue;
+            lo.x = fminf(lo.x, llo[i].x); lo.y = fminf(lo.y, llo[i].y); lo.z = fminf(lo.z, llo[i].z);
+            hi.x = fmaxf(hi.x, lhi[i].x); hi.y = fmaxf(hi.y, lhi[i].y); hi.z = fmaxf(hi.z, lhi[i].z);
+            cnt += lcnt[i];
+        }
+        hi.w = cost[S];
+        bool col;
+        node_cost(half_area(lo, hi), __fadd_rn(cost[split[S]], cost[S ^ split[S]]), cnt, min_leaf, max_leaf, col);
+        __stcg(nlo + me, lo);
+        __stcg(nhi + me, hi);
+        __stcg(ncount + me, cnt);
+        collapse[me] = col ? 1 : 0;
+    }
+}
+
 // One thread per leaf climbs while it is the second to reach a node; the
-// first one stops.  Node box = union of the children; tree cost
-// = 0.5 A + cost(left) + cost(right); leaf cost = count A (A = half area).
-// A node becomes a leaf when it holds at most min_leaf faces (the reference's
-// rule: fewer than LeafThreshold = 4 faces, bvh_builder.cpp:10,99), or at most
-// max_leaf faces at a leaf cost not above its tree cost.
+// first one stops.  At each node reached second: restructure its treelet
+// (when treelet >= 3), then box = union of the children, count, SAH cost and
+// the leaf decision of node_cost.
 __global__ void __launch_bounds__(kLbThreads) k_lbvh_bottom_up(
-    const uint2* __restrict__ child, const uint32_t* __restrict__ parent_inner,
-    const uint32_t* __restrict__ parent_leaf, const uint32_t* __restrict__ sorted, const float4* __restrict__ blo,
-    const float4* __restrict__ bhi, uint32_t n, uint32_t min_leaf, uint32_t max_leaf, float4* nlo, float4* nhi,
-    uint32_t* ncount,
-    uint8_t* __restrict__ collapse, uint32_t* __restrict__ counter) {
+    uint2* child, uint32_t* parent_inner, uint32_t* parent_leaf, const uint32_t* __restrict__ sorted,
+    const float4* __restrict__ blo, const float4* __restrict__ bhi, uint32_t n, uint32_t min_leaf, uint32_t max_leaf,
+    int treelet, float4* nlo, float4* nhi, uint32_t* ncount, uint8_t* __restrict__ collapse,
+    uint32_t* __restrict__ counter, uint32_t* __restrict__ fault) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
-        uint32_t node = parent_leaf[p];
-        while (node != kNone) {
+        uint32_t node = __ldcg(parent_leaf + p);
+        for (uint32_t steps = 0; node != kNone; ++steps) {
+            if (steps >= kMaxWalk) { atomicExch(fault, 1u); break; }
             __threadfence();
             if (atomicAdd(counter + node, 1u) == 0) break;
-            const uint2 ch = child[node];
+            if (treelet >= 3)
+                restructure(node, treelet, child, parent_inner, parent_leaf, sorted, blo, bhi, nlo, nhi, ncount,
+                            collapse, min_leaf, max_leaf);
+            const uint2 ch = __ldcg(child + node);
             const ChildInfo a = child_info(ch.x, sorted, blo, bhi, nlo, nhi, ncount);
             const ChildInfo b = child_info(ch.y, sorted, blo, bhi, nlo, nhi, ncount);
             float4 lo = make_float4(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y), fminf(a.lo.z, b.lo.z), 0.f);
             float4 hi = make_float4(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z), 0.f);
-            const float area = half_area(lo, hi);
-            const float tree = __fadd_rn(__fadd_rn(__fmul_rn(0.5f, area), a.hi.w), b.hi.w);
             const uint32_t cnt = a.count + b.count;
-            const float leaf = __fmul_rn(__uint2float_rn(cnt), area);
-            const bool col = cnt <= min_leaf || (cnt <= max_leaf && leaf <= tree);
-            hi.w = col ? leaf : tree;
+            bool col;
+            hi.w = node_cost(half_area(lo, hi), __fadd_rn(a.hi.w, b.hi.w), cnt, min_leaf, max_leaf, col);
             __stcg(nlo + node, lo);
             __stcg(nhi + node, hi);
             __stcg(ncount + node, cnt);
             collapse[node] = col ? 1 : 0;
-            node = parent_inner[node];
+            node = __ldcg(parent_inner + node);
         }
     }
 }
 
-// keep[i] = inner node i survives (neither it nor an ancestor became a leaf);
-// depth[0] = max over survivors of (edges from the root + 1).
+__device__ __forceinline__ uint32_t ref_count(uint32_t c, const uint32_t* __restrict__ ncount) {
+    return (c & kLeafBit) ? 1u : ncount[c];
+}
+
+// Per inner node i, walking to the root: keep[i] = neither it nor an
+// ancestor became a leaf; offset[i] = its first face in depth-first order
+// (the faces of the left siblings of it and its ancestors); depth[0] = max
+// over survivors of (edges from the root + 1).
 __global__ void __launch_bounds__(kLbThreads) k_lbvh_keep(const uint8_t* __restrict__ collapse,
-                                                         const uint32_t* __restrict__ parent_inner, uint32_t m,
-                                                         uint32_t* __restrict__ keep, uint32_t* __restrict__ depth) {
+                                                         const uint32_t* __restrict__ parent_inner,
+                                                         const uint2* __restrict__ child,
+                                                         const uint32_t* __restrict__ ncount, uint32_t m,
+                                                         uint32_t* __restrict__ keep, uint32_t* __restrict__ offset,
+                                                         uint32_t* __restrict__ depth, uint32_t* __restrict__ fault) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t mr = (m + 31u) & ~31u;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < mr; i += stride) {
         uint32_t kp = 0, dd = 0;
-        if (i < m && !collapse[i]) {
-            kp = 1;
-            for (uint32_t a = parent_inner[i]; a != kNone; a = parent_inner[a]) {
-                if (collapse[a]) { kp = 0; break; }
+        if (i < m) {
+            kp = collapse[i] ? 0u : 1u;
+            uint32_t off = 0;
+            for (uint32_t c = i, a = parent_inner[i]; a != kNone; c = a, a = parent_inner[a]) {
+                if (dd >= kMaxWalk) { atomicExch(fault, 1u); break; }
+                if (collapse[a]) kp = 0;
+                const uint2 ch = child[a];
+                if (ch.y == c) off += ref_count(ch.x, ncount);
                 ++dd;
             }
             keep[i] = kp;
-        } else if (i < m) {
-            keep[i] = 0;
+            offset[i] = off;
         }
         const uint32_t wmax = __reduce_max_sync(0xffffffffu, kp ? dd + 1 : 0u);
         if ((threadIdx.x & 31) == 0 && wmax) atomicMax(depth, wmax);
+    }
+}
+
+// Depth-first position of every face: its parent's offset, plus the left
+// sibling's faces when it is a right child.  With one face, position 0.
+__global__ void __launch_bounds__(kLbThreads) k_lbvh_positions(const uint32_t* __restrict__ parent_leaf,
+                                                              const uint2* __restrict__ child,
+                                                              const uint32_t* __restrict__ ncount,
+                                                              const uint32_t* __restrict__ offset, uint32_t n,
+                                                              uint32_t* __restrict__ pos) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        const uint32_t a = parent_leaf[p];
+        if (a == kNone) { pos[p] = 0; continue; }
+        const uint2 ch = child[a];
+        pos[p] = offset[a] + (ch.y == (kLeafBit | p) ? ref_count(ch.x, ncount) : 0u);
     }
 }
 
@@ -295,50 +475,53 @@ __global__ void __launch_bounds__(kLbThreads) k_lbvh_keep(const uint8_t* __restr
 // gets a zero record.
 __global__ void __launch_bounds__(kLbThreads) k_lbvh_gather(const pt_vertex* __restrict__ v, uint32_t nv,
                                                            const pt_face* __restrict__ f,
-                                                           const uint32_t* __restrict__ sorted, uint32_t n,
+                                                           const uint32_t* __restrict__ sorted,
+                                                           const uint32_t* __restrict__ pos, uint32_t n,
                                                            pt_face* __restrict__ fout, float4* __restrict__ tout) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
         const pt_face fc = f[sorted[p]];
-        fout[p] = fc;
+        const uint32_t q = pos[p];
+        if (q >= n) continue;   // only a malformed tree; the host walk rejects it
+        fout[q] = fc;
         if (fc.v0 >= nv || fc.v1 >= nv || fc.v2 >= nv) {
             const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-            tout[3 * p + 0] = z;
-            tout[3 * p + 1] = z;
-            tout[3 * p + 2] = z;
+            tout[3 * q + 0] = z;
+            tout[3 * q + 1] = z;
+            tout[3 * q + 2] = z;
             continue;
         }
         const float* p0 = v[fc.v0].position;
         const float* p1 = v[fc.v1].position;
         const float* p2 = v[fc.v2].position;
         const float x0 = p0[0], y0 = p0[1], z0 = p0[2];
-        tout[3 * p + 0] = make_float4(x0, y0, z0, __fsub_rn(p1[0], x0));
-        tout[3 * p + 1] = make_float4(__fsub_rn(p1[1], y0), __fsub_rn(p1[2], z0), __fsub_rn(p2[0], x0),
+        tout[3 * q + 0] = make_float4(x0, y0, z0, __fsub_rn(p1[0], x0));
+        tout[3 * q + 1] = make_float4(__fsub_rn(p1[1], y0), __fsub_rn(p1[2], z0), __fsub_rn(p2[0], x0),
                                       __fsub_rn(p2[1], y0));
-        tout[3 * p + 2] = make_float4(__fsub_rn(p2[2], z0), 0.f, 0.f, 0.f);
+        tout[3 * q + 2] = make_float4(__fsub_rn(p2[2], z0), 0.f, 0.f, 0.f);
     }
 }
 
 __device__ __forceinline__ void child_ref(uint32_t c, const uint32_t* __restrict__ sorted,
                                           const float4* __restrict__ blo, const float4* __restrict__ bhi,
                                           const float4* __restrict__ nlo, const float4* __restrict__ nhi,
-                                          const uint8_t* __restrict__ collapse, const uint2* __restrict__ range,
-                                          const uint32_t* __restrict__ scan, float4& lo, float4& hi,
-                                          uint32_t& ref, uint32_t& last) {
+                                          const uint8_t* __restrict__ collapse, const uint32_t* __restrict__ ncount,
+                                          const uint32_t* __restrict__ offset, const uint32_t* __restrict__ pos,
+                                          const uint32_t* __restrict__ scan, float4& lo, float4& hi, uint32_t& ref,
+                                          uint32_t& last) {
     if (c & kLeafBit) {
         const uint32_t p = c & ~kLeafBit;
         const uint32_t f = sorted[p];
         lo = blo[f];
         hi = bhi[f];
-        ref = c;
-        last = p;
+        ref = kLeafBit | pos[p];
+        last = pos[p];
     } else {
         lo = nlo[c];
         hi = nhi[c];
         if (collapse[c]) {
-            const uint2 r = range[c];
-            ref = kLeafBit | r.x;
-            last = r.y;
+            ref = kLeafBit | offset[c];
+            last = offset[c] + ncount[c] - 1u;
         } else {
             ref = scan[c];
             last = kNone;
@@ -348,11 +531,11 @@ __device__ __forceinline__ void child_ref(uint32_t c, const uint32_t* __restrict
 
 // Surviving inner node i -> InnerNode scan[i]; leaves flag their last record.
 __global__ void __launch_bounds__(kLbThreads) k_lbvh_emit(
-    const uint2* __restrict__ child, const uint2* __restrict__ range, const uint32_t* __restrict__ sorted,
-    const float4* __restrict__ blo, const float4* __restrict__ bhi, const float4* __restrict__ nlo,
-    const float4* __restrict__ nhi, const uint8_t* __restrict__ collapse, const uint32_t* __restrict__ keep,
-    const uint32_t* __restrict__ scan, uint32_t m, InnerNode* __restrict__ out, float4* __restrict__ tris,
-    uint32_t* __restrict__ leaves) {
+    const uint2* __restrict__ child, const uint32_t* __restrict__ sorted, const float4* __restrict__ blo,
+    const float4* __restrict__ bhi, const float4* __restrict__ nlo, const float4* __restrict__ nhi,
+    const uint8_t* __restrict__ collapse, const uint32_t* __restrict__ ncount, const uint32_t* __restrict__ offset,
+    const uint32_t* __restrict__ pos, const uint32_t* __restrict__ keep, const uint32_t* __restrict__ scan,
+    uint32_t m, uint32_t n, InnerNode* __restrict__ out, float4* __restrict__ tris, uint32_t* __restrict__ leaves) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t mr = (m + 31u) & ~31u;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < mr; i += stride) {
@@ -361,10 +544,11 @@ __global__ void __launch_bounds__(kLbThreads) k_lbvh_emit(
             const uint2 ch = child[i];
             float4 l0, h0, l1, h1;
             uint32_t r0, r1, last0, last1;
-            child_ref(ch.x, sorted, blo, bhi, nlo, nhi, collapse, range, scan, l0, h0, r0, last0);
-            child_ref(ch.y, sorted, blo, bhi, nlo, nhi, collapse, range, scan, l1, h1, r1, last1);
-            if (last0 != kNone) { tris[3 * last0 + 2].y = __uint_as_float(1u); ++nleaf; }
-            if (last1 != kNone) { tris[3 * last1 + 2].y = __uint_as_float(1u); ++nleaf; }
+            child_ref(ch.x, sorted, blo, bhi, nlo, nhi, collapse, ncount, offset, pos, scan, l0, h0, r0, last0);
+            child_ref(ch.y, sorted, blo, bhi, nlo, nhi, collapse, ncount, offset, pos, scan, l1, h1, r1, last1);
+            // (last >= n only in a malformed tree, which the host walk rejects)
+            if (last0 != kNone) { if (last0 < n) tris[3 * last0 + 2].y = __uint_as_float(1u); ++nleaf; }
+            if (last1 != kNone) { if (last1 < n) tris[3 * last1 + 2].y = __uint_as_float(1u); ++nleaf; }
             // child order rule: the node's max-extent axis and the child centres on it
             const float4 pl = nlo[i], ph = nhi[i];
             const float dx = __fsub_rn(ph.x, pl.x), dy = __fsub_rn(ph.y, pl.y), dz = __fsub_rn(ph.z, pl.z);
@@ -385,6 +569,50 @@ __global__ void __launch_bounds__(kLbThreads) k_lbvh_emit(
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Walk the built tree from its root on the host before anything traverses it:
+// every inner node reached once, every face in exactly one leaf (a leaf runs
+// to its flagged record), and the longest root-leaf path (edges).
+bool check_tree(const SceneTables& t, uint32_t n, uint32_t& depth, std::string& why) {
+    const uint32_t ni = static_cast<uint32_t>(t.inner.size());
+    std::vector<uint8_t> inner_seen(ni, 0), face_seen(n, 0);
+    uint32_t faces = 0;
+    depth = 0;
+    auto leaf = [&](uint32_t first, uint32_t d) {
+        for (uint32_t i = first;; ++i) {
+            if (i >= n || face_seen[i]) { why = "leaf at " + std::to_string(first) + " overlaps or overruns"; return false; }
+            face_seen[i] = 1;
+            ++faces;
+            if (t.tris[i].flags & 1u) break;
+        }
+        if (d > depth) depth = d;
+        return true;
+    };
+    if (t.root_ref & kLeafBit) {
+        if (!leaf(t.root_ref & ~kLeafBit, 0)) return false;
+    } else {
+        if (ni == 0) { why = "no inner nodes"; return false; }
+        std::vector<std::pair<uint32_t, uint32_t>> stack{{0u, 0u}};
+        inner_seen[0] = 1;
+        while (!stack.empty()) {
+            const auto [k, d] = stack.back();
+            stack.pop_back();
+            for (const uint32_t r : {t.inner[k].ref0, t.inner[k].ref1}) {
+                if (r & kLeafBit) {
+                    if (!leaf(r & ~kLeafBit, d + 1)) return false;
+                } else {
+                    if (r >= ni || inner_seen[r]) { why = "inner node " + std::to_string(r) + " reached twice"; return false; }
+                    inner_seen[r] = 1;
+                    stack.push_back({r, d + 1});
+                }
+            }
+        }
+        for (uint32_t k = 0; k < ni; ++k)
+            if (!inner_seen[k]) { why = "inner node " + std::to_string(k) + " unreachable"; return false; }
+    }
+    if (faces != n) { why = "leaves hold " + std::to_string(faces) + " of " + std::to_string(n) + " faces"; return false; }
+    return true;
+}
+
 int grid_for(uint32_t n, int sms) {
     const uint64_t want = (static_cast<uint64_t>(n) + kLbThreads - 1) / kLbThreads;
     const uint64_t cap = static_cast<uint64_t>(sms) * 8;
@@ -393,7 +621,7 @@ int grid_for(uint32_t n, int sms) {
 
 }  // namespace
 
-int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, pt_build_stats* stats) {
+int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, pt_build_stats* stats) {
     using clock = std::chrono::steady_clock;
     const auto t_start = clock::now();
     HostScene& hs = s->host;
@@ -429,11 +657,11 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, pt_build_stat
     size_t off = 0;
     auto take = [&](size_t bytes) { const size_t o = off; off += align_up(bytes ? bytes : 1); return o; };
     const size_t o_v = take(size_t(nv) * sizeof(pt_vertex)), o_f = take(size_t(n) * sizeof(pt_face));
-    const size_t o_blo = take(size_t(n) * 16), o_bhi = take(size_t(n) * 16), o_cb = take(8 * 4);
+    const size_t o_blo = take(size_t(n) * 16), o_bhi = take(size_t(n) * 16), o_cb = take(16 * 4);
     const size_t o_k0 = take(size_t(n) * 8), o_k1 = take(size_t(n) * 8);
     const size_t o_i0 = take(size_t(n) * 4), o_i1 = take(size_t(n) * 4);
     const size_t o_sort = take(sort_tmp), o_scan = take(scan_tmp);
-    const size_t o_child = take(size_t(m) * 8), o_range = take(size_t(m) * 8);
+    const size_t o_child = take(size_t(m) * 8), o_off = take(size_t(m) * 4), o_pos = take(size_t(n) * 4);
     const size_t o_pin = take(size_t(m) * 4), o_pleaf = take(size_t(n) * 4);
     const size_t o_nlo = take(size_t(m) * 16), o_nhi = take(size_t(m) * 16), o_ncnt = take(size_t(m) * 4);
     const size_t o_col = take(size_t(m)), o_ctr = take(size_t(m) * 4);
@@ -454,7 +682,8 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, pt_build_stat
     uint32_t* i0 = static_cast<uint32_t*>(at(o_i0));
     uint32_t* i1 = static_cast<uint32_t*>(at(o_i1));
     uint2* child = static_cast<uint2*>(at(o_child));
-    uint2* range = static_cast<uint2*>(at(o_range));
+    uint32_t* offset = static_cast<uint32_t*>(at(o_off));
+    uint32_t* pos = static_cast<uint32_t*>(at(o_pos));
     uint32_t* pin = static_cast<uint32_t*>(at(o_pin));
     uint32_t* pleaf = static_cast<uint32_t*>(at(o_pleaf));
     float4* nlo = static_cast<float4*>(at(o_nlo));
@@ -480,36 +709,39 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, pt_build_stat
     LB_CU(cudaMemcpyAsync(d_f, hs.faces.data(), size_t(n) * sizeof(pt_face), cudaMemcpyHostToDevice, stream));
     LB_CU(cudaEventRecord(ev[1], stream));
 
-    // centre bounds start empty; cb[6] = first bad face; cb[7] = depth
-    const uint32_t init[8] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u, 0xffffffffu, 0u};
+    // centre bounds start empty; cb[6] = first bad face; cb[7] = depth; cb[8] = a climb
+    // that did not reach the root
+    const uint32_t init[9] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u, 0xffffffffu, 0u, 0u};
     LB_CU(cudaMemcpyAsync(cb, init, sizeof(init), cudaMemcpyHostToDevice, stream));
     const int g = grid_for(n, sms);
     k_lbvh_boxes<<<g, kLbThreads, 0, stream>>>(d_v, nv, d_f, n, static_cast<int32_t>(hs.materials.size()), blo, bhi,
                                                cb);
     k_lbvh_morton<<<g, kLbThreads, 0, stream>>>(blo, bhi, n, cb, k0, i0);
     LB_CU(cub::DeviceRadixSort::SortPairs(at(o_sort), sort_tmp, k0, k1, i0, i1, static_cast<int>(n), 0, 63, stream));
+    LB_CU(cudaMemsetAsync(pleaf, 0xff, size_t(n) * 4, stream));
     if (m > 0) {
         const int gm = grid_for(m, sms);
-        LB_CU(cudaMemsetAsync(ctr, 0, size_t(m) * 4, stream));
-        k_lbvh_tree<<<gm, kLbThreads, 0, stream>>>(k1, n, child, range, pin, pleaf);
         const uint32_t min_leaf = max_leaf < 3 ? max_leaf : 3;
-        k_lbvh_bottom_up<<<g, kLbThreads, 0, stream>>>(child, pin, pleaf, i1, blo, bhi, n, min_leaf, max_leaf, nlo,
-                                                       nhi, ncnt, col, ctr);
-        k_lbvh_keep<<<gm, kLbThreads, 0, stream>>>(col, pin, m, keep, cb + 7);
+        LB_CU(cudaMemsetAsync(ctr, 0, size_t(m) * 4, stream));
+        k_lbvh_tree<<<gm, kLbThreads, 0, stream>>>(k1, n, child, pin, pleaf);
+        k_lbvh_bottom_up<<<g, kLbThreads, 0, stream>>>(child, pin, pleaf, i1, blo, bhi, n, min_leaf, max_leaf, treelet,
+                                                       nlo, nhi, ncnt, col, ctr, cb + 8);
+        k_lbvh_keep<<<gm, kLbThreads, 0, stream>>>(col, pin, child, ncnt, m, keep, offset, cb + 7, cb + 8);
         LB_CU(cub::DeviceScan::ExclusiveSum(at(o_scan), scan_tmp, keep, scn, static_cast<int>(m), stream));
     }
-    k_lbvh_gather<<<g, kLbThreads, 0, stream>>>(d_v, nv, d_f, i1, n, d_fout, d_tris);
+    k_lbvh_positions<<<g, kLbThreads, 0, stream>>>(pleaf, child, ncnt, offset, n, pos);
+    k_lbvh_gather<<<g, kLbThreads, 0, stream>>>(d_v, nv, d_f, i1, pos, n, d_fout, d_tris);
     if (m > 0) {
         // the bottom-up arrival counters are done with: ctr[0] counts leaves
         LB_CU(cudaMemsetAsync(ctr, 0, 4, stream));
-        k_lbvh_emit<<<grid_for(m, sms), kLbThreads, 0, stream>>>(child, range, i1, blo, bhi, nlo, nhi, col, keep, scn,
-                                                                 m, d_inner, d_tris, ctr);
+        k_lbvh_emit<<<grid_for(m, sms), kLbThreads, 0, stream>>>(child, i1, blo, bhi, nlo, nhi, col, ncnt, offset, pos,
+                                                                 keep, scn, m, n, d_inner, d_tris, ctr);
     }
     LB_CU(cudaGetLastError());
     LB_CU(cudaEventRecord(ev[2], stream));
 
     // scalars: bad face, depth, leaves, survivors, root collapse, root box
-    uint32_t h_cb[8];
+    uint32_t h_cb[9];
     uint32_t h_leaves = 0, h_keep_last = 0, h_scan_last = 0;
     float4 h_root[2] = {};
     LB_CU(cudaMemcpyAsync(h_cb, cb, sizeof(h_cb), cudaMemcpyDeviceToHost, stream));
@@ -532,6 +764,10 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, pt_build_stat
                   std::to_string(hs.materials.size()) + " materials)");
         return PT_ERR_INVALID;
     }
+    if (h_cb[8]) {
+        set_error("GPU BVH build: a climb to the root did not end (malformed tree)");
+        return PT_ERR_DEVICE;
+    }
     const uint32_t kept = m > 0 ? h_scan_last + h_keep_last : 0;
     const uint32_t depth = h_cb[7];
     if (depth >= static_cast<uint32_t>(kStackDepth)) {
@@ -551,18 +787,22 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, pt_build_stat
     LB_CU(cudaStreamSynchronize(stream));
     const auto t_dl = clock::now();
 
+    {
+        uint32_t walked = 0;
+        std::string why;
+        if (kept == 0) t.tris[n - 1].flags |= 1u;
+        t.root_ref = kept == 0 ? kLeafBit : 0u;
+        if (!check_tree(t, n, walked, why) || walked != depth) {
+            set_error("GPU BVH build produced a malformed tree (" + (why.empty() ? "depth mismatch" : why) + ")");
+            t = SceneTables{};
+            return PT_ERR_DEVICE;
+        }
+    }
     for (int a = 0; a < 3; ++a) {
         t.root_lo[a] = (&h_root[0].x)[a];
         t.root_hi[a] = (&h_root[1].x)[a];
     }
-    if (kept == 0) {   // the whole scene is one leaf
-        t.root_ref = kLeafBit;
-        t.tris[n - 1].flags |= 1u;
-        t.num_leaves = 1;
-    } else {
-        t.root_ref = 0;
-        t.num_leaves = h_leaves;
-    }
+    t.num_leaves = kept == 0 ? 1u : h_leaves;   // kept == 0: the whole scene is one leaf
     t.bvh_depth = depth;
     build_emissive_tables(hs, t);
     build_env_tables(hs, t);

@@ -37,16 +37,19 @@ CASES = {
     "soup_dups": lambda: _soup_scene(5000, 5, dup=700),
     "cornell": lambda: (lambda sa: (sa.scene(), sa.vertices, sa.faces))(scenes.cornell_box(width=32, height=32)),
     "spheres": lambda: (lambda sa: (sa.scene(), sa.vertices, sa.faces))(
+        scenes.icosphere_field(n_spheres=8, subdiv=3, width=32, height=18, env_size=(16, 8))),
+    "spheres_large": lambda: (lambda sa: (sa.scene(), sa.vertices, sa.faces))(
         scenes.icosphere_field(n_spheres=40, subdiv=3, width=32, height=18, env_size=(16, 8))),
 }
+EXACT = [k for k in CASES if k != "spheres_large"]
 
 
-@pytest.mark.parametrize("name", list(CASES))
-@pytest.mark.parametrize("max_leaf", [1, 8])
-def test_device_build_bit_exact(name, max_leaf):
+@pytest.mark.parametrize("name", EXACT)
+@pytest.mark.parametrize("max_leaf,treelet", [(1, 1), (8, 1), (1, 7), (8, 7), (8, 4)])
+def test_device_build_bit_exact(name, max_leaf, treelet):
     s, v, f = CASES[name]()
-    st = s.build_accel(builder="device", max_leaf=max_leaf)
-    res = lbvh_ref.build(v["position"], f, max_leaf)
+    st = s.build_accel(builder="device", max_leaf=max_leaf, treelet=treelet)
+    res = lbvh_ref.build(v["position"], f, max_leaf, treelet if treelet >= 3 else 0)
     faces = s.faces()
     assert np.array_equal(faces.view(np.uint32), f[res["order"]].view(np.uint32))
     inner, tris, root = s.traversal_layout()
@@ -60,7 +63,7 @@ def test_device_build_bit_exact(name, max_leaf):
     nodes = s.bvh_nodes()
     assert np.array_equal(nodes.view(np.uint32).reshape(-1, 8), lbvh_ref.reference_nodes(res, len(f)))
     # deterministic
-    s.build_accel(builder="device", max_leaf=max_leaf)
+    s.build_accel(builder="device", max_leaf=max_leaf, treelet=treelet)
     inner2, tris2, _ = s.traversal_layout()
     assert np.array_equal(inner, inner2) and np.array_equal(tris, tris2)
 
@@ -73,7 +76,7 @@ def _rays(n, lo, hi, seed):
     return o, d
 
 
-@pytest.mark.parametrize("name", ["cornell", "spheres", "soup_dups"])
+@pytest.mark.parametrize("name", ["cornell", "spheres_large", "soup_dups"])
 def test_device_tree_hits(oracle, name):
     s, v, f = CASES[name]()
     s.build_accel(builder="device")

@@ -1,7 +1,8 @@
 """The GPU BVH builder's float32 restatement (oracle/lbvh_ref.py) on its own:
-Morton codes of known points, and trees that are valid BVHs whose traversal
-finds the same closest hits as the reference-order tree (both traversed by the
-oracle's C restatement of the reference's traversal)."""
+Morton codes of known points, trees (with and without treelet restructuring)
+that are valid BVHs, restructuring that lowers the SAH cost, and traversal
+that finds the same closest hits as in the reference-order tree (both
+traversed by the oracle's C restatement of the reference's traversal)."""
 import numpy as np
 import pytest
 
@@ -37,11 +38,12 @@ def test_morton_known_values():
     assert full == 2097151
 
 
-@pytest.mark.parametrize("n,dup,max_leaf", [(1, 0, 8), (2, 0, 8), (7, 0, 8), (500, 0, 8), (3000, 400, 8),
-                                            (3000, 0, 1), (3000, 0, 4)])
-def test_oracle_tree_is_a_bvh(n, dup, max_leaf):
+@pytest.mark.parametrize("treelet", [0, 7])
+@pytest.mark.parametrize("n,dup,max_leaf", [(1, 0, 8), (2, 0, 8), (7, 0, 8), (500, 0, 8), (1500, 300, 8),
+                                            (1500, 0, 1), (1500, 0, 4)])
+def test_oracle_tree_is_a_bvh(n, dup, max_leaf, treelet):
     v, f = soup(n, n + dup, dup)
-    res = lbvh_ref.build(v["position"], f, max_leaf)
+    res = lbvh_ref.build(v["position"], f, max_leaf, treelet)
     lo, hi = lbvh_ref.face_boxes(v["position"], f)
     order = res["order"]
     assert sorted(order.tolist()) == list(range(n))
@@ -68,10 +70,17 @@ def test_oracle_tree_is_a_bvh(n, dup, max_leaf):
     assert depth == res["depth"]
 
 
+def test_restructuring_lowers_sah_cost():
+    v, f = soup(2000, 11)
+    plain = lbvh_ref.build(v["position"], f, 8, 0)["sah_cost"]
+    opt = lbvh_ref.build(v["position"], f, 8, 7)["sah_cost"]
+    assert opt < 0.95 * plain, (opt, plain)
+
+
 @pytest.mark.parametrize("name", ["cornell", "spheres"])
 def test_oracle_tree_finds_the_reference_tree_hits(oracle, name):
     sa = {"cornell": lambda: scenes.cornell_box(width=32, height=32),
-          "spheres": lambda: scenes.icosphere_field(n_spheres=12, subdiv=3, width=32, height=18,
+          "spheres": lambda: scenes.icosphere_field(n_spheres=6, subdiv=3, width=32, height=18,
                                                     env_size=(16, 8))}[name]()
     res = lbvh_ref.build(sa.vertices["position"], sa.faces)
     faces = sa.faces[res["order"]]
