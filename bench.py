@@ -53,11 +53,16 @@ def parse_args():
                    help="skip the CPU baseline leg (profiling runs; the line then carries cpu_baseline null)")
     p.add_argument("--paths-in-flight", type=int, default=0,
                    help="wavefront path slots of the render (0: the library default)")
-    p.add_argument("--workload", choices=["render", "batch", "large"], default="render",
+    p.add_argument("--workload", choices=["render", "batch", "large", "build"], default="render",
                    help="render: the bench line; batch: the 64-scene uneven batch in one launch; large: the "
-                        "20M-triangle 16-camera case (separate lines)")
+                        "20M-triangle 16-camera case; build: host vs GPU BVH build of the bench scene "
+                        "(separate lines)")
     p.add_argument("--large-spp", type=int, default=32, help="samples per pixel per camera of --workload large")
     p.add_argument("--large-train-spp", type=int, default=16, help="guide training spp of --workload large")
+    p.add_argument("--builder", choices=["host", "device"], default="host",
+                   help="BVH builder of --workload large: host = the reference's SAH build (node for node), "
+                        "device = the GPU builder (linear BVH + treelet restructuring); both build times are "
+                        "reported")
     p.add_argument("--no-convergence", action="store_true",
                    help="skip the guided-vs-plain convergence leg (the line then carries convergence null)")
     return p.parse_args()
@@ -523,6 +528,12 @@ def large_workload(args):
     t0 = time.perf_counter()
     scene.build_accel()
     t_build = time.perf_counter() - t0
+    d = sa.scene()
+    d.build_accel(builder="device")                            # warm-up: first CUDA use, allocator
+    dev_build = d.build_accel(builder="device")
+    if args.builder == "device":
+        scene = d
+    del d
     t0 = time.perf_counter()
     scene.upload_to_device(0)
     t_upload = time.perf_counter() - t0
@@ -551,9 +562,12 @@ def large_workload(args):
     rays_g = stg["camera_rays"] + stg["extension_rays"] + stg["shadow_rays"]
     g.close()
     print(json.dumps({
-        "metric": METRIC, "workload": f"large scene {info['num_faces']} tri (BVH {info['num_bvh_nodes']} nodes, depth "
-                                      f"{info['bvh_max_depth']}), 16 cameras 1920x1080, {spp} spp each, depth 16",
+        "metric": METRIC, "workload": f"large scene {info['num_faces']} tri ({args.builder}-built BVH "
+                                      f"{info['num_bvh_nodes']} nodes, depth {info['bvh_max_depth']}), 16 cameras "
+                                      f"1920x1080, {spp} spp each, depth 16",
+        "builder": args.builder,
         "host_seconds": {"generate": round(t_gen, 1), "bvh_build": round(t_build, 1), "upload": round(t_upload, 2)},
+        "device_build": {k: (round(v, 2) if isinstance(v, float) else v) for k, v in dev_build.items()},
         "device_bytes": int(info["device_bytes"]),
         "plain": {"value": round(rays / t_plain / 1e6, 2), "unit": METRIC, "seconds": round(t_plain, 3),
                   "paths": int(st["paths"]), "rays": int(rays)},
@@ -561,9 +575,68 @@ def large_workload(args):
                    "train_spp": args.large_train_spp, "train_seconds": round(t_train, 3), "rays": int(rays_g)}}))
 
 
+def build_workload(args):
+    """--workload build: the bench scene (2,048,002 triangles) built by the
+    reference-order host SAH builder and by the GPU builder (defaults: linear
+    BVH, two treelet passes), each tree then traced by the same integrator:
+    64 spp of the 1080p render, best of two, CUDA events.  --steps timed GPU
+    builds after --warmup untimed ones (their median is reported)."""
+    import statistics
+    import torch
+    import pathtracingtutorial_b200 as pt
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    sa = workload(args.small)
+
+    def trace_rate(scene):
+        r = pt.Renderer(scene, stream=stream.cuda_stream)
+        best = None
+        for _ in range(3):
+            r.reset_accumulation()
+            scene.set_frame_count(0)
+            r.integrator.reset_stats()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            r.render_frames(64 // sa.sample_per_frame)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            st = r.integrator.stats()
+            rate = (st["camera_rays"] + st["extension_rays"] + st["shadow_rays"]) / e0.elapsed_time(e1) / 1e3
+            best = rate if best is None else max(best, rate)
+        return best
+
+    host = sa.scene()
+    t0 = time.perf_counter()
+    host.build_accel()
+    host_s = time.perf_counter() - t0
+    host.upload_to_device(0)
+    hi = host.info()
+    host_rate = trace_rate(host)
+    del host
+    dev = sa.scene()
+    for _ in range(max(1, args.warmup)):
+        dev.build_accel(builder="device")
+    runs = [dev.build_accel(builder="device") for _ in range(max(1, args.steps))]
+    dev.upload_to_device(0)
+    di = dev.info()
+    dev_rate = trace_rate(dev)
+    med = {k: round(statistics.median(r[k] for r in runs), 2) for k in runs[0] if k.endswith("_ms")}
+    print(json.dumps({
+        "metric": "BVH build ms", "workload": f"{sa.name} {di['num_faces']} tri", "steps": len(runs),
+        "host": {"build_ms": round(host_s * 1e3, 1), "nodes": hi["num_bvh_nodes"], "depth": hi["bvh_max_depth"],
+                 "trace_mrays": round(host_rate, 1)},
+        "device": {"build_ms": med, "nodes": di["num_bvh_nodes"], "depth": di["bvh_max_depth"],
+                   "trace_mrays": round(dev_rate, 1)},
+        "build_speedup": round(host_s * 1e3 / med["total_ms"], 2),
+        "trace_ratio": round(dev_rate / host_rate, 3)}))
+
+
 def main():
     args = parse_args()
-    if args.workload == "batch":
+    if args.workload == "build":
+        build_workload(args)
+    elif args.workload == "batch":
         batch_workload(args)
     elif args.workload == "large":
         large_workload(args)

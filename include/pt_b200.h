@@ -214,31 +214,38 @@ int pt_scene_build_accel(pt_scene* scene);
 
 /* The same prep with the BVH built on `device` instead of by the reference's
  * host builder (BVHBuilder::build, Part_2/src/accel/bvh_builder.cpp:56-221):
- * a linear BVH over 63-bit Morton codes (Karras radix tree) whose subtrees
- * become leaves by the reference's two rules: at most 3 faces (fewer than its
- * LeafThreshold of 4), or at most `max_leaf` faces (0 = 8) where its SAH cost
- * model (traversal 0.5, intersection 1) prefers a leaf; max_leaf below 3 also
- * caps the first rule.  Before the leaf decisions every inner node's treelet
- * of `treelet_leaves` leaves (0 = 7, 1-2 = off) is re-topologised to its least
- * SAH cost (Karras and Aila's treelet restructuring, one bottom-up pass), and
- * faces are laid out in the final tree's depth-first order.  The tree is
- * walked on the host before it is accepted (PT_ERR_DEVICE if malformed).  Faces are reordered
- * into leaf order as by pt_scene_build_accel; light and environment tables are
- * then built on the host.  Closest-hit distances equal those of the host-built
- * tree; triangle ids, the light table order and hence the images' sample
- * streams differ from the reference's.  Deterministic: the same scene gives
- * the same tree.  Fails with PT_ERR_INVALID when a face indexes a missing
- * vertex or material or the tree is deeper than the traversal stack (64).
- * `stats` may be null. */
+ * a linear BVH over 63-bit Morton codes (Karras radix tree); then, in
+ * `passes` bottom-up passes (0 = 2), every inner node's treelet of
+ * `treelet_leaves` leaves (0 = 7, 1-2 = off) is re-topologised to its least
+ * SAH cost (Karras and Aila's treelet restructuring); subtrees become leaves
+ * by the reference's two rules: at most 3 faces (fewer than its LeafThreshold
+ * of 4), or at most `max_leaf` faces (0 = 8) where the SAH cost model (a
+ * node visit costs `traversal_cost` triangle tests; 0 = 1.0, which traces
+ * faster here than the reference's 0.5) prefers a leaf (max_leaf below 3 also
+ * caps the first rule).  Faces are reordered into the tree's depth-first order as
+ * pt_scene_build_accel reorders them; light and environment tables are then
+ * built on the host, and the tree is walked on the host before it is accepted
+ * (PT_ERR_DEVICE if malformed).  Closest-hit distances equal those of the
+ * host-built tree; triangle ids, the light table order and hence the images'
+ * sample streams differ from the reference's.  Deterministic: the same scene
+ * and options give the same tree.  PT_ERR_INVALID when a face indexes a
+ * missing vertex or material or the tree is deeper than the traversal stack
+ * (64).  `options` and `stats` may be null. */
+typedef struct pt_build_options {
+    uint32_t max_leaf;        /* 0 = 8, at most 64             */
+    uint32_t treelet_leaves;  /* 0 = 7, 1-2 = no restructuring */
+    uint32_t passes;          /* 0 = 2, at most 8              */
+    float    traversal_cost;  /* SAH cost of a node visit in triangle tests; 0 = 1.0 (the reference: 0.5) */
+} pt_build_options;
 typedef struct pt_build_stats {
     double   total_ms;      /* the whole call, host wall time                 */
     double   upload_ms;     /* vertices and faces to the device (CUDA events)  */
-    double   device_ms;     /* boxes, codes, sort, tree, collapse, emission    */
+    double   device_ms;     /* boxes, codes, sort, tree, treelets, emission    */
     double   download_ms;   /* nodes, triangle records, reordered faces back   */
     double   tables_ms;     /* tree check, emissive and environment tables    */
     uint32_t inner_nodes, leaves, depth, max_leaf;
 } pt_build_stats;
-int pt_scene_build_accel_device(pt_scene* scene, int32_t device, uint32_t max_leaf, uint32_t treelet_leaves,
+int pt_scene_build_accel_device(pt_scene* scene, int32_t device, const pt_build_options* options,
                                 pt_build_stats* stats);
 /* ---- scene: upload (SceneManager::uploadToDevice / DeviceScene::uploadFrom,
  *      Part_2/src/scene/device_scene.cu:8-57) ---- */

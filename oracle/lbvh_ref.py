@@ -25,7 +25,9 @@ for bit:
       descending-submask order of the splits holding the lowest leaf, inner
       nodes reused depth first from a LIFO stack); then box = union of the
       children; A = dx dy + dy dz + dz dx;
-      tree cost = 0.5 A + (cost_left + cost_right) (a single face costs its A),
+      tree cost = ct A + (cost_left + cost_right) (ct = traversal_cost, 1.0
+      by default as on the device, the reference's model has 0.5; a single
+      face costs its A),
       leaf cost = count * A, the node becomes a leaf when count <= min(3,
       max_leaf) (the reference's LeafThreshold rule, bvh_builder.cpp:10,99) or
       when count <= max_leaf and leaf cost <= tree cost;
@@ -76,8 +78,8 @@ def _half_area(lo, hi) -> np.float32:
     return F(F(F(dx * dy) + F(dy * dz)) + F(dz * dx))
 
 
-def _node_cost(area, children, cnt, min_leaf, max_leaf):
-    tree = F(F(F(0.5) * area) + children)
+def _node_cost(area, children, cnt, min_leaf, max_leaf, ct=F(0.5)):
+    tree = F(F(F(ct) * area) + children)
     leaf = F(F(cnt) * area)
     col = cnt <= min_leaf or (cnt <= max_leaf and leaf <= tree)
     return (leaf if col else tree), col
@@ -87,12 +89,15 @@ def _low_index(x: int) -> int:
     return (x & -x).bit_length() - 1
 
 
-def build(positions: np.ndarray, faces: np.ndarray, max_leaf: int = 8, treelet: int = 7) -> dict:
+def build(positions: np.ndarray, faces: np.ndarray, max_leaf: int = 8, treelet: int = 7, passes: int = 2,
+          traversal_cost: float = 1.0) -> dict:
     """The device builder's outputs: order (face index per final position),
     inner (uint32[k, 16]), leaf_last (positions whose record ends a leaf),
-    root_ref, root box, depth, leaves.  treelet < 3: no restructuring."""
+    root_ref, root box, depth, leaves.  treelet < 3: no restructuring;
+    otherwise `passes` bottom-up passes, each over the tree the last one left."""
     n = len(faces)
     min_leaf = min(max_leaf, 3)
+    ct = F(traversal_cost)
     lo, hi = face_boxes(positions, faces)
     codes = morton_codes(lo, hi)
     order = np.argsort(codes, kind="stable")
@@ -187,7 +192,7 @@ def build(positions: np.ndarray, faces: np.ndarray, max_leaf: int = 8, treelet: 
                     if best is None or c < best:
                         best, bp = c, P
                 P = (P - 1) & S
-            dp[S] = _node_cost(_half_area(blo, bhi), best, k, min_leaf, max_leaf)[0]
+            dp[S] = _node_cost(_half_area(blo, bhi), best, k, min_leaf, max_leaf, ct)[0]
             split[S] = bp
         stack = [(full, node)]
         nxt = 1
@@ -210,16 +215,24 @@ def build(positions: np.ndarray, faces: np.ndarray, max_leaf: int = 8, treelet: 
             blo, bhi, k = members(S)
             nlo[me], nhi[me], cnt[me] = blo, bhi, k
             cost[me] = dp[S]
-            col[me] = _node_cost(_half_area(blo, bhi), F(dp[split[S]] + dp[S ^ split[S]]), k, min_leaf, max_leaf)[1]
+            col[me] = _node_cost(_half_area(blo, bhi), F(dp[split[S]] + dp[S ^ split[S]]), k, min_leaf, max_leaf, ct)[1]
 
-    for node in reversed(pre):                   # every node after its subtree
-        if treelet >= 3:
-            restructure(node)
-        la, ha, ca, na = info(child[node][0])
-        lb, hb, cbb, nb = info(child[node][1])
-        blo, bhi = np.minimum(la, lb), np.maximum(ha, hb)
-        nlo[node], nhi[node], cnt[node] = blo, bhi, na + nb
-        cost[node], col[node] = _node_cost(_half_area(blo, bhi), F(ca + cbb), na + nb, min_leaf, max_leaf)
+    for _ in range(passes if treelet >= 3 else 1):
+        if m > 0 and not pre:                    # preorder of the tree the last pass left
+            stack = [0]
+            while stack:
+                x = stack.pop()
+                pre.append(x)
+                stack.extend(c for c in child[x] if not c & LEAF)
+        for node in reversed(pre):               # every node after its subtree
+            if treelet >= 3:
+                restructure(node)
+            la, ha, ca, na = info(child[node][0])
+            lb, hb, cbb, nb = info(child[node][1])
+            blo, bhi = np.minimum(la, lb), np.maximum(ha, hb)
+            nlo[node], nhi[node], cnt[node] = blo, bhi, na + nb
+            cost[node], col[node] = _node_cost(_half_area(blo, bhi), F(ca + cbb), na + nb, min_leaf, max_leaf, ct)
+        pre = []
 
     def count_of(c):
         return 1 if c & LEAF else cnt[c]

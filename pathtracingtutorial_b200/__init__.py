@@ -171,18 +171,21 @@ class SceneManager:
 
     # -- prep / upload --
     def build_accel(self, builder: str = "host", device: int = 0, max_leaf: int = 0,
-                    treelet: int = 0) -> dict | None:
+                    treelet: int = 0, passes: int = 0, traversal_cost: float = 0.0) -> dict | None:
         """SceneManager::buildAccel.  builder="host" is the reference's SAH
         build (node for node); builder="device" builds a linear BVH on
         `device`, re-topologises its treelets of `treelet` leaves (0 = 7, 1 =
-        off) and collapses leaves by the SAH, and returns its timings and sizes."""
+        off) in `passes` passes (0 = 2) and collapses leaves by the SAH (a node
+        visit costs `traversal_cost` triangle tests, 0 = 1.0), and returns its
+        timings and sizes."""
         if builder == "host":
             check(lib().pt_scene_build_accel(self._h))
             return None
         if builder != "device":
             raise ValueError(f"unknown builder {builder!r} (host or device)")
         st = _ffi.BuildStats()
-        check(lib().pt_scene_build_accel_device(self._h, device, max_leaf, treelet, C.byref(st)))
+        opt = _ffi.BuildOptions(max_leaf, treelet, passes, traversal_cost)
+        check(lib().pt_scene_build_accel_device(self._h, device, C.byref(opt), C.byref(st)))
         return st.as_dict()
 
     def upload_to_device(self, device: int = 0) -> None:

@@ -73,6 +73,11 @@ class RenderSettings(C.Structure):
                 ("flags", C.c_int32), ("paths_in_flight", C.c_int32)]
 
 
+class BuildOptions(C.Structure):
+    _fields_ = [("max_leaf", C.c_uint32), ("treelet_leaves", C.c_uint32), ("passes", C.c_uint32),
+                ("traversal_cost", C.c_float)]
+
+
 class BuildStats(C.Structure):
     _fields_ = [("total_ms", C.c_double), ("upload_ms", C.c_double), ("device_ms", C.c_double),
                 ("download_ms", C.c_double), ("tables_ms", C.c_double), ("inner_nodes", C.c_uint32),
@@ -137,7 +142,7 @@ _SIGS = [
     ("pt_scene_set_camera", C.c_int, [_P, _P]),
     ("pt_scene_get_camera", C.c_int, [_P, _P]),
     ("pt_scene_build_accel", C.c_int, [_P]),
-    ("pt_scene_build_accel_device", C.c_int, [_P, C.c_int32, C.c_uint32, C.c_uint32, C.POINTER(BuildStats)]),
+    ("pt_scene_build_accel_device", C.c_int, [_P, C.c_int32, C.POINTER(BuildOptions), C.POINTER(BuildStats)]),
     ("pt_scene_get_traversal", C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
     ("pt_scene_upload", C.c_int, [_P, C.c_int32]),
     ("pt_scene_info_get", C.c_int, [_P, C.POINTER(SceneInfo)]),

@@ -10,7 +10,8 @@ DeviceScene device_view(const pt_scene* s);
 void free_scene_device(pt_scene* s);
 void unpin_host_arrays(pt_scene* s);
 int  upload_scene(pt_scene* s, int device);
-int  build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, pt_build_stats* stats);
+int  build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, int passes, float ct,
+                         pt_build_stats* stats);
 
 int  film_alloc(pt_film* f);
 void film_free(pt_film* f);

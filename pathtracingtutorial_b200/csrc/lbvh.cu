@@ -231,13 +231,14 @@ __device__ __forceinline__ ChildInfo child_info(uint32_t c, const uint32_t* __re
 }
 
 // SAH cost of a node of `cnt` faces and half area `area` whose children cost
-// `children` together: tree = 0.5 A + children, leaf = cnt A.  It becomes a
+// `children` together: tree = ct A + children, leaf = cnt A (ct = cost of a
+// node visit in triangle tests; the reference's model has 0.5).  It becomes a
 // leaf when it holds at most min_leaf faces (the reference's rule: fewer than
 // LeafThreshold = 4, bvh_builder.cpp:10,99) or at most max_leaf faces at a
 // leaf cost not above its tree cost.
 __device__ __forceinline__ float node_cost(float area, float children, uint32_t cnt, uint32_t min_leaf,
-                                           uint32_t max_leaf, bool& col) {
-    const float tree = __fadd_rn(__fmul_rn(0.5f, area), children);
+                                           uint32_t max_leaf, float ct, bool& col) {
+    const float tree = __fadd_rn(__fmul_rn(ct, area), children);
     const float leaf = __fmul_rn(__uint2float_rn(cnt), area);
     col = cnt <= min_leaf || (cnt <= max_leaf && leaf <= tree);
     return col ? leaf : tree;
@@ -273,7 +274,7 @@ __device__ void restructure(uint32_t node, int max_leaves, uint2* child, uint32_
                             uint32_t* parent_leaf, const uint32_t* __restrict__ sorted,
                             const float4* __restrict__ blo, const float4* __restrict__ bhi, float4* nlo,
                             float4* nhi, uint32_t* ncount, uint8_t* __restrict__ collapse, uint32_t min_leaf,
-                            uint32_t max_leaf) {
+                            uint32_t max_leaf, float ct) {
     uint32_t leaf[kMaxTreelet];
     float larea[kMaxTreelet];
     uint32_t inner[kMaxTreelet - 1];
@@ -321,16 +322,19 @@ __device__ void restructure(uint32_t node, int max_leaves, uint2* child, uint32_
             hi.x = fmaxf(hi.x, lhi[i].x); hi.y = fmaxf(hi.y, lhi[i].y); hi.z = fmaxf(hi.z, lhi[i].z);
             cnt += lcnt[i];
         }
-        const uint32_t low = S & (0u - S);
+        // the splits P holding S's lowest leaf, in descending order: P = low | Q
+        // for the submasks Q of the other leaves R, Q < R descending
+        const uint32_t low = S & (0u - S), R = S ^ low;
         float best = INFINITY;
         uint32_t bp = low;
-        for (uint32_t P = (S - 1u) & S; P; P = (P - 1u) & S) {
-            if (!(P & low)) continue;
-            const float c = __fadd_rn(cost[P], cost[S ^ P]);
+        for (uint32_t Q = (R - 1u) & R;; Q = (Q - 1u) & R) {
+            const uint32_t P = Q | low;
+            const float c = __fadd_rn(cost[P], cost[R ^ Q]);
             if (c < best) { best = c; bp = P; }
+            if (Q == 0) break;
         }
         bool col;
-        cost[S] = node_cost(half_area(lo, hi), best, cnt, min_leaf, max_leaf, col);
+        cost[S] = node_cost(half_area(lo, hi), best, cnt, min_leaf, max_leaf, ct, col);
         split[S] = static_cast<uint8_t>(bp);
     }
     // write the topology: (subset, inner node) on a LIFO stack
@@ -374,7 +378,7 @@ __device__ void restructure(uint32_t node, int max_leaves, uint2* child, uint32_
         }
         hi.w = cost[S];
         bool col;
-        node_cost(half_area(lo, hi), __fadd_rn(cost[split[S]], cost[S ^ split[S]]), cnt, min_leaf, max_leaf, col);
+        node_cost(half_area(lo, hi), __fadd_rn(cost[split[S]], cost[S ^ split[S]]), cnt, min_leaf, max_leaf, ct, col);
         __stcg(nlo + me, lo);
         __stcg(nhi + me, hi);
         __stcg(ncount + me, cnt);
@@ -389,7 +393,7 @@ __device__ void restructure(uint32_t node, int max_leaves, uint2* child, uint32_
 __global__ void __launch_bounds__(kLbThreads) k_lbvh_bottom_up(
     uint2* child, uint32_t* parent_inner, uint32_t* parent_leaf, const uint32_t* __restrict__ sorted,
     const float4* __restrict__ blo, const float4* __restrict__ bhi, uint32_t n, uint32_t min_leaf, uint32_t max_leaf,
-    int treelet, float4* nlo, float4* nhi, uint32_t* ncount, uint8_t* __restrict__ collapse,
+    float ct, int treelet, float4* nlo, float4* nhi, uint32_t* ncount, uint8_t* __restrict__ collapse,
     uint32_t* __restrict__ counter, uint32_t* __restrict__ fault) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
@@ -400,7 +404,7 @@ __global__ void __launch_bounds__(kLbThreads) k_lbvh_bottom_up(
             if (atomicAdd(counter + node, 1u) == 0) break;
             if (treelet >= 3)
                 restructure(node, treelet, child, parent_inner, parent_leaf, sorted, blo, bhi, nlo, nhi, ncount,
-                            collapse, min_leaf, max_leaf);
+                            collapse, min_leaf, max_leaf, ct);
             const uint2 ch = __ldcg(child + node);
             const ChildInfo a = child_info(ch.x, sorted, blo, bhi, nlo, nhi, ncount);
             const ChildInfo b = child_info(ch.y, sorted, blo, bhi, nlo, nhi, ncount);
@@ -408,7 +412,7 @@ __global__ void __launch_bounds__(kLbThreads) k_lbvh_bottom_up(
             float4 hi = make_float4(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z), 0.f);
             const uint32_t cnt = a.count + b.count;
             bool col;
-            hi.w = node_cost(half_area(lo, hi), __fadd_rn(a.hi.w, b.hi.w), cnt, min_leaf, max_leaf, col);
+            hi.w = node_cost(half_area(lo, hi), __fadd_rn(a.hi.w, b.hi.w), cnt, min_leaf, max_leaf, ct, col);
             __stcg(nlo + node, lo);
             __stcg(nhi + node, hi);
             __stcg(ncount + node, cnt);
@@ -569,59 +573,59 @@ __global__ void __launch_bounds__(kLbThreads) k_lbvh_emit(
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Walk the built tree from its root on the host before anything traverses it:
-// every inner node reached once, every face in exactly one leaf (a leaf runs
-// to its flagged record), and the longest root-leaf path (edges).
-bool check_tree(const SceneTables& t, uint32_t n, uint32_t& depth, std::string& why) {
-    const uint32_t ni = static_cast<uint32_t>(t.inner.size());
-    std::vector<uint8_t> inner_seen(ni, 0), face_seen(n, 0);
-    uint32_t faces = 0;
-    depth = 0;
-    auto leaf = [&](uint32_t first, uint32_t d) {
-        for (uint32_t i = first;; ++i) {
-            if (i >= n || face_seen[i]) { why = "leaf at " + std::to_string(first) + " overlaps or overruns"; return false; }
-            face_seen[i] = 1;
-            ++faces;
-            if (t.tris[i].flags & 1u) break;
-        }
-        if (d > depth) depth = d;
-        return true;
-    };
-    if (t.root_ref & kLeafBit) {
-        if (!leaf(t.root_ref & ~kLeafBit, 0)) return false;
-    } else {
-        if (ni == 0) { why = "no inner nodes"; return false; }
-        std::vector<std::pair<uint32_t, uint32_t>> stack{{0u, 0u}};
-        inner_seen[0] = 1;
-        while (!stack.empty()) {
-            const auto [k, d] = stack.back();
-            stack.pop_back();
-            for (const uint32_t r : {t.inner[k].ref0, t.inner[k].ref1}) {
-                if (r & kLeafBit) {
-                    if (!leaf(r & ~kLeafBit, d + 1)) return false;
-                } else {
-                    if (r >= ni || inner_seen[r]) { why = "inner node " + std::to_string(r) + " reached twice"; return false; }
-                    inner_seen[r] = 1;
-                    stack.push_back({r, d + 1});
-                }
-            }
-        }
-        for (uint32_t k = 0; k < ni; ++k)
-            if (!inner_seen[k]) { why = "inner node " + std::to_string(k) + " unreachable"; return false; }
-    }
-    if (faces != n) { why = "leaves hold " + std::to_string(faces) + " of " + std::to_string(n) + " faces"; return false; }
-    return true;
-}
-
 int grid_for(uint32_t n, int sms) {
     const uint64_t want = (static_cast<uint64_t>(n) + kLbThreads - 1) / kLbThreads;
     const uint64_t cap = static_cast<uint64_t>(sms) * 8;
     return static_cast<int>(want < 1 ? 1 : (want > cap ? cap : want));
 }
 
+// Check the built tree on the host before anything traverses it, in linear
+// passes: every child reference in range, every inner node but the root
+// referenced exactly once and the root never (so the part reachable from the
+// root is a tree), and the leaves tiling the triangle records exactly (each
+// leaf starts where the previous flagged record ends, the last record is
+// flagged).  Traversal then ends and reads only within the arrays.
+bool check_tree(const SceneTables& t, uint32_t n, std::string& why) {
+    const uint32_t ni = static_cast<uint32_t>(t.inner.size());
+    std::vector<uint8_t> indeg(ni, 0), starts(n, 0);
+    auto leaf = [&](uint32_t first) {
+        if (first >= n) { why = "leaf start " + std::to_string(first) + " out of range"; return false; }
+        if (starts[first]++) { why = "two leaves start at " + std::to_string(first); return false; }
+        return true;
+    };
+    if (t.root_ref & kLeafBit) {
+        if (ni != 0 || (t.root_ref & ~kLeafBit) != 0) { why = "one-leaf tree with inner nodes"; return false; }
+        if (!leaf(0)) return false;
+    } else {
+        if (ni == 0 || t.root_ref != 0) { why = "no root"; return false; }
+        for (uint32_t k = 0; k < ni; ++k) {
+            for (const uint32_t r : {t.inner[k].ref0, t.inner[k].ref1}) {
+                if (r & kLeafBit) {
+                    if (!leaf(r & ~kLeafBit)) return false;
+                } else if (r == 0 || r >= ni || indeg[r]++) {
+                    why = "inner node reference " + std::to_string(r) + " out of range or repeated";
+                    return false;
+                }
+            }
+        }
+        for (uint32_t k = 1; k < ni; ++k)
+            if (!indeg[k]) { why = "inner node " + std::to_string(k) + " unreferenced"; return false; }
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const bool should_start = i == 0 || (t.tris[i - 1].flags & 1u);
+        if (static_cast<bool>(starts[i]) != should_start) {
+            why = "leaves do not tile the triangle records at " + std::to_string(i);
+            return false;
+        }
+    }
+    if (!(t.tris[n - 1].flags & 1u)) { why = "last triangle record not flagged"; return false; }
+    return true;
+}
+
 }  // namespace
 
-int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, pt_build_stats* stats) {
+int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, int passes, float ct,
+                       pt_build_stats* stats) {
     using clock = std::chrono::steady_clock;
     const auto t_start = clock::now();
     HostScene& hs = s->host;
@@ -722,10 +726,13 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, 
     if (m > 0) {
         const int gm = grid_for(m, sms);
         const uint32_t min_leaf = max_leaf < 3 ? max_leaf : 3;
-        LB_CU(cudaMemsetAsync(ctr, 0, size_t(m) * 4, stream));
         k_lbvh_tree<<<gm, kLbThreads, 0, stream>>>(k1, n, child, pin, pleaf);
-        k_lbvh_bottom_up<<<g, kLbThreads, 0, stream>>>(child, pin, pleaf, i1, blo, bhi, n, min_leaf, max_leaf, treelet,
-                                                       nlo, nhi, ncnt, col, ctr, cb + 8);
+        // later passes restructure the treelets of the restructured tree
+        for (int pass = 0; pass < (treelet >= 3 ? passes : 1); ++pass) {
+            LB_CU(cudaMemsetAsync(ctr, 0, size_t(m) * 4, stream));
+            k_lbvh_bottom_up<<<g, kLbThreads, 0, stream>>>(child, pin, pleaf, i1, blo, bhi, n, min_leaf, max_leaf,
+                                                           ct, treelet, nlo, nhi, ncnt, col, ctr, cb + 8);
+        }
         k_lbvh_keep<<<gm, kLbThreads, 0, stream>>>(col, pin, child, ncnt, m, keep, offset, cb + 7, cb + 8);
         LB_CU(cub::DeviceScan::ExclusiveSum(at(o_scan), scan_tmp, keep, scn, static_cast<int>(m), stream));
     }
@@ -788,12 +795,11 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, 
     const auto t_dl = clock::now();
 
     {
-        uint32_t walked = 0;
         std::string why;
         if (kept == 0) t.tris[n - 1].flags |= 1u;
         t.root_ref = kept == 0 ? kLeafBit : 0u;
-        if (!check_tree(t, n, walked, why) || walked != depth) {
-            set_error("GPU BVH build produced a malformed tree (" + (why.empty() ? "depth mismatch" : why) + ")");
+        if (!check_tree(t, n, why)) {
+            set_error("GPU BVH build produced a malformed tree (" + why + ")");
             t = SceneTables{};
             return PT_ERR_DEVICE;
         }

@@ -45,11 +45,16 @@ EXACT = [k for k in CASES if k != "spheres_large"]
 
 
 @pytest.mark.parametrize("name", EXACT)
-@pytest.mark.parametrize("max_leaf,treelet", [(1, 1), (8, 1), (1, 7), (8, 7), (8, 4)])
-def test_device_build_bit_exact(name, max_leaf, treelet):
+@pytest.mark.parametrize("max_leaf,treelet,passes,ct", [(1, 1, 1, 0.5), (8, 1, 1, 0.5), (1, 7, 1, 0.5), (8, 7, 1, 0.5),
+                                                        (8, 4, 1, 0.5), (8, 7, 2, 1.0), (0, 0, 0, 0.0)])
+def test_device_build_bit_exact(name, max_leaf, treelet, passes, ct):
     s, v, f = CASES[name]()
-    st = s.build_accel(builder="device", max_leaf=max_leaf, treelet=treelet)
-    res = lbvh_ref.build(v["position"], f, max_leaf, treelet if treelet >= 3 else 0)
+    kw = dict(builder="device", max_leaf=max_leaf, treelet=treelet, passes=passes, traversal_cost=ct)
+    st = s.build_accel(**kw)
+    if (max_leaf, treelet, passes, ct) == (0, 0, 0, 0.0):      # the library's defaults
+        res = lbvh_ref.build(v["position"], f)
+    else:
+        res = lbvh_ref.build(v["position"], f, max_leaf, treelet if treelet >= 3 else 0, passes, ct)
     faces = s.faces()
     assert np.array_equal(faces.view(np.uint32), f[res["order"]].view(np.uint32))
     inner, tris, root = s.traversal_layout()
@@ -63,7 +68,7 @@ def test_device_build_bit_exact(name, max_leaf, treelet):
     nodes = s.bvh_nodes()
     assert np.array_equal(nodes.view(np.uint32).reshape(-1, 8), lbvh_ref.reference_nodes(res, len(f)))
     # deterministic
-    s.build_accel(builder="device", max_leaf=max_leaf, treelet=treelet)
+    s.build_accel(**kw)
     inner2, tris2, _ = s.traversal_layout()
     assert np.array_equal(inner, inner2) and np.array_equal(tris, tris2)
 

@@ -38,12 +38,12 @@ def test_morton_known_values():
     assert full == 2097151
 
 
-@pytest.mark.parametrize("treelet", [0, 7])
+@pytest.mark.parametrize("treelet,passes,ct", [(0, 1, 0.5), (7, 1, 0.5), (7, 2, 1.0)])
 @pytest.mark.parametrize("n,dup,max_leaf", [(1, 0, 8), (2, 0, 8), (7, 0, 8), (500, 0, 8), (1500, 300, 8),
                                             (1500, 0, 1), (1500, 0, 4)])
-def test_oracle_tree_is_a_bvh(n, dup, max_leaf, treelet):
+def test_oracle_tree_is_a_bvh(n, dup, max_leaf, treelet, passes, ct):
     v, f = soup(n, n + dup, dup)
-    res = lbvh_ref.build(v["position"], f, max_leaf, treelet)
+    res = lbvh_ref.build(v["position"], f, max_leaf, treelet, passes, ct)
     lo, hi = lbvh_ref.face_boxes(v["position"], f)
     order = res["order"]
     assert sorted(order.tolist()) == list(range(n))
