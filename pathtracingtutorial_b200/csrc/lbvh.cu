@@ -259,22 +259,53 @@ __device__ __forceinline__ void set_parent(uint32_t c, uint32_t p, uint32_t* par
     else __stcg(parent_inner + c, p);
 }
 
+// Leaf subsets of a treelet ordered by size (then value): the dynamic program
+// handles one size at a time, the subsets of a size in parallel.
+struct SubsetTable {
+    uint8_t mask[127];
+    uint8_t start[9];   // subsets of size k: mask[start[k] .. start[k + 1])
+};
+constexpr SubsetTable make_subset_table() {
+    SubsetTable t{};
+    int j = 0;
+    for (int k = 0; k <= 8; ++k) {
+        t.start[k] = static_cast<uint8_t>(j);
+        for (int m = 1; m < 128 && k >= 1; ++m) {
+            int bits = 0;
+            for (int b = 0; b < 7; ++b) bits += (m >> b) & 1;
+            if (bits == k) t.mask[j++] = static_cast<uint8_t>(m);
+        }
+    }
+    return t;
+}
+__constant__ SubsetTable c_subsets = make_subset_table();
+
+// One warp's tables for the treelet it is restructuring.
+struct TreeletScratch {
+    float4 lo[kMaxTreelet], hi[kMaxTreelet];   // leaf boxes, hi.w = leaf cost
+    uint32_t cnt[kMaxTreelet];
+    float cost[1 << kMaxTreelet];
+    uint8_t split[1 << kMaxTreelet];
+};
+
 // Treelet restructuring (Karras and Aila, "Fast parallel construction of
-// high-quality bounding volume hierarchies", HPG 2013), one pass.  The treelet
-// of `node`: start from its two children and repeatedly open the inner-node
-// leaf of largest area (first on ties) until `max_leaves` leaves; the treelet's
-// inner nodes (node first, then in opening order) are reused.  Dynamic
-// programming over the 2^k leaf subsets finds the topology of least SAH cost
-// (subsets in increasing order; for subset S the splits P containing S's
-// lowest leaf, in descending submask order, the first strict minimum wins;
-// P becomes the left child).  The new topology is written with the inner
-// nodes handed out depth first, right part first (a LIFO stack), and the
-// moved nodes' summaries are recomputed children first.
-__device__ void restructure(uint32_t node, int max_leaves, uint2* child, uint32_t* parent_inner,
-                            uint32_t* parent_leaf, const uint32_t* __restrict__ sorted,
-                            const float4* __restrict__ blo, const float4* __restrict__ bhi, float4* nlo,
-                            float4* nhi, uint32_t* ncount, uint8_t* __restrict__ collapse, uint32_t min_leaf,
-                            uint32_t max_leaf, float ct) {
+// high-quality bounding volume hierarchies", HPG 2013), by all 32 lanes of a
+// warp for one node.  The treelet of `node`: start from its two children and
+// repeatedly open the inner-node leaf of largest area (first on ties) until
+// `max_leaves` leaves; the treelet's inner nodes (node first, then in opening
+// order) are reused.  Dynamic programming over the leaf subsets, smaller
+// subsets first (one subset per lane), finds the topology of least SAH cost:
+// for subset S the splits P containing S's lowest leaf, in descending order,
+// the first strict minimum wins; P becomes the left child.  Lane 0 writes
+// the new topology with the inner nodes handed out depth first, right part
+// first (a LIFO stack), and recomputes the moved nodes' summaries children
+// first.
+__device__ void warp_restructure(uint32_t node, int max_leaves, int lane, TreeletScratch& ts, uint2* child,
+                                 uint32_t* parent_inner, uint32_t* parent_leaf, const uint32_t* __restrict__ sorted,
+                                 const float4* __restrict__ blo, const float4* __restrict__ bhi, float4* nlo,
+                                 float4* nhi, uint32_t* ncount, uint8_t* __restrict__ collapse, uint32_t min_leaf,
+                                 uint32_t max_leaf, float ct) {
+    // treelet formation: every lane computes the same (reads broadcast)
     uint32_t leaf[kMaxTreelet];
     float larea[kMaxTreelet];
     uint32_t inner[kMaxTreelet - 1];
@@ -300,124 +331,157 @@ __device__ void restructure(uint32_t node, int max_leaves, uint2* child, uint32_
         larea[nl] = ref_area(cc.y, sorted, blo, bhi, nlo, nhi);
         ++nl;
     }
-    if (nl < 3) return;
-    float4 llo[kMaxTreelet], lhi[kMaxTreelet];
-    uint32_t lcnt[kMaxTreelet];
-    for (int i = 0; i < nl; ++i) {
-        const ChildInfo ci = child_info(leaf[i], sorted, blo, bhi, nlo, nhi, ncount);
-        llo[i] = ci.lo;
-        lhi[i] = ci.hi;
-        lcnt[i] = ci.count;
+    if (nl < 3) return;   // the same on every lane
+    if (lane < nl) {
+        const ChildInfo ci = child_info(leaf[lane], sorted, blo, bhi, nlo, nhi, ncount);
+        ts.lo[lane] = ci.lo;
+        ts.hi[lane] = ci.hi;
+        ts.cnt[lane] = ci.count;
+        ts.cost[1u << lane] = ci.hi.w;
     }
-    float cost[1 << kMaxTreelet];
-    uint8_t split[1 << kMaxTreelet];
+    __syncwarp();
     const uint32_t full = (1u << nl) - 1u;
-    for (uint32_t S = 1; S <= full; ++S) {
-        if ((S & (S - 1)) == 0) { cost[S] = lhi[__ffs(S) - 1].w; continue; }
-        float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
-        uint32_t cnt = 0;
-        for (int i = 0; i < nl; ++i) {
-            if (!((S >> i) & 1u)) continue;
-            lo.x = fminf(lo.x, llo[i].x); lo.y = fminf(lo.y, llo[i].y); lo.z = fminf(lo.z, llo[i].z);
-            hi.x = fmaxf(hi.x, lhi[i].x); hi.y = fmaxf(hi.y, lhi[i].y); hi.z = fmaxf(hi.z, lhi[i].z);
-            cnt += lcnt[i];
-        }
-        // the splits P holding S's lowest leaf, in descending order: P = low | Q
-        // for the submasks Q of the other leaves R, Q < R descending
-        const uint32_t low = S & (0u - S), R = S ^ low;
-        float best = INFINITY;
-        uint32_t bp = low;
-        for (uint32_t Q = (R - 1u) & R;; Q = (Q - 1u) & R) {
-            const uint32_t P = Q | low;
-            const float c = __fadd_rn(cost[P], cost[R ^ Q]);
-            if (c < best) { best = c; bp = P; }
-            if (Q == 0) break;
-        }
-        bool col;
-        cost[S] = node_cost(half_area(lo, hi), best, cnt, min_leaf, max_leaf, ct, col);
-        split[S] = static_cast<uint8_t>(bp);
-    }
-    // write the topology: (subset, inner node) on a LIFO stack
-    uint8_t st_s[kMaxTreelet];
-    uint32_t st_n[kMaxTreelet];
-    uint8_t made_s[kMaxTreelet - 1];
-    uint32_t made_n[kMaxTreelet - 1];
-    int sp = 0, next = 1, nm = 0;
-    st_s[sp] = static_cast<uint8_t>(full);
-    st_n[sp++] = node;
-    while (sp) {
-        --sp;
-        const uint32_t S = st_s[sp], me = st_n[sp];
-        made_s[nm] = static_cast<uint8_t>(S);
-        made_n[nm++] = me;
-        const uint32_t parts[2] = {split[S], S ^ split[S]};
-        uint32_t ref[2];
-        for (int k = 0; k < 2; ++k) {
-            if ((parts[k] & (parts[k] - 1u)) == 0) {
-                ref[k] = leaf[__ffs(parts[k]) - 1];
-            } else {
-                ref[k] = inner[next++];
-                st_s[sp] = static_cast<uint8_t>(parts[k]);
-                st_n[sp++] = ref[k];
+    for (int k = 2; k <= nl; ++k) {
+        for (int j = c_subsets.start[k] + lane; j < c_subsets.start[k + 1]; j += 32) {
+            const uint32_t S = c_subsets.mask[j];
+            if (S > full) continue;
+            float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+            uint32_t cnt = 0;
+            for (int i = 0; i < nl; ++i) {
+                if (!((S >> i) & 1u)) continue;
+                const float4 a = ts.lo[i], b = ts.hi[i];
+                lo.x = fminf(lo.x, a.x); lo.y = fminf(lo.y, a.y); lo.z = fminf(lo.z, a.z);
+                hi.x = fmaxf(hi.x, b.x); hi.y = fmaxf(hi.y, b.y); hi.z = fmaxf(hi.z, b.z);
+                cnt += ts.cnt[i];
             }
-            set_parent(ref[k], me, parent_inner, parent_leaf);
+            // the splits P holding S's lowest leaf, in descending order: P = low | Q
+            // for the submasks Q of the other leaves R, Q < R descending
+            const uint32_t low = S & (0u - S), R = S ^ low;
+            float best = INFINITY;
+            uint32_t bp = low;
+            for (uint32_t Q = (R - 1u) & R;; Q = (Q - 1u) & R) {
+                const float c = __fadd_rn(ts.cost[Q | low], ts.cost[R ^ Q]);
+                if (c < best) { best = c; bp = Q | low; }
+                if (Q == 0) break;
+            }
+            bool col;
+            ts.cost[S] = node_cost(half_area(lo, hi), best, cnt, min_leaf, max_leaf, ct, col);
+            ts.split[S] = static_cast<uint8_t>(bp);
         }
-        __stcg(child + me, make_uint2(ref[0], ref[1]));
+        __syncwarp();
     }
-    // summaries of the moved inner nodes, children first (the root's is
-    // written by the caller)
-    for (int j = nm - 1; j >= 1; --j) {
-        const uint32_t S = made_s[j], me = made_n[j];
-        float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
-        uint32_t cnt = 0;
-        for (int i = 0; i < nl; ++i) {
-            if (!((S >> i) & 1u)) continue;
-            lo.x = fminf(lo.x, llo[i].x); lo.y = fminf(lo.y, llo[i].y); lo.z = fminf(lo.z, llo[i].z);
-            hi.x = fmaxf(hi.x, lhi[i].x); hi.y = fmaxf(hi.y, lhi[i].y); hi.z = fmaxf(hi.z, lhi[i].z);
-            cnt += lcnt[i];
+    if (lane == 0) {
+        // write the topology: (subset, inner node) on a LIFO stack
+        uint8_t st_s[kMaxTreelet];
+        uint32_t st_n[kMaxTreelet];
+        uint8_t made_s[kMaxTreelet - 1];
+        uint32_t made_n[kMaxTreelet - 1];
+        int sp = 0, next = 1, nm = 0;
+        st_s[sp] = static_cast<uint8_t>(full);
+        st_n[sp++] = node;
+        while (sp) {
+            --sp;
+            const uint32_t S = st_s[sp], me = st_n[sp];
+            made_s[nm] = static_cast<uint8_t>(S);
+            made_n[nm++] = me;
+            const uint32_t parts[2] = {ts.split[S], S ^ ts.split[S]};
+            uint32_t ref[2];
+            for (int q = 0; q < 2; ++q) {
+                if ((parts[q] & (parts[q] - 1u)) == 0) {
+                    ref[q] = leaf[__ffs(parts[q]) - 1];
+                } else {
+                    ref[q] = inner[next++];
+                    st_s[sp] = static_cast<uint8_t>(parts[q]);
+                    st_n[sp++] = ref[q];
+                }
+                set_parent(ref[q], me, parent_inner, parent_leaf);
+            }
+            __stcg(child + me, make_uint2(ref[0], ref[1]));
         }
-        hi.w = cost[S];
-        bool col;
-        node_cost(half_area(lo, hi), __fadd_rn(cost[split[S]], cost[S ^ split[S]]), cnt, min_leaf, max_leaf, ct, col);
-        __stcg(nlo + me, lo);
-        __stcg(nhi + me, hi);
-        __stcg(ncount + me, cnt);
-        collapse[me] = col ? 1 : 0;
+        // summaries of the moved inner nodes, children first (the root's is
+        // written by the caller)
+        for (int j = nm - 1; j >= 1; --j) {
+            const uint32_t S = made_s[j], me = made_n[j];
+            float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+            uint32_t cnt = 0;
+            for (int i = 0; i < nl; ++i) {
+                if (!((S >> i) & 1u)) continue;
+                const float4 a = ts.lo[i], b = ts.hi[i];
+                lo.x = fminf(lo.x, a.x); lo.y = fminf(lo.y, a.y); lo.z = fminf(lo.z, a.z);
+                hi.x = fmaxf(hi.x, b.x); hi.y = fmaxf(hi.y, b.y); hi.z = fmaxf(hi.z, b.z);
+                cnt += ts.cnt[i];
+            }
+            hi.w = ts.cost[S];
+            bool col;
+            node_cost(half_area(lo, hi), __fadd_rn(ts.cost[ts.split[S]], ts.cost[S ^ ts.split[S]]), cnt, min_leaf,
+                      max_leaf, ct, col);
+            __stcg(nlo + me, lo);
+            __stcg(nhi + me, hi);
+            __stcg(ncount + me, cnt);
+            collapse[me] = col ? 1 : 0;
+        }
     }
+    __syncwarp();
 }
 
 // One thread per leaf climbs while it is the second to reach a node; the
-// first one stops.  At each node reached second: restructure its treelet
-// (when treelet >= 3), then box = union of the children, count, SAH cost and
-// the leaf decision of node_cost.
+// first one stops.  At each node reached second: the warp restructures the
+// node's treelet (when treelet >= 3; the warp takes its lanes' nodes one at a
+// time), then the owner lane writes box = union of the children, count, SAH
+// cost and the leaf decision of node_cost.  Every climb ends within kMaxWalk
+// steps or raises `fault`.
 __global__ void __launch_bounds__(kLbThreads) k_lbvh_bottom_up(
     uint2* child, uint32_t* parent_inner, uint32_t* parent_leaf, const uint32_t* __restrict__ sorted,
     const float4* __restrict__ blo, const float4* __restrict__ bhi, uint32_t n, uint32_t min_leaf, uint32_t max_leaf,
     float ct, int treelet, float4* nlo, float4* nhi, uint32_t* ncount, uint8_t* __restrict__ collapse,
     uint32_t* __restrict__ counter, uint32_t* __restrict__ fault) {
+    __shared__ TreeletScratch scratch[kLbThreads / 32];
+    const int lane = threadIdx.x & 31;
+    TreeletScratch& ts = scratch[threadIdx.x >> 5];
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
-        uint32_t node = __ldcg(parent_leaf + p);
-        for (uint32_t steps = 0; node != kNone; ++steps) {
-            if (steps >= kMaxWalk) { atomicExch(fault, 1u); break; }
-            __threadfence();
-            if (atomicAdd(counter + node, 1u) == 0) break;
-            if (treelet >= 3)
-                restructure(node, treelet, child, parent_inner, parent_leaf, sorted, blo, bhi, nlo, nhi, ncount,
-                            collapse, min_leaf, max_leaf, ct);
-            const uint2 ch = __ldcg(child + node);
-            const ChildInfo a = child_info(ch.x, sorted, blo, bhi, nlo, nhi, ncount);
-            const ChildInfo b = child_info(ch.y, sorted, blo, bhi, nlo, nhi, ncount);
-            float4 lo = make_float4(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y), fminf(a.lo.z, b.lo.z), 0.f);
-            float4 hi = make_float4(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z), 0.f);
-            const uint32_t cnt = a.count + b.count;
-            bool col;
-            hi.w = node_cost(half_area(lo, hi), __fadd_rn(a.hi.w, b.hi.w), cnt, min_leaf, max_leaf, ct, col);
-            __stcg(nlo + node, lo);
-            __stcg(nhi + node, hi);
-            __stcg(ncount + node, cnt);
-            collapse[node] = col ? 1 : 0;
-            node = __ldcg(parent_inner + node);
+    const uint32_t nr = (n + 31u) & ~31u;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < nr; p += stride) {   // whole warps
+        uint32_t node = p < n ? __ldcg(parent_leaf + p) : kNone;
+        uint32_t steps = 0;
+        while (__any_sync(0xffffffffu, node != kNone)) {
+            bool mine = false;
+            if (node != kNone) {
+                if (steps++ >= kMaxWalk) {
+                    atomicExch(fault, 1u);
+                    node = kNone;
+                } else {
+                    __threadfence();
+                    mine = atomicAdd(counter + node, 1u) != 0;
+                    if (mine) __threadfence();
+                    else node = kNone;
+                }
+            }
+            if (treelet >= 3) {
+                uint32_t need = __ballot_sync(0xffffffffu, mine);
+                __syncwarp();
+                while (need) {
+                    const int src = __ffs(need) - 1;
+                    need &= need - 1u;
+                    const uint32_t t = __shfl_sync(0xffffffffu, node, src);
+                    warp_restructure(t, treelet, lane, ts, child, parent_inner, parent_leaf, sorted, blo, bhi, nlo,
+                                     nhi, ncount, collapse, min_leaf, max_leaf, ct);
+                }
+            }
+            if (mine) {
+                const uint2 ch = __ldcg(child + node);
+                const ChildInfo a = child_info(ch.x, sorted, blo, bhi, nlo, nhi, ncount);
+                const ChildInfo b = child_info(ch.y, sorted, blo, bhi, nlo, nhi, ncount);
+                float4 lo = make_float4(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y), fminf(a.lo.z, b.lo.z), 0.f);
+                float4 hi = make_float4(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z), 0.f);
+                const uint32_t cnt = a.count + b.count;
+                bool col;
+                hi.w = node_cost(half_area(lo, hi), __fadd_rn(a.hi.w, b.hi.w), cnt, min_leaf, max_leaf, ct, col);
+                __stcg(nlo + node, lo);
+                __stcg(nhi + node, hi);
+                __stcg(ncount + node, cnt);
+                collapse[node] = col ? 1 : 0;
+                node = __ldcg(parent_inner + node);
+            }
         }
     }
 }
