@@ -243,6 +243,7 @@ typedef struct pt_build_stats {
     double   device_ms;     /* boxes, codes, sort, tree, treelets, emission    */
     double   download_ms;   /* nodes, triangle records, reordered faces back   */
     double   tables_ms;     /* tree check, emissive and environment tables    */
+    double   setup_ms;      /* device arena, stream and events                */
     uint32_t inner_nodes, leaves, depth, max_leaf;
 } pt_build_stats;
 int pt_scene_build_accel_device(pt_scene* scene, int32_t device, const pt_build_options* options,

@@ -80,14 +80,15 @@ class BuildOptions(C.Structure):
 
 class BuildStats(C.Structure):
     _fields_ = [("total_ms", C.c_double), ("upload_ms", C.c_double), ("device_ms", C.c_double),
-                ("download_ms", C.c_double), ("tables_ms", C.c_double), ("inner_nodes", C.c_uint32),
+                ("download_ms", C.c_double), ("tables_ms", C.c_double), ("setup_ms", C.c_double),
+                ("inner_nodes", C.c_uint32),
                 ("leaves", C.c_uint32), ("depth", C.c_uint32), ("max_leaf", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-assert C.sizeof(BuildStats) == 56
+assert C.sizeof(BuildStats) == 64
 
 
 class SceneInfo(C.Structure):

@@ -2,7 +2,11 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "pt_internal.h"
@@ -26,6 +30,22 @@ struct HostScene {
     std::string                    output_file = "output.hdr";
 };
 
+// Allocator whose resize() leaves new elements default-initialised (plain
+// records: uninitialised), for large arrays that are written in full right
+// after they are sized.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U> struct rebind { using other = NoInitAlloc<U>; };
+    NoInitAlloc() = default;
+    template <class U> NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <class U> void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A> void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+
 // Prep results (SceneManager::buildAccel, Part_2/src/scene/scene_manager.cpp:28-41).
 struct SceneTables {
     bool built = false;
@@ -38,8 +58,8 @@ struct SceneTables {
     std::vector<pt_alias_entry>  env_alias;
     int32_t                      env_w = 0, env_h = 0;
     // traversal layout
-    std::vector<InnerNode>       inner;
-    std::vector<TriRecord>       tris;
+    std::vector<InnerNode, NoInitAlloc<InnerNode>> inner;   // every record written by its builder
+    std::vector<TriRecord, NoInitAlloc<TriRecord>> tris;
     float                        root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
     uint32_t                     root_ref = 0;
     uint32_t                     num_leaves = 0;

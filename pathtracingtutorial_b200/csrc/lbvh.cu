@@ -31,9 +31,11 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "device_api.h"
@@ -637,6 +639,23 @@ __global__ void __launch_bounds__(kLbThreads) k_lbvh_emit(
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Fault in freshly allocated host pages from several cores (each thread
+// zeroes its own slice) before a device-to-host copy writes them: the copy
+// then runs at the speed of resident memory.
+void touch_pages(void* p, size_t bytes) {
+    if (bytes < (size_t(64) << 20)) { std::memset(p, 0, bytes); return; }
+    const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    const size_t chunk = (bytes + nt - 1) / nt;
+    std::vector<std::thread> pool;
+    for (unsigned i = 0; i < nt; ++i) {
+        const size_t a = i * chunk;
+        if (a >= bytes) break;
+        const size_t len = std::min(chunk, bytes - a);
+        pool.emplace_back([p, a, len] { std::memset(static_cast<char*>(p) + a, 0, len); });
+    }
+    for (std::thread& t : pool) t.join();
+}
+
 int grid_for(uint32_t n, int sms) {
     const uint64_t want = (static_cast<uint64_t>(n) + kLbThreads - 1) / kLbThreads;
     const uint64_t cap = static_cast<uint64_t>(sms) * 8;
@@ -772,6 +791,7 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, 
     for (auto& e : ev) LB_CU(cudaEventCreate(&e));
     struct EFree { cudaEvent_t* e; ~EFree() { for (int i = 0; i < 3; ++i) cudaEventDestroy(e[i]); } } eguard{ev};
 
+    const auto t_setup = clock::now();
     LB_CU(cudaEventRecord(ev[0], stream));
     LB_CU(cudaMemcpyAsync(d_v, hs.vertices.data(), size_t(nv) * sizeof(pt_vertex), cudaMemcpyHostToDevice, stream));
     LB_CU(cudaMemcpyAsync(d_f, hs.faces.data(), size_t(n) * sizeof(pt_face), cudaMemcpyHostToDevice, stream));
@@ -811,6 +831,11 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, 
     LB_CU(cudaGetLastError());
     LB_CU(cudaEventRecord(ev[2], stream));
 
+    // the environment tables do not depend on the tree: build them while the device works
+    const auto t_env0 = clock::now();
+    build_env_tables(hs, t);
+    const double env_ms = std::chrono::duration<double, std::milli>(clock::now() - t_env0).count();
+
     // scalars: bad face, depth, leaves, survivors, root collapse, root box
     uint32_t h_cb[9];
     uint32_t h_leaves = 0, h_keep_last = 0, h_scan_last = 0;
@@ -847,9 +872,11 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, 
         return PT_ERR_INVALID;
     }
 
+    const auto t_dl0 = clock::now();
     t.inner.resize(kept);
     t.tris.resize(n);
-    const auto t_dl0 = clock::now();
+    touch_pages(t.inner.data(), size_t(kept) * sizeof(InnerNode));
+    touch_pages(t.tris.data(), size_t(n) * sizeof(TriRecord));
     if (kept)
         LB_CU(cudaMemcpyAsync(t.inner.data(), d_inner, size_t(kept) * sizeof(InnerNode), cudaMemcpyDeviceToHost,
                               stream));
@@ -875,7 +902,6 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, 
     t.num_leaves = kept == 0 ? 1u : h_leaves;   // kept == 0: the whole scene is one leaf
     t.bvh_depth = depth;
     build_emissive_tables(hs, t);
-    build_env_tables(hs, t);
     t.built = true;
     const auto t_end = clock::now();
 
@@ -885,7 +911,8 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, 
     st.upload_ms = ms_up;
     st.device_ms = ms_build;
     st.download_ms = std::chrono::duration<double, std::milli>(t_dl - t_dl0).count();
-    st.tables_ms = std::chrono::duration<double, std::milli>(t_end - t_dl).count();
+    st.tables_ms = std::chrono::duration<double, std::milli>(t_end - t_dl).count() + env_ms;
+    st.setup_ms = std::chrono::duration<double, std::milli>(t_setup - t_start).count();
     st.total_ms = std::chrono::duration<double, std::milli>(t_end - t_start).count();
     st.inner_nodes = kept;
     st.leaves = t.num_leaves;
