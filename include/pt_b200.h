@@ -257,6 +257,7 @@ int pt_scene_build_params(const pt_scene* scene, pt_scene_params* out);         
 int pt_scene_get_vertices(const pt_scene* scene, pt_vertex* out, uint32_t cap);
 int pt_scene_get_faces(const pt_scene* scene, pt_face* out, uint32_t cap);
 int pt_scene_get_materials(const pt_scene* scene, pt_material* out, uint32_t cap);
+int pt_scene_get_punctual_lights(const pt_scene* scene, pt_punctual_light* out, uint32_t cap);
 int pt_scene_get_bvh(const pt_scene* scene, pt_bvh_node* out, uint32_t cap);
 int pt_scene_get_emissive(const pt_scene* scene, pt_emissive_ref* refs, uint32_t cap_refs,
                           float* face_pmf, uint32_t cap_pmf,

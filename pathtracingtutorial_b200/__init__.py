@@ -217,6 +217,11 @@ class SceneManager:
         check(lib().pt_scene_get_materials(self._h, ptr(out), len(out)))
         return out
 
+    def punctual_lights(self) -> np.ndarray:
+        out = np.zeros(self.info()["num_punctual_lights"], PUNCTUAL_DTYPE)
+        check(lib().pt_scene_get_punctual_lights(self._h, ptr(out), len(out)))
+        return out
+
     def bvh_nodes(self) -> np.ndarray:
         out = np.zeros(self.info()["num_bvh_nodes"], BVH_NODE_DTYPE)
         check(lib().pt_scene_get_bvh(self._h, ptr(out), len(out)))

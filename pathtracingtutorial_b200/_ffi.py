@@ -151,6 +151,7 @@ _SIGS = [
     ("pt_scene_get_vertices", C.c_int, [_P, _P, C.c_uint32]),
     ("pt_scene_get_faces", C.c_int, [_P, _P, C.c_uint32]),
     ("pt_scene_get_materials", C.c_int, [_P, _P, C.c_uint32]),
+    ("pt_scene_get_punctual_lights", C.c_int, [_P, _P, C.c_uint32]),
     ("pt_scene_get_bvh", C.c_int, [_P, _P, C.c_uint32]),
     ("pt_scene_get_emissive", C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32]),
     ("pt_scene_get_env_tables", C.c_int, [_P, _P, _P, C.c_uint32]),

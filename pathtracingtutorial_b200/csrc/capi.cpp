@@ -290,6 +290,10 @@ int pt_scene_get_materials(const pt_scene* s, pt_material* out, uint32_t cap) {
     PT_REQUIRE(s, "null scene");
     return copy_out(s->host.materials, out, cap);
 }
+int pt_scene_get_punctual_lights(const pt_scene* s, pt_punctual_light* out, uint32_t cap) {
+    PT_REQUIRE(s, "null scene");
+    return copy_out(s->host.punctual, out, cap);
+}
 int pt_scene_get_bvh(const pt_scene* s, pt_bvh_node* out, uint32_t cap) {
     PT_REQUIRE(s, "null scene");
     PT_GUARD_BEGIN

@@ -8,9 +8,9 @@
 //   materials{name:{...}}   -- indexed in sorted key order, as the reference's
 //                              JSON library stores objects in a sorted map
 //   lights[{type,position,direction,color,intensity,range,innerCone,outerCone}]
-//   objects[{type: quad|mesh, vertices|file, material, transform}]
-// glTF objects are not supported (the glTF importer is outside this library);
-// such a scene is rejected with an error instead of being rendered without them.
+//   objects[{type: quad|mesh|gltf, vertices|file, material, transform,
+//            materialOverrides}]
+// A path ending in .gltf / .glb is read as a glTF scene (see load_gltf).
 #include <cctype>
 #include <cerrno>
 #include <cmath>
@@ -515,9 +515,506 @@ bool load_obj(const std::string& path, int mat, const float xform[16],
 }
 
 // ---------------------------------------------------------------------------
+// glTF 2.0 (GltfSceneLoader::load, Part_2/src/io/gltf_loader.cpp:588-734):
+// .gltf (JSON with external or data-URI buffers) and .glb (JSON and BIN
+// chunks).  The default scene's node tree is walked with world = parent *
+// local (a node's matrix, else T * R * S); every triangle primitive adds its
+// vertices (positions by the world transform, normals by its inverse
+// transpose and normalised, tangents by the world transform; normals that
+// are absent are the normalised sums of the primitive's face normals) and its
+// faces (indexed by 8/16/32-bit indices, else consecutive triples), on
+// material `offset + material` or 0 when it has none.  Materials: the metal-
+// rough factors and the emissive, ior, transmission, clearcoat, sheen,
+// specular, volume and anisotropy extensions and the alpha mode
+// (loadMaterials, gltf_loader.cpp:172-347); KHR_lights_punctual lights sit at
+// their node's origin looking down its -z.  Vertex attributes must be FLOAT
+// (the reference reads them as floats).  Files with textures or images are
+// rejected: this library has no image decoder and samples no textures.
+// ---------------------------------------------------------------------------
+namespace {
+
+std::string read_binary_file(const std::string& path) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in) throw json::Error{"cannot open " + path};
+    std::stringstream ss;
+    ss << in.rdbuf();
+    return ss.str();
+}
+
+std::string base64_decode(const std::string& s, size_t from) {
+    auto val = [](char c) -> int {
+        if (c >= 'A' && c <= 'Z') return c - 'A';
+        if (c >= 'a' && c <= 'z') return c - 'a' + 26;
+        if (c >= '0' && c <= '9') return c - '0' + 52;
+        if (c == '+' || c == '-') return 62;
+        if (c == '/' || c == '_') return 63;
+        return -1;
+    };
+    std::string out;
+    uint32_t acc = 0;
+    int bits = 0;
+    for (size_t i = from; i < s.size(); ++i) {
+        if (s[i] == '=') break;
+        const int v = val(s[i]);
+        if (v < 0) continue;
+        acc = (acc << 6) | static_cast<uint32_t>(v);
+        bits += 6;
+        if (bits >= 8) { bits -= 8; out.push_back(static_cast<char>((acc >> bits) & 0xffu)); }
+    }
+    return out;
+}
+
+struct GltfDoc {
+    json::Value root;
+    std::vector<std::string> buffers;
+};
+
+GltfDoc read_gltf(const std::string& path) {
+    GltfDoc d;
+    const std::string bytes = read_binary_file(path);
+    std::string text, bin;
+    bool have_bin = false;
+    if (lower_ext(path) == ".glb") {
+        auto u32 = [&](size_t o) {
+            if (o + 4 > bytes.size()) throw json::Error{"truncated .glb"};
+            uint32_t v;
+            std::memcpy(&v, bytes.data() + o, 4);
+            return v;
+        };
+        if (u32(0) != 0x46546C67u || u32(4) != 2u) throw json::Error{"not a glTF 2.0 binary"};
+        size_t o = 12;
+        while (o + 8 <= bytes.size()) {
+            const uint32_t len = u32(o), type = u32(o + 4);
+            if (o + 8 + static_cast<size_t>(len) > bytes.size()) throw json::Error{"truncated .glb chunk"};
+            if (type == 0x4E4F534Au) text.assign(bytes, o + 8, len);
+            else if (type == 0x004E4942u && !have_bin) { bin.assign(bytes, o + 8, len); have_bin = true; }
+            o += 8 + ((static_cast<size_t>(len) + 3) & ~size_t(3));
+        }
+        if (text.empty()) throw json::Error{".glb without a JSON chunk"};
+    } else {
+        text = bytes;
+    }
+    d.root = json::Parser(text).parse();
+    if (d.root.kind != json::Value::Obj) throw json::Error{"glTF root must be an object"};
+    if ((d.root.has("images") && d.root["images"].size()) || (d.root.has("textures") && d.root["textures"].size()))
+        throw json::Error{"glTF textures are not supported (no image decoder in this library)"};
+    if (d.root.has("buffers")) {
+        const json::Value& bs = d.root["buffers"];
+        for (size_t i = 0; i < bs.size(); ++i) {
+            const json::Value& b = bs[i];
+            std::string data;
+            if (b.has("uri")) {
+                const std::string& uri = json::as_string(b["uri"]);
+                if (uri.compare(0, 5, "data:") == 0) {
+                    const size_t comma = uri.find(',');
+                    if (comma == std::string::npos) throw json::Error{"bad data URI"};
+                    data = base64_decode(uri, comma + 1);
+                } else {
+                    data = read_binary_file(resolve_relative(path, uri));
+                }
+            } else if (i == 0 && have_bin) {
+                data = bin;
+            } else {
+                throw json::Error{"buffer " + std::to_string(i) + " has no data"};
+            }
+            if (b.has("byteLength") && data.size() < static_cast<size_t>(json::as_int(b["byteLength"])))
+                throw json::Error{"buffer " + std::to_string(i) + " is shorter than its byteLength"};
+            d.buffers.push_back(std::move(data));
+        }
+    }
+    return d;
+}
+
+int get_int(const json::Value& o, const char* k, int dflt) { return o.has(k) ? json::as_int(o[k]) : dflt; }
+float get_num(const json::Value& o, const char* k, float dflt) { return o.has(k) ? json::as_float(o[k]) : dflt; }
+
+struct GltfAccessor {
+    const unsigned char* base = nullptr;
+    size_t stride = 0, count = 0, elem = 0, avail = 0;   // avail: bytes from base to the buffer's end
+    int comp = 0;
+};
+
+GltfAccessor gltf_accessor(const GltfDoc& d, int idx, size_t default_elem) {
+    const json::Value& accs = d.root["accessors"];
+    if (idx < 0 || static_cast<size_t>(idx) >= accs.size()) throw json::Error{"accessor index out of range"};
+    const json::Value& a = accs[idx];
+    if (!a.has("bufferView")) throw json::Error{"accessor without a bufferView (sparse accessors are not supported)"};
+    const int bvi = json::as_int(a["bufferView"]);
+    const json::Value& bvs = d.root["bufferViews"];
+    if (bvi < 0 || static_cast<size_t>(bvi) >= bvs.size()) throw json::Error{"bufferView index out of range"};
+    const json::Value& bv = bvs[bvi];
+    const int bi = json::as_int(bv["buffer"]);
+    if (bi < 0 || static_cast<size_t>(bi) >= d.buffers.size()) throw json::Error{"buffer index out of range"};
+    const std::string& buf = d.buffers[bi];
+    const size_t off = static_cast<size_t>(get_int(bv, "byteOffset", 0)) + static_cast<size_t>(get_int(a, "byteOffset", 0));
+    if (off > buf.size()) throw json::Error{"accessor offset outside its buffer"};
+    GltfAccessor r;
+    r.base = reinterpret_cast<const unsigned char*>(buf.data()) + off;
+    r.avail = buf.size() - off;
+    const int stride = get_int(bv, "byteStride", 0);
+    r.stride = stride > 0 ? static_cast<size_t>(stride) : default_elem;
+    r.count = static_cast<size_t>(json::as_int(a["count"]));
+    r.comp = json::as_int(a["componentType"]);
+    r.elem = default_elem;
+    return r;
+}
+
+const float* acc_float(const GltfAccessor& a, size_t i, size_t nfloats) {
+    const size_t at = i * a.stride;
+    if (at + nfloats * 4 > a.avail) throw json::Error{"accessor reads past its buffer"};
+    return reinterpret_cast<const float*>(a.base + at);
+}
+
+// glTF's column-major matrix or T * R * S (gltf_loader.cpp:53-88).
+M4 gltf_node_transform(const json::Value& n) {
+    if (n.has("matrix") && n["matrix"].size() == 16) {
+        float m[16];
+        for (int i = 0; i < 16; ++i) m[i] = json::as_float(n["matrix"][i]);
+        M4 r;
+        for (int row = 0; row < 4; ++row)
+            for (int col = 0; col < 4; ++col) r.m[row * 4 + col] = m[col * 4 + row];
+        return r;
+    }
+    M4 T = m4_identity(), R = m4_identity(), S = m4_identity();
+    if (n.has("translation") && n["translation"].size() == 3)
+        T = m4_translation(mk(json::as_float(n["translation"][0]), json::as_float(n["translation"][1]),
+                              json::as_float(n["translation"][2])));
+    if (n.has("rotation") && n["rotation"].size() == 4) {
+        const float qx = json::as_float(n["rotation"][0]), qy = json::as_float(n["rotation"][1]);
+        const float qz = json::as_float(n["rotation"][2]), qw = json::as_float(n["rotation"][3]);
+        const float xx = qx * qx, yy = qy * qy, zz = qz * qz, xy = qx * qy, xz = qx * qz, yz = qy * qz;
+        const float wx = qw * qx, wy = qw * qy, wz = qw * qz;
+        const float r[16] = {1 - 2 * (yy + zz), 2 * (xy - wz), 2 * (xz + wy), 0,
+                             2 * (xy + wz), 1 - 2 * (xx + zz), 2 * (yz - wx), 0,
+                             2 * (xz - wy), 2 * (yz + wx), 1 - 2 * (xx + yy), 0,
+                             0, 0, 0, 1};
+        std::memcpy(R.m, r, sizeof(r));
+    }
+    if (n.has("scale") && n["scale"].size() == 3) {
+        S.m[0] = json::as_float(n["scale"][0]);
+        S.m[5] = json::as_float(n["scale"][1]);
+        S.m[10] = json::as_float(n["scale"][2]);
+    }
+    return m4_mul(m4_mul(T, R), S);
+}
+
+void gltf_materials(const GltfDoc& d, std::vector<pt_material>& out, std::vector<std::string>& names) {
+    if (!d.root.has("materials")) return;
+    const json::Value& ms = d.root["materials"];
+    for (size_t i = 0; i < ms.size(); ++i) {
+        const json::Value& g = ms[i];
+        pt_material m = default_material();
+        names.push_back(g.has("name") ? json::as_string(g["name"]) : std::string());
+        // glTF defaults: base colour (1, 1, 1, 1), metallic 1, roughness 1, no emission
+        float bc[4] = {1.0f, 1.0f, 1.0f, 1.0f};
+        float metallic = 1.0f, roughness = 1.0f;
+        if (g.has("pbrMetallicRoughness")) {
+            const json::Value& p = g["pbrMetallicRoughness"];
+            if (p.has("baseColorFactor"))
+                for (size_t k = 0; k < 4 && k < p["baseColorFactor"].size(); ++k) bc[k] = json::as_float(p["baseColorFactor"][k]);
+            metallic = get_num(p, "metallicFactor", 1.0f);
+            roughness = get_num(p, "roughnessFactor", 1.0f);
+        }
+        m.base_color[0] = bc[0]; m.base_color[1] = bc[1]; m.base_color[2] = bc[2];
+        m.base_alpha = bc[3];
+        m.metallic = metallic;
+        m.roughness = roughness;
+        float em[3] = {0.0f, 0.0f, 0.0f};
+        if (g.has("emissiveFactor"))
+            for (size_t k = 0; k < 3 && k < g["emissiveFactor"].size(); ++k) em[k] = json::as_float(g["emissiveFactor"][k]);
+        m.emissive[0] = em[0]; m.emissive[1] = em[1]; m.emissive[2] = em[2];
+        if (em[0] > 0 || em[1] > 0 || em[2] > 0) m.emissive_strength = 1.0f;
+        m.double_sided = (g.has("doubleSided") && json::as_bool(g["doubleSided"])) ? 1 : 0;
+        if (g.has("extensions")) {
+            const json::Value& x = g["extensions"];
+            auto ext = [&](const char* k) -> const json::Value* { return x.has(k) ? &x[k] : nullptr; };
+            if (const json::Value* e = ext("KHR_materials_emissive_strength"))
+                if (e->has("emissiveStrength")) m.emissive_strength = json::as_float((*e)["emissiveStrength"]);
+            if (const json::Value* e = ext("KHR_materials_ior"))
+                if (e->has("ior")) m.ior = json::as_float((*e)["ior"]);
+            if (const json::Value* e = ext("KHR_materials_transmission"))
+                if (e->has("transmissionFactor")) m.spec_trans = json::as_float((*e)["transmissionFactor"]);
+            if (const json::Value* e = ext("KHR_materials_clearcoat")) {
+                if (e->has("clearcoatFactor")) m.clearcoat = json::as_float((*e)["clearcoatFactor"]);
+                if (e->has("clearcoatRoughnessFactor"))
+                    m.clearcoat_roughness = json::as_float((*e)["clearcoatRoughnessFactor"]);
+            }
+            if (const json::Value* e = ext("KHR_materials_sheen")) {
+                if (e->has("sheenRoughnessFactor")) m.sheen = json::as_float((*e)["sheenRoughnessFactor"]);
+                if (e->has("sheenColorFactor") && (*e)["sheenColorFactor"].size() >= 3) {
+                    const json::Value& c = (*e)["sheenColorFactor"];
+                    m.sheen_color_r = json::as_float(c[0]); m.sheen_color_g = json::as_float(c[1]);
+                    m.sheen_color_b = json::as_float(c[2]);
+                }
+            }
+            if (const json::Value* e = ext("KHR_materials_specular")) {
+                if (e->has("specularFactor")) m.specular_factor = json::as_float((*e)["specularFactor"]);
+                if (e->has("specularColorFactor") && (*e)["specularColorFactor"].size() >= 3) {
+                    const json::Value& c = (*e)["specularColorFactor"];
+                    m.specular_color_r = json::as_float(c[0]); m.specular_color_g = json::as_float(c[1]);
+                    m.specular_color_b = json::as_float(c[2]);
+                }
+            }
+            if (const json::Value* e = ext("KHR_materials_volume")) {
+                if (e->has("thicknessFactor")) m.thickness_factor = json::as_float((*e)["thicknessFactor"]);
+                if (e->has("attenuationDistance")) m.attenuation_distance = json::as_float((*e)["attenuationDistance"]);
+                if (e->has("attenuationColor") && (*e)["attenuationColor"].size() >= 3) {
+                    const json::Value& c = (*e)["attenuationColor"];
+                    m.att_color_r = json::as_float(c[0]); m.att_color_g = json::as_float(c[1]);
+                    m.att_color_b = json::as_float(c[2]);
+                }
+            }
+            if (const json::Value* e = ext("KHR_materials_anisotropy")) {
+                if (e->has("anisotropyStrength")) m.anisotropic = json::as_float((*e)["anisotropyStrength"]);
+                if (e->has("anisotropyRotation")) m.anisotropy_rotation = json::as_float((*e)["anisotropyRotation"]);
+            }
+        }
+        const std::string mode = g.has("alphaMode") ? json::as_string(g["alphaMode"]) : std::string("OPAQUE");
+        if (mode == "MASK") { m.alpha_mode = 1; m.alpha_cutoff = get_num(g, "alphaCutoff", 0.5f); }
+        else if (mode == "BLEND") m.alpha_mode = 2;
+        out.push_back(m);
+    }
+}
+
+void gltf_primitive(const GltfDoc& d, const json::Value& prim, const M4& world, int mat_offset,
+                    std::vector<pt_vertex>& verts, std::vector<pt_face>& faces) {
+    const int mode = get_int(prim, "mode", -1);
+    if (mode != 4 && mode != -1) return;
+    if (!prim.has("attributes") || !prim["attributes"].has("POSITION")) return;
+    const json::Value& at = prim["attributes"];
+    auto float_attr = [&](const char* name, size_t n) {
+        GltfAccessor a = gltf_accessor(d, json::as_int(at[name]), n * 4);
+        if (a.comp != 5126) throw json::Error{std::string("glTF attribute ") + name + " must be FLOAT"};
+        return a;
+    };
+    const GltfAccessor pos = float_attr("POSITION", 3);
+    const bool has_n = at.has("NORMAL"), has_uv = at.has("TEXCOORD_0"), has_t = at.has("TANGENT");
+    GltfAccessor nrm, uv, tan;
+    if (has_n) nrm = float_attr("NORMAL", 3);
+    if (has_uv) uv = float_attr("TEXCOORD_0", 2);
+    if (has_t) tan = float_attr("TANGENT", 4);
+    const M4 nmat = m4_transpose(m4_inverse(world));
+    const uint32_t base = static_cast<uint32_t>(verts.size());
+    const size_t nv = pos.count;
+    for (size_t v = 0; v < nv; ++v) {
+        pt_vertex o{};
+        const float* p = acc_float(pos, v, 3);
+        st3(o.position, m4_point(world, mk(p[0], p[1], p[2])));
+        if (has_n) {
+            const float* q = acc_float(nrm, v, 3);
+            st3(o.normal, normalize(m4_vector(nmat, mk(q[0], q[1], q[2]))));
+        }
+        if (has_uv) {
+            const float* q = acc_float(uv, v, 2);
+            o.uv[0] = q[0]; o.uv[1] = q[1];
+        }
+        if (has_t) {
+            const float* q = acc_float(tan, v, 4);
+            const f3 t = normalize(m4_vector(world, mk(q[0], q[1], q[2])));
+            o.tangent[0] = t.x; o.tangent[1] = t.y; o.tangent[2] = t.z; o.tangent[3] = q[3];
+        }
+        verts.push_back(o);
+    }
+    const int mat = prim.has("material") && json::as_int(prim["material"]) >= 0
+                        ? json::as_int(prim["material"]) + mat_offset : 0;
+    size_t expected;
+    if (prim.has("indices") && json::as_int(prim["indices"]) >= 0) {
+        const GltfAccessor ia = gltf_accessor(d, json::as_int(prim["indices"]), 1);
+        const size_t tris = ia.count / 3;
+        expected = tris;
+        const size_t width = ia.comp == 5121 ? 1 : (ia.comp == 5123 ? 2 : (ia.comp == 5125 ? 4 : 0));
+        if (width && tris * 3 * width > ia.avail) throw json::Error{"index accessor reads past its buffer"};
+        for (size_t t = 0; t < tris; ++t) {
+            uint32_t i[3];
+            for (int k = 0; k < 3; ++k) {
+                const unsigned char* src = ia.base + (t * 3 + k) * width;
+                if (width == 1) i[k] = src[0];
+                else if (width == 2) { uint16_t x; std::memcpy(&x, src, 2); i[k] = x; }
+                else if (width == 4) std::memcpy(&i[k], src, 4);
+            }
+            if (!width) continue;   // other index types: no faces (as the reference)
+            for (int k = 0; k < 3; ++k)
+                if (i[k] >= nv) throw json::Error{"glTF index " + std::to_string(i[k]) + " out of range"};
+            faces.push_back({base + i[0], base + i[1], base + i[2], mat});
+        }
+    } else {
+        expected = nv / 3;
+        for (size_t t = 0; t < nv / 3; ++t) {
+            const uint32_t i = static_cast<uint32_t>(t * 3);
+            faces.push_back({base + i, base + i + 1, base + i + 2, mat});
+        }
+    }
+    if (!has_n) {
+        for (size_t v = 0; v < nv; ++v) st3(verts[base + v].normal, mk(0.0f));
+        const size_t first = faces.size() >= expected ? faces.size() - expected : 0;
+        for (size_t fi = first; fi < faces.size(); ++fi) {
+            const pt_face& f = faces[fi];
+            const f3 fn = cross(ld3(verts[f.v1].position) - ld3(verts[f.v0].position),
+                                ld3(verts[f.v2].position) - ld3(verts[f.v0].position));
+            for (uint32_t vi : {f.v0, f.v1, f.v2}) st3(verts[vi].normal, ld3(verts[vi].normal) + fn);
+        }
+        for (size_t v = 0; v < nv; ++v) {
+            const f3 n = ld3(verts[base + v].normal);
+            const float len = length(n);
+            if (len > 0.0f) st3(verts[base + v].normal, n / len);
+        }
+    }
+}
+
+struct GltfLight { int type = 0; f3 color = mk(1.0f); float intensity = 1.0f, range = 1e30f, inner = 0.0f, outer = 0.7853982f; };
+
+struct GltfOptions {
+    M4 transform = m4_identity();
+    bool load_camera = true, auto_fit_camera = true, add_default_lights = true, load_environment = true;
+};
+
+// PunctualLight's defaults (Part_2/src/lights/punctual_light.h:14-25).
+pt_punctual_light default_punctual() {
+    pt_punctual_light L{};
+    st3(L.position, mk(0.0f)); L.range = FLT_MAX; st3(L.color, mk(1.0f)); L.intensity = 1.0f;
+    st3(L.direction, mk(0.0f, -1.0f, 0.0f)); L.inner_cone = 0.0f; L.outer_cone = 0.7071068f; L.type = 0;
+    return L;
+}
+
+void gltf_nodes(const GltfDoc& d, int idx, const M4& parent, int mat_offset, const std::vector<GltfLight>& lights,
+                HostScene& hs, bool& camera_set, int depth) {
+    const json::Value& nodes = d.root["nodes"];
+    if (idx < 0 || static_cast<size_t>(idx) >= nodes.size()) return;
+    if (depth > 256) throw json::Error{"glTF node hierarchy too deep (a cycle?)"};
+    const json::Value& n = nodes[idx];
+    const M4 world = m4_mul(parent, gltf_node_transform(n));
+    const int mesh = get_int(n, "mesh", -1);
+    if (mesh >= 0 && d.root.has("meshes") && static_cast<size_t>(mesh) < d.root["meshes"].size()) {
+        const json::Value& m = d.root["meshes"][mesh];
+        if (m.has("primitives"))
+            for (size_t p = 0; p < m["primitives"].size(); ++p)
+                gltf_primitive(d, m["primitives"][p], world, mat_offset, hs.vertices, hs.faces);
+    }
+    const int cam = get_int(n, "camera", -1);
+    if (!camera_set && cam >= 0 && d.root.has("cameras") && static_cast<size_t>(cam) < d.root["cameras"].size()) {
+        const json::Value& c = d.root["cameras"][cam];
+        if (c.has("type") && json::as_string(c["type"]) == "perspective" && c.has("perspective")) {
+            const json::Value& p = c["perspective"];
+            const f3 pos = m4_point(world, mk(0.0f));
+            st3(hs.camera.position, pos);
+            st3(hs.camera.look_at, pos + normalize(m4_vector(world, mk(0.0f, 0.0f, -1.0f))));
+            st3(hs.camera.up, normalize(m4_vector(world, mk(0.0f, 1.0f, 0.0f))));
+            const double yfov = p.has("yfov") ? (p["yfov"].kind == json::Value::Int ? double(p["yfov"].i) : p["yfov"].d) : 0.0;
+            hs.camera.fov = static_cast<float>(yfov * 180.0 / 3.14159265358979323846);
+            const double aspect = p.has("aspectRatio") ? (p["aspectRatio"].kind == json::Value::Int ? double(p["aspectRatio"].i) : p["aspectRatio"].d) : 0.0;
+            if (aspect > 0.0) hs.camera.width = static_cast<int>(aspect * hs.camera.height);
+            camera_set = true;
+        }
+    }
+    if (n.has("extensions") && n["extensions"].has("KHR_lights_punctual") &&
+        n["extensions"]["KHR_lights_punctual"].has("light")) {
+        const int li = json::as_int(n["extensions"]["KHR_lights_punctual"]["light"]);
+        if (li >= 0 && static_cast<size_t>(li) < lights.size()) {
+            const GltfLight& g = lights[li];
+            pt_punctual_light L = default_punctual();
+            L.type = g.type;
+            st3(L.color, g.color);
+            L.intensity = g.intensity;
+            L.range = g.range;
+            st3(L.position, m4_point(world, mk(0.0f)));
+            st3(L.direction, normalize(m4_vector(world, mk(0.0f, 0.0f, -1.0f))));
+            L.inner_cone = std::cos(g.inner);
+            L.outer_cone = std::cos(g.outer);
+            hs.punctual.push_back(L);
+        }
+    }
+    if (n.has("children"))
+        for (size_t c = 0; c < n["children"].size(); ++c)
+            gltf_nodes(d, json::as_int(n["children"][c]), world, mat_offset, lights, hs, camera_set, depth + 1);
+}
+
+// Appends one glTF file to `hs`; returns the names of its materials.
+std::vector<std::string> load_gltf(const std::string& path, HostScene& hs, const GltfOptions& opt) {
+    const GltfDoc d = read_gltf(path);
+    const int mat_offset = static_cast<int>(hs.materials.size());
+    std::vector<std::string> names;
+    gltf_materials(d, hs.materials, names);
+    if (hs.materials.empty()) hs.materials.push_back(default_material());
+    std::vector<GltfLight> lights;
+    if (d.root.has("extensions") && d.root["extensions"].has("KHR_lights_punctual") &&
+        d.root["extensions"]["KHR_lights_punctual"].has("lights")) {
+        const json::Value& ls = d.root["extensions"]["KHR_lights_punctual"]["lights"];
+        for (size_t i = 0; i < ls.size(); ++i) {
+            const json::Value& l = ls[i];
+            GltfLight g;
+            if (l.has("type")) {
+                const std::string& t = json::as_string(l["type"]);
+                g.type = t == "directional" ? 1 : (t == "spot" ? 2 : 0);
+            }
+            if (l.has("color") && l["color"].size() >= 3) g.color = to_f3(l["color"]);
+            g.intensity = get_num(l, "intensity", g.intensity);
+            g.range = get_num(l, "range", g.range);
+            if (l.has("spot")) {
+                g.inner = get_num(l["spot"], "innerConeAngle", g.inner);
+                g.outer = get_num(l["spot"], "outerConeAngle", g.outer);
+            }
+            lights.push_back(g);
+        }
+    }
+    bool camera_set = !opt.load_camera;
+    const int scene = get_int(d.root, "scene", 0) >= 0 ? get_int(d.root, "scene", 0) : 0;
+    if (d.root.has("scenes") && static_cast<size_t>(scene) < d.root["scenes"].size() && d.root.has("nodes")) {
+        const json::Value& s = d.root["scenes"][scene];
+        if (s.has("nodes"))
+            for (size_t i = 0; i < s["nodes"].size(); ++i)
+                gltf_nodes(d, json::as_int(s["nodes"][i]), opt.transform, mat_offset, lights, hs, camera_set, 0);
+    }
+    if (opt.auto_fit_camera && !camera_set && !hs.vertices.empty()) auto_fit_camera(hs.vertices, hs.camera);
+    if (opt.load_environment && hs.env_w <= 0 && hs.env_h <= 0) {
+        // the reference looks upward from the file for models/<its default sky>
+        std::string dir = path;
+        for (int up = 0; up < 64; ++up) {
+            const size_t slash = dir.find_last_of('/');
+            if (slash == std::string::npos) break;
+            dir = dir.substr(0, slash);
+            const std::string cand = (dir.empty() ? std::string() : dir) + "/models/kloofendal_48d_partly_cloudy_puresky_4k.hdr";
+            std::ifstream probe(cand, std::ios::binary);
+            if (probe) {
+                if (!load_hdr(cand, hs.env_rgba, hs.env_w, hs.env_h)) { hs.env_rgba.clear(); hs.env_w = hs.env_h = 0; }
+                break;
+            }
+            if (dir.empty()) break;
+        }
+    }
+    bool emissive = false;
+    for (const pt_material& m : hs.materials)
+        if (m.emissive_strength > 0.0f && (m.emissive[0] > 0.0f || m.emissive[1] > 0.0f || m.emissive[2] > 0.0f)) emissive = true;
+    if (opt.add_default_lights && !(hs.env_w > 0 && hs.env_h > 0) && !emissive && hs.punctual.empty()) {
+        pt_punctual_light key = default_punctual(), fill = default_punctual();
+        key.type = 1; st3(key.direction, normalize(mk(-0.5f, -0.8f, -0.6f))); st3(key.color, mk(1.0f, 0.95f, 0.9f));
+        key.intensity = 3.0f;
+        fill.type = 1; st3(fill.direction, normalize(mk(0.6f, -0.3f, 0.5f))); st3(fill.color, mk(0.7f, 0.8f, 1.0f));
+        fill.intensity = 1.0f;
+        hs.punctual.push_back(key);
+        hs.punctual.push_back(fill);
+    }
+    return names;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
 // Scene JSON.
 // ---------------------------------------------------------------------------
 bool load_json_scene(const std::string& path, HostScene& hs) {
+    const std::string ext = lower_ext(path);
+    if (ext == ".gltf" || ext == ".glb") {   // SceneLoader::load (scene_loader.cpp:280-289)
+        try {
+            load_gltf(path, hs, GltfOptions{});
+        } catch (const json::Error& e) {
+            set_error(path + ": " + e.msg);
+            return false;
+        } catch (const std::exception& e) {
+            set_error(path + ": " + e.what());
+            return false;
+        }
+        return true;
+    }
     std::ifstream in(path, std::ios::binary);
     if (!in) { set_error("cannot open " + path); return false; }
     std::stringstream buf;
@@ -611,7 +1108,21 @@ bool load_json_scene(const std::string& path, HostScene& hs) {
                     const M4 T = parse_transform(o);
                     if (!load_obj(file, mid, T.m, hs.vertices, hs.faces)) return false;
                 } else if (type == "gltf") {
-                    throw json::Error{"glTF objects are not supported by this library"};
+                    // SceneLoader's glTF objects (scene_loader.cpp:162-193): the object's
+                    // transform, no camera / default lights / environment, then the
+                    // object's materialOverrides applied by glTF material name
+                    GltfOptions opt;
+                    opt.transform = parse_transform(o);
+                    opt.load_camera = opt.auto_fit_camera = opt.add_default_lights = opt.load_environment = false;
+                    const int first = static_cast<int>(hs.materials.size());
+                    const std::vector<std::string> names =
+                        load_gltf(resolve_relative(path, json::as_string(o["file"])), hs, opt);
+                    if (o.has("materialOverrides")) {
+                        for (const auto& kv : *o["materialOverrides"].o)
+                            for (size_t k = 0; k < names.size(); ++k)
+                                if (names[k] == kv.first && first + k < hs.materials.size())
+                                    apply_material_override(kv.second, hs.materials[first + k]);
+                    }
                 }
             }
         }
