@@ -281,6 +281,8 @@ int pt_film_destroy(pt_film* film);
 int pt_film_clear(pt_film* film);
 int pt_film_download(const pt_film* film, float* host_rgba);       /* Film::downloadAccumulated */
 int pt_film_download_new(const pt_film* film, float* host_rgba);   /* the last launch's mean     */
+/* Film::downloadAccumulated into a host or (dst_is_device) device buffer of the film's device. */
+int pt_film_download_to(const pt_film* film, float* dst_rgba, int32_t dst_is_device);
 
 /* ---- integrator plugin (Integrator, Part_2/src/integrators/integrator.h:10-20) ---- */
 int         pt_integrator_create(const char* name, pt_integrator** out);          /* "path" */

@@ -159,6 +159,7 @@ _SIGS = [
     ("pt_film_destroy", C.c_int, [_P]),
     ("pt_film_clear", C.c_int, [_P]),
     ("pt_film_download", C.c_int, [_P, _P]),
+    ("pt_film_download_to", C.c_int, [_P, _P, C.c_int32]),
     ("pt_film_download_new", C.c_int, [_P, _P]),
     ("pt_integrator_create", C.c_int, [C.c_char_p, C.POINTER(_P)]),
     ("pt_integrator_destroy", C.c_int, [_P]),

@@ -359,6 +359,10 @@ int pt_film_download(const pt_film* f, float* host_rgba) {
     PT_REQUIRE(f && host_rgba, "null argument");
     return film_download(f, host_rgba, false, true);
 }
+int pt_film_download_to(const pt_film* f, float* dst, int32_t dst_is_device) {
+    PT_REQUIRE(f && dst, "null argument");
+    return film_download(f, dst, false, dst_is_device == 0);
+}
 int pt_film_download_new(const pt_film* f, float* host_rgba) {
     PT_REQUIRE(f && host_rgba, "null argument");
     return film_download(f, host_rgba, true, true);
