@@ -534,11 +534,19 @@ bool load_obj(const std::string& path, int mat, const float xform[16],
 namespace {
 
 std::string read_binary_file(const std::string& path) {
-    std::ifstream in(path, std::ios::binary);
-    if (!in) throw json::Error{"cannot open " + path};
-    std::stringstream ss;
-    ss << in.rdbuf();
-    return ss.str();
+    std::FILE* fp = std::fopen(path.c_str(), "rb");
+    if (!fp) throw json::Error{"cannot open " + path};
+    std::string out;
+    if (std::fseek(fp, 0, SEEK_END) == 0) {
+        const long len = std::ftell(fp);
+        if (len > 0) {
+            out.resize(static_cast<size_t>(len));
+            std::fseek(fp, 0, SEEK_SET);
+            if (std::fread(&out[0], 1, out.size(), fp) != out.size()) { std::fclose(fp); throw json::Error{"cannot read " + path}; }
+        }
+    }
+    std::fclose(fp);
+    return out;
 }
 
 std::string base64_decode(const std::string& s, size_t from) {
@@ -564,15 +572,24 @@ std::string base64_decode(const std::string& s, size_t from) {
     return out;
 }
 
+struct GltfBuffer {
+    const char* data = nullptr;
+    size_t size = 0;
+};
+
 struct GltfDoc {
     json::Value root;
-    std::vector<std::string> buffers;
+    std::string file;                 // the .glb (its BIN chunk is buffer 0)
+    std::vector<std::string> owned;   // external and data-URI buffers
+    std::vector<GltfBuffer> buffers;
 };
 
 GltfDoc read_gltf(const std::string& path) {
     GltfDoc d;
-    const std::string bytes = read_binary_file(path);
-    std::string text, bin;
+    d.file = read_binary_file(path);
+    const std::string& bytes = d.file;
+    std::string text;
+    size_t bin_off = 0, bin_len = 0;
     bool have_bin = false;
     if (lower_ext(path) == ".glb") {
         auto u32 = [&](size_t o) {
@@ -587,7 +604,7 @@ GltfDoc read_gltf(const std::string& path) {
             const uint32_t len = u32(o), type = u32(o + 4);
             if (o + 8 + static_cast<size_t>(len) > bytes.size()) throw json::Error{"truncated .glb chunk"};
             if (type == 0x4E4F534Au) text.assign(bytes, o + 8, len);
-            else if (type == 0x004E4942u && !have_bin) { bin.assign(bytes, o + 8, len); have_bin = true; }
+            else if (type == 0x004E4942u && !have_bin) { bin_off = o + 8; bin_len = len; have_bin = true; }
             o += 8 + ((static_cast<size_t>(len) + 3) & ~size_t(3));
         }
         if (text.empty()) throw json::Error{".glb without a JSON chunk"};
@@ -600,26 +617,30 @@ GltfDoc read_gltf(const std::string& path) {
         throw json::Error{"glTF textures are not supported (no image decoder in this library)"};
     if (d.root.has("buffers")) {
         const json::Value& bs = d.root["buffers"];
+        d.owned.reserve(bs.size());
         for (size_t i = 0; i < bs.size(); ++i) {
             const json::Value& b = bs[i];
-            std::string data;
+            GltfBuffer buf;
             if (b.has("uri")) {
                 const std::string& uri = json::as_string(b["uri"]);
                 if (uri.compare(0, 5, "data:") == 0) {
                     const size_t comma = uri.find(',');
                     if (comma == std::string::npos) throw json::Error{"bad data URI"};
-                    data = base64_decode(uri, comma + 1);
+                    d.owned.push_back(base64_decode(uri, comma + 1));
                 } else {
-                    data = read_binary_file(resolve_relative(path, uri));
+                    d.owned.push_back(read_binary_file(resolve_relative(path, uri)));
                 }
+                buf.data = d.owned.back().data();
+                buf.size = d.owned.back().size();
             } else if (i == 0 && have_bin) {
-                data = bin;
+                buf.data = bytes.data() + bin_off;
+                buf.size = bin_len;
             } else {
                 throw json::Error{"buffer " + std::to_string(i) + " has no data"};
             }
-            if (b.has("byteLength") && data.size() < static_cast<size_t>(json::as_int(b["byteLength"])))
+            if (b.has("byteLength") && buf.size < static_cast<size_t>(json::as_int(b["byteLength"])))
                 throw json::Error{"buffer " + std::to_string(i) + " is shorter than its byteLength"};
-            d.buffers.push_back(std::move(data));
+            d.buffers.push_back(buf);
         }
     }
     return d;
@@ -645,12 +666,12 @@ GltfAccessor gltf_accessor(const GltfDoc& d, int idx, size_t default_elem) {
     const json::Value& bv = bvs[bvi];
     const int bi = json::as_int(bv["buffer"]);
     if (bi < 0 || static_cast<size_t>(bi) >= d.buffers.size()) throw json::Error{"buffer index out of range"};
-    const std::string& buf = d.buffers[bi];
+    const GltfBuffer& buf = d.buffers[bi];
     const size_t off = static_cast<size_t>(get_int(bv, "byteOffset", 0)) + static_cast<size_t>(get_int(a, "byteOffset", 0));
-    if (off > buf.size()) throw json::Error{"accessor offset outside its buffer"};
+    if (off > buf.size) throw json::Error{"accessor offset outside its buffer"};
     GltfAccessor r;
-    r.base = reinterpret_cast<const unsigned char*>(buf.data()) + off;
-    r.avail = buf.size() - off;
+    r.base = reinterpret_cast<const unsigned char*>(buf.data) + off;
+    r.avail = buf.size - off;
     const int stride = get_int(bv, "byteStride", 0);
     r.stride = stride > 0 ? static_cast<size_t>(stride) : default_elem;
     r.count = static_cast<size_t>(json::as_int(a["count"]));
@@ -796,6 +817,8 @@ void gltf_primitive(const GltfDoc& d, const json::Value& prim, const M4& world, 
     const M4 nmat = m4_transpose(m4_inverse(world));
     const uint32_t base = static_cast<uint32_t>(verts.size());
     const size_t nv = pos.count;
+    if (nv * pos.stride > pos.avail + pos.stride) throw json::Error{"POSITION accessor reads past its buffer"};
+    verts.reserve(verts.size() + nv);
     for (size_t v = 0; v < nv; ++v) {
         pt_vertex o{};
         const float* p = acc_float(pos, v, 3);
@@ -822,6 +845,7 @@ void gltf_primitive(const GltfDoc& d, const json::Value& prim, const M4& world, 
         const GltfAccessor ia = gltf_accessor(d, json::as_int(prim["indices"]), 1);
         const size_t tris = ia.count / 3;
         expected = tris;
+        faces.reserve(faces.size() + tris);
         const size_t width = ia.comp == 5121 ? 1 : (ia.comp == 5123 ? 2 : (ia.comp == 5125 ? 4 : 0));
         if (width && tris * 3 * width > ia.avail) throw json::Error{"index accessor reads past its buffer"};
         for (size_t t = 0; t < tris; ++t) {

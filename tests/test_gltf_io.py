@@ -237,3 +237,58 @@ def test_gltf_with_textures_is_rejected(tmp_path):
     p.write_text(json.dumps(g))
     with pytest.raises(pt.PTError, match="textures"):
         pt.SceneManager.load(str(p))
+
+
+def _write_big_glb(path, sa):
+    """One mesh of the scene's triangles (positions, normals, uvs, u32 indices) as a .glb."""
+    v, f = sa.vertices, sa.faces
+    pos = np.ascontiguousarray(v["position"], np.float32)
+    nrm = np.ascontiguousarray(v["normal"], np.float32)
+    uv = np.ascontiguousarray(v["uv"], np.float32)
+    idx = np.ascontiguousarray(np.stack([f["v0"], f["v1"], f["v2"]], 1).astype(np.uint32))
+    parts = [pos.tobytes(), nrm.tobytes(), uv.tobytes(), idx.tobytes()]
+    offs = np.cumsum([0] + [len(p) for p in parts])[:-1]
+    views = [{"buffer": 0, "byteOffset": int(o), "byteLength": len(p)} for o, p in zip(offs, parts)]
+    acc = [{"bufferView": 0, "componentType": 5126, "count": len(pos), "type": "VEC3"},
+           {"bufferView": 1, "componentType": 5126, "count": len(pos), "type": "VEC3"},
+           {"bufferView": 2, "componentType": 5126, "count": len(pos), "type": "VEC2"},
+           {"bufferView": 3, "componentType": 5125, "count": idx.size, "type": "SCALAR"}]
+    blob = b"".join(parts)
+    g = {"asset": {"version": "2.0"}, "scene": 0, "scenes": [{"nodes": [0]}],
+         "nodes": [{"mesh": 0, "scale": [1.0, 1.0, 1.0]}],
+         "meshes": [{"primitives": [{"attributes": {"POSITION": 0, "NORMAL": 1, "TEXCOORD_0": 2}, "indices": 3,
+                                     "material": 0}]}],
+         "materials": [{"name": "m", "pbrMetallicRoughness": {"baseColorFactor": [0.7, 0.7, 0.7, 1.0]}}],
+         "accessors": acc, "bufferViews": views, "buffers": [{"byteLength": len(blob)}]}
+    js = json.dumps(g).encode()
+    js += b" " * ((-len(js)) % 4)
+    blob += b"\0" * ((-len(blob)) % 4)
+    out = struct.pack("<III", 0x46546C67, 2, 12 + 8 + len(js) + 8 + len(blob))
+    out += struct.pack("<II", len(js), 0x4E4F534A) + js + struct.pack("<II", len(blob), 0x004E4942) + blob
+    path.write_bytes(out)
+
+
+def test_gltf_load_speed_against_reference_loader(ref, tmp_path):
+    """A 524,802-triangle .glb (the icosphere field at 100 spheres) loaded by
+    both loaders on the host: the same arrays, and one JSON line with the
+    wall times (best of two)."""
+    import time
+    from pathtracingtutorial_b200 import scenes
+    sa = scenes.icosphere_field(n_spheres=100, subdiv=4, width=64, height=36, env_size=(16, 8))
+    p = tmp_path / "big.glb"
+    _write_big_glb(p, sa)
+    t_ours, t_ref = [], []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        s = pt.SceneManager.load(str(p))
+        t_ours.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        r = ref.load_json(str(p))
+        t_ref.append(time.perf_counter() - t0)
+    v = s.vertices()
+    assert len(s.faces()) == len(sa.faces) and np.array_equal(s.faces().view(np.uint32), r["faces"].view(np.uint32))
+    assert np.array_equal(np.ascontiguousarray(v["position"]).view(np.uint32),
+                          np.ascontiguousarray(r["vertices"]["position"]).view(np.uint32))
+    print(json.dumps({"workload": f"glb of {len(sa.faces)} triangles", "ours_ms": round(min(t_ours) * 1e3, 1),
+                      "reference_loader_ms": round(min(t_ref) * 1e3, 1),
+                      "speedup": round(min(t_ref) / min(t_ours), 2)}))
