@@ -8,7 +8,9 @@ restatement (oracle/lbvh_ref.py) and against the host-built reference tree.
     hits the oracle's traversal finds in the same tree, and have the same
     closest distances as the host-built tree;
   * renders of a device-built scene agree with renders of the host-built one
-    within the noise of two independent renders;
+    within the noise of two independent renders, and with the FP64 oracle
+    rendering the same device-built tree and light tables on the same sample
+    streams to FP32 rounding;
   * a face with a vertex index out of range is reported, not traced.
 """
 import numpy as np
@@ -139,3 +141,30 @@ def test_bad_vertex_index_is_reported():
         bad.build_accel(builder="device")
     with pytest.raises(pt.PTError):
         bad.upload_to_device(0)
+
+
+@pytest.mark.parametrize("name", ["cornell", "spheres"])
+def test_device_built_radiance_correlated_with_fp64_oracle(oracle, name):
+    """The FP64 oracle renders with the device-built tree, its face order and
+    its light tables (read back through the C ABI) on the same sample streams:
+    the images agree to FP32 rounding, as for host-built scenes."""
+    from oracle.pyoracle import Prepared
+    sa = {"cornell": lambda: scenes.cornell_box(width=48, height=48),
+          "spheres": lambda: scenes.icosphere_field(n_spheres=20, subdiv=3, width=64, height=36,
+                                                    env_size=(128, 64))}[name]()
+    spp = 8
+    s = sa.scene()
+    s.build_accel(builder="device")
+    s.upload_to_device(0)
+    img = pt.render(s, spp)[..., :3].astype(np.float64)
+    base = oracle.prepare(sa)
+    refs, pmf, alias = s.emissive_tables()
+    prep = Prepared(base.vertices, np.ascontiguousarray(s.faces()), base.materials,
+                    np.ascontiguousarray(s.bvh_nodes()), s.info()["bvh_max_depth"], refs, pmf, alias, base.env,
+                    base.env_pmf, base.env_alias, base.camera_frame, base.width, base.height, base.punctual)
+    (mean, _), _ = oracle.render(prep, sa.sample_per_frame, sa.max_depth, sa.sampler, frames=spp // sa.sample_per_frame,
+                                 first_frame=0, precision=64, rtl=pt.DEVICE_ARG_ORDER, pcg_seed=sa.pcg_seed)
+    assert mean.mean() > 0
+    rel = np.abs(img - mean) / np.maximum(np.abs(mean), 1e-3)
+    assert np.median(rel) < 1e-4, np.median(rel)
+    assert float(np.mean((img - mean) ** 2 / (mean ** 2 + 1e-2))) < 1e-3
