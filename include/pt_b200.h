@@ -273,6 +273,15 @@ int pt_scene_get_env_tables(const pt_scene* scene, float* pmf, pt_alias_entry* a
 int pt_scene_get_traversal(const pt_scene* scene, void* inner, uint32_t cap_inner, void* tris, uint32_t cap_tris,
                            uint32_t* root_ref);
 
+/* ---- images (ImageIO, Part_2/src/io/image_io.cpp) ----
+ * pt_write_hdr: ImageIO::write for .hdr (lines 79-121): w x h RGBA floats,
+ * rows swapped when flip_y (the reference's default), written as the
+ * reference's stb_image_write v1.16 writes them (RLE RGBE), byte for byte.
+ * pt_read_hdr: a Radiance .hdr (flat or RLE) into RGBA floats (alpha 1);
+ * with rgba null it only reports the size. */
+int pt_write_hdr(const char* path, const float* rgba, int32_t width, int32_t height, int32_t flip_y);
+int pt_read_hdr(const char* path, float* rgba, uint64_t cap_floats, int32_t* width, int32_t* height);
+
 /* ---- film (Film, Part_2/src/film/film.h:9-40) ----
  * Per pixel: compensated FP32 sum (Neumaier), compensation, sample count, and
  * the mean of the last launch (the reference's "new" surface). */

@@ -220,6 +220,14 @@ class RefHarness:
         n = self.L.ref_struct_layout(_p(out), C.c_int(256))
         return out[:n]
 
+    def write_image(self, path, rgba, flip_y=True):
+        """ImageIO::write of an (H, W, 4) float image."""
+        a = np.ascontiguousarray(rgba, np.float32)
+        rc = self.L.ref_write_image(os.fsencode(path), _p(a), C.c_int(a.shape[1]), C.c_int(a.shape[0]),
+                                    C.c_int(1 if flip_y else 0))
+        if rc != 0:
+            raise RuntimeError(f"reference writer failed on {path}")
+
     def load_json(self, path):
         counts = np.zeros(6, np.uint32)
         cam = np.zeros(80, np.uint8)

@@ -75,6 +75,7 @@ inline bool ptref_occluded(const Ray& r, const BVHNode* n, const Vertex* v, cons
 #include "lights/light_sampler.h"
 #include "scene/scene.h"
 #include "scene/scene_loader.h"
+#include "io/image_io.h"
 
 using namespace pt;
 
@@ -187,6 +188,17 @@ int ref_load_json(const char* path, uint32_t* counts, void* camera_out, int32_t*
     settings[2] = g_loaded.settings.maxDepth;
     settings[3] = g_loaded.settings.samplerType;
     return 0;
+}
+
+// ImageIO::write (Part_2/src/io/image_io.cpp:79-121) of a w x h RGBA image.
+int ref_write_image(const char* path, const float* rgba, int w, int h, int flip_y) {
+    Silence quiet;
+    Image img;
+    img.width = w;
+    img.height = h;
+    img.channel = 4;
+    img.data.assign(rgba, rgba + static_cast<size_t>(w) * h * 4);
+    return ImageIO::write(img, path, flip_y != 0) ? 0 : 1;
 }
 
 int ref_loaded_arrays(void* verts, void* faces, void* mats, void* lights, float* env) {

@@ -627,33 +627,19 @@ def rmse_to_db(rmse: float) -> float:
 
 # ---- Radiance RGBE files ----
 def write_hdr(path: str, img: np.ndarray, flip_y: bool = True) -> None:
-    """Write (H, W, 3|4) float radiance as flat RGBE; rows flipped like ImageIO::write's default."""
-    rgb = np.asarray(img, np.float32)[..., :3]
-    if flip_y:
-        rgb = rgb[::-1]
-    h, w = rgb.shape[:2]
-    v = rgb.max(axis=2)
-    mant, expo = np.frexp(v)
-    scale = np.where(v > 1e-32, mant * 256.0 / np.where(v > 1e-32, v, 1.0), 0.0)
-    out = np.zeros((h, w, 4), np.uint8)
-    out[..., :3] = np.clip(rgb * scale[..., None], 0, 255).astype(np.uint8)
-    out[..., 3] = np.where(v > 1e-32, expo + 128, 0).astype(np.uint8)
-    with open(path, "wb") as f:
-        f.write(b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n")
-        f.write(f"-Y {h} +X {w}\n".encode())
-        f.write(out.tobytes())
+    """ImageIO::write for .hdr: (H, W, 3|4) float radiance as run-length coded
+    RGBE, rows flipped by default, byte for byte as the reference writes it."""
+    a = np.asarray(img, np.float32)
+    h, w = a.shape[:2]
+    rgba = np.ones((h, w, 4), np.float32)
+    rgba[..., :3] = a[..., :3]
+    check(lib().pt_write_hdr(os.fsencode(path), ptr(rgba), w, h, 1 if flip_y else 0))
 
 
 def read_hdr(path: str) -> np.ndarray:
-    """Read a flat (non-RLE) RGBE file as written by write_hdr -> (H, W, 4)."""
-    with open(path, "rb") as f:
-        data = f.read()
-    head, _, rest = data.partition(b"\n\n")
-    line, _, pix = rest.partition(b"\n")
-    _, hh, _, ww = line.split()
-    h, w = int(hh), int(ww)
-    px = np.frombuffer(pix[: h * w * 4], np.uint8).reshape(h, w, 4).astype(np.float32)
-    scale = np.where(px[..., 3] > 0, np.ldexp(1.0, px[..., 3].astype(np.int32) - 136), 0.0)
-    out = np.ones((h, w, 4), np.float32)
-    out[..., :3] = px[..., :3] * scale[..., None]
+    """A Radiance .hdr (flat or run-length coded) -> (H, W, 4) float32, alpha 1."""
+    w, h = C.c_int32(), C.c_int32()
+    check(lib().pt_read_hdr(os.fsencode(path), None, 0, C.byref(w), C.byref(h)))
+    out = np.zeros((h.value, w.value, 4), np.float32)
+    check(lib().pt_read_hdr(os.fsencode(path), ptr(out), out.size, C.byref(w), C.byref(h)))
     return out

@@ -160,6 +160,8 @@ _SIGS = [
     ("pt_film_clear", C.c_int, [_P]),
     ("pt_film_download", C.c_int, [_P, _P]),
     ("pt_film_download_to", C.c_int, [_P, _P, C.c_int32]),
+    ("pt_write_hdr", C.c_int, [C.c_char_p, _P, C.c_int32, C.c_int32, C.c_int32]),
+    ("pt_read_hdr", C.c_int, [C.c_char_p, _P, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("pt_film_download_new", C.c_int, [_P, _P]),
     ("pt_integrator_create", C.c_int, [C.c_char_p, C.POINTER(_P)]),
     ("pt_integrator_destroy", C.c_int, [_P]),

@@ -359,6 +359,28 @@ int pt_film_download(const pt_film* f, float* host_rgba) {
     PT_REQUIRE(f && host_rgba, "null argument");
     return film_download(f, host_rgba, false, true);
 }
+int pt_write_hdr(const char* path, const float* rgba, int32_t w, int32_t h, int32_t flip_y) {
+    PT_REQUIRE(path && rgba, "null argument");
+    PT_REQUIRE(w > 0 && h > 0, "image size must be positive");
+    PT_GUARD_BEGIN
+    return write_hdr(path, rgba, w, h, flip_y != 0) ? PT_OK : PT_ERR_IO;
+    PT_GUARD_END
+}
+int pt_read_hdr(const char* path, float* rgba, uint64_t cap, int32_t* w, int32_t* h) {
+    PT_REQUIRE(path && w && h, "null argument");
+    PT_GUARD_BEGIN
+    std::vector<float> px;
+    int32_t ww = 0, hh = 0;
+    if (!load_hdr(path, px, ww, hh)) return PT_ERR_IO;
+    *w = ww;
+    *h = hh;
+    if (rgba) {
+        PT_REQUIRE(cap >= px.size(), "output capacity too small");
+        std::memcpy(rgba, px.data(), px.size() * sizeof(float));
+    }
+    return PT_OK;
+    PT_GUARD_END
+}
 int pt_film_download_to(const pt_film* f, float* dst, int32_t dst_is_device) {
     PT_REQUIRE(f && dst, "null argument");
     return film_download(f, dst, false, dst_is_device == 0);

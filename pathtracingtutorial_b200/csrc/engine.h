@@ -109,6 +109,8 @@ void add_quad(const float a[3], const float b[3], const float c[3], const float 
               std::vector<pt_vertex>& verts, std::vector<pt_face>& faces);
 // Scene JSON (SceneLoader::loadFromJson, Part_2/src/scene/scene_loader.cpp:240-276).
 bool load_json_scene(const std::string& path, HostScene& hs);
+bool load_hdr(const std::string& path, std::vector<float>& rgba, int32_t& w, int32_t& h);
+bool write_hdr(const std::string& path, const float* rgba, int32_t w, int32_t h, bool flip_y);
 // Radiance RGBE .hdr reader (as ImageIO::load, Part_2/src/io/image_io.cpp:19-49).
 bool load_hdr(const std::string& path, std::vector<float>& rgba, int32_t& w, int32_t& h);
 // Wavefront OBJ (MeshLoader::loadObj, Part_2/src/io/mesh_loader.cpp:23-112).

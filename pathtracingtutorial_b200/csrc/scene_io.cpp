@@ -11,6 +11,7 @@
 //   objects[{type: quad|mesh|gltf, vertices|file, material, transform,
 //            materialOverrides}]
 // A path ending in .gltf / .glb is read as a glTF scene (see load_gltf).
+#include <algorithm>
 #include <cctype>
 #include <cerrno>
 #include <cmath>
@@ -441,6 +442,98 @@ bool load_hdr(const std::string& path, std::vector<float>& rgba, int32_t& w, int
         decode(y);
     }
     return true;
+}
+
+// ---------------------------------------------------------------------------
+// Radiance RGBE writer: ImageIO::write for .hdr (Part_2/src/io/image_io.cpp:
+// 79-121: RGBA -> RGB, rows swapped when flip_y) through the reference's
+// vendored stb_image_write v1.16 (stbi_write_hdr), restated from its
+// published algorithm so that the files are byte for byte the same:
+//   header "#?RADIANCE", "# Written by stb_image_write.h",
+//     "FORMAT=32-bit_rle_rgbe", "EXPOSURE=          1.0000000000000", "",
+//     "-Y <h> +X <w>";
+//   pixel -> RGBE: m = max(r, max(g, b)); m < 1e-32 -> 0 0 0 0, else
+//     s = frexp(m, e) * 256 / m, bytes (r s, g s, b s) truncated, e + 128;
+//   scanline: width < 8 or >= 32768 -> flat RGBE; otherwise 2 2 w>>8 w&255
+//     and each of the four byte planes run-length coded: literal stretches of
+//     at most 128 bytes up to the next run of three equal bytes, runs of at
+//     most 127 (length + 128, byte).
+// ---------------------------------------------------------------------------
+namespace {
+
+void rgbe_of(const float* lin, unsigned char* out) {
+    const float m12 = lin[1] > lin[2] ? lin[1] : lin[2];
+    const float m = lin[0] > m12 ? lin[0] : m12;
+    if (m < 1e-32f) { out[0] = out[1] = out[2] = out[3] = 0; return; }
+    int e = 0;
+    const float s = static_cast<float>(std::frexp(m, &e)) * 256.0f / m;
+    for (int c = 0; c < 3; ++c) out[c] = static_cast<unsigned char>(static_cast<int>(lin[c] * s));
+    out[3] = static_cast<unsigned char>(e + 128);
+}
+
+void hdr_scanline(std::string& o, int width, const float* rgb, std::vector<unsigned char>& plane) {
+    if (width < 8 || width >= 32768) {
+        unsigned char q[4];
+        for (int x = 0; x < width; ++x) { rgbe_of(rgb + 3 * x, q); o.append(reinterpret_cast<char*>(q), 4); }
+        return;
+    }
+    plane.resize(static_cast<size_t>(width) * 4);
+    for (int x = 0; x < width; ++x) {
+        unsigned char q[4];
+        rgbe_of(rgb + 3 * x, q);
+        for (int c = 0; c < 4; ++c) plane[static_cast<size_t>(c) * width + x] = q[c];
+    }
+    o.push_back(2); o.push_back(2);
+    o.push_back(static_cast<char>((width & 0xff00) >> 8)); o.push_back(static_cast<char>(width & 0xff));
+    for (int c = 0; c < 4; ++c) {
+        const unsigned char* b = plane.data() + static_cast<size_t>(c) * width;
+        int x = 0;
+        while (x < width) {
+            int r = x;   // start of the next run of three equal bytes, else width
+            while (r + 2 < width && !(b[r] == b[r + 1] && b[r] == b[r + 2])) ++r;
+            if (r + 2 >= width) r = width;
+            while (x < r) {
+                const int len = std::min(r - x, 128);
+                o.push_back(static_cast<char>(len));
+                o.append(reinterpret_cast<const char*>(b + x), len);
+                x += len;
+            }
+            if (r + 2 < width) {
+                while (r < width && b[r] == b[x]) ++r;
+                while (x < r) {
+                    const int len = std::min(r - x, 127);
+                    o.push_back(static_cast<char>(len + 128));
+                    o.push_back(static_cast<char>(b[x]));
+                    x += len;
+                }
+            }
+        }
+    }
+}
+
+}  // namespace
+
+bool write_hdr(const std::string& path, const float* rgba, int32_t w, int32_t h, bool flip_y) {
+    if (!rgba || w <= 0 || h <= 0) { set_error("invalid image"); return false; }
+    const size_t px = static_cast<size_t>(w) * h;
+    std::vector<float> rgb(px * 3);
+    for (size_t i = 0; i < px; ++i)
+        for (int c = 0; c < 3; ++c) rgb[i * 3 + c] = rgba[i * 4 + c];
+    if (flip_y) {
+        const size_t row = static_cast<size_t>(w) * 3;
+        for (int y = 0; y < h / 2; ++y)
+            std::swap_ranges(rgb.begin() + y * row, rgb.begin() + (y + 1) * row, rgb.begin() + (h - 1 - y) * row);
+    }
+    std::string o = "#?RADIANCE\n# Written by stb_image_write.h\nFORMAT=32-bit_rle_rgbe\n";
+    o += "EXPOSURE=          1.0000000000000\n\n-Y " + std::to_string(h) + " +X " + std::to_string(w) + "\n";
+    std::vector<unsigned char> plane;
+    for (int y = 0; y < h; ++y) hdr_scanline(o, w, rgb.data() + static_cast<size_t>(y) * w * 3, plane);
+    std::FILE* fp = std::fopen(path.c_str(), "wb");
+    if (!fp) { set_error("cannot write " + path); return false; }
+    const bool ok = std::fwrite(o.data(), 1, o.size(), fp) == o.size();
+    std::fclose(fp);
+    if (!ok) set_error("cannot write " + path);
+    return ok;
 }
 
 // ---------------------------------------------------------------------------

@@ -258,3 +258,29 @@ def test_tonemap_oracle_known_values():
     assert out[0, 0, 0] == 0 and out[0, 0, 1] == round(12.92 * t * 255)
     assert out[0, 0, 2] == round((1.055 * (1 - math.exp(-1.0)) ** (1 / 2.4) - 0.055) * 255) == 208
     assert (out[0, 1, :3] == 255).all() and (out[..., 3] == 255).all()
+
+
+@pytest.mark.parametrize("shape,flip", [((13, 40), True), ((13, 40), False), ((6, 5), True), ((3, 300), False),
+                                        ((2, 129), True)])
+def test_hdr_writer_bytes_match_reference_writer(ref, tmp_path, shape, flip):
+    """pt_write_hdr against the reference's ImageIO::write (its vendored
+    stb_image_write, built from its tree): identical files, for run-length
+    coded rows (width >= 8: runs, literal stretches longer than 128, runs
+    longer than 127) and flat rows (width < 8), zeros, tiny values and both
+    row orders; and the file reads back to the RGBE-quantised image."""
+    h, w = shape
+    rng = np.random.default_rng(h * 1000 + w)
+    img = np.ones((h, w, 4), np.float32)
+    img[..., :3] = rng.lognormal(0.0, 2.0, (h, w, 3)).astype(np.float32)
+    img[0, : w // 2, :3] = 0.25                        # a run
+    img[h - 1, :, :3] = 0.0                            # a zero row
+    img[h // 2, : min(w, 4), :3] = 1e-35               # below the RGBE floor
+    ours, theirs = tmp_path / "ours.hdr", tmp_path / "ref.hdr"
+    pt.write_hdr(str(ours), img, flip_y=flip)
+    ref.write_image(str(theirs), img, flip_y=flip)
+    assert ours.read_bytes() == theirs.read_bytes()
+    back = pt.read_hdr(str(ours))
+    if flip:
+        back = back[::-1]
+    err = np.abs(back[..., :3] - img[..., :3])            # RGBE keeps 8 bits below each pixel's largest channel
+    assert np.all(err <= img[..., :3].max(axis=2, keepdims=True) / 128 + 1e-30)
