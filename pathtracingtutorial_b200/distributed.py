@@ -54,6 +54,7 @@ def render_distributed(scene, spp: int, group=None, renderer=None):
     img = torch.zeros((h, w, 4), dtype=torch.float32, device=f"cuda:{r.film.device}")
     if count:
         r.render_frames(count)
+        r.synchronize()   # the integrator's stream does not order with the copy's
         check(lib().pt_film_download_to(r.film._h, C.c_void_p(img.data_ptr()), 1))
         img *= float(count * spf)
     torch.cuda.synchronize(img.device)
