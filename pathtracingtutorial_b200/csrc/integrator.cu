@@ -1289,8 +1289,13 @@ void film_free(pt_film* f) {
     f->sum = f->comp = f->batch = f->fresh = f->resolve = nullptr;
 }
 
+// Film::clear and Film::downloadAccumulated are blocking calls on the legacy
+// stream in the reference (film.cu:8-59), ordered after every render launch;
+// renders here run on the integrator's or the caller's stream, so both wait
+// for the device first.
 int film_clear(pt_film* f) {
     if (int rc = ensure_device(f->device)) return rc;
+    PT_CU(cudaDeviceSynchronize());
     const size_t bytes = static_cast<size_t>(f->width) * f->height * sizeof(float4);
     void* bufs[] = {f->sum, f->comp, f->batch, f->fresh};
     for (void* b : bufs) PT_CU(cudaMemset(b, 0, bytes));
@@ -1299,6 +1304,7 @@ int film_clear(pt_film* f) {
 
 int film_download(const pt_film* f, float* host, bool fresh, bool host_ptr) {
     if (int rc = ensure_device(f->device)) return rc;
+    PT_CU(cudaDeviceSynchronize());
     const int n = f->width * f->height;
     const size_t bytes = static_cast<size_t>(n) * sizeof(float4);
     if (fresh) {

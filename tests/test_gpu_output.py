@@ -33,3 +33,19 @@ def test_tonemap_of_a_render():
     out = pt.tonemap(img)
     assert np.abs(out.astype(int) - tonemap_ref(img).astype(int)).max() <= 1
     assert out[..., :3].mean() > 10
+
+
+def test_film_download_waits_for_the_render():
+    """Renderer.render_frames returns with the render queued on the
+    integrator's stream; the film download (Film::downloadAccumulated) still
+    returns the finished image, as the reference's blocking copy does."""
+    sa = scenes.cornell_box(width=96, height=96)
+    s = sa.scene()
+    s.build_accel()
+    s.upload_to_device(0)
+    r = pt.Renderer(s)
+    r.reset_accumulation()
+    r.render_frames(16)
+    img = r.download_current_image()          # no synchronize in between
+    ref = pt.render(s, 64)
+    assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))

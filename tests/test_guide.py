@@ -172,7 +172,10 @@ def test_guided_render_unbiased_and_lower_error():
     guided = guided[..., :3].astype(np.float64)
 
     def relmse(x):
-        return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
+        # per-pixel squared relative error, each pixel's term capped at 1: at 64
+        # spp a single firefly pixel otherwise decides the comparison, and the
+        # guide's online training (FP32 atomics) differs from run to run
+        return float(np.mean(np.minimum((x - ref) ** 2 / (ref ** 2 + 1e-2), 1.0)))
 
     m_ref, m_plain, m_guided = ref.mean(), plain.mean(), guided.mean()
     assert abs(m_plain / m_ref - 1) < 0.03
