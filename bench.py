@@ -599,7 +599,7 @@ def large_workload(args):
 def build_workload(args):
     """--workload build: the bench scene (2,048,002 triangles) built by the
     reference-order host SAH builder and by the GPU builder (defaults: linear
-    BVH, two treelet passes), each tree then traced by the same integrator:
+    BVH, three treelet passes), each tree then traced by the same integrator:
     64 spp of the 1080p render, best of two, CUDA events.  --steps timed GPU
     builds after --warmup untimed ones (their median is reported)."""
     import statistics

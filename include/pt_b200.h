@@ -215,7 +215,7 @@ int pt_scene_build_accel(pt_scene* scene);
 /* The same prep with the BVH built on `device` instead of by the reference's
  * host builder (BVHBuilder::build, Part_2/src/accel/bvh_builder.cpp:56-221):
  * a linear BVH over 63-bit Morton codes (Karras radix tree); then, in
- * `passes` bottom-up passes (0 = 2), every inner node's treelet of
+ * `passes` bottom-up passes (0 = 3), every inner node's treelet of
  * `treelet_leaves` leaves (0 = 7, 1-2 = off) is re-topologised to its least
  * SAH cost (Karras and Aila's treelet restructuring); subtrees become leaves
  * by the reference's two rules: at most 3 faces (fewer than its LeafThreshold
@@ -234,7 +234,7 @@ int pt_scene_build_accel(pt_scene* scene);
 typedef struct pt_build_options {
     uint32_t max_leaf;        /* 0 = 8, at most 64             */
     uint32_t treelet_leaves;  /* 0 = 7, 1-2 = no restructuring */
-    uint32_t passes;          /* 0 = 2, at most 8              */
+    uint32_t passes;          /* 0 = 3, at most 8              */
     float    traversal_cost;  /* SAH cost of a node visit in triangle tests; 0 = 1.0 (the reference: 0.5) */
 } pt_build_options;
 typedef struct pt_build_stats {

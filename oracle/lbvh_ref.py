@@ -89,7 +89,7 @@ def _low_index(x: int) -> int:
     return (x & -x).bit_length() - 1
 
 
-def build(positions: np.ndarray, faces: np.ndarray, max_leaf: int = 8, treelet: int = 7, passes: int = 2,
+def build(positions: np.ndarray, faces: np.ndarray, max_leaf: int = 8, treelet: int = 7, passes: int = 3,
           traversal_cost: float = 1.0) -> dict:
     """The device builder's outputs: order (face index per final position),
     inner (uint32[k, 16]), leaf_last (positions whose record ends a leaf),

@@ -175,7 +175,7 @@ class SceneManager:
         """SceneManager::buildAccel.  builder="host" is the reference's SAH
         build (node for node); builder="device" builds a linear BVH on
         `device`, re-topologises its treelets of `treelet` leaves (0 = 7, 1 =
-        off) in `passes` passes (0 = 2) and collapses leaves by the SAH (a node
+        off) in `passes` passes (0 = 3) and collapses leaves by the SAH (a node
         visit costs `traversal_cost` triangle tests, 0 = 1.0), and returns its
         timings and sizes."""
         if builder == "host":

@@ -227,8 +227,8 @@ int pt_scene_build_accel_device(pt_scene* s, int32_t device, const pt_build_opti
     const uint32_t leaf = o.max_leaf ? o.max_leaf : 8u;
     const int treelet = o.treelet_leaves == 0 ? 7 : (o.treelet_leaves < 3 ? 0 : static_cast<int>(o.treelet_leaves));
     // defaults measured on the 2M-triangle icosphere field and the 20M-triangle
-    // scene: two passes, a node visit costed as one triangle test
-    const int passes = o.passes ? static_cast<int>(o.passes) : 2;
+    // scene: three passes, a node visit costed as one triangle test
+    const int passes = o.passes ? static_cast<int>(o.passes) : 3;
     const float ct = o.traversal_cost > 0.0f ? o.traversal_cost : 1.0f;
     const int rc = build_accel_device(s, device, leaf, treelet, passes, ct, stats);
     if (rc != PT_OK) s->tables = SceneTables{};
