@@ -213,11 +213,64 @@ inline float mt(const float o[3], const float d[3], const Vtx& a, const Vtx& b, 
     return t;
 }
 
+// Watertight mode (added; the reference has none): the slab test of the
+// reference with the exit distance widened by kWtExit (Ize 2013: the slab
+// distances are within a factor 1 +- gamma(3) of exact, and 1 + 4 ulp covers
+// (1 + gamma(3)) / (1 - gamma(3)) and the product's own rounding), and Woop,
+// Benthin and Wald's triangle test (JCGT 2013) on the shared vertex
+// positions.  The tmax of the reference's recurrence is compared apart from
+// the widened exit.
+constexpr float kWtExit = 1.0f + 4.0f * 1.1920929e-7f;
+
+inline bool slab_wt(const float o[3], const float inv[3], const Node& n, float tmax) {
+    float tn = 0.0f, tf = INFINITY;
+    for (int i = 0; i < 3; ++i) {
+        const float t1 = (n.lo[i] - o[i]) * inv[i];
+        const float t2 = (n.hi[i] - o[i]) * inv[i];
+        tn = std::fmin(std::fmax(t1, tn), std::fmax(t2, tn));
+        tf = std::fmax(std::fmin(t1, tf), std::fmin(t2, tf));
+    }
+    return tn <= tf * kWtExit && tn <= tmax;
+}
+
+inline float woop(const float o[3], const float d[3], const Vtx& p0, const Vtx& p1, const Vtx& p2, bool shadow,
+                  float& uu, float& vv) {
+    const float adx = std::fabs(d[0]), ady = std::fabs(d[1]), adz = std::fabs(d[2]);
+    int kz = (adx > ady) ? (adx > adz ? 0 : 2) : (ady > adz ? 1 : 2);
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    if (d[kz] < 0.0f) std::swap(kx, ky);
+    const float sx = d[kx] / d[kz], sy = d[ky] / d[kz], sz = 1.0f / d[kz];
+    float a[3], b[3], c[3];
+    for (int k = 0; k < 3; ++k) { a[k] = p0.p[k] - o[k]; b[k] = p1.p[k] - o[k]; c[k] = p2.p[k] - o[k]; }
+    const float ax = a[kx] - sx * a[kz], ay = a[ky] - sy * a[kz];
+    const float bx = b[kx] - sx * b[kz], by = b[ky] - sy * b[kz];
+    const float cx = c[kx] - sx * c[kz], cy = c[ky] - sy * c[kz];
+    float U = cx * by - cy * bx, V = ax * cy - ay * cx, W = bx * ay - by * ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = static_cast<float>(double(cx) * double(by) - double(cy) * double(bx));
+        V = static_cast<float>(double(ax) * double(cy) - double(ay) * double(cx));
+        W = static_cast<float>(double(bx) * double(ay) - double(by) * double(ax));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return -1.0f;
+    const float det = U + V + W;
+    if (det == 0.0f) return -1.0f;
+    const float az = sz * a[kz], bz = sz * b[kz], cz = sz * c[kz];
+    const float T = U * az + V * bz + W * cz;
+    const float inv = 1.0f / det;
+    const float t = T * inv;
+    if (shadow) { if (!(t > 1e-4f)) return -1.0f; }
+    else if (t < 1e-4f) return -1.0f;
+    uu = V * inv; vv = W * inv;
+    return t;
+}
+
 struct Geo {
     const Node* nodes;
     const Vtx* v;
     const Face* f;
     uint32_t nn;
+    bool wt = false;
 };
 
 Hit closest(const Geo& g, const float o[3], const float d[3], Cnt& c) {
@@ -231,14 +284,15 @@ Hit closest(const Geo& g, const float o[3], const float d[3], Cnt& c) {
     while (top > 0) {
         const Node& n = g.nodes[st[--top]];
         ++c.pops;
-        if (!slab(o, inv, n, h.t)) continue;
+        if (!(g.wt ? slab_wt(o, inv, n, h.t) : slab(o, inv, n, h.t))) continue;
         if (n.d0 & kLeaf) {
             const uint32_t first = n.d0 & ~kLeaf;
             for (uint32_t i = 0; i < n.d1; ++i) {
                 const Face& f = g.f[first + i];
                 float u = 0, v = 0;
                 ++c.tris;
-                const float t = mt(o, d, g.v[f.v0], g.v[f.v1], g.v[f.v2], false, u, v);
+                const float t = g.wt ? woop(o, d, g.v[f.v0], g.v[f.v1], g.v[f.v2], false, u, v)
+                                     : mt(o, d, g.v[f.v0], g.v[f.v1], g.v[f.v2], false, u, v);
                 if (t >= 0.0f && t < h.t) { h.hit = true; h.t = t; h.prim = static_cast<int>(first + i); h.u = u; h.v = v; }
             }
         } else {
@@ -264,14 +318,15 @@ bool occluded(const Geo& g, const float o[3], const float d[3], float tmax, Cnt&
     while (top > 0) {
         const Node& n = g.nodes[st[--top]];
         ++c.pops;
-        if (!slab(o, inv, n, tmax)) continue;
+        if (!(g.wt ? slab_wt(o, inv, n, tmax) : slab(o, inv, n, tmax))) continue;
         if (n.d0 & kLeaf) {
             const uint32_t first = n.d0 & ~kLeaf;
             for (uint32_t i = 0; i < n.d1; ++i) {
                 const Face& f = g.f[first + i];
                 float u, v;
                 ++c.tris;
-                const float t = mt(o, d, g.v[f.v0], g.v[f.v1], g.v[f.v2], true, u, v);
+                const float t = g.wt ? woop(o, d, g.v[f.v0], g.v[f.v1], g.v[f.v2], true, u, v)
+                                     : mt(o, d, g.v[f.v0], g.v[f.v1], g.v[f.v2], true, u, v);
                 if (t > 0.0f && t < tmax) return true;
             }
         } else {
@@ -1136,22 +1191,50 @@ int oracle_sampler_stream(int32_t type, int32_t w, int32_t h, uint32_t frame, in
 
 int oracle_trace(const void* nodes, const void* vertices, const void* faces, const float* rays, uint32_t n,
                  int32_t any, float* hits_out, uint8_t* occl_out, oracle_counters* counters) {
-    Geo g{static_cast<const Node*>(nodes), static_cast<const Vtx*>(vertices), static_cast<const Face*>(faces), 1};
-    Cnt c;
-    for (uint32_t i = 0; i < n; ++i) {
-        const float* r = rays + static_cast<size_t>(i) * 8;
-        const float o[3] = {r[0], r[1], r[2]}, d[3] = {r[4], r[5], r[6]};
-        if (any) {
-            occl_out[i] = occluded(g, o, d, r[7], c) ? 1 : 0;
-        } else {
-            const Hit h = closest(g, o, d, c);
-            float* out = hits_out + static_cast<size_t>(i) * 4;
-            out[0] = h.t;
-            std::memcpy(&out[1], &h.prim, 4);
-            out[2] = h.u;
-            out[3] = h.v;
+    return oracle_trace_mode(nodes, vertices, faces, rays, n, any, 0, hits_out, occl_out, counters);
+}
+
+int oracle_trace_mode(const void* nodes, const void* vertices, const void* faces, const float* rays, uint32_t n,
+                      int32_t any, int32_t watertight, float* hits_out, uint8_t* occl_out,
+                      oracle_counters* counters) {
+    Geo g{static_cast<const Node*>(nodes), static_cast<const Vtx*>(vertices), static_cast<const Face*>(faces), 1,
+          watertight != 0};
+    // rays in blocks of 4096 handed out to the host threads; counters summed
+    const uint32_t block = 4096;
+    const uint32_t nblocks = (n + block - 1) / block;
+    const int threads = static_cast<int>(std::min<uint32_t>(std::max(1u, std::thread::hardware_concurrency()),
+                                                            std::max(1u, nblocks)));
+    std::atomic<uint32_t> next{0};
+    std::atomic<uint64_t> pops{0}, tris{0};
+    auto worker = [&]() {
+        Cnt c;
+        for (uint32_t b = next++; b < nblocks; b = next++) {
+            const uint32_t end = std::min(n, (b + 1) * block);
+            for (uint32_t i = b * block; i < end; ++i) {
+                const float* r = rays + static_cast<size_t>(i) * 8;
+                const float o[3] = {r[0], r[1], r[2]}, d[3] = {r[4], r[5], r[6]};
+                if (any) {
+                    occl_out[i] = occluded(g, o, d, r[7], c) ? 1 : 0;
+                } else {
+                    const Hit h = closest(g, o, d, c);
+                    float* out = hits_out + static_cast<size_t>(i) * 4;
+                    out[0] = h.t;
+                    std::memcpy(&out[1], &h.prim, 4);
+                    out[2] = h.u;
+                    out[3] = h.v;
+                }
+            }
         }
-    }
+        pops += c.pops;
+        tris += c.tris;
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    Cnt c;
+    c.pops = pops;
+    c.tris = tris;
     if (counters) {
         std::memset(counters, 0, sizeof(*counters));
         if (any) { counters->shadow_rays = n; counters->shadow_node_pops = c.pops; counters->shadow_tri_tests = c.tris; }
@@ -1164,7 +1247,7 @@ int oracle_render(const oracle_scene* sc, const oracle_render_args* a, float* ou
                   double* out_var, oracle_counters* counters) {
     Ctx c{};
     c.geo = Geo{static_cast<const Node*>(sc->nodes), static_cast<const Vtx*>(sc->vertices),
-                static_cast<const Face*>(sc->faces), sc->num_nodes};
+                static_cast<const Face*>(sc->faces), sc->num_nodes, a->watertight != 0};
     c.mats = static_cast<const Mat*>(sc->materials);
     c.nmat = sc->num_materials;
     c.em = sc->num_emissive ? static_cast<const EmRef*>(sc->emissive) : nullptr;
@@ -1190,15 +1273,18 @@ int oracle_render(const oracle_scene* sc, const oracle_render_args* a, float* ou
     const uint32_t nfaces = sc->num_faces;
     int threads = a->threads > 0 ? a->threads : static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
     const int step = a->row_step > 0 ? a->row_step : 1;
+    const int y_end = a->row_end > 0 ? std::min(a->row_end, h) : h;
+    const int x0 = std::max(a->col0, 0), x1 = a->col1 > 0 ? std::min(a->col1, w) : w;
     std::vector<int> rows;
-    for (int y = a->row0; y < h; y += step) rows.push_back(y);
+    for (int y = a->row0; y < y_end; y += step) rows.push_back(y);
     std::atomic<uint64_t> acc_c{0}, acc_s{0}, np{0}, nt{0}, snp{0}, snt{0};
+    std::atomic<size_t> next_row{0};
     const auto t0 = std::chrono::steady_clock::now();
-    auto worker = [&](int tid) {
+    auto worker = [&](int) {
         Stats st;
-        for (size_t k = static_cast<size_t>(tid); k < rows.size(); k += static_cast<size_t>(threads)) {
+        for (size_t k = next_row++; k < rows.size(); k = next_row++) {
             const int y = rows[k];
-            for (int x = 0; x < w; ++x) {
+            for (int x = x0; x < x1; ++x) {
                 const size_t p = static_cast<size_t>(y) * w + x;
                 if (a->precision == 64) {
                     double s[3] = {0, 0, 0}, q[3] = {0, 0, 0};
@@ -1250,7 +1336,7 @@ int oracle_render(const oracle_scene* sc, const oracle_render_args* a, float* ou
         counters->closest_rays = acc_c; counters->shadow_rays = acc_s;
         counters->node_pops = np; counters->tri_tests = nt;
         counters->shadow_node_pops = snp; counters->shadow_tri_tests = snt;
-        counters->paths = static_cast<uint64_t>(rows.size()) * w * c.spf * a->num_frames;
+        counters->paths = static_cast<uint64_t>(rows.size()) * static_cast<uint64_t>(std::max(x1 - x0, 0)) * c.spf * a->num_frames;
         counters->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
     return 0;

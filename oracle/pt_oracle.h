@@ -37,6 +37,9 @@ typedef struct oracle_render_args {
     uint32_t first_frame, num_frames;
     int32_t  row0, row_step, threads;
     int32_t  precision;         /* 32 or 64 */
+    int32_t  col0, col1;        /* pixel columns [col0, col1) (col1 0 = width)  */
+    int32_t  row_end;           /* rows row0, row0 + row_step, ... below row_end (0 = height) */
+    int32_t  watertight;        /* 1: the watertight triangle and box tests (added mode) */
     int32_t  _pad;
 } oracle_render_args;
 
@@ -57,6 +60,11 @@ int oracle_sampler_stream(int32_t type, int32_t w, int32_t h, uint32_t frame, in
 /* rays: n x 8 floats (o, -, d, tmax).  hits: n x 4 (t, prim bits, u, v). */
 int oracle_trace(const void* nodes, const void* vertices, const void* faces, const float* rays, uint32_t n,
                  int32_t any, float* hits_out, uint8_t* occl_out, oracle_counters* counters);
+/* the same with watertight = 1: Woop et al.'s triangle test on the shared
+ * vertices and the widened box exit (an added mode, not the reference's) */
+int oracle_trace_mode(const void* nodes, const void* vertices, const void* faces, const float* rays, uint32_t n,
+                      int32_t any, int32_t watertight, float* hits_out, uint8_t* occl_out,
+                      oracle_counters* counters);
 /* precision 32: out_f32 = the reference's accumulated film (w*h*4, running mean).
  * precision 64: out_mean / out_var = per-pixel mean and sample variance of the
  * clamped per-sample radiance (w*h*3 doubles each). */

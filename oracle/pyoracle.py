@@ -44,7 +44,8 @@ class RenderArgs(C.Structure):
     _fields_ = [("sample_per_frame", C.c_int32), ("max_depth", C.c_int32), ("sampler_type", C.c_int32),
                 ("arg_rtl", C.c_int32), ("pcg_seed", C.c_uint32), ("first_frame", C.c_uint32),
                 ("num_frames", C.c_uint32), ("row0", C.c_int32), ("row_step", C.c_int32), ("threads", C.c_int32),
-                ("precision", C.c_int32), ("_pad", C.c_int32)]
+                ("precision", C.c_int32), ("col0", C.c_int32), ("col1", C.c_int32),
+                ("row_end", C.c_int32), ("watertight", C.c_int32), ("_pad", C.c_int32)]
 
 
 class Counters(C.Structure):
@@ -158,14 +159,16 @@ class Oracle:
                                      C.c_int32(spf), C.c_int32(sif), C.c_uint32(ndims), C.c_uint32(pcg_seed), _p(out))
         return out
 
-    def trace(self, nodes, vertices, faces, rays, any_hit=False):
+    def trace(self, nodes, vertices, faces, rays, any_hit=False, watertight=False):
         rays = np.ascontiguousarray(rays, np.float32)
         n = len(rays)
         hits = np.zeros((n, 4), np.float32)
         occ = np.zeros(n, np.uint8)
         cnt = Counters()
-        self.L.oracle_trace(_p(nodes), _p(np.ascontiguousarray(vertices, VERTEX)), _p(np.ascontiguousarray(faces, FACE)),
-                            _p(rays), C.c_uint32(n), C.c_int32(1 if any_hit else 0), _p(hits), _p(occ), C.byref(cnt))
+        self.L.oracle_trace_mode(_p(nodes), _p(np.ascontiguousarray(vertices, VERTEX)),
+                                 _p(np.ascontiguousarray(faces, FACE)), _p(rays), C.c_uint32(n),
+                                 C.c_int32(1 if any_hit else 0), C.c_int32(1 if watertight else 0), _p(hits), _p(occ),
+                                 C.byref(cnt))
         return (occ.astype(bool) if any_hit else hits), cnt.as_dict()
 
     def bsdf_eval(self, materials, records):
@@ -188,11 +191,13 @@ class Oracle:
                         int(sa.camera["height"]), punct)
 
     def render(self, prep: Prepared, spf, max_depth, sampler, frames, first_frame=0, precision=64, rtl=1,
-               pcg_seed=0, row0=0, row_step=1, threads=0):
-        """precision 32: the reference's film (H, W, 4).  precision 64: (mean, var) of shape (H, W, 3)."""
+               pcg_seed=0, row0=0, row_step=1, threads=0, crop=None, watertight=False):
+        """precision 32: the reference's film (H, W, 4).  precision 64: (mean, var) of shape (H, W, 3).
+        crop = (x0, y0, x1, y1) renders only those pixels (the rest stay zero)."""
         sc = prep.struct()
-        a = RenderArgs(spf, max_depth, sampler, rtl, pcg_seed, first_frame, frames, row0, row_step, threads,
-                       precision, 0)
+        x0, y0, x1, y1 = crop if crop is not None else (0, row0, 0, 0)
+        a = RenderArgs(spf, max_depth, sampler, rtl, pcg_seed, first_frame, frames, y0, row_step, threads,
+                       precision, x0, x1, y1, 1 if watertight else 0, 0)
         cnt = Counters()
         h, w = prep.height, prep.width
         if precision == 32:
