@@ -161,6 +161,18 @@ def combine_over_ranks(ms: float, rays: float, dist, device: str):
     return float(t[0]), float(r[0])
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the CPU baseline's record."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def reference_arm(args):
     """The reference's own CPU integrator on the host cores, bounded sample."""
     rank, world, _ = dist_env()
@@ -199,6 +211,7 @@ def reference_arm(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": cfg,
             "cpu_baseline": {"value": round(value, 3), "unit": METRIC, "cores": cores, "kind": "reference",
+                             "cpu_model": cpu_model(), "build": "reference host sources, g++ -O3",
                              "sample": sample},
             "e2e": {"value": round(value, 3), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -240,6 +253,8 @@ def cpu_baseline(sa, spp, seconds):
         rays, secs, paths, frames = s["closest_rays"] + s["shadow_rays"], s["seconds"], s["paths"], 1
         kind = "port"
     return {"value": round(float(rays / secs / 1e6), 3), "unit": METRIC, "cores": cores, "kind": kind,
+            "cpu_model": cpu_model(),
+            "build": "reference host sources, g++ -O3" if kind == "reference" else "oracle restatement, g++ -O2",
             "sample": f"every {stride}th row of {int(sa.camera['width'])}x{h}, {frames * sa.sample_per_frame} spp "
                       f"({frames} frames of {sa.sample_per_frame}), {int(paths)} paths, {int(rays)} rays, "
                       f"{secs:.1f} s"}

@@ -400,11 +400,17 @@ int pt_trace_closest(pt_scene* scene, const float* rays, uint32_t n, pt_hit* hit
 int pt_trace_any(pt_scene* scene, const float* rays, uint32_t n, uint8_t* occluded,
                  int32_t ptrs_are_device);
 /* Added, no reference counterpart: pt_trace_closest for HOST rays and hits
- * that allocates nothing.  Rays and hits pass through a fixed file-scope
- * device array of PT_STATIC_TRACE_MAX_RAYS rays (3 MiB); n above that is
- * rejected with PT_ERR_INVALID.  Calls on one device share the array and must
- * not overlap; the first call on a device looks up the array's address (and
- * may load the module), so make it before any stream capture on that device. */
+ * that allocates nothing, for callers that cannot allocate device memory (a
+ * host whose own pool allocator owns the device, or code where a cudaMalloc
+ * is not allowed).  Rays and hits pass through a fixed file-scope device
+ * array of PT_STATIC_TRACE_MAX_RAYS rays (3 MiB, held on every device that
+ * loads the library until exit); n above that is rejected with
+ * PT_ERR_INVALID.  The work runs on the calling thread's per-thread default
+ * stream and the call returns once it is done.  Calls on one device share the
+ * array and must not overlap; the first call on a device looks up the
+ * array's address (and may load the module), so make it before any stream
+ * capture on that device.  Resetting the device between calls is not
+ * supported (the looked-up address belongs to the old context). */
 #define PT_STATIC_TRACE_MAX_RAYS 65536
 int pt_trace_closest_static(pt_scene* scene, const float* rays, uint32_t n, pt_hit* hits);
 /* Sampler streams: out[(y*width + x)*ndims + k] = dimension k of pixel (x,y) for the

@@ -64,8 +64,19 @@ def _p(a):
     return C.c_void_p(a.ctypes.data)
 
 
-def build(ref: bool = False) -> None:
-    """Compile liboracle.so (and, when the reference tree is present, _ref/libptref.so)."""
+def reference_dir() -> str | None:
+    """The reference tree oracle/Makefile would build from (PT_REF_DIR, else
+    its default search), or None when there is none."""
+    r = subprocess.run(["make", "-s", "-C", HERE, "ref-dir"], capture_output=True, text=True)
+    path = r.stdout.strip()
+    return path if r.returncode == 0 and path else None
+
+
+def build(ref: bool | None = None) -> None:
+    """Compile liboracle.so and, with ref (default: when a reference tree is
+    found), the reference's host and GPU builds under _ref/."""
+    if ref is None:
+        ref = reference_dir() is not None
     targets = ["oracle", "ref", "ref-gpu"] if ref else ["oracle"]
     r = subprocess.run(["make", "-C", HERE, "-j8", *targets], capture_output=True, text=True)
     if r.returncode != 0:

@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -875,13 +876,17 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, 
     const auto t_dl0 = clock::now();
     t.inner.resize(kept);
     t.tris.resize(n);
+    // the reordered faces land in a staging array and replace the scene's
+    // only once the tree has passed its check
+    std::unique_ptr<pt_face[]> faces_out(new pt_face[n]);
     touch_pages(t.inner.data(), size_t(kept) * sizeof(InnerNode));
     touch_pages(t.tris.data(), size_t(n) * sizeof(TriRecord));
+    touch_pages(faces_out.get(), size_t(n) * sizeof(pt_face));
     if (kept)
         LB_CU(cudaMemcpyAsync(t.inner.data(), d_inner, size_t(kept) * sizeof(InnerNode), cudaMemcpyDeviceToHost,
                               stream));
     LB_CU(cudaMemcpyAsync(t.tris.data(), d_tris, size_t(n) * sizeof(TriRecord), cudaMemcpyDeviceToHost, stream));
-    LB_CU(cudaMemcpyAsync(hs.faces.data(), d_fout, size_t(n) * sizeof(pt_face), cudaMemcpyDeviceToHost, stream));
+    LB_CU(cudaMemcpyAsync(faces_out.get(), d_fout, size_t(n) * sizeof(pt_face), cudaMemcpyDeviceToHost, stream));
     LB_CU(cudaStreamSynchronize(stream));
     const auto t_dl = clock::now();
 
@@ -895,6 +900,7 @@ int build_accel_device(pt_scene* s, int device, uint32_t max_leaf, int treelet, 
             return PT_ERR_DEVICE;
         }
     }
+    std::memcpy(hs.faces.data(), faces_out.get(), size_t(n) * sizeof(pt_face));
     for (int a = 0; a < 3; ++a) {
         t.root_lo[a] = (&h_root[0].x)[a];
         t.root_hi[a] = (&h_root[1].x)[a];

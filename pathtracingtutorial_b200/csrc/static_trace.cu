@@ -1,17 +1,31 @@
 // static_trace.cu -- pt_trace_closest_static: closest hits of host rays
 // without any allocation (an added entry point; the reference has none).
 //
-// Rays and hits travel through one file-scope device array of fixed size,
-// kStaticTraceMaxRays rays (2 MiB of rays, 1 MiB of hits).  Its address is
-// looked up once per device with cudaGetSymbolAddress and checked; after
-// that a call is: copy the rays in, clear the error word, one launch of the
+// Some callers cannot allocate device memory: a host that has handed the
+// whole device to its own pool allocator, or code that runs where a
+// cudaMalloc would synchronise the device or is forbidden outright.  For
+// them, rays and hits travel through one file-scope device array of fixed
+// size, kStaticTraceMaxRays rays (2 MiB of rays, 1 MiB of hits), which every
+// GPU that loads the library holds until the process exits.
+//
+// Set-up, once per device (on the first call there, with that device
+// current): the array's device address is looked up with
+// cudaGetSymbolAddress (the host-side name of a __device__ variable is not a
+// device address) and the SM count is read; both are cached.  After that a
+// call is: copy the rays in, clear the error word, one launch of the
 // warp-scheduled closest-hit loop the wavefront uses, copy the hits and the
-// error word out.  No cudaMalloc, cudaFree or allocating library call is
-// made.  Calls on one device share the array, so they must not overlap (one
-// host thread at a time per device; a mutex serialises calls within this
-// library).  The first call on a device performs the symbol lookup, which
-// loads the module if needed: make it before any stream capture on that
-// device.
+// error word out -- all on the per-thread default stream, waited for with a
+// stream synchronisation (other streams of the process are not waited on).
+// No cudaMalloc, cudaFree or allocating library call is made.
+//
+// Calls on one device share the array, which keeps the previous call's
+// contents (the error word is cleared on every call; hits are written for
+// every ray of the call), so calls whose GPU work overlaps would race: a
+// mutex serialises the calls made through this library.  The first call on
+// a device may load the module: make it before any stream capture on that
+// device.  The cached addresses are only valid for the device contexts that
+// were current at set-up: resetting a device (cudaDeviceReset) between calls
+// is not supported.
 
 #include <cuda_runtime.h>
 
@@ -41,6 +55,7 @@ namespace {
 
 std::mutex g_static_mu;
 StaticTraceScratch* g_static_addr[kStaticTraceMaxDevices] = {};
+int g_static_sms[kStaticTraceMaxDevices] = {};
 
 __global__ void __launch_bounds__(128) k_trace_closest_static(DeviceScene s, StaticTraceScratch* sc, uint32_t n,
                                                               int watertight) {
@@ -86,25 +101,33 @@ int trace_closest_static(pt_scene* s, const float* rays, uint32_t n, pt_hit* hit
         e = cudaGetSymbolAddress(&p, g_static_trace);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
         if (!p) { set_error("trace (static scratch): null symbol address"); return PT_ERR_CUDA; }
+        int sms = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return cuda_fail(e, "SM count");
+        g_static_sms[dev] = sms > 0 ? sms : 1;
         g_static_addr[dev] = static_cast<StaticTraceScratch*>(p);
     }
     StaticTraceScratch* sc = g_static_addr[dev];
-    e = cudaMemcpy(sc->rays, rays, static_cast<size_t>(n) * 2 * sizeof(float4), cudaMemcpyHostToDevice);
+    const cudaStream_t st = cudaStreamPerThread;
+    e = cudaMemcpyAsync(sc->rays, rays, static_cast<size_t>(n) * 2 * sizeof(float4), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_fail(e, "ray upload");
-    e = cudaMemset(&sc->err, 0, sizeof(uint32_t));
+    e = cudaMemsetAsync(&sc->err, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return cuda_fail(e, "clear");
     const DeviceScene v = device_view(s);
     const int wt = (s->host.settings.flags & PT_FLAG_WATERTIGHT) ? 1 : 0;
-    const int blocks = static_cast<int>(std::min<uint32_t>((n + 127) / 128, 148u * 16u));
-    k_trace_closest_static<<<blocks, 128>>>(v, sc, n, wt);
+    // 16 resident blocks of 128 threads per SM; the loop strides over the rays
+    const uint32_t max_blocks = static_cast<uint32_t>(g_static_sms[dev]) * 16u;
+    const int blocks = static_cast<int>(std::min<uint32_t>((n + 127) / 128, max_blocks));
+    k_trace_closest_static<<<blocks, 128, 0, st>>>(v, sc, n, wt);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "launch");
-    e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) return cuda_fail(e, "kernel");
     uint32_t err = 0;
-    e = cudaMemcpy(&err, &sc->err, sizeof(uint32_t), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(hits, sc->hits, static_cast<size_t>(n) * sizeof(pt_hit), cudaMemcpyDeviceToHost);
+    e = cudaMemcpyAsync(&err, &sc->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hits, sc->hits, static_cast<size_t>(n) * sizeof(pt_hit), cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return cuda_fail(e, "download");
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel");
     if (err) { set_error("traversal stack overflow"); return PT_ERR_DEVICE; }
     return PT_OK;
 }

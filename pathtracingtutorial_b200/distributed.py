@@ -38,7 +38,10 @@ def reduce_to_root(weighted, dist, group=None):
 def render_distributed(scene, spp: int, group=None, renderer=None):
     """render(scene, spp) over the ranks of `group` (default: the world).
     Every rank calls it with the same scene and spp, its scene uploaded to its
-    own device.  Returns the (H, W, 4) image on rank 0, None elsewhere."""
+    own device.  Returns the (H, W, 4) image on rank 0, None elsewhere.
+    Afterwards every rank's scene stands at the frame count a single-GPU
+    render of spp leaves (all of the render's frames), so a later render
+    continues from the same sample index on every rank."""
     import torch
     import torch.distributed as dist
     from . import Renderer
@@ -58,6 +61,7 @@ def render_distributed(scene, spp: int, group=None, renderer=None):
         check(lib().pt_film_download_to(r.film._h, C.c_void_p(img.data_ptr()), 1))
         img *= float(count * spf)
     torch.cuda.synchronize(img.device)
+    scene.set_frame_count(frames)
     reduce_to_root(img, dist, group)
     if rank != 0:
         return None

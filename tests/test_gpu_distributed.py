@@ -29,6 +29,7 @@ def test_one_rank_equals_single_gpu_render():
         sc.build_accel()
         sc.upload_to_device(0)
         img = render_distributed(sc, 32)
+        assert sc.info()["frame_count"] == 32 // sa.sample_per_frame   # as a single-GPU render leaves it
         ref = pt.render(sc, 32)
         assert img.shape == ref.shape and img[..., :3].mean() > 0
         assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))

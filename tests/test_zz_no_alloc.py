@@ -1,9 +1,14 @@
 """The allocation-free closest-hit entry point (pt_trace_closest_static).
 
+It serves callers that cannot allocate device memory (a host whose own pool
+allocator owns the device, or code where a cudaMalloc is not allowed): rays
+and hits pass through a fixed array that the library holds on every device.
+
 Collected last on purpose: it must give the same hits as pt_trace_closest
-whether it runs alone or after every other test of the session, on two calls
-in a row (the second call reuses the static array the first one filled), and
-it rejects more rays than its array holds without touching the device.
+and as the oracle's traversal, bit for bit, whether it runs alone or after
+every other test of the session, on two calls in a row (the second call
+reuses the static array the first one filled), and it rejects more rays than
+its array holds without touching the device.
 """
 import numpy as np
 import pytest
@@ -30,7 +35,7 @@ def _rays(n, lo, hi, seed):
 
 
 @pytest.mark.parametrize("name", ["cornell", "spheres"])
-def test_static_trace_matches_trace_closest_twice(name):
+def test_static_trace_matches_trace_closest_twice(oracle, name):
     sa = scenes.cornell_box(width=32, height=32) if name == "cornell" else \
         scenes.icosphere_field(n_spheres=40, subdiv=3, width=32, height=18, env_size=(64, 32))
     s = _scene(sa)
@@ -42,6 +47,13 @@ def test_static_trace_matches_trace_closest_twice(name):
     assert np.array_equal(first.view(np.uint8), ref.view(np.uint8))
     assert np.array_equal(second.view(np.uint8), ref.view(np.uint8))
     assert (ref["prim"] >= 0).mean() > 0.3
+    # and the oracle's restatement of the reference's traversal, directly
+    prep = oracle.prepare(sa)
+    rays = np.zeros((len(o), 8), np.float32)
+    rays[:, :3], rays[:, 4:7] = o, d
+    orc, _ = oracle.trace(prep.nodes, prep.vertices, prep.faces, rays)
+    gpu = np.stack([first["t"], first["prim"].view(np.float32), first["u"], first["v"]], 1)
+    assert np.array_equal(gpu.view(np.uint32), orc.view(np.uint32))
     # a smaller call after a full one: only its own rays come back
     o2, d2 = _rays(1000, lo, hi, 6)
     assert np.array_equal(pt.trace_closest_static(s, o2, d2).view(np.uint8), pt.trace_closest(s, o2, d2).view(np.uint8))
