@@ -72,11 +72,17 @@ PT_HD float x_add(float a, float b) { return __fadd_rn(a, b); }
 PT_HD float x_sub(float a, float b) { return __fsub_rn(a, b); }
 PT_HD float x_mul(float a, float b) { return __fmul_rn(a, b); }
 PT_HD float x_rcp(float a) { return __frcp_rn(a); }
+PT_HD float x_div(float a, float b) { return __fdiv_rn(a, b); }
+PT_HD double xd_mul(double a, double b) { return __dmul_rn(a, b); }
+PT_HD double xd_sub(double a, double b) { return __dsub_rn(a, b); }
 #else
 PT_HD float x_add(float a, float b) { return a + b; }
 PT_HD float x_sub(float a, float b) { return a - b; }
 PT_HD float x_mul(float a, float b) { return a * b; }
 PT_HD float x_rcp(float a) { return 1.0f / a; }
+PT_HD float x_div(float a, float b) { return a / b; }
+PT_HD double xd_mul(double a, double b) { return a * b; }
+PT_HD double xd_sub(double a, double b) { return a - b; }
 #endif
 
 // ---------------------------------------------------------------------------

@@ -21,6 +21,14 @@
 //  * Closest hit keeps the first hit found under strict '<' (ties resolved
 //    exactly as in the reference); any-hit returns on the first triangle with
 //    1e-4 < t < tMax, which is order independent.
+//
+// Watertight mode (PT_FLAG_WATERTIGHT; the reference has none): the triangle
+// test is Woop, Benthin and Wald's (JCGT 2013) on the triangle's own shared
+// vertex positions, so that two triangles sharing an edge see bit-identical
+// transformed edge endpoints and exactly opposite edge functions, and the box
+// test's exit distance is widened (Ize 2013, "Robust BVH Ray Traversal"), so
+// no box that the ray touches is culled by rounding.  Visit order and the
+// acceptance rules (t >= 1e-4, shadow t > 1e-4) are those of the default mode.
 #pragma once
 
 #include "pt_internal.h"
@@ -35,15 +43,24 @@ struct RayInv {
     float ox, oy, oz;
     float dx, dy, dz;
     float ix, iy, iz;
+    float xs;          // box exit scale: 1 (the reference's test) or kWatertightExitScale
     int   sx, sy, sz;
     bool  nan_free;
 };
+
+// Widening of a box's exit distance.  A slab distance (l - o) * (1 / d) is
+// off by a factor in [1 - gamma(3), 1 + gamma(3)], gamma(n) = n u / (1 - n u),
+// u = 2^-24 (Ize 2013), so a box the ray touches passes whenever the exit is
+// scaled by (1 + gamma(3)) / (1 - gamma(3)), just above 1 + 2 gamma(3) =
+// 1 + 3.0000005 ulp; 1 + 4 ulp covers it and the rounding of the product.
+constexpr float kWatertightExitScale = 1.0f + 4.0f * 1.1920929e-7f;
 
 PT_HD RayInv make_ray_inv(float ox, float oy, float oz, float dx, float dy, float dz) {
     RayInv r;
     r.ox = ox; r.oy = oy; r.oz = oz;
     r.dx = dx; r.dy = dy; r.dz = dz;
     r.ix = x_rcp(dx); r.iy = x_rcp(dy); r.iz = x_rcp(dz);
+    r.xs = 1.0f;
     r.sx = r.ix < 0.0f ? 1 : 0;
     r.sy = r.iy < 0.0f ? 1 : 0;
     r.sz = r.iz < 0.0f ? 1 : 0;
@@ -51,7 +68,10 @@ PT_HD RayInv make_ray_inv(float ox, float oy, float oz, float dx, float dy, floa
     return r;
 }
 
-// entry / exit of a box, with the reference's arithmetic.
+PT_HD float exit_scale(bool watertight) { return watertight ? kWatertightExitScale : 1.0f; }
+
+// entry / exit of a box, with the reference's arithmetic; the exit is
+// multiplied by r.xs (exact for the default 1).
 PT_HD void box_span(const RayInv& r, float lx, float ly, float lz, float hx, float hy, float hz,
                     float& entry, float& exit_) {
     const float t1x = x_mul(x_sub(lx, r.ox), r.ix), t2x = x_mul(x_sub(hx, r.ox), r.ix);
@@ -59,14 +79,14 @@ PT_HD void box_span(const RayInv& r, float lx, float ly, float lz, float hx, flo
     const float t1z = x_mul(x_sub(lz, r.oz), r.iz), t2z = x_mul(x_sub(hz, r.oz), r.iz);
     if (r.nan_free) {
         entry = fmaxf(fmaxf(fminf(t1x, t2x), fminf(t1y, t2y)), fmaxf(fminf(t1z, t2z), 0.0f));
-        exit_ = fminf(fminf(fmaxf(t1x, t2x), fmaxf(t1y, t2y)), fmaxf(t1z, t2z));
+        exit_ = x_mul(fminf(fminf(fmaxf(t1x, t2x), fmaxf(t1y, t2y)), fmaxf(t1z, t2z)), r.xs);
     } else {
         // literal recurrence (bvh_traversal.cuh:33-39) with t_max starting at +inf
         float tn = 0.0f, tf = INFINITY;
         tn = fminf(fmaxf(t1x, tn), fmaxf(t2x, tn)); tf = fmaxf(fminf(t1x, tf), fminf(t2x, tf));
         tn = fminf(fmaxf(t1y, tn), fmaxf(t2y, tn)); tf = fmaxf(fminf(t1y, tf), fminf(t2y, tf));
         tn = fminf(fmaxf(t1z, tn), fmaxf(t2z, tn)); tf = fmaxf(fminf(t1z, tf), fminf(t2z, tf));
-        entry = tn; exit_ = tf;
+        entry = tn; exit_ = x_mul(tf, r.xs);
     }
 }
 
@@ -96,45 +116,50 @@ PT_HD float tri_mt(const RayInv& r, float v0x, float v0y, float v0z,
     return t;
 }
 
-// Watertight ray/triangle test (Woop, Benthin, Wald 2013): shear/scale so the
-// ray is +z, 2D edge functions with a double-precision fallback on exact
-// zeros.  Used when PT_FLAG_WATERTIGHT is set; not bit-comparable with the
-// reference (which has no watertight mode).
-PT_HD float tri_watertight(const RayInv& r, float v0x, float v0y, float v0z,
-                           float e1x, float e1y, float e1z, float e2x, float e2y, float e2z,
-                           bool shadow, float& u_out, float& v_out) {
-    // dominant axis
+// Watertight ray/triangle test (Woop, Benthin, Wald 2013) on the absolute
+// vertex positions p0, p1, p2 (the shared vertices of the mesh, not a
+// per-triangle edge record): translate to the ray origin, shear and scale so
+// the ray runs along +z, evaluate the three 2D edge functions, and redo them
+// in double when one is exactly zero (products of floats are exact in
+// double, so the signs are exact).  Every operation is explicitly rounded, so
+// host and device agree bit for bit.  Barycentrics as the default test:
+// u weights p1, v weights p2.
+PT_HD float tri_watertight(const RayInv& r, const float* p0, const float* p1, const float* p2, bool shadow,
+                           float& u_out, float& v_out) {
     const float adx = fabsf(r.dx), ady = fabsf(r.dy), adz = fabsf(r.dz);
     int kz = (adx > ady) ? (adx > adz ? 0 : 2) : (ady > adz ? 1 : 2);
     int kx = kz + 1 == 3 ? 0 : kz + 1;
     int ky = kx + 1 == 3 ? 0 : kx + 1;
     const float d[3] = {r.dx, r.dy, r.dz};
-    if (d[kz] < 0.0f) { int t = kx; kx = ky; ky = t; }
-    const float sx = d[kx] / d[kz], sy = d[ky] / d[kz], sz = 1.0f / d[kz];
-    const float a[3] = {v0x - r.ox, v0y - r.oy, v0z - r.oz};
-    const float b[3] = {a[0] + e1x, a[1] + e1y, a[2] + e1z};
-    const float c[3] = {a[0] + e2x, a[1] + e2y, a[2] + e2z};
-    const float ax = a[kx] - sx * a[kz], ay = a[ky] - sy * a[kz];
-    const float bx = b[kx] - sx * b[kz], by = b[ky] - sy * b[kz];
-    const float cx = c[kx] - sx * c[kz], cy = c[ky] - sy * c[kz];
-    float U = cx * by - cy * bx;
-    float V = ax * cy - ay * cx;
-    float W = bx * ay - by * ax;
+    if (d[kz] < 0.0f) { const int t = kx; kx = ky; ky = t; }
+    const float sx = x_div(d[kx], d[kz]), sy = x_div(d[ky], d[kz]), sz = x_rcp(d[kz]);
+    const float o[3] = {r.ox, r.oy, r.oz};
+    float a[3], b[3], c[3];
+    for (int k = 0; k < 3; ++k) {
+        a[k] = x_sub(p0[k], o[k]);
+        b[k] = x_sub(p1[k], o[k]);
+        c[k] = x_sub(p2[k], o[k]);
+    }
+    const float ax = x_sub(a[kx], x_mul(sx, a[kz])), ay = x_sub(a[ky], x_mul(sy, a[kz]));
+    const float bx = x_sub(b[kx], x_mul(sx, b[kz])), by = x_sub(b[ky], x_mul(sy, b[kz]));
+    const float cx = x_sub(c[kx], x_mul(sx, c[kz])), cy = x_sub(c[ky], x_mul(sy, c[kz]));
+    float U = x_sub(x_mul(cx, by), x_mul(cy, bx));
+    float V = x_sub(x_mul(ax, cy), x_mul(ay, cx));
+    float W = x_sub(x_mul(bx, ay), x_mul(by, ax));
     if (U == 0.0f || V == 0.0f || W == 0.0f) {
-        U = (float)((double)cx * (double)by - (double)cy * (double)bx);
-        V = (float)((double)ax * (double)cy - (double)ay * (double)cx);
-        W = (float)((double)bx * (double)ay - (double)by * (double)ax);
+        U = static_cast<float>(xd_sub(xd_mul(cx, by), xd_mul(cy, bx)));
+        V = static_cast<float>(xd_sub(xd_mul(ax, cy), xd_mul(ay, cx)));
+        W = static_cast<float>(xd_sub(xd_mul(bx, ay), xd_mul(by, ax)));
     }
     if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return -1.0f;
-    const float det = U + V + W;
+    const float det = x_add(x_add(U, V), W);
     if (det == 0.0f) return -1.0f;
-    const float az = sz * a[kz], bz = sz * b[kz], cz = sz * c[kz];
-    const float T = U * az + V * bz + W * cz;
-    const float inv = 1.0f / det;
-    const float t = T * inv;
+    const float az = x_mul(sz, a[kz]), bz = x_mul(sz, b[kz]), cz = x_mul(sz, c[kz]);
+    const float T = x_add(x_add(x_mul(U, az), x_mul(V, bz)), x_mul(W, cz));
+    const float inv = x_rcp(det);
+    const float t = x_mul(T, inv);
     if (shadow ? !(t > 1e-4f) : (t < 1e-4f)) return -1.0f;
-    // barycentrics w.r.t. (v0, v1, v2): weight of v1 is V, of v2 is W
-    u_out = V * inv; v_out = W * inv;
+    u_out = x_mul(V, inv); v_out = x_mul(W, inv);
     return t;
 }
 
@@ -151,18 +176,27 @@ struct TraceCounters { uint32_t inner; uint32_t tris; };
 PT_HD float tri_test(const DeviceScene& s, const RayInv& r, uint32_t ti, bool shadow, bool watertight,
                      float& u, float& v, bool& last) {
     const float* base = reinterpret_cast<const float*>(s.tris + ti);
+    if (watertight) {
+        last = (__float_as_uint_hd(PT_LDG4(base + 8).y) & 1u) != 0u;
+        const uint4 f = PT_LDGU4(s.faces + ti);
+        const float4 p0 = PT_LDG4(s.vertices[f.x].position);
+        const float4 p1 = PT_LDG4(s.vertices[f.y].position);
+        const float4 p2 = PT_LDG4(s.vertices[f.z].position);
+        const float q0[3] = {p0.x, p0.y, p0.z}, q1[3] = {p1.x, p1.y, p1.z}, q2[3] = {p2.x, p2.y, p2.z};
+        return tri_watertight(r, q0, q1, q2, shadow, u, v);
+    }
     const float4 a = PT_LDG4(base);
     const float4 b = PT_LDG4(base + 4);
     const float4 c = PT_LDG4(base + 8);
     last = (__float_as_uint_hd(c.y) & 1u) != 0u;
-    if (watertight)
-        return tri_watertight(r, a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, shadow, u, v);
     return tri_mt(r, a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, shadow, u, v);
 }
 
 // Closest hit.  Returns prim (BVH-ordered face index) or -1; t = FLT_MAX on miss.
-PT_HD int trace_closest(const DeviceScene& s, const RayInv& r, bool watertight,
+PT_HD int trace_closest(const DeviceScene& s, const RayInv& ray, bool watertight,
                         float& t_out, float& u_out, float& v_out, uint32_t& err, TraceCounters& cnt) {
+    RayInv r = ray;
+    r.xs = exit_scale(watertight);
     float best = FLT_MAX;
     int prim = -1;
     float bu = 0.0f, bv = 0.0f;
@@ -230,9 +264,11 @@ PT_HD int trace_closest(const DeviceScene& s, const RayInv& r, bool watertight,
 }
 
 // Any hit in (1e-4, tmax).
-PT_HD bool trace_any(const DeviceScene& s, const RayInv& r, float tmax, bool watertight,
+PT_HD bool trace_any(const DeviceScene& s, const RayInv& ray, float tmax, bool watertight,
                      uint32_t& err, TraceCounters& cnt) {
     if (s.num_faces == 0) return false;
+    RayInv r = ray;
+    r.xs = exit_scale(watertight);
     float en, ex;
     box_span(r, s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], en, ex);
     if (!(en <= tmax && en <= ex)) return false;
@@ -391,6 +427,7 @@ __device__ __forceinline__ void closest_loop(const DeviceScene& s, uint32_t i, u
     for (;;) {
         while (!have && i < n) {
             fetch(i, w.r);
+            w.r.xs = exit_scale(watertight);
             if (closest_begin(s, w)) { have = true; }
             else { done(i, w); i += stride; }
         }
@@ -488,6 +525,7 @@ __device__ __forceinline__ void any_loop(const DeviceScene& s, uint32_t i, uint3
     for (;;) {
         while (!have && i < n) {
             fetch(i, w);
+            w.r.xs = exit_scale(watertight);
             if (any_begin(s, w)) { have = true; }
             else { done(i, false); i += stride; }
         }
