@@ -21,9 +21,11 @@
 // incident radiance to q with the one-sample estimate
 // -L_in(w) |cos| / p(w) * log q(w | x)  per recorded path vertex, in
 // minibatches interleaved over the whole image; the backward pass runs on the
-// tensor cores too
-// (dX = dY W and dW = dY^T X per CTA tile), the hash-grid gradient is scattered
-// with FP32 atomics, and Adam updates FP32 master copies.
+// tensor cores too (dX = dY W and dW = dY^T X per warp tile), and Adam
+// updates FP32 master copies.  Training is deterministic: the samples are
+// stored in path order (count, scan, write), and every gradient sum is
+// accumulated in 64-bit fixed point (units of 2^-40) with integer atomics,
+// whose result does not depend on the order in which they land.
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -66,20 +68,37 @@ constexpr int kGSmemW = kGHid * (kGIn + 8) + 2 * kGHid * (kGHid + 8) + kGOutPad 
 struct GuideNet {
     __half2*        grid;        // kGLevels * kGTable (inference copy)
     float2*         grid_master; // FP32 master
-    float2*         grid_grad;
+    unsigned long long* grid_grad;   // 2 per entry, fixed point (kGFix)
     float2*         grid_m;
     float2*         grid_v;
     __nv_bfloat16*  w;           // kGWeights (inference copy), layer-packed [out][in]
     float*          w_master;
-    float*          w_grad;
+    unsigned long long* w_grad;  // kGWeights, fixed point (kGFix)
     float*          w_m;
     float*          w_v;
     float           lo[3];       // scene bounds (positions mapped to [0,1]^3)
     float           inv_ext[3];
     float           scale[kGLevels];
     uint32_t        dense_limit; // levels with (res+1)^3 <= table use direct indexing
-    float*          loss;        // [0] sum of w (-log q), [1] samples, [2] mean of the last pass
+    float*          loss;        // [2] mean loss of the last pass
+    unsigned long long* loss_fix;    // [0] sum of w (-log q) (kGLossFix units), [1] samples
 };
+
+// Fixed-point gradient sums: a contribution x is added as round(x * 2^40)
+// (clamped to +-2^20, far above any gradient of a mean loss), so a sum holds
+// up to +-2^23 with a resolution of 2^-40.  Loss sums use 2^-20 units.
+constexpr float kGFix = 1099511627776.0f;              // 2^40
+constexpr double kGFixInv = 1.0 / 1099511627776.0;
+constexpr float kGLossFix = 1048576.0f;                // 2^20
+__host__ __device__ __forceinline__ float g_unfix(unsigned long long v) {
+    return static_cast<float>(static_cast<double>(static_cast<long long>(v)) * kGFixInv);
+}
+#if defined(__CUDACC__)
+__device__ __forceinline__ unsigned long long g_fix(float x) {
+    x = fminf(fmaxf(x, -1048576.0f), 1048576.0f);
+    return static_cast<unsigned long long>(__float2ll_rn(x * kGFix));
+}
+#endif
 
 // ---------------------------------------------------------------------------
 // mma helpers
@@ -380,9 +399,10 @@ __device__ __forceinline__ void store_t(const uint32_t (&a)[K / 16][4], __nv_bfl
     }
 }
 
-// dW[out][in] += DYT[out][16] . XT[in][16]^T  (K = the warp's 16 rows), into FP32 shared dW.
+// dW[out][in] += DYT[out][16] . XT[in][16]^T  (K = the warp's 16 rows), into the
+// fixed-point shared dW.
 template <int OUT, int IN>
-__device__ __forceinline__ void accum_dw(const __nv_bfloat16* DYT, const __nv_bfloat16* XT, float* sdw) {
+__device__ __forceinline__ void accum_dw(const __nv_bfloat16* DYT, const __nv_bfloat16* XT, unsigned long long* sdw) {
     const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
 #pragma unroll
     for (int mt = 0; mt < OUT / 16; ++mt) {
@@ -401,10 +421,10 @@ __device__ __forceinline__ void accum_dw(const __nv_bfloat16* DYT, const __nv_bf
             float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
             mma_bf16(acc, a, b0, b1);
             const int m0 = mt * 16 + g, n0 = nt * 8 + 2 * c;
-            atomicAdd(&sdw[m0 * IN + n0], acc[0]);
-            atomicAdd(&sdw[m0 * IN + n0 + 1], acc[1]);
-            atomicAdd(&sdw[(m0 + 8) * IN + n0], acc[2]);
-            atomicAdd(&sdw[(m0 + 8) * IN + n0 + 1], acc[3]);
+            atomicAdd(&sdw[m0 * IN + n0], g_fix(acc[0]));
+            atomicAdd(&sdw[m0 * IN + n0 + 1], g_fix(acc[1]));
+            atomicAdd(&sdw[(m0 + 8) * IN + n0], g_fix(acc[2]));
+            atomicAdd(&sdw[(m0 + 8) * IN + n0 + 1], g_fix(acc[3]));
         }
     }
 }
@@ -474,10 +494,9 @@ __host__ __device__ __forceinline__ uint32_t steps_before(uint32_t n, int mb, in
 }
 
 // Gradient of the mean loss over minibatch mb (of nmb) of the collected samples.
-// Training CTAs hold one copy of both weight layouts and the FP32 weight
-// gradient in shared memory for kGTrainWarps warps (one CTA per SM fits):
-// 6 warps instead of 4 hide more of the gradient scatter's latency.
-constexpr int kGTrainWarps = 6;
+// Training CTAs hold one copy of both weight layouts and the fixed-point
+// weight gradient in shared memory for kGTrainWarps warps (one CTA per SM).
+constexpr int kGTrainWarps = 4;
 __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net, const GuideSample* __restrict__ samples_all,
                                                      const uint32_t* count, uint32_t cap, int mb, int nmb) {
     const uint32_t n = minibatch_size(min(*count, cap), mb, nmb);
@@ -489,7 +508,7 @@ __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net,
     extern __shared__ __align__(16) unsigned char g_smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(g_smem);                       // W  [out][in+8]
     __nv_bfloat16* swt = sw + kGSmemW;                                                 // WT [in][out+8]
-    float* sdw = reinterpret_cast<float*>(swt + kGSmemW + 64);                         // dW fp32, packed
+    unsigned long long* sdw = reinterpret_cast<unsigned long long*>(swt + kGSmemW + 64);   // dW fixed point, packed
     unsigned char* scratch0 = reinterpret_cast<unsigned char*>(sdw + kGWeights);
     load_weights_smem(net, sw);
     // transposed weights: layer l, WT[in][out] with row length out + 8
@@ -502,7 +521,7 @@ __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net,
             swt[woff + k * (out + 8) + o] = net.w[g_woff(l) + i];
         }
     }
-    for (int i = threadIdx.x; i < kGWeights; i += blockDim.x) sdw[i] = 0.0f;
+    for (int i = threadIdx.x; i < kGWeights; i += blockDim.x) sdw[i] = 0ull;
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
     unsigned char* my = scratch0 + warp * kGWarpScratch;
@@ -568,10 +587,15 @@ __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net,
                 DYT[j * 24 + lane] = b;
             }
         }
-        for (int o = 16; o > 0; o >>= 1) row_loss += __shfl_xor_sync(0xffffffffu, row_loss, o);
-        if (lane == 0 && net.loss) {
-            atomicAdd(net.loss, row_loss);
-            atomicAdd(net.loss + 1, static_cast<float>(min(16u, n - tile * 16)));
+        if (net.loss_fix) {
+            unsigned long long lf = lane < 16 ? static_cast<unsigned long long>(
+                                                    __float2ll_rn(fminf(fmaxf(row_loss, -1e12f), 1e12f) * kGLossFix))
+                                              : 0ull;
+            for (int o = 16; o > 0; o >>= 1) lf += __shfl_xor_sync(0xffffffffu, lf, o);
+            if (lane == 0) {
+                atomicAdd(net.loss_fix, lf);
+                atomicAdd(net.loss_fix + 1, static_cast<unsigned long long>(min(16u, n - tile * 16)));
+            }
         }
         __syncwarp();
         // layer 3 (48 x 64)
@@ -613,11 +637,13 @@ __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net,
                 const float bx = floorf(fx), by = floorf(fy), bz = floorf(fz);
                 const float tx = fx - bx, ty = fy - by, tz = fz - bz;
                 const uint32_t ix = static_cast<uint32_t>(bx), iy = static_cast<uint32_t>(by), iz = static_cast<uint32_t>(bz);
-                float2* gg = net.grid_grad + static_cast<size_t>(level) * kGTable;
+                unsigned long long* gg = net.grid_grad + static_cast<size_t>(level) * kGTable * 2;
                 for (int cidx = 0; cidx < 8; ++cidx) {
                     const uint32_t cx = cidx & 1, cy = (cidx >> 1) & 1, cz = (cidx >> 2) & 1;
                     const float w = (cx ? tx : 1.0f - tx) * (cy ? ty : 1.0f - ty) * (cz ? tz : 1.0f - tz);
-                    atomicAdd(&gg[grid_index(net, level, ix + cx, iy + cy, iz + cz)], make_float2(w * gx, w * gy));
+                    const uint32_t e = grid_index(net, level, ix + cx, iy + cy, iz + cz);
+                    atomicAdd(&gg[2 * e], g_fix(w * gx));
+                    atomicAdd(&gg[2 * e + 1], g_fix(w * gy));
                 }
             }
         }
@@ -625,16 +651,16 @@ __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net,
     }
     __syncthreads();
     for (int i = threadIdx.x; i < kGWeights; i += blockDim.x)
-        if (sdw[i] != 0.0f) atomicAdd(&net.w_grad[i], sdw[i]);
+        if (sdw[i] != 0ull) atomicAdd(&net.w_grad[i], sdw[i]);
 }
 
 // Adam on the MLP weights (FP32 master -> BF16 copy) and the hash grid
 // (FP32 master -> FP16 copy); gradients are cleared.
 // dynamic shared memory of the two network kernels (4 warps per CTA)
 constexpr int kGInferSmem = kGSmemW * 2 + kGInferWarps * 16 * kGOutPad * 4;
-constexpr int kGTrainSmem = (2 * kGSmemW + 64) * 2 + kGWeights * 4 + kGTrainWarps * kGWarpScratch;
+constexpr int kGTrainSmem = (2 * kGSmemW + 64) * 2 + kGWeights * 8 + kGTrainWarps * kGWarpScratch;
 static_assert(kGTrainSmem <= 227 * 1024, "training kernel shared memory");
-static_assert(((2 * kGSmemW + 64) * 2) % 16 == 0 && (kGWeights * 4) % 16 == 0 && kGWarpScratch % 16 == 0,
+static_assert(((2 * kGSmemW + 64) * 2) % 16 == 0 && (kGWeights * 8) % 16 == 0 && kGWarpScratch % 16 == 0,
               "shared memory carve alignment");
 
 // Host-side state of one guide: the network, its optimiser state and the
@@ -653,6 +679,10 @@ struct GuideState {
     GuideSample* samples = nullptr;
     uint32_t     sample_cap = 0;
     uint32_t*    counters = nullptr;  // [0] samples collected in the current pass (work buffer)
+    uint32_t*    scan_counts = nullptr;   // training samples per path (npix + 1)
+    uint32_t*    scan_offsets = nullptr;  // their exclusive prefix sums
+    void*        scan_tmp = nullptr;      // the scan's temporary storage
+    size_t       scan_tmp_bytes = 0;
     uint32_t*    step = nullptr;      // optimiser steps taken (with the parameters: survives work resizes)
     int          mode = 0;            // 0 off, PT_GUIDE_USE, PT_GUIDE_TRAIN
     float        lr = 1e-2f;
@@ -661,12 +691,15 @@ struct GuideState {
 
 // After a pass's minibatches: advance the step counter by the steps taken
 // and empty the sample buffer.
-__global__ void k_guide_step(uint32_t* sample_count, uint32_t* step, float* loss, uint32_t cap, int nmb) {
+__global__ void k_guide_step(uint32_t* sample_count, uint32_t* step, float* loss, unsigned long long* loss_fix,
+                             uint32_t cap, int nmb) {
     *step += steps_before(min(*sample_count, cap), nmb, nmb);
     *sample_count = 0u;
-    if (loss[1] > 0.0f) loss[2] = loss[0] / loss[1];
-    loss[0] = 0.0f;
-    loss[1] = 0.0f;
+    if (loss_fix[1] > 0ull)
+        loss[2] = static_cast<float>(static_cast<double>(static_cast<long long>(loss_fix[0])) / kGLossFix /
+                                     static_cast<double>(loss_fix[1]));
+    loss_fix[0] = 0ull;
+    loss_fix[1] = 0ull;
 }
 
 // Adam step for minibatch mb (skipped when it is empty); the step number is
@@ -682,23 +715,25 @@ __global__ void k_guide_adam(GuideNet net, const uint32_t* count, uint32_t cap, 
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < nw + ng;
          i += static_cast<size_t>(gridDim.x) * blockDim.x) {
         if (i < nw) {
-            const float gr = net.w_grad[i];
+            const float gr = g_unfix(net.w_grad[i]);
             const float m = b1 * net.w_m[i] + (1.0f - b1) * gr;
             const float v = b2 * net.w_v[i] + (1.0f - b2) * gr * gr;
-            net.w_m[i] = m; net.w_v[i] = v; net.w_grad[i] = 0.0f;
+            net.w_m[i] = m; net.w_v[i] = v; net.w_grad[i] = 0ull;
             const float p = net.w_master[i] - lr_w * (m / bc1) / (sqrtf(v / bc2) + eps);
             net.w_master[i] = p;
             net.w[i] = __float2bfloat16_rn(p);
         } else {
             const size_t j = i - nw;
-            const float2 gr = net.grid_grad[j];
-            if (gr.x == 0.0f && gr.y == 0.0f && net.grid_m[j].x == 0.0f && net.grid_m[j].y == 0.0f) continue;
+            const ulonglong2 gi = reinterpret_cast<const ulonglong2*>(net.grid_grad)[j];
+            if (gi.x == 0ull && gi.y == 0ull && net.grid_m[j].x == 0.0f && net.grid_m[j].y == 0.0f) continue;
+            const float2 gr = make_float2(g_unfix(gi.x), g_unfix(gi.y));
             float2 m = net.grid_m[j], v = net.grid_v[j], p = net.grid_master[j];
             m.x = b1 * m.x + (1.0f - b1) * gr.x; m.y = b1 * m.y + (1.0f - b1) * gr.y;
             v.x = b2 * v.x + (1.0f - b2) * gr.x * gr.x; v.y = b2 * v.y + (1.0f - b2) * gr.y * gr.y;
             p.x -= lr_g * (m.x / bc1) / (sqrtf(v.x / bc2) + eps);
             p.y -= lr_g * (m.y / bc1) / (sqrtf(v.y / bc2) + eps);
-            net.grid_m[j] = m; net.grid_v[j] = v; net.grid_master[j] = p; net.grid_grad[j] = make_float2(0.0f, 0.0f);
+            net.grid_m[j] = m; net.grid_v[j] = v; net.grid_master[j] = p;
+            reinterpret_cast<ulonglong2*>(net.grid_grad)[j] = make_ulonglong2(0ull, 0ull);
             net.grid[j] = __floats2half2_rn(p.x, p.y);
         }
     }

@@ -48,29 +48,32 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     const size_t ng = static_cast<size_t>(kGLevels) * kGTable;
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t off_master = al(ng * sizeof(__half2));
-    const size_t off_grad = off_master + al(ng * sizeof(float2));
-    const size_t off_m = off_grad + al(ng * sizeof(float2));
+    const size_t off_grad = off_master + al(ng * sizeof(float2));       // 2 x u64 per entry
+    const size_t off_m = off_grad + al(ng * 2 * sizeof(unsigned long long));
     const size_t off_v = off_m + al(ng * sizeof(float2));
     const size_t off_w = off_v + al(ng * sizeof(float2));
     const size_t off_wm = off_w + al(kGWeights * sizeof(__nv_bfloat16));
     const size_t wf = al(kGWeights * sizeof(float));
-    const size_t off_step = off_wm + 4 * wf;
+    const size_t off_wg = off_wm + wf;                                    // u64 per weight
+    const size_t wg = al(kGWeights * sizeof(unsigned long long));
+    const size_t off_step = off_wg + wg + 2 * wf;
     const size_t total = off_step + 256;
     if (!guide_cuda_ok(cudaMalloc(&g.params, total), "parameter allocation")) return PT_ERR_NOMEM;
     g.param_bytes = total;
     char* base = static_cast<char*>(g.params);
     g.net.grid = reinterpret_cast<__half2*>(base);
     g.net.grid_master = reinterpret_cast<float2*>(base + off_master);
-    g.net.grid_grad = reinterpret_cast<float2*>(base + off_grad);
+    g.net.grid_grad = reinterpret_cast<unsigned long long*>(base + off_grad);
     g.net.grid_m = reinterpret_cast<float2*>(base + off_m);
     g.net.grid_v = reinterpret_cast<float2*>(base + off_v);
     g.net.w = reinterpret_cast<__nv_bfloat16*>(base + off_w);
     g.net.w_master = reinterpret_cast<float*>(base + off_wm);
-    g.net.w_grad = reinterpret_cast<float*>(base + off_wm + wf);
-    g.net.w_m = reinterpret_cast<float*>(base + off_wm + 2 * wf);
-    g.net.w_v = reinterpret_cast<float*>(base + off_wm + 3 * wf);
+    g.net.w_grad = reinterpret_cast<unsigned long long*>(base + off_wg);
+    g.net.w_m = reinterpret_cast<float*>(base + off_wg + wg);
+    g.net.w_v = reinterpret_cast<float*>(base + off_wg + wg + wf);
     g.step = reinterpret_cast<uint32_t*>(base + off_step);
     g.net.loss = reinterpret_cast<float*>(base + off_step + 16);
+    g.net.loss_fix = reinterpret_cast<unsigned long long*>(base + off_step + 32);
     // host-side initial values
     std::mt19937 rng(seed);
     std::vector<float> gm(2 * ng);
@@ -92,10 +95,10 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     for (int i = 0; i < kGWeights; ++i) wb[i] = __float2bfloat16_rn(w[i]);
     bool ok = guide_cuda_ok(cudaMemcpy(g.net.grid, gh.data(), ng * sizeof(__half2), cudaMemcpyHostToDevice), "upload") &&
               guide_cuda_ok(cudaMemcpy(g.net.grid_master, gm.data(), ng * sizeof(float2), cudaMemcpyHostToDevice), "upload") &&
-              guide_cuda_ok(cudaMemset(g.net.grid_grad, 0, 3 * al(ng * sizeof(float2))), "clear") &&
+              guide_cuda_ok(cudaMemset(g.net.grid_grad, 0, off_w - off_grad), "clear") &&
               guide_cuda_ok(cudaMemcpy(g.net.w, wb.data(), kGWeights * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice), "upload") &&
               guide_cuda_ok(cudaMemcpy(g.net.w_master, w.data(), kGWeights * sizeof(float), cudaMemcpyHostToDevice), "upload") &&
-              guide_cuda_ok(cudaMemset(g.net.w_grad, 0, 3 * wf), "clear") &&
+              guide_cuda_ok(cudaMemset(g.net.w_grad, 0, wg + 2 * wf), "clear") &&
               guide_cuda_ok(cudaMemset(g.step, 0, 256), "clear") &&
               guide_cuda_ok(cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kGTrainSmem), "smem") &&
               guide_cuda_ok(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kGInferSmem), "smem");
@@ -117,14 +120,25 @@ inline int guide_prepare_work(GuideState& g, int npix, int depth, bool records) 
     const size_t b_mix = al(P * kGMix * sizeof(float));
     const size_t b_rec = records ? al(D * P * 4 * sizeof(float4)) : 0;
     const size_t b_smp = al(cap * sizeof(GuideSample));
-    const size_t total = b_mix + b_rec + b_smp + 256;
+    size_t scan_tmp = 0;
+    if (records &&
+        !guide_cuda_ok(cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, static_cast<uint32_t*>(nullptr),
+                                                     static_cast<uint32_t*>(nullptr), static_cast<int>(P + 1)),
+                       "scan size"))
+        return PT_ERR_CUDA;
+    const size_t b_scan = records ? 2 * al((P + 1) * sizeof(uint32_t)) + al(scan_tmp) : 0;
+    const size_t total = b_mix + b_rec + b_smp + b_scan + 256;
     if (!guide_cuda_ok(cudaMalloc(&g.work, total), "work allocation")) return PT_ERR_NOMEM;
     g.work_bytes = total;
     char* base = static_cast<char*>(g.work);
     g.mix = reinterpret_cast<float*>(base);
     g.rec = records ? reinterpret_cast<float4*>(base + b_mix) : nullptr;
     g.samples = records ? reinterpret_cast<GuideSample*>(base + b_mix + b_rec) : nullptr;
-    g.counters = reinterpret_cast<uint32_t*>(base + b_mix + b_rec + b_smp);
+    g.counters = reinterpret_cast<uint32_t*>(base + b_mix + b_rec + b_smp + b_scan);
+    g.scan_counts = records ? reinterpret_cast<uint32_t*>(base + b_mix + b_rec + b_smp) : nullptr;
+    g.scan_offsets = records ? reinterpret_cast<uint32_t*>(base + b_mix + b_rec + b_smp + al((P + 1) * 4)) : nullptr;
+    g.scan_tmp = records ? base + b_mix + b_rec + b_smp + 2 * al((P + 1) * 4) : nullptr;
+    g.scan_tmp_bytes = records ? scan_tmp : 0;
     g.sample_cap = static_cast<uint32_t>(cap);
     g.npix = npix;
     g.depth = depth;

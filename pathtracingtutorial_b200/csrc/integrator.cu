@@ -30,6 +30,8 @@
 #include "engine.h"
 #include "bsdf.h"
 #include "traverse.h"
+#include <cub/device/device_scan.cuh>
+
 #include "guide.cuh"
 #include "guide_host.cuh"
 
@@ -806,33 +808,64 @@ __global__ void __launch_bounds__(256) k_finalize(WaveParams P, int s0, int coun
 // vertex, the incident radiance along its sampled direction is the part of the
 // path's final estimate gathered after it, divided by the throughput after it
 // (luminance, clamped like a sample); weight = L_in |cos| / p, so the guide
-// learns the cosine-weighted incident radiance.  Records are cleared.
-__global__ void __launch_bounds__(256) k_guide_collect(WaveParams P, int npaths, GuideNet net, GuideSample* out,
-                                                       uint32_t* count, uint32_t cap) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npaths; p += gridDim.x * blockDim.x) {
-        f3 Lf = f3of(P.lo[p]);
-        for (int k = 0; k < P.n_slots; ++k) Lf += f3of(P.nee[static_cast<size_t>(k) * P.npath + p]);
-        for (int d = 0; d + 1 < P.max_depth; ++d) {
-            float4* r = P.grec + (static_cast<size_t>(d) * P.npath + p) * 4;
-            const float4 r1 = r[1];
-            float w = 0.0f;
-            float4 r0 = make_float4(0, 0, 0, 0);
-            if (r1.w != 0.0f) {
-                r[1].w = 0.0f;
-                r0 = r[0];
-                const f3 Ta = f3of(r[2]);
-                const f3 S = f3of(r[3]);
-                const f3 Lin = mk(Ta.x > 0.0f ? (Lf.x - S.x) / Ta.x : 0.0f, Ta.y > 0.0f ? (Lf.y - S.y) / Ta.y : 0.0f,
-                                  Ta.z > 0.0f ? (Lf.z - S.z) / Ta.z : 0.0f);
-                const float lum = fminf(fmaxf(luminance(Lin), 0.0f), 100.0f) * r[2].w;
-                w = r0.w > 0.0f ? lum / r0.w : 0.0f;
-                if (!(w < 1e30f)) w = 0.0f;
+// learns the cosine-weighted incident radiance.  The samples are stored in
+// path order, each path's in depth order (k_guide_count, an exclusive scan of
+// the counts, k_guide_collect), so the minibatches -- and with them the
+// trained network -- are the same on every run.  Records are cleared.
+__device__ __forceinline__ float guide_record_weight(const WaveParams& P, int p, int d, f3 Lf, float4& r0,
+                                                    float4& r1) {
+    const float4* r = P.grec + (static_cast<size_t>(d) * P.npath + p) * 4;
+    r1 = r[1];
+    r0 = make_float4(0, 0, 0, 0);
+    if (r1.w == 0.0f) return 0.0f;
+    r0 = r[0];
+    const f3 Ta = f3of(r[2]);
+    const f3 S = f3of(r[3]);
+    const f3 Lin = mk(Ta.x > 0.0f ? (Lf.x - S.x) / Ta.x : 0.0f, Ta.y > 0.0f ? (Lf.y - S.y) / Ta.y : 0.0f,
+                      Ta.z > 0.0f ? (Lf.z - S.z) / Ta.z : 0.0f);
+    const float lum = fminf(fmaxf(luminance(Lin), 0.0f), 100.0f) * r[2].w;
+    float w = r0.w > 0.0f ? lum / r0.w : 0.0f;
+    if (!(w < 1e30f)) w = 0.0f;
+    return w;
+}
+
+__device__ __forceinline__ f3 guide_path_estimate(const WaveParams& P, int p) {
+    f3 Lf = f3of(P.lo[p]);
+    for (int k = 0; k < P.n_slots; ++k) Lf += f3of(P.nee[static_cast<size_t>(k) * P.npath + p]);
+    return Lf;
+}
+
+// counts[p] = training samples of path p; counts[npaths] = 0 (the scan's total).
+__global__ void __launch_bounds__(256) k_guide_count(WaveParams P, int npaths, uint32_t* counts) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= npaths; p += gridDim.x * blockDim.x) {
+        uint32_t k = 0;
+        if (p < npaths) {
+            const f3 Lf = guide_path_estimate(P, p);
+            for (int d = 0; d + 1 < P.max_depth; ++d) {
+                float4 r0, r1;
+                k += guide_record_weight(P, p, d, Lf, r0, r1) > 0.0f ? 1u : 0u;
             }
-            const bool want = w > 0.0f;
-            const uint32_t j = warp_append(count, want);
-            if (want && j < cap) {
-                const f3 x = guide_normalise(net, mk(r0.x, r0.y, r0.z));
-                out[j] = GuideSample{make_float4(x.x, x.y, x.z, w), make_float4(r1.x, r1.y, r1.z, 0.0f)};
+        }
+        counts[p] = k;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_guide_collect(WaveParams P, int npaths, GuideNet net, GuideSample* out,
+                                                       const uint32_t* offsets, uint32_t* count, uint32_t cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *count = offsets[npaths];
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npaths; p += gridDim.x * blockDim.x) {
+        const f3 Lf = guide_path_estimate(P, p);
+        uint32_t j = offsets[p];
+        for (int d = 0; d + 1 < P.max_depth; ++d) {
+            float4 r0, r1;
+            const float w = guide_record_weight(P, p, d, Lf, r0, r1);
+            if (r1.w != 0.0f) P.grec[(static_cast<size_t>(d) * P.npath + p) * 4 + 1].w = 0.0f;
+            if (w > 0.0f) {
+                if (j < cap) {
+                    const f3 x = guide_normalise(net, mk(r0.x, r0.y, r0.z));
+                    out[j] = GuideSample{make_float4(x.x, x.y, x.z, w), make_float4(r1.x, r1.y, r1.z, 0.0f)};
+                }
+                ++j;
             }
         }
     }
@@ -1090,7 +1123,11 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
         if (int rc = timed(3, [&] { k_finalize<<<wf.grid_finalize, 256, 0, st>>>(P, s0, count); })) return rc;
         if (train) {
             if (int rc = timed(4, [&] {
-                    k_guide_collect<<<wf.grid_finalize, 256, 0, st>>>(P, P.npix * count, gs->net, gs->samples,
+                    const int np = P.npix * count;
+                    k_guide_count<<<wf.grid_finalize, 256, 0, st>>>(P, np, gs->scan_counts);
+                    size_t tmp = gs->scan_tmp_bytes;
+                    cub::DeviceScan::ExclusiveSum(gs->scan_tmp, tmp, gs->scan_counts, gs->scan_offsets, np + 1, st);
+                    k_guide_collect<<<wf.grid_finalize, 256, 0, st>>>(P, np, gs->net, gs->samples, gs->scan_offsets,
                                                                       gs->counters, gs->sample_cap);
                     // optimiser steps over this pass's samples in minibatches
                     const int nmb = guide_minibatches(P.npix * count);
@@ -1100,7 +1137,8 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
                         k_guide_adam<<<wf.sms * 8, 256, 0, st>>>(gs->net, gs->counters, gs->sample_cap, mb, nmb,
                                                                  gs->step, gs->lr, gs->lr, 0.9f, 0.99f, 1e-10f);
                     }
-                    k_guide_step<<<1, 1, 0, st>>>(gs->counters, gs->step, gs->net.loss, gs->sample_cap, nmb);
+                    k_guide_step<<<1, 1, 0, st>>>(gs->counters, gs->step, gs->net.loss, gs->net.loss_fix,
+                                                  gs->sample_cap, nmb);
                 })) return rc;
         }
     }
@@ -1458,7 +1496,7 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     if (!timing) wf.extend_launches += passes * static_cast<uint64_t>(P.max_depth);
     wf.kernel_launches += 1 + passes * (1 + 4 * static_cast<uint64_t>(P.max_depth));
     if (P.gmix)
-        wf.kernel_launches += passes * (P.max_depth + (P.grec ? 2 + 2 * guide_minibatches(P.npix * lanes) : 0));
+        wf.kernel_launches += passes * (P.max_depth + (P.grec ? 5 + 2 * guide_minibatches(P.npix * lanes) : 0));
     return PT_OK;
 }
 
@@ -1785,20 +1823,29 @@ int guide_backward(pt_guide* h, const float* samples, uint32_t n, float* wgrad, 
     const size_t ng = static_cast<size_t>(kGLevels) * kGTable;
     cudaError_t e = cudaMemcpy(ds, samples, static_cast<size_t>(n) * sizeof(GuideSample), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(dn, &n, 4, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(h->g.net.w_grad, 0, kGWeights * sizeof(float));
-    if (e == cudaSuccess) e = cudaMemset(h->g.net.grid_grad, 0, ng * sizeof(float2));
+    if (e == cudaSuccess) e = cudaMemset(h->g.net.w_grad, 0, kGWeights * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(h->g.net.grid_grad, 0, ng * 2 * sizeof(unsigned long long));
     if (e == cudaSuccess) {
         GuideNet net = h->g.net;
-        net.loss = nullptr;   // leave the training-loss record alone
+        net.loss_fix = nullptr;   // leave the training-loss record alone
         k_guide_train<<<148, 32 * kGTrainWarps, kGTrainSmem>>>(net, ds, dn, n, 0, 1);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
     }
-    if (e == cudaSuccess) e = cudaMemcpy(wgrad, h->g.net.w_grad, kGWeights * sizeof(float), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && ggrad) e = cudaMemcpy(ggrad, h->g.net.grid_grad, ng * sizeof(float2), cudaMemcpyDeviceToHost);
+    // gradients come back as floats (fixed point on the device)
+    if (e == cudaSuccess) {
+        std::vector<unsigned long long> wg(kGWeights);
+        e = cudaMemcpy(wg.data(), h->g.net.w_grad, kGWeights * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+        for (int i = 0; i < kGWeights && e == cudaSuccess; ++i) wgrad[i] = g_unfix(wg[i]);
+    }
+    if (e == cudaSuccess && ggrad) {
+        std::vector<unsigned long long> gg(ng * 2);
+        e = cudaMemcpy(gg.data(), h->g.net.grid_grad, ng * 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+        for (size_t i = 0; i < ng * 2 && e == cudaSuccess; ++i) ggrad[i] = g_unfix(gg[i]);
+    }
     // leave the optimiser state as it was
-    cudaMemset(h->g.net.w_grad, 0, kGWeights * sizeof(float));
-    cudaMemset(h->g.net.grid_grad, 0, ng * sizeof(float2));
+    cudaMemset(h->g.net.w_grad, 0, kGWeights * sizeof(unsigned long long));
+    cudaMemset(h->g.net.grid_grad, 0, ng * 2 * sizeof(unsigned long long));
     cudaFree(ds);
     cudaFree(dn);
     if (e != cudaSuccess) { set_error(std::string("guide backward: ") + cudaGetErrorString(e)); return PT_ERR_CUDA; }

@@ -158,27 +158,59 @@ def test_guide_forward_and_gradients_after_training():
 
 
 @pytest.mark.gpu
-def test_guided_render_unbiased_and_lower_error():
-    """Guided vs plain on the hidden-light room at equal samples per pixel:
-    both agree in the mean with a high-spp plain render, and the trained
-    guide lowers the relative MSE."""
+def test_guide_training_is_deterministic():
+    """Two guides trained from the same seed on the same samples end with the
+    same parameters bit for bit, and render the same image: the samples are
+    collected in path order and every gradient is summed in fixed point."""
     import pathtracingtutorial_b200 as pt
     from pathtracingtutorial_b200 import scenes
-    sa = scenes.hidden_light_room(width=64, height=64, n_boxes=40, box_subdiv=2, spp=64, max_depth=10)
+    sa = scenes.hidden_light_room(width=64, height=64, n_boxes=40, box_subdiv=2, spp=16, max_depth=10)
+    s = _scene(sa)
+    runs = []
+    for _ in range(2):
+        img, g, _ = pt.render_guided(s, train_spp=64, spp=16, guide=pt.Guide(s, seed=3))
+        p = g.params(with_grid=True)
+        runs.append((img, p["weights"], p["grid"], g.info()["steps"], g.loss()))
+        g.close()
+    (i0, w0, g0, n0, l0), (i1, w1, g1, n1, l1) = runs
+    assert n0 == n1 > 0
+    assert np.array_equal(w0.view(np.uint32), w1.view(np.uint32))
+    assert np.array_equal(g0.view(np.uint32), g1.view(np.uint32))
+    assert np.array_equal(i0.view(np.uint32), i1.view(np.uint32))
+    assert l0 == l1
+
+
+@pytest.mark.gpu
+def test_guided_render_unbiased_and_lower_error():
+    """Guided vs plain on the hidden-light room at equal samples per pixel
+    (256): the image means agree with an 8192-spp plain render within four
+    standard errors (estimated from eight independent 32-spp parts of each
+    render), and the trained guide lowers the relative MSE against it."""
+    import pathtracingtutorial_b200 as pt
+    from pathtracingtutorial_b200 import scenes
+    sa = scenes.hidden_light_room(width=64, height=64, n_boxes=40, box_subdiv=2, spp=256, max_depth=10)
     s = _scene(sa)
     ref = _render_from(s, 8192, 1_000_000)[..., :3].astype(np.float64)
-    plain = pt.render(s, 64)[..., :3].astype(np.float64)
-    guided, g, _ = pt.render_guided(s, train_spp=256, spp=64)
-    guided = guided[..., :3].astype(np.float64)
+    g = pt.Guide(s, seed=1)
+    pt.render_guided(s, train_spp=256, spp=4, guide=g)
+    spf = sa.sample_per_frame
+    parts_plain = [_render_from(s, 32, k * (32 // spf))[..., :3].astype(np.float64) for k in range(8)]
+    parts_guided = [pt.render_batch([(s, 32, k * (32 // spf), None, g)])[0][0][..., :3].astype(np.float64)
+                    for k in range(8)]
+    plain, guided = np.mean(parts_plain, 0), np.mean(parts_guided, 0)
 
     def relmse(x):
-        # per-pixel squared relative error, each pixel's term capped at 1: at 64
-        # spp a single firefly pixel otherwise decides the comparison, and the
-        # guide's online training (FP32 atomics) differs from run to run
-        return float(np.mean(np.minimum((x - ref) ** 2 / (ref ** 2 + 1e-2), 1.0)))
+        return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
 
-    m_ref, m_plain, m_guided = ref.mean(), plain.mean(), guided.mean()
-    assert abs(m_plain / m_ref - 1) < 0.03
-    assert abs(m_guided / m_ref - 1) < 0.03, (m_guided, m_ref)
-    assert relmse(guided) < relmse(plain), (relmse(guided), relmse(plain))
+    def se(parts):
+        m = np.array([p.mean() for p in parts])
+        return m.std(ddof=1) / np.sqrt(len(m))
+
+    se_ref = se(parts_plain) * np.sqrt(256 / 8192)
+    for img, parts in ((plain, parts_plain), (guided, parts_guided)):
+        bound = 4 * np.sqrt(se(parts) ** 2 + se_ref ** 2)
+        assert abs(img.mean() - ref.mean()) < bound, (img.mean(), ref.mean(), bound)
+    e_plain, e_guided = relmse(plain), relmse(guided)
+    print(f"relMSE at 256 spp: plain {e_plain:.4g}, guided {e_guided:.4g}")
+    assert e_guided < e_plain, (e_guided, e_plain)
     g.close()
