@@ -10,10 +10,10 @@ graph-captured launch of wavefront passes of up to 2^27 path slots (64 spp at
 1080p); scene resident in HBM.  Rays = camera + extension + shadow rays traced.
 
 The line also carries the second half of the metric, measured on the
-hidden-light room (1024x1024, depth 16): relMSE of the plain and the guided
-integrator against a 4096-spp plain reference, and their extrapolated time to
-relMSE 1e-3 (key "convergence"); and the BVH build of the bench scene by the
-host SAH builder and by the GPU builder (key "bvh_build").
+hidden-light room (1024x1024, depth 16): the wall time at which the plain
+integrator and the guided, batched one reach relMSE 1e-3 against the FP64
+oracle on a 128 x 128 crop (key "convergence"); and the BVH build of the
+bench scene by the host SAH builder and by the GPU builder (key "bvh_build").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -260,73 +260,148 @@ def cpu_baseline(sa, spp, seconds):
                       f"{secs:.1f} s"}
 
 
-def convergence(local: int, stream, small: bool):
-    """Guided vs plain on the hidden-light room (202,002 triangles, 1024x1024,
-    depth 16, Sobol): relMSE against a 4096-spp plain render on independent
-    sample indices, each arm timed with CUDA events; the guide trains online
-    for 64 spp (timed) before it renders.  Time to relMSE 1e-3 is extrapolated
-    with relMSE ~ 1/time (both estimators are unbiased), after subtracting the
-    reference's own noise (estimated from the plain arm, whose relMSE is its
-    own noise c / spp plus the reference's c / 4096)."""
+ROOM_CROP_FIXTURE = os.path.join(ROOT, "tests", "golden", "room_crop_fp64.npz")
+TARGET_RELMSE = 1e-3
+
+
+def crossing_time(trace, target):
+    """First checkpoint of a progressive trace [(spp, ms, relmse), ...] whose
+    relMSE is at or below `target`, and the time of the crossing
+    interpolated log-log between it and the checkpoint before; (None, None)
+    when the trace never gets there."""
+    import math
+    for k, (spp, ms, e) in enumerate(trace):
+        if e <= target:
+            if k == 0:
+                return ms, ms
+            s0, m0, e0 = trace[k - 1]
+            if e0 <= e or m0 <= 0 or e <= 0:
+                return ms, ms
+            f = math.log(e0 / target) / math.log(e0 / e)
+            return ms, m0 * (ms / m0) ** f
+    return None, None
+
+
+def convergence(local: int, stream, small: bool, plain_cap: int = 8192, guided_cap: int = 4096,
+                chunk: int = 64, train_spp: int = 64):
+    """Guided + batched vs plain on the hidden-light room (202,002 triangles,
+    1024 x 1024, depth 16, Sobol): wall time to relMSE 1e-3 against the FP64
+    oracle on the room's central 128 x 128 crop (tests/golden/room_crop_fp64.npz,
+    the FP64 restatement at tens of thousands of spp on disjoint sample
+    indices; its own noise is recorded with it).
+
+    Plain: the plain integrator (Renderer.render_frames) in chunks of `chunk`
+    spp; guided: a guide trained online for `train_spp` spp (timed), then
+    rendered through pt_render_batch with the trained guide as the item's
+    guide, chunk by chunk (consecutive first frames), the chunks averaged.
+    Each arm's clock runs from its start to every checkpoint and includes the
+    image read-back (as Renderer::runConvergenceBenchmark, renderer.cu:138-173);
+    relMSE = mean over crop pixels and channels of (I - R)^2 / (R^2 + 1e-2).
+    The crossing is measured: the first checkpoint at or below 1e-3 (and the
+    log-log interpolated crossing between it and the previous checkpoint)."""
     import numpy as np
     import torch
     import pathtracingtutorial_b200 as pt
     from pathtracingtutorial_b200 import scenes
-    w = 256 if small else 1024
-    n_ref, n_plain, n_train, n_guided = (256, 64, 16, 64) if small else (4096, 256, 64, 256)
-    sa = scenes.hidden_light_room(width=w, height=w)
+    if small or not os.path.exists(ROOM_CROP_FIXTURE):
+        return None
+    z = np.load(ROOM_CROP_FIXTURE)
+    x0, y0, x1, y1 = (int(v) for v in z["crop"])
+    ref = z["mean"].astype(np.float64)
+    eps = float(z["eps_rel"])
+    ref_noise = float(z["noise_relmse"])
+    sa = scenes.hidden_light_room(width=int(z["width"]), height=int(z["height"]))
     scene = sa.scene()
     scene.build_accel()
     scene.upload_to_device(local)
     spf = sa.sample_per_frame
     handle = stream.cuda_stream
 
-    def timed(fn):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
+    def relmse(img):
+        c = img[y0:y1, x0:x1, :3].astype(np.float64)
+        return float(np.mean((c - ref) ** 2 / (ref * ref + eps)))
 
+    def sync():
+        torch.cuda.synchronize(local)
+
+    # plain arm
     r = pt.Renderer(scene, device=local, stream=handle)
     r.reset_accumulation()
-    scene.set_frame_count(1_000_000)
-    ref_ms = timed(lambda: r.render_frames(n_ref // spf))
-    ref = r.download_current_image()[..., :3].astype(np.float64)
-
-    def relmse(img):
-        return float(np.mean((img[..., :3].astype(np.float64) - ref) ** 2 / (ref ** 2 + 1e-2)))
-
+    scene.set_frame_count(0)
+    r.render_frames(chunk // spf)            # warm-up: graph capture and arena
+    sync()
     r.reset_accumulation()
     scene.set_frame_count(0)
-    t_plain = timed(lambda: r.render_frames(n_plain // spf))
-    e_plain = relmse(r.download_current_image())
+    plain = []
+    t0 = time.perf_counter()
+    spp = 0
+    while spp < plain_cap:
+        r.render_frames(chunk // spf)
+        sync()
+        img = r.download_current_image()
+        spp += chunk
+        e = relmse(img)
+        plain.append((spp, (time.perf_counter() - t0) * 1e3, e))
+        if e <= TARGET_RELMSE:
+            break
+    r.integrator.close()
+    r.film.close()
+
+    # guided arm: online training, then batched rendering with the trained guide
     g = pt.Guide(scene, seed=1)
+    pt.render_batch([(scene, chunk, 200_000, None, g)], mode=pt.BATCH_WAVEFRONT, autotune=False)   # warm-up
     rg = pt.Renderer(scene, device=local, stream=handle)
+    sync()
+    t0 = time.perf_counter()
     g.attach(rg.integrator, pt.Guide.TRAIN)
     rg.reset_accumulation()
-    scene.set_frame_count(100_000)
-    t_train = timed(lambda: rg.render_frames(n_train // spf))
-    g.attach(rg.integrator, pt.Guide.USE)
-    rg.reset_accumulation()
-    scene.set_frame_count(0)
-    t_guided = timed(lambda: rg.render_frames(n_guided // spf))
-    e_guided = relmse(rg.download_current_image())
+    scene.set_frame_count(100_000)           # training samples are independent of the image's
+    rg.render_frames(train_spp // spf)
+    sync()
+    train_ms = (time.perf_counter() - t0) * 1e3
+    g.attach(rg.integrator, pt.Guide.OFF)
+    rg.integrator.close()
+    rg.film.close()
+    guided = []
+    acc = None
+    spp = 0
+    while spp < guided_cap:
+        imgs, _, _ = pt.render_batch([(scene, chunk, spp // spf, None, g)], mode=pt.BATCH_WAVEFRONT,
+                                     autotune=False)
+        img = imgs[0].astype(np.float64)
+        acc = img if acc is None else acc + (img - acc) * (chunk / (spp + chunk))
+        spp += chunk
+        e = relmse(acc)
+        guided.append((spp, (time.perf_counter() - t0) * 1e3, e))
+        if e <= TARGET_RELMSE:
+            break
     g.close()
-    # plain: e_plain = c / n_plain + c / n_ref (its own noise plus the reference's)
-    e_ref = e_plain * n_plain / (n_plain + n_ref)
-    tp = t_plain * max(e_plain - e_ref, 1e-12) / 1e-3
-    tg = t_train + t_guided * max(e_guided - e_ref, 1e-12) / 1e-3
-    return {"scene": f"hidden_light_room {len(sa.faces)} tri, {w}x{w}, depth {sa.max_depth}, sobol",
-            "reference": f"plain, {n_ref} spp, independent samples ({ref_ms:.0f} ms)",
-            "plain": {"spp": n_plain, "ms": round(t_plain, 1), "relmse": round(e_plain, 6)},
-            "guided": {"train_spp": n_train, "train_ms": round(t_train, 1), "spp": n_guided,
-                       "ms": round(t_guided, 1), "relmse": round(e_guided, 6)},
-            "reference_noise_relmse": round(e_ref, 6),
-            "time_to_relmse_1e-3_ms": {"plain": round(tp, 1), "guided": round(tg, 1)},
-            "guided_speedup": round(tp / tg, 3)}
+    tp_chk, tp = crossing_time(plain, TARGET_RELMSE)
+    tg_chk, tg = crossing_time(guided, TARGET_RELMSE)
+    # secondary: the same with the reference's own noise taken out
+    tpc = crossing_time([(a, b, c - ref_noise) for a, b, c in plain], TARGET_RELMSE)[1]
+    tgc = crossing_time([(a, b, c - ref_noise) for a, b, c in guided], TARGET_RELMSE)[1]
+
+    def brief(tr):
+        keep = {2 ** k for k in range(6, 16)}
+        return [[a, round(b, 1), round(c, 6)] for a, b, c in tr if a in keep or (a, b, c) == tr[-1]]
+
+    return {"scene": f"hidden_light_room {len(sa.faces)} tri, {int(z['width'])}x{int(z['height'])}, "
+                     f"depth {sa.max_depth}, sobol",
+            "reference": f"FP64 oracle, crop x {x0}-{x1} y {y0}-{y1}, {int(z['spp'])} spp, "
+                         f"noise relMSE {ref_noise:.2e}",
+            "eps_rel": eps, "chunk_spp": chunk,
+            "plain": {"path": "Renderer.render_frames (pt_renderer_render_frames)", "trace": brief(plain)},
+            "guided": {"path": "pt_render_batch, wavefront item with its trained guide", "train_spp": train_spp,
+                       "train_ms": round(train_ms, 1), "trace": brief(guided)},
+            "time_to_relmse_1e-3_ms": {"plain": None if tp is None else round(tp, 1),
+                                       "guided": None if tg is None else round(tg, 1)},
+            "first_checkpoint_below_1e-3_ms": {"plain": None if tp_chk is None else round(tp_chk, 1),
+                                               "guided": None if tg_chk is None else round(tg_chk, 1)},
+            "noise_corrected_time_ms": {"plain": None if tpc is None else round(tpc, 1),
+                                        "guided": None if tgc is None else round(tgc, 1)},
+            "guided_speedup": None if (tp is None or tg is None) else round(tp / tg, 3),
+            "target_speedup": 3.0}
 
 
 def build_leg(sa):
