@@ -162,6 +162,8 @@ typedef struct pt_scene_info {
     uint32_t bvh_max_depth, num_inner_nodes, num_leaves;
     uint32_t frame_count;
     uint64_t device_bytes;
+    uint32_t num_textures;           /* material textures (HostScene::textures) */
+    uint32_t _pad;
 } pt_scene_info;
 
 typedef struct pt_render_stats {
@@ -202,6 +204,26 @@ int pt_scene_create(const pt_vertex* vertices, uint32_t num_vertices,
                     pt_scene** out);
 int pt_scene_destroy(pt_scene* scene);
 int pt_scene_set_punctual_lights(pt_scene* scene, const pt_punctual_light* lights, uint32_t n);
+/* Material textures (HostScene::textures, Part_2/src/scene/scene.h:24-35; the
+ * reference fills them from glTF images, gltf_loader.cpp:112-147, and uploads
+ * each as a CudaTexture, cuda/cuda_texture.cu:37-62): width * height RGBA
+ * floats (8-bit images as value / 255, no colour decoding -- base colour and
+ * sheen colour texels are raised to 2.2 when sampled), GL wrap modes (10497
+ * repeat, 33071 clamp to edge, 33648 mirrored repeat), bilinear filtering and
+ * normalized coordinates on the device.  A material's *_tex fields index this
+ * list.  pt_scene_add_texture appends one (out_index = its index; 0 x 0 with
+ * rgba null adds a texture without an image, as a glTF texture without a
+ * source becomes; lookups skip it); pt_scene_get_texture reads one back (rgba
+ * may be null). */
+int pt_scene_add_texture(pt_scene* scene, const float* rgba, int32_t width, int32_t height, int32_t wrap_s,
+                         int32_t wrap_t, int32_t* out_index);
+int pt_scene_get_texture(const pt_scene* scene, int32_t index, float* rgba, uint64_t cap_floats, int32_t* width,
+                         int32_t* height, int32_t* wrap_s, int32_t* wrap_t);
+/* PNG or baseline JPEG bytes -> 8-bit RGBA (grey, grey + alpha and RGB
+ * expanded as the reference's stb_image call with four channels does,
+ * gltf_loader.cpp:21-39).  With rgba8 null only the size is reported. */
+int pt_decode_image(const uint8_t* bytes, uint64_t size, uint8_t* rgba8, uint64_t cap, int32_t* width,
+                    int32_t* height);
 int pt_scene_set_render_settings(pt_scene* scene, const pt_render_settings* s);   /* setSpp/setSampler/setMaxDepth */
 int pt_scene_get_render_settings(const pt_scene* scene, pt_render_settings* s);
 int pt_scene_set_camera(pt_scene* scene, const pt_camera* cam);                   /* SceneManager::updateCamera */

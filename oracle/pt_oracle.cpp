@@ -633,10 +633,15 @@ template <class R> R power(R a, R b) {
 // ---------------------------------------------------------------------------
 // Scene context and lights (direct_lighting.cuh, light_pdf.cuh, envmap.h)
 // ---------------------------------------------------------------------------
+// A material texture: float RGBA texels and the address modes of its glTF sampler.
+struct OTex { const float* rgba; int32_t width, height, wrap_s, wrap_t; };
+
 struct Ctx {
     Geo geo;
     const Mat* mats;
     uint32_t nmat;
+    const OTex* texs;     // material textures (null / 0 when the scene has none)
+    uint32_t ntex;
     const EmRef* em;
     uint32_t nem;
     const float* tri_pmf;
@@ -689,6 +694,45 @@ template <class R> R env_pdf(const Ctx& c, const V3<R>& d) {
 }
 template <class R> V3<R> vpos(const Ctx& c, uint32_t i) { return ld<R>(c.geo.v[i].p); }
 template <class R> V3<R> vnr(const Ctx& c, uint32_t i) { return ld<R>(c.geo.v[i].n); }
+
+// ---- material textures (shading_utils.cuh:17-68, disney_bsdf.cuh:79-116) ----
+enum { kTexBase = 0, kTexMR = 1, kTexNormal = 2, kTexCC = 5, kTexCCR = 6, kTexTrans = 8, kTexSheenC = 9,
+       kTexSheenR = 10 };
+inline bool tex_live(const Ctx& c, int32_t id) {
+    return id >= 0 && static_cast<uint32_t>(id) < c.ntex && c.texs[id].rgba != nullptr && c.texs[id].width > 0 &&
+           c.texs[id].height > 0;
+}
+// the device's tex2D<float4> (bilinear, normalized coordinates, the sampler's
+// address modes), through the measured B200 filter model
+inline float4 tex_at(const Ctx& c, int32_t id, float u, float v) {
+    const OTex& t = c.texs[id];
+    const HostTexture h{t.rgba, t.width, t.height};
+    return ptref_tex_fetch_mode(&h, u, v, ptref_gl_mode(t.wrap_s), ptref_gl_mode(t.wrap_t));
+}
+template <class R> V3<R> tex_linear(float4 t) {
+    return {std::pow(R(t.x), R(2.2f)), std::pow(R(t.y), R(2.2f)), std::pow(R(t.z), R(2.2f))};
+}
+
+// fetchMaterial with textures: factors times texel channels, then the clamps.
+template <class R> ME<R> fetch_tex(const Ctx& c, const Mat& m, float u, float v) {
+    ME<R> e = fetch<R>(m);
+    R rough = R(m.roughness), metal = R(m.metallic), ccr = R(m.cc_roughness);
+    if (tex_live(c, m.tex[kTexBase])) e.base = e.base * tex_linear<R>(tex_at(c, m.tex[kTexBase], u, v));
+    if (tex_live(c, m.tex[kTexMR])) {
+        const float4 t = tex_at(c, m.tex[kTexMR], u, v);
+        rough = rough * R(t.y);
+        metal = metal * R(t.z);
+    }
+    if (tex_live(c, m.tex[kTexCC])) e.clearcoat = e.clearcoat * R(tex_at(c, m.tex[kTexCC], u, v).x);
+    if (tex_live(c, m.tex[kTexCCR])) ccr = ccr * R(tex_at(c, m.tex[kTexCCR], u, v).y);
+    if (tex_live(c, m.tex[kTexTrans])) e.spec_trans = e.spec_trans * R(tex_at(c, m.tex[kTexTrans], u, v).x);
+    if (tex_live(c, m.tex[kTexSheenC])) e.sheen_color = e.sheen_color * tex_linear<R>(tex_at(c, m.tex[kTexSheenC], u, v));
+    if (tex_live(c, m.tex[kTexSheenR])) e.sheen = e.sheen * R(tex_at(c, m.tex[kTexSheenR], u, v).w);
+    e.roughness = clampr(rough, R(0.001f), R(1));
+    e.metallic = clampr(metal, R(0), R(1));
+    e.cc_roughness = clampr(ccr, R(0.001f), R(1));
+    return e;
+}
 template <class R> R face_area(const Ctx& c, const Face& f) {
     return R(0.5f) * len(cross(vpos<R>(c, f.v1) - vpos<R>(c, f.v0), vpos<R>(c, f.v2) - vpos<R>(c, f.v0)));
 }
@@ -888,8 +932,47 @@ template <class R> V3<R> path(const Ctx& c, uint32_t nfaces, int x, int y, Smp& 
         if (mat.double_sided && !entering) { gn = -n; entering = true; }
         else gn = entering ? n : -n;
         const V3<R> wo = -rd;
-        const V3<R> N = gn;
-        const ME<R> me = fetch<R>(mat);
+        V3<R> N = gn;
+        float su = 0.0f, sv = 0.0f, tu = 0.0f, tv = 0.0f;
+        if (c.ntex > 0) {
+            // surface uv (triangle.h:46), applyUvTransform, applyNormalMap with
+            // interpolateTangent (shading_utils.cuh:17-68)
+            const Vtx& a = c.geo.v[f.v0];
+            const Vtx& b = c.geo.v[f.v1];
+            const Vtx& cc = c.geo.v[f.v2];
+            const R u = bw * R(a.uv[0]) + bu * R(b.uv[0]) + bv * R(cc.uv[0]);
+            const R v = bw * R(a.uv[1]) + bu * R(b.uv[1]) + bv * R(cc.uv[1]);
+            su = static_cast<float>(u);
+            sv = static_cast<float>(v);
+            R ttu = u, ttv = v;
+            if (!(mat.uvrot == 0.0f && mat.uvsx == 1.0f && mat.uvsy == 1.0f && mat.uvox == 0.0f && mat.uvoy == 0.0f)) {
+                const R cr = std::cos(R(mat.uvrot)), sr = std::sin(R(mat.uvrot));
+                const R ru = cr * u + sr * v, rv = -sr * u + cr * v;
+                ttu = ru * R(mat.uvsx) + R(mat.uvox);
+                ttv = rv * R(mat.uvsy) + R(mat.uvoy);
+            }
+            tu = static_cast<float>(ttu);
+            tv = static_cast<float>(ttv);
+            if (tex_live(c, mat.tex[kTexNormal])) {
+                V3<R> Tg = nrm(V3<R>(bw * R(a.t[0]) + bu * R(b.t[0]) + bv * R(cc.t[0]),
+                                     bw * R(a.t[1]) + bu * R(b.t[1]) + bv * R(cc.t[1]),
+                                     bw * R(a.t[2]) + bu * R(b.t[2]) + bv * R(cc.t[2])));
+                const R sign = a.t[3] >= 0.0f ? R(1) : R(-1);
+                const float4 nm = tex_at(c, mat.tex[kTexNormal], tu, tv);
+                V3<R> mn(R(nm.x) * R(2) - R(1), R(nm.y) * R(2) - R(1), R(nm.z) * R(2) - R(1));
+                mn.x = mn.x * R(mat.normal_scale);
+                mn.y = mn.y * R(mat.normal_scale);
+                mn = nrm(mn);
+                if (Tg.x != R(0) || Tg.y != R(0) || Tg.z != R(0)) {
+                    Tg = nrm(Tg - gn * dot(gn, Tg));
+                    const V3<R> B = cross(gn, Tg) * sign;
+                    N = nrm(Tg * mn.x + B * mn.y + gn * mn.z);
+                } else {
+                    N = nrm(Frm<R>(gn).world(mn));
+                }
+            }
+        }
+        const ME<R> me = c.ntex > 0 ? fetch_tex<R>(c, mat, tu, tv) : fetch<R>(mat);
         if (emits(mat)) {
             R w = R(1);
             if (d > 0 && !last_delta) w = power(last_pdf, emissive_pdf(c, h.prim, t, rd, nfaces));
@@ -897,10 +980,12 @@ template <class R> V3<R> path(const Ctx& c, uint32_t nfaces, int x, int y, Smp& 
             break;
         }
         if (mat.alpha_mode == 1) {
-            const R alpha = R(1);
+            R alpha = R(1);
+            if (tex_live(c, mat.tex[kTexBase])) alpha = R(tex_at(c, mat.tex[kTexBase], su, sv).w);
             if (alpha < R(mat.alpha_cutoff)) { ray = make_ray(hp + rd * R(1e-4f), rd); continue; }
         } else if (mat.alpha_mode == 2) {
-            const R alpha = R(mat.base_alpha);
+            R alpha = R(mat.base_alpha);
+            if (tex_live(c, mat.tex[kTexBase])) alpha = alpha * R(tex_at(c, mat.tex[kTexBase], su, sv).w);
             if (R(rng.next()) >= alpha) { ray = make_ray(hp + rd * R(1e-4f), rd); continue; }
         }
         const bool delta_surface = (me.metallic >= R(1) && me.roughness < R(0.01f)) ||
@@ -1250,6 +1335,8 @@ int oracle_render(const oracle_scene* sc, const oracle_render_args* a, float* ou
                 static_cast<const Face*>(sc->faces), sc->num_nodes, a->watertight != 0};
     c.mats = static_cast<const Mat*>(sc->materials);
     c.nmat = sc->num_materials;
+    c.texs = static_cast<const OTex*>(sc->textures);
+    c.ntex = sc->textures ? sc->num_textures : 0u;
     c.em = sc->num_emissive ? static_cast<const EmRef*>(sc->emissive) : nullptr;
     c.nem = sc->num_emissive;
     c.tri_pmf = sc->tri_pmf;

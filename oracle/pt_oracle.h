@@ -29,7 +29,14 @@ typedef struct oracle_scene {
     const void*  punctual;  uint32_t num_punctual;     /* pt_punctual_light (112 B)       */
     const void*  camera_frame;                         /* pt_camera_frame (64 B)          */
     int32_t      width, height;
+    const void*  textures;  uint32_t num_textures;     /* oracle_texture per material texture */
 } oracle_scene;
+
+/* a material texture: width * height RGBA floats, GL wrap modes of its sampler */
+typedef struct oracle_texture {
+    const float* rgba;
+    int32_t width, height, wrap_s, wrap_t;
+} oracle_texture;
 
 typedef struct oracle_render_args {
     int32_t  sample_per_frame, max_depth, sampler_type, arg_rtl;

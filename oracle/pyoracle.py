@@ -37,7 +37,13 @@ class Scene(C.Structure):
                 ("env_rgba", C.c_void_p), ("env_w", C.c_int32), ("env_h", C.c_int32), ("env_pmf", C.c_void_p),
                 ("env_alias", C.c_void_p), ("num_env_texels", C.c_uint32), ("env_tw", C.c_int32),
                 ("env_th", C.c_int32), ("punctual", C.c_void_p), ("num_punctual", C.c_uint32),
-                ("camera_frame", C.c_void_p), ("width", C.c_int32), ("height", C.c_int32)]
+                ("camera_frame", C.c_void_p), ("width", C.c_int32), ("height", C.c_int32),
+                ("textures", C.c_void_p), ("num_textures", C.c_uint32)]
+
+
+class OTex(C.Structure):
+    _fields_ = [("rgba", C.c_void_p), ("width", C.c_int32), ("height", C.c_int32), ("wrap_s", C.c_int32),
+                ("wrap_t", C.c_int32)]
 
 
 class RenderArgs(C.Structure):
@@ -87,12 +93,15 @@ class Prepared:
     """Scene prepared with the oracle's own builder (BVH order, light tables)."""
 
     def __init__(self, vertices, faces, materials, nodes, depth, em_refs, tri_pmf, tri_alias, env, env_pmf,
-                 env_alias, camera_frame, width, height, punctual=None):
+                 env_alias, camera_frame, width, height, punctual=None, textures=None):
         self.vertices, self.faces, self.materials, self.nodes, self.depth = vertices, faces, materials, nodes, depth
         self.em_refs, self.tri_pmf, self.tri_alias = em_refs, tri_pmf, tri_alias
         self.env, self.env_pmf, self.env_alias = env, env_pmf, env_alias
         self.camera_frame, self.width, self.height = camera_frame, width, height
         self.punctual = punctual
+        # material textures: [{"rgba": (H, W, 4) float32, "wrap_s": gl, "wrap_t": gl}, ...]
+        self.textures = [dict(t, rgba=np.ascontiguousarray(t["rgba"], np.float32)) for t in (textures or [])]
+        self._tex_table = None
 
     def struct(self) -> Scene:
         s = Scene()
@@ -111,6 +120,14 @@ class Prepared:
             s.punctual, s.num_punctual = _p(self.punctual), len(self.punctual)
         s.camera_frame = _p(self.camera_frame)
         s.width, s.height = self.width, self.height
+        if self.textures:
+            tab = (OTex * len(self.textures))()
+            for k, t in enumerate(self.textures):
+                a = t["rgba"]
+                tab[k] = OTex(a.ctypes.data if a.size else None, a.shape[1], a.shape[0],
+                              int(t.get("wrap_s", 10497)), int(t.get("wrap_t", 10497)))
+            self._tex_table = tab
+            s.textures, s.num_textures = C.cast(tab, C.c_void_p), len(self.textures)
         return s
 
 
@@ -199,7 +216,7 @@ class Oracle:
         punct = getattr(sa, "punctual", None)
         return Prepared(np.ascontiguousarray(sa.vertices, VERTEX), faces, np.ascontiguousarray(sa.materials), nodes,
                         depth, refs, pmf, alias, env, env_pmf, env_alias, cf, int(sa.camera["width"]),
-                        int(sa.camera["height"]), punct)
+                        int(sa.camera["height"]), punct, getattr(sa, "textures", None))
 
     def render(self, prep: Prepared, spf, max_depth, sampler, frames, first_frame=0, precision=64, rtl=1,
                pcg_seed=0, row0=0, row_step=1, threads=0, crop=None, watertight=False):
@@ -260,6 +277,29 @@ class RefHarness:
         self.L.ref_loaded_arrays(_p(v), _p(f), _p(m), _p(lights), _p(env) if env is not None else None)
         return {"vertices": v, "faces": f, "materials": m, "lights": lights, "env": env, "camera": cam,
                 "settings": settings}
+
+    def loaded_textures(self):
+        """Material textures of the last load_json: [{"rgba": (H, W, 4), "wrap_s", "wrap_t"}]."""
+        self.L.ref_loaded_texture_count.restype = C.c_uint32
+        out = []
+        for i in range(int(self.L.ref_loaded_texture_count())):
+            info = np.zeros(5, np.int32)
+            self.L.ref_loaded_texture(C.c_uint32(i), _p(info), None)
+            rgba = np.zeros((max(int(info[1]), 0), max(int(info[0]), 0), 4), np.float32)
+            if rgba.size:
+                self.L.ref_loaded_texture(C.c_uint32(i), _p(info), _p(rgba))
+            out.append({"rgba": rgba, "wrap_s": int(info[3]), "wrap_t": int(info[4]), "channel": int(info[2])})
+        return out
+
+    def decode_image(self, data: bytes):
+        """The reference's stb_image decode with four channels forced -> (H, W, 4) uint8."""
+        buf = np.frombuffer(bytes(data), np.uint8)
+        w, h = C.c_int32(), C.c_int32()
+        if self.L.ref_decode_image(_p(buf), C.c_int(len(buf)), None, C.c_int(0), C.byref(w), C.byref(h)) != 0:
+            raise RuntimeError("reference decoder rejected the image")
+        out = np.zeros((h.value, w.value, 4), np.uint8)
+        self.L.ref_decode_image(_p(buf), C.c_int(len(buf)), _p(out), C.c_int(out.size), C.byref(w), C.byref(h))
+        return out
 
     def build(self, vertices, faces, materials, env=None):
         v = np.ascontiguousarray(vertices, VERTEX)
@@ -351,9 +391,16 @@ class RefGpu:
         ew, eh = (env.shape[1], env.shape[0]) if env is not None else (0, 0)
         st = np.array([sa.spp, sa.sample_per_frame, sa.max_depth, sa.sampler], np.int32)
         h = C.c_void_p()
-        rc = self.L.refgpu_create(_p(v), C.c_uint32(len(v)), _p(f), C.c_uint32(len(f)), _p(m),
-                                  C.c_uint32(m.nbytes // 256), _p(env), C.c_int(ew), C.c_int(eh), _p(cam), _p(st),
-                                  C.c_int(device), C.byref(h))
+        texs = [dict(t, rgba=np.ascontiguousarray(t["rgba"], np.float32)) for t in getattr(sa, "textures", [])]
+        tab = (OTex * max(1, len(texs)))()
+        for k, t in enumerate(texs):
+            a = t["rgba"]
+            tab[k] = OTex(a.ctypes.data if a.size else None, a.shape[1], a.shape[0], int(t.get("wrap_s", 10497)),
+                          int(t.get("wrap_t", 10497)))
+        rc = self.L.refgpu_create_textured(_p(v), C.c_uint32(len(v)), _p(f), C.c_uint32(len(f)), _p(m),
+                                           C.c_uint32(m.nbytes // 256), _p(env), C.c_int(ew), C.c_int(eh), _p(cam),
+                                           _p(st), C.cast(tab, C.c_void_p), C.c_uint32(len(texs)), C.c_int(device),
+                                           C.byref(h))
         if rc != 0:
             raise RuntimeError(f"reference GPU scene setup failed ({rc})")
         self._h = h

@@ -51,11 +51,28 @@ struct RefGpu {
 
 extern "C" {
 
+// A material texture as passed in: RGBA floats and GL wrap modes (the
+// layout of oracle_texture in pt_oracle.h).
+struct RefTexture { const float* rgba; int32_t width, height, wrap_s, wrap_t; };
+
+int refgpu_create_textured(const void* verts, uint32_t nv, const void* faces, uint32_t nf, const void* mats,
+                           uint32_t nm, const float* env, int ew, int eh, const void* camera, const int32_t* settings,
+                           const void* textures, uint32_t ntex, int device, void** out);
+
 // settings = {targetSamples, samplePerFrame, maxDepth, samplerType}.
 // Scene prep is SceneManager::buildAccel's; the upload is DeviceScene::uploadFrom.
 int refgpu_create(const void* verts, uint32_t nv, const void* faces, uint32_t nf, const void* mats, uint32_t nm,
                   const float* env, int ew, int eh, const void* camera, const int32_t* settings, int device,
                   void** out) {
+    return refgpu_create_textured(verts, nv, faces, nf, mats, nm, env, ew, eh, camera, settings, nullptr, 0, device,
+                                  out);
+}
+
+// The same with material textures (HostScene::textures, uploaded by
+// DeviceScene::uploadFrom as CudaTextures, device_scene.cu:29-41).
+int refgpu_create_textured(const void* verts, uint32_t nv, const void* faces, uint32_t nf, const void* mats,
+                           uint32_t nm, const float* env, int ew, int eh, const void* camera, const int32_t* settings,
+                           const void* textures, uint32_t ntex, int device, void** out) {
     if (cudaSetDevice(device) != cudaSuccess) return 1;
     Quiet quiet;
     RefGpu* r = new RefGpu();
@@ -71,6 +88,20 @@ int refgpu_create(const void* verts, uint32_t nv, const void* faces, uint32_t nf
         hs.hdrImage.height = eh;
         hs.hdrImage.channel = 4;
         hs.hdrImage.data.assign(env, env + static_cast<size_t>(ew) * eh * 4);
+    }
+    const RefTexture* tx = static_cast<const RefTexture*>(textures);
+    for (uint32_t k = 0; k < ntex; ++k) {
+        Image img;
+        img.width = tx[k].width;
+        img.height = tx[k].height;
+        img.channel = 4;
+        img.wrapS = tx[k].wrap_s;
+        img.wrapT = tx[k].wrap_t;
+        if (tx[k].rgba && tx[k].width > 0 && tx[k].height > 0)
+            img.data.assign(tx[k].rgba, tx[k].rgba + static_cast<size_t>(tx[k].width) * tx[k].height * 4);
+        else
+            img.channel = 0;   // no image: CudaTexture creates no texture for it
+        hs.textures.push_back(std::move(img));
     }
     std::memcpy(static_cast<void*>(&hs.camera), camera, sizeof(Camera));
     hs.settings.targetSamples = settings[0];

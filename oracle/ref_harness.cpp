@@ -76,6 +76,7 @@ inline bool ptref_occluded(const Ray& r, const BVHNode* n, const Vertex* v, cons
 #include "scene/scene.h"
 #include "scene/scene_loader.h"
 #include "io/image_io.h"
+#include "stb/stb_image.h"
 
 using namespace pt;
 
@@ -199,6 +200,35 @@ int ref_write_image(const char* path, const float* rgba, int w, int h, int flip_
     img.channel = 4;
     img.data.assign(rgba, rgba + static_cast<size_t>(w) * h * 4);
     return ImageIO::write(img, path, flip_y != 0) ? 0 : 1;
+}
+
+// Material textures of the last loaded scene: count, then per texture its size,
+// wrap modes and RGBA floats (HostScene::textures as the reference's loaders fill it).
+uint32_t ref_loaded_texture_count() { return static_cast<uint32_t>(g_loaded.textures.size()); }
+int ref_loaded_texture(uint32_t i, int32_t* info, float* rgba) {
+    if (i >= g_loaded.textures.size()) return 1;
+    const Image& t = g_loaded.textures[i];
+    info[0] = t.width;
+    info[1] = t.height;
+    info[2] = t.channel;
+    info[3] = t.wrapS;
+    info[4] = t.wrapT;
+    if (rgba && !t.data.empty()) std::memcpy(rgba, t.data.data(), t.data.size() * sizeof(float));
+    return 0;
+}
+
+// The reference's image decoder as its glTF loader calls it (stb_image from
+// its 3rdparty tree, four channels forced, gltf_loader.cpp:21-39).
+int ref_decode_image(const unsigned char* bytes, int size, unsigned char* rgba, int cap, int32_t* w, int32_t* h) {
+    int ww = 0, hh = 0, comp = 0;
+    unsigned char* data = stbi_load_from_memory(bytes, size, &ww, &hh, &comp, 4);
+    if (!data) return 1;
+    *w = ww;
+    *h = hh;
+    const int n = ww * hh * 4;
+    if (rgba && cap >= n) std::memcpy(rgba, data, static_cast<size_t>(n));
+    stbi_image_free(data);
+    return 0;
 }
 
 int ref_loaded_arrays(void* verts, void* faces, void* mats, void* lights, float* env) {

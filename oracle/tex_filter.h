@@ -37,6 +37,17 @@ inline int ptref_wrap(int i, int n) {
     return r < 0 ? r + n : r;
 }
 
+// Texel index under a CUDA address mode: 0 wrap, 1 clamp to the edge,
+// 2 mirror (the texel row reflected at both ends, period 2n).
+inline int ptref_address(int i, int n, int mode) {
+    if (mode == 1) return i < 0 ? 0 : (i >= n ? n - 1 : i);
+    if (mode == 2) {
+        int r = ptref_wrap(i, 2 * n);
+        return r < n ? r : 2 * n - 1 - r;
+    }
+    return ptref_wrap(i, n);
+}
+
 // Bilinear fetch with normalized coordinates and wrap addressing.
 inline float4 ptref_tex_fetch(const HostTexture* t, float u, float v) {
     const float x = (u - std::floor(u)) * static_cast<float>(t->width) - 0.5f;
@@ -59,3 +70,36 @@ inline float4 ptref_tex_fetch(const HostTexture* t, float u, float v) {
         r[c] = static_cast<float>((w00 * p00[c] + w10 * p10[c] + w01 * p01[c] + w11 * p11[c]) / 256.0);
     return make_float4(r[0], r[1], r[2], r[3]);
 }
+
+// The same bilinear model with an address mode per axis (0 wrap, 1 clamp,
+// 2 mirror).  Wrap reduces the coordinate to [0, 1) first, as the fetch
+// above; clamp and mirror address the two neighbouring texels of
+// x = u * W - 1/2 by their index rule.
+inline float4 ptref_tex_fetch_mode(const HostTexture* t, float u, float v, int mode_s, int mode_t) {
+    const float uu = mode_s == 0 ? u - std::floor(u) : u;
+    const float vv = mode_t == 0 ? v - std::floor(v) : v;
+    const float x = uu * static_cast<float>(t->width) - 0.5f;
+    const float y = vv * static_cast<float>(t->height) - 0.5f;
+    const float fx = std::floor(x), fy = std::floor(y);
+    const double a8 = std::nearbyint(static_cast<double>(x - fx) * 256.0);
+    const double b8 = std::nearbyint(static_cast<double>(y - fy) * 256.0);
+    const double w00 = std::nearbyint((256.0 - a8) * (256.0 - b8) / 256.0);
+    const double w10 = std::nearbyint(a8 * (256.0 - b8) / 256.0);
+    const double w01 = std::nearbyint((256.0 - a8) * b8 / 256.0);
+    const double w11 = std::nearbyint(a8 * b8 / 256.0);
+    const int i0 = ptref_address(static_cast<int>(fx), t->width, mode_s);
+    const int i1 = ptref_address(static_cast<int>(fx) + 1, t->width, mode_s);
+    const int j0 = ptref_address(static_cast<int>(fy), t->height, mode_t);
+    const int j1 = ptref_address(static_cast<int>(fy) + 1, t->height, mode_t);
+    const float* p00 = t->rgba + (static_cast<size_t>(j0) * t->width + i0) * 4;
+    const float* p10 = t->rgba + (static_cast<size_t>(j0) * t->width + i1) * 4;
+    const float* p01 = t->rgba + (static_cast<size_t>(j1) * t->width + i0) * 4;
+    const float* p11 = t->rgba + (static_cast<size_t>(j1) * t->width + i1) * 4;
+    float r[4];
+    for (int c = 0; c < 4; ++c)
+        r[c] = static_cast<float>((w00 * p00[c] + w10 * p10[c] + w01 * p01[c] + w11 * p11[c]) / 256.0);
+    return make_float4(r[0], r[1], r[2], r[3]);
+}
+
+// GL wrap mode of a glTF sampler -> the address mode above.
+inline int ptref_gl_mode(int gl) { return gl == 33071 ? 1 : (gl == 33648 ? 2 : 0); }

@@ -32,7 +32,7 @@ from ._ffi import SAMPLER_PCG, SAMPLER_SOBOL, FLAG_WATERTIGHT, FLAG_STAGE_TIMING
     FLAG_COUNT_TRAVERSAL, ARGS_LTR, ARGS_RTL
 
 __all__ = ["SceneManager", "PathIntegrator", "Film", "Renderer", "render", "default_material", "make_camera",
-           "trace_closest", "trace_any", "sampler_stream", "bsdf_eval", "write_hdr", "read_hdr", "tonemap",
+           "trace_closest", "trace_any", "sampler_stream", "bsdf_eval", "write_hdr", "read_hdr", "tonemap", "decode_image",
            "compute_rmse", "rmse_to_db", "PTError", "VERTEX_DTYPE", "FACE_DTYPE", "MATERIAL_DTYPE",
            "CAMERA_DTYPE", "PUNCTUAL_DTYPE", "BVH_NODE_DTYPE", "SAMPLER_PCG", "SAMPLER_SOBOL",
            "FLAG_WATERTIGHT", "FLAG_STAGE_TIMING", "FLAG_NO_GRAPH", "FLAG_COUNT_TRAVERSAL",
@@ -164,6 +164,28 @@ class SceneManager:
     def update_camera(self, cam: np.ndarray) -> None:
         c = np.ascontiguousarray(cam, dtype=CAMERA_DTYPE)
         check(lib().pt_scene_set_camera(self._h, ptr(c)))
+
+    def add_texture(self, rgba: np.ndarray, wrap_s: int = 10497, wrap_t: int = 10497) -> int:
+        """Append a material texture ((H, W, 4) float texels; GL wrap modes) and
+        return its index for the materials' *_tex fields."""
+        a = np.ascontiguousarray(rgba, np.float32)
+        if a.ndim != 3 or a.shape[2] != 4:
+            raise ValueError("texture must be (H, W, 4)")
+        idx = C.c_int32()
+        check(lib().pt_scene_add_texture(self._h, ptr(a) if a.size else None, a.shape[1], a.shape[0], int(wrap_s),
+                                         int(wrap_t), C.byref(idx)))
+        return idx.value
+
+    def texture(self, index: int) -> dict:
+        """Material texture `index`: {"rgba": (H, W, 4) float32, "wrap_s", "wrap_t"}."""
+        w, h, ws, wt = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().pt_scene_get_texture(self._h, int(index), None, 0, C.byref(w), C.byref(h), C.byref(ws),
+                                         C.byref(wt)))
+        out = np.zeros((h.value, w.value, 4), np.float32)
+        if out.size:
+            check(lib().pt_scene_get_texture(self._h, int(index), ptr(out), out.size, C.byref(w), C.byref(h), None,
+                                             None))
+        return {"rgba": out, "wrap_s": ws.value, "wrap_t": wt.value}
 
     def set_punctual_lights(self, lights: np.ndarray) -> None:
         L = np.ascontiguousarray(lights, dtype=PUNCTUAL_DTYPE)
@@ -612,6 +634,16 @@ def tonemap(img: np.ndarray, exposure: float = -2.8, device: int = 0) -> np.ndar
         a = np.ascontiguousarray(np.concatenate([a, np.ones((h, w, 1), np.float32)], 2))
     out = np.zeros((h, w, 4), np.uint8)
     check(lib().pt_tonemap(ptr(a), w, h, float(exposure), ptr(out), 0, device))
+    return out
+
+
+def decode_image(data: bytes) -> np.ndarray:
+    """PNG or baseline JPEG bytes -> (H, W, 4) uint8 RGBA (the library's decoder)."""
+    buf = np.frombuffer(bytes(data), np.uint8)
+    w, h = C.c_int32(), C.c_int32()
+    check(lib().pt_decode_image(ptr(buf), len(buf), None, 0, C.byref(w), C.byref(h)))
+    out = np.zeros((h.value, w.value, 4), np.uint8)
+    check(lib().pt_decode_image(ptr(buf), len(buf), ptr(out), out.size, C.byref(w), C.byref(h)))
     return out
 
 

@@ -96,7 +96,8 @@ class SceneInfo(C.Structure):
                 ("num_bvh_nodes", C.c_uint32), ("num_emissive_triangles", C.c_uint32),
                 ("num_punctual_lights", C.c_uint32), ("env_width", C.c_int32), ("env_height", C.c_int32),
                 ("bvh_max_depth", C.c_uint32), ("num_inner_nodes", C.c_uint32), ("num_leaves", C.c_uint32),
-                ("frame_count", C.c_uint32), ("device_bytes", C.c_uint64)]
+                ("frame_count", C.c_uint32), ("device_bytes", C.c_uint64), ("num_textures", C.c_uint32),
+                ("_pad", C.c_uint32)]
 
 
 class RenderStats(C.Structure):
@@ -138,6 +139,10 @@ _SIGS = [
                                   C.POINTER(_P)]),
     ("pt_scene_destroy", C.c_int, [_P]),
     ("pt_scene_set_punctual_lights", C.c_int, [_P, _P, C.c_uint32]),
+    ("pt_scene_add_texture", C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    ("pt_scene_get_texture", C.c_int, [_P, C.c_int32, _P, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    ("pt_decode_image", C.c_int, [_P, C.c_uint64, _P, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("pt_scene_set_render_settings", C.c_int, [_P, C.POINTER(RenderSettings)]),
     ("pt_scene_get_render_settings", C.c_int, [_P, C.POINTER(RenderSettings)]),
     ("pt_scene_set_camera", C.c_int, [_P, _P]),

@@ -21,9 +21,9 @@ LIB = os.path.join(HERE, "libpt_b200.so")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
-CXX_SOURCES = ["host_prep.cpp", "scene_io.cpp", "capi.cpp"]
+CXX_SOURCES = ["host_prep.cpp", "scene_io.cpp", "image_decode.cpp", "capi.cpp"]
 CU_SOURCES = ["integrator.cu", "static_trace.cu", "lbvh.cu"]
-HEADERS = ["pt_internal.h", "sampler.h", "bsdf.h", "traverse.h", "engine.h", "device_api.h", "batch.cuh", "guide.cuh", "guide_host.cuh"]
+HEADERS = ["image_decode.h", "pt_internal.h", "sampler.h", "bsdf.h", "traverse.h", "engine.h", "device_api.h", "batch.cuh", "guide.cuh", "guide_host.cuh"]
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXXFLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-Wall",
@@ -69,7 +69,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         with ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
             list(ex.map(_run_verbose if (verbose or ptxas_info) else _run, jobs))
     if jobs or _stale(LIB, objs):
-        _run([NVCC, *GENCODE, "-shared", "-o", LIB, *objs, "-cudart", "static", "-lpthread"])
+        _run([NVCC, *GENCODE, "-shared", "-o", LIB, *objs, "-cudart", "static", "-lpthread", "-lz"])
     return LIB
 
 

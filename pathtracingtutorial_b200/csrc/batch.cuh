@@ -476,12 +476,19 @@ int render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batc
         set_error("unknown batch mode");
         return PT_ERR_INVALID;
     }
-    bool guided = false;
-    for (uint32_t k = 0; k < n; ++k) guided = guided || in[k].guide != nullptr;
-    if (guided) {
-        // the persistent kernel traces whole paths per thread and has no
-        // warp-wide network evaluation: guided items run in wavefront mode
-        if (req_mode == PT_BATCH_PERSISTENT) { set_error("guided batch items need wavefront mode"); return PT_ERR_INVALID; }
+    bool guided = false, textured = false;
+    for (uint32_t k = 0; k < n; ++k) {
+        guided = guided || in[k].guide != nullptr;
+        textured = textured || !in[k].scene->host.textures.empty();
+    }
+    if (guided || textured) {
+        // the persistent kernel traces whole paths per thread with the
+        // untextured shading and has no warp-wide network evaluation: guided
+        // items and scenes with material textures run in wavefront mode
+        if (req_mode == PT_BATCH_PERSISTENT) {
+            set_error(guided ? "guided batch items need wavefront mode" : "textured scenes need wavefront mode");
+            return PT_ERR_INVALID;
+        }
         req_mode = PT_BATCH_WAVEFRONT;
     }
     const int64_t budget = cfg && cfg->paths_in_flight > 0 ? cfg->paths_in_flight : kDefaultPathsInFlight;

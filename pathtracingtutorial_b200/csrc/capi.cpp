@@ -15,6 +15,7 @@
 
 #include "device_api.h"
 #include "engine.h"
+#include "image_decode.h"
 
 namespace ptb {
 
@@ -155,6 +156,59 @@ int pt_scene_set_punctual_lights(pt_scene* s, const pt_punctual_light* lights, u
     return PT_OK;
 }
 
+int pt_scene_add_texture(pt_scene* s, const float* rgba, int32_t width, int32_t height, int32_t wrap_s,
+                         int32_t wrap_t, int32_t* out_index) {
+    PT_REQUIRE(s && out_index, "null argument");
+    PT_REQUIRE((width > 0 && height > 0 && rgba) || (width == 0 && height == 0),
+               "texture size must be positive (or 0 x 0 for a texture without an image)");
+    PT_REQUIRE(static_cast<uint64_t>(width) * height <= (uint64_t(1) << 28), "texture too large");
+    PT_GUARD_BEGIN
+    HostTextureImage t;
+    t.width = width;
+    t.height = height;
+    t.wrap_s = wrap_s;
+    t.wrap_t = wrap_t;
+    if (width > 0) t.rgba.assign(rgba, rgba + static_cast<size_t>(width) * height * 4);
+    s->host.textures.push_back(std::move(t));
+    *out_index = static_cast<int32_t>(s->host.textures.size() - 1);
+    if (s->dev.uploaded) free_scene_device(s);
+    return PT_OK;
+    PT_GUARD_END
+}
+
+int pt_scene_get_texture(const pt_scene* s, int32_t index, float* rgba, uint64_t cap_floats, int32_t* width,
+                         int32_t* height, int32_t* wrap_s, int32_t* wrap_t) {
+    PT_REQUIRE(s && width && height, "null argument");
+    PT_REQUIRE(index >= 0 && static_cast<size_t>(index) < s->host.textures.size(), "texture index out of range");
+    const HostTextureImage& t = s->host.textures[static_cast<size_t>(index)];
+    *width = t.width;
+    *height = t.height;
+    if (wrap_s) *wrap_s = t.wrap_s;
+    if (wrap_t) *wrap_t = t.wrap_t;
+    if (rgba) {
+        PT_REQUIRE(cap_floats >= t.rgba.size(), "output capacity too small");
+        std::memcpy(rgba, t.rgba.data(), t.rgba.size() * sizeof(float));
+    }
+    return PT_OK;
+}
+
+int pt_decode_image(const uint8_t* bytes, uint64_t size, uint8_t* rgba8, uint64_t cap, int32_t* width,
+                    int32_t* height) {
+    PT_REQUIRE(bytes && width && height, "null argument");
+    PT_GUARD_BEGIN
+    DecodedImage img;
+    std::string err;
+    if (!decode_image(bytes, static_cast<size_t>(size), img, err)) { set_error(err); return PT_ERR_IO; }
+    *width = img.width;
+    *height = img.height;
+    if (rgba8) {
+        PT_REQUIRE(cap >= img.rgba.size(), "output capacity too small");
+        std::memcpy(rgba8, img.rgba.data(), img.rgba.size());
+    }
+    return PT_OK;
+    PT_GUARD_END
+}
+
 int pt_scene_set_render_settings(pt_scene* s, const pt_render_settings* st) {
     PT_REQUIRE(s && st, "null argument");
     PT_REQUIRE(st->sample_per_frame > 0, "sample_per_frame must be positive");
@@ -262,6 +316,7 @@ int pt_scene_info_get(const pt_scene* s, pt_scene_info* info) {
     info->num_leaves = s->tables.num_leaves;
     info->frame_count = s->frame_count;
     info->device_bytes = s->dev.bytes;
+    info->num_textures = static_cast<uint32_t>(s->host.textures.size());
     return PT_OK;
 }
 

@@ -18,10 +18,20 @@ void set_error(const std::string& msg);
 const std::string& get_error();
 
 // ---- host scene (HostScene, Part_2/src/scene/scene.h:24-35) ----
+// A material texture as the reference keeps it (Image, Part_2/src/io/image_io.h,
+// filled by loadTextures, gltf_loader.cpp:112-147): float RGBA texels (8-bit
+// values / 255, no colour decoding) and the glTF sampler's GL wrap modes.
+struct HostTextureImage {
+    int32_t width = 0, height = 0;
+    int32_t wrap_s = 10497, wrap_t = 10497;    // GL_REPEAT
+    std::vector<float> rgba;                    // width * height * 4
+};
+
 struct HostScene {
     std::vector<pt_vertex>         vertices;
     std::vector<pt_face>           faces;
     std::vector<pt_material>       materials;
+    std::vector<HostTextureImage>  textures;
     std::vector<pt_punctual_light> punctual;
     pt_camera                      camera{};
     std::vector<float>             env_rgba;   // env_w * env_h * 4
@@ -82,6 +92,11 @@ struct DeviceSceneBuffers {
     void*    punctual = nullptr;
     void*    env_array = nullptr;          // cudaArray_t
     unsigned long long env_tex = 0;        // cudaTextureObject_t
+    std::vector<void*> tex_arrays;         // per material texture: cudaArray_t (null when empty)
+    std::vector<unsigned long long> tex_objs;   // cudaTextureObject_t (0 when empty)
+    void*    tex_table = nullptr;          // device copy of tex_objs
+    std::vector<size_t> tex_sizes;         // texels per uploaded texture
+    std::vector<int32_t> tex_wraps;        // its wrap modes (s << 16 ^ t)
     uint64_t bytes = 0;
     size_t   sizes[11] = {};               // bytes of the buffers above, in declaration order
     int      env_w = 0, env_h = 0;

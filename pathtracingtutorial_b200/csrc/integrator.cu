@@ -152,6 +152,115 @@ __device__ __forceinline__ pt_face load_face(const DeviceScene& s, uint32_t i) {
     pt_face r; r.v0 = f.x; r.v1 = f.y; r.v2 = f.z; r.material_id = static_cast<int32_t>(f.w);
     return r;
 }
+// ---- material textures (Part_2/src/materials/shading_utils.cuh:17-68 and
+//      disney_bsdf.cuh:79-116) ----
+// A texture id is looked up only when it names a texture with an image.
+__device__ __forceinline__ bool tex_live(const DeviceScene& s, int32_t id) {
+    return id >= 0 && static_cast<uint32_t>(id) < s.num_textures && s.textures[id] != 0ull;
+}
+__device__ __forceinline__ float4 tex_at(const DeviceScene& s, int32_t id, float u, float v) {
+    return tex2D<float4>(static_cast<cudaTextureObject_t>(s.textures[id]), u, v);
+}
+// texel colour to linear (the reference's pow(c, 2.2) per channel)
+__device__ __forceinline__ f3 tex_linear(float4 c) { return mk(powf(c.x, 2.2f), powf(c.y, 2.2f), powf(c.z, 2.2f)); }
+__device__ __forceinline__ float2 vuv(const DeviceScene& s, uint32_t i) {
+    return __ldg(reinterpret_cast<const float2*>(s.vertices + i) + 4);
+}
+__device__ __forceinline__ float4 vtan(const DeviceScene& s, uint32_t i) {
+    return __ldg(reinterpret_cast<const float4*>(s.vertices + i) + 3);
+}
+
+// fetchMaterial with textures: the factors times the texel channels, then
+// the reference's clamps.  (The emissive texture only changes the evaluated
+// material's emission, which the path loop never reads: emission comes from
+// the material record, path.cu:105-111.)
+__device__ MatEval resolve_material_textured(const DeviceScene& s, const pt_material& m, float u, float v) {
+    MatEval e = resolve_material(m);
+    float rough = m.roughness, metal = m.metallic, ccr = m.clearcoat_roughness;
+    if (tex_live(s, m.base_color_tex)) e.base = e.base * tex_linear(tex_at(s, m.base_color_tex, u, v));
+    if (tex_live(s, m.metallic_roughness_tex)) {
+        const float4 t = tex_at(s, m.metallic_roughness_tex, u, v);
+        rough *= t.y;
+        metal *= t.z;
+    }
+    if (tex_live(s, m.clearcoat_tex)) e.clearcoat *= tex_at(s, m.clearcoat_tex, u, v).x;
+    if (tex_live(s, m.clearcoat_roughness_tex)) ccr *= tex_at(s, m.clearcoat_roughness_tex, u, v).y;
+    if (tex_live(s, m.transmission_tex)) e.spec_trans *= tex_at(s, m.transmission_tex, u, v).x;
+    if (tex_live(s, m.sheen_color_tex)) e.sheen_color = e.sheen_color * tex_linear(tex_at(s, m.sheen_color_tex, u, v));
+    if (tex_live(s, m.sheen_roughness_tex)) e.sheen *= tex_at(s, m.sheen_roughness_tex, u, v).w;
+    e.roughness = clampf(rough, 0.001f, 1.0f);
+    e.metallic = clampf(metal, 0.0f, 1.0f);
+    e.cc_roughness = clampf(ccr, 0.001f, 1.0f);
+    return e;
+}
+
+// The surface at a hit as the path loop sees it (path.cu:84-102): the
+// interpolated normal oriented towards the ray (double-sided materials
+// flipped), and -- for textured scenes -- the surface uv, the material's
+// transformed uv and the normal-mapped shading normal.  Front and back
+// shading kernels both call it, so they see the same surface.
+struct SurfaceAt {
+    f3    gn, N;          // oriented geometric normal, shading normal
+    bool  entering;
+    float su, sv;         // interpolated uv (alpha lookups)
+    float tu, tv;         // after the material's uv transform (texture lookups)
+};
+
+template <bool Textured>
+__device__ __forceinline__ void surface_at(const DeviceScene& s, const pt_face& f, const pt_material& m, float bu,
+                                           float bv, f3 rd, SurfaceAt& g) {
+    const float bw = 1.0f - bu - bv;
+    const f3 n = normalize(bw * vnrm(s, f.v0) + bu * vnrm(s, f.v1) + bv * vnrm(s, f.v2));
+    bool entering = dot(n, rd) < 0.0f;
+    if (m.double_sided && !entering) { g.gn = -n; entering = true; }
+    else g.gn = entering ? n : -n;
+    g.entering = entering;
+    g.N = g.gn;
+    g.su = g.sv = g.tu = g.tv = 0.0f;
+    if (!Textured) return;
+    const float2 a = vuv(s, f.v0), b = vuv(s, f.v1), c = vuv(s, f.v2);
+    g.su = bw * a.x + bu * b.x + bv * c.x;
+    g.sv = bw * a.y + bu * b.y + bv * c.y;
+    // applyUvTransform (shading_utils.cuh:17-28)
+    g.tu = g.su;
+    g.tv = g.sv;
+    if (!(m.uv_rotation == 0.0f && m.uv_scale_x == 1.0f && m.uv_scale_y == 1.0f && m.uv_offset_x == 0.0f &&
+          m.uv_offset_y == 0.0f)) {
+        const float cr = cosf(m.uv_rotation), sr = sinf(m.uv_rotation);
+        const float ru = cr * g.su + sr * g.sv;
+        const float rv = -sr * g.su + cr * g.sv;
+        g.tu = ru * m.uv_scale_x + m.uv_offset_x;
+        g.tv = rv * m.uv_scale_y + m.uv_offset_y;
+    }
+    // applyNormalMap (shading_utils.cuh:43-68) with interpolateTangent (:30-41);
+    // the reference's tangent flip for double-sided back faces cannot trigger
+    // (entering is true by then), so none is applied here either
+    if (tex_live(s, m.normal_tex)) {
+        const float4 t0 = vtan(s, f.v0), t1 = vtan(s, f.v1), t2 = vtan(s, f.v2);
+        f3 T = normalize(mk(bw * t0.x + bu * t1.x + bv * t2.x, bw * t0.y + bu * t1.y + bv * t2.y,
+                            bw * t0.z + bu * t1.z + bv * t2.z));
+        const float sign = t0.w >= 0.0f ? 1.0f : -1.0f;
+        const float4 nm = tex_at(s, m.normal_tex, g.tu, g.tv);
+        f3 mn = mk(nm.x * 2.0f - 1.0f, nm.y * 2.0f - 1.0f, nm.z * 2.0f - 1.0f);
+        mn.x *= m.normal_scale;
+        mn.y *= m.normal_scale;
+        mn = normalize(mn);
+        if (T.x != 0.0f || T.y != 0.0f || T.z != 0.0f) {
+            T = normalize(T - g.gn * dot(g.gn, T));
+            const f3 B = cross(g.gn, T) * sign;
+            g.N = normalize(T * mn.x + B * mn.y + g.gn * mn.z);
+        } else {
+            const Frame tbn = make_frame(g.gn);
+            g.N = normalize(to_world(tbn, mn));
+        }
+    }
+}
+
+// hit point o + t d with explicit fused multiply-adds (the same value wherever computed)
+__device__ __forceinline__ f3 hit_point(f3 o, f3 d, float t) {
+    return mk(fmaf(t, d.x, o.x), fmaf(t, d.y, o.y), fmaf(t, d.z, o.z));
+}
+
 // emissiveTrianglePdf (light_pdf.cuh:31-54)
 __device__ float emissive_pdf(const DeviceScene& s, int prim, float dist, f3 dir) {
     if (prim < 0 || prim >= static_cast<int>(s.num_faces) || s.tri_light_pmf == nullptr) return 0.0f;
@@ -340,7 +449,7 @@ struct InlineSink {
 
 // The shading point a bounce continues from.
 struct ShadePoint {
-    f3 hp, gn;
+    f3 hp, gn, N;        // N: the shading normal (gn unless a normal map bends it)
     bool entering;
     MatEval me;
     const float* gmix;   // guided vertex: its mixture, else nullptr
@@ -350,7 +459,7 @@ struct ShadePoint {
 // emitter hit (the path ends), alpha pass-through, next-event estimation.
 // Returns 0 when the path ends here, 1 when it continues by sampling at `sp`
 // (shade_back), 2 when it continues straight through with ray (no, nd).
-template <bool Guided, class Sink>
+template <bool Guided, class Sink, bool Textured = false>
 __device__ int shade_front(const DeviceScene& s, int arg_rtl, int depth, f3 ro, f3 rd, float4 h, const f3& T,
                            float last_pdf, bool last_delta, f3& L, PathRng& rng, f3& no, f3& nd, Sink& sink,
                            GuideVertex gv, ShadePoint& sp) {
@@ -366,29 +475,45 @@ __device__ int shade_front(const DeviceScene& s, int arg_rtl, int depth, f3 ro, 
     }
     const float t = h.x, bu = h.z, bv = h.w;
     const pt_face f = load_face(s, static_cast<uint32_t>(prim));
-    const f3 hp = ro + t * rd;
-    const float bw = 1.0f - bu - bv;
-    const f3 n = normalize(bw * vnrm(s, f.v0) + bu * vnrm(s, f.v1) + bv * vnrm(s, f.v2));
     const pt_material& m = s.materials[f.material_id];
-    bool entering = dot(n, rd) < 0.0f;
-    f3 gn;
-    if (m.double_sided && !entering) { gn = -n; entering = true; }
-    else gn = entering ? n : -n;
+    f3 hp, gn, N;
+    bool entering;
+    SurfaceAt g;
+    if (Textured) {
+        hp = hit_point(ro, rd, t);
+        surface_at<true>(s, f, m, bu, bv, rd, g);
+        gn = g.gn;
+        N = g.N;
+        entering = g.entering;
+    } else {
+        hp = ro + t * rd;
+        const float bw = 1.0f - bu - bv;
+        const f3 n = normalize(bw * vnrm(s, f.v0) + bu * vnrm(s, f.v1) + bv * vnrm(s, f.v2));
+        entering = dot(n, rd) < 0.0f;
+        if (m.double_sided && !entering) { gn = -n; entering = true; }
+        else gn = entering ? n : -n;
+        N = gn;   // no normal map without textures
+    }
     const f3 wo = -rd;
-    const f3 N = gn;   // no normal map without textures
     if (material_emits(m)) {
         float w = 1.0f;
         if (depth > 0 && !last_delta) w = power_heuristic(last_pdf, emissive_pdf(s, prim, t, rd));
         L += T * material_emission(m) * w;
         return 0;
     }
-    // alpha (path.cu:136-158); untextured: MASK alpha is 1, BLEND alpha is baseAlpha
+    // alpha (path.cu:136-158): MASK alpha is the base colour texture's alpha
+    // (else 1), BLEND alpha is baseAlpha times it; both looked up at the
+    // surface's own uv, without the material's uv transform, as the reference does
     if (m.alpha_mode == 1) {
-        if (1.0f < m.alpha_cutoff) { no = hp + rd * 1e-4f; nd = normalize(rd); return 2; }
+        float alpha = 1.0f;
+        if (Textured && tex_live(s, m.base_color_tex)) alpha = tex_at(s, m.base_color_tex, g.su, g.sv).w;
+        if (alpha < m.alpha_cutoff) { no = hp + rd * 1e-4f; nd = normalize(rd); return 2; }
     } else if (m.alpha_mode == 2) {
-        if (rng_next(rng) >= m.base_alpha) { no = hp + rd * 1e-4f; nd = normalize(rd); return 2; }
+        float alpha = m.base_alpha;
+        if (Textured && tex_live(s, m.base_color_tex)) alpha *= tex_at(s, m.base_color_tex, g.su, g.sv).w;
+        if (rng_next(rng) >= alpha) { no = hp + rd * 1e-4f; nd = normalize(rd); return 2; }
     }
-    const MatEval me = resolve_material(m);
+    const MatEval me = Textured ? resolve_material_textured(s, m, g.tu, g.tv) : resolve_material(m);
     const bool delta_surface = (me.metallic >= 1.0f && me.roughness < 0.01f) ||
                                (me.spec_trans >= 1.0f && me.roughness < 0.01f);
     // guided vertex: a mixture is available and no lobe can be a delta
@@ -502,6 +627,7 @@ __device__ int shade_front(const DeviceScene& s, int arg_rtl, int depth, f3 ro, 
     }
     sp.hp = hp;
     sp.gn = gn;
+    sp.N = N;
     sp.entering = entering;
     sp.me = me;
     sp.gmix = gmix;
@@ -515,7 +641,7 @@ template <bool Guided>
 __device__ bool shade_back(int arg_rtl, int depth, f3 rd, const ShadePoint& sp, f3& T, float& last_pdf,
                            bool& last_delta, PathRng& rng, f3& no, f3& nd, GuideVertex gv, float* rr_w) {
     const MatEval& me = sp.me;
-    const f3 hp = sp.hp, gn = sp.gn, N = sp.gn, wo = -rd;
+    const f3 hp = sp.hp, gn = sp.gn, N = sp.N, wo = -rd;
     const bool entering = sp.entering;
     const float* gmix = Guided ? sp.gmix : nullptr;
     BsdfSample bs;
@@ -636,7 +762,7 @@ __device__ __forceinline__ void push_continuation(const WaveParams& P, int q, bo
 // blocks of 128 per SM (80 registers): 224 ms against 243 ms at 5 blocks.
 constexpr uint32_t kEnteringBit = 0x40000000u;
 
-template <bool Guided>
+template <bool Guided, bool Textured = false>
 __global__ void __launch_bounds__(128, 6) k_shade_front(WaveParams P, int q, int depth, int s0) {
     const uint32_t cap = static_cast<uint32_t>(P.npath);
     const uint32_t n = min(P.counts[q], cap);
@@ -672,11 +798,15 @@ __global__ void __launch_bounds__(128, 6) k_shade_front(WaveParams P, int q, int
             }
         }
         ShadePoint sp;
-        const int r = shade_front<Guided>(P.scene, P.arg_rtl, depth, f3of(o4), f3of(d4), h, T, thr.w, lo.w != 0.0f,
-                                          L, rng, no, nd, sink, gv, sp);
+        const int r = shade_front<Guided, QueueSink, Textured>(P.scene, P.arg_rtl, depth, f3of(o4), f3of(d4), h, T,
+                                                               thr.w, lo.w != 0.0f, L, rng, no, nd, sink, gv, sp);
         P.lo[p] = f4of(L, lo.w);
         P.rng[p] = rng.s;
-        if (r == 1 && !last) {
+        if (Textured) {
+            // the back kernel recomputes the surface from the untouched hit and
+            // ray; a negative primitive tells it that this path needs no sampling
+            if (!(r == 1 && !last)) P.hit[i].y = __int_as_float(-1);
+        } else if (r == 1 && !last) {
             const uint32_t prim = static_cast<uint32_t>(__float_as_int(h.y));
             P.hit[i] = make_float4(sp.hp.x, sp.hp.y, sp.hp.z, __uint_as_float(prim | (sp.entering ? kEnteringBit : 0u)));
             P.ray_o[q][i] = make_float4(sp.gn.x, sp.gn.y, sp.gn.z, o4.w);
@@ -687,7 +817,7 @@ __global__ void __launch_bounds__(128, 6) k_shade_front(WaveParams P, int q, int
     }
 }
 
-template <bool Guided>
+template <bool Guided, bool Textured = false>
 __global__ void __launch_bounds__(128, 6) k_shade_back(WaveParams P, int q, int depth, int s0) {
     const uint32_t cap = static_cast<uint32_t>(P.npath);
     const uint32_t n = min(P.counts[q], cap);
@@ -695,7 +825,7 @@ __global__ void __launch_bounds__(128, 6) k_shade_back(WaveParams P, int q, int 
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const float4 h = P.hit[i];
-        const int code = __float_as_int(h.w);
+        const int code = Textured ? __float_as_int(h.y) : __float_as_int(h.w);
         bool cont = false;
         uint32_t p = 0;
         f3 no = mk(0.0f), nd = mk(0.0f);
@@ -711,11 +841,24 @@ __global__ void __launch_bounds__(128, 6) k_shade_back(WaveParams P, int q, int 
             bool last_delta = lo.w != 0.0f;
             PathRng rng = path_rng(P, p, sidx0);
             ShadePoint sp;
-            sp.hp = mk(h.x, h.y, h.z);
-            sp.gn = f3of(o4);
-            sp.entering = (static_cast<uint32_t>(code) & kEnteringBit) != 0u;
-            const pt_face f = load_face(P.scene, static_cast<uint32_t>(code) & ~kEnteringBit);
-            sp.me = resolve_material(P.scene.materials[f.material_id]);
+            if (Textured) {
+                const pt_face f = load_face(P.scene, static_cast<uint32_t>(code));
+                const pt_material& m = P.scene.materials[f.material_id];
+                SurfaceAt g;
+                surface_at<true>(P.scene, f, m, h.z, h.w, f3of(d4), g);
+                sp.hp = hit_point(f3of(o4), f3of(d4), h.x);
+                sp.gn = g.gn;
+                sp.N = g.N;
+                sp.entering = g.entering;
+                sp.me = resolve_material_textured(P.scene, m, g.tu, g.tv);
+            } else {
+                sp.hp = mk(h.x, h.y, h.z);
+                sp.gn = f3of(o4);
+                sp.N = sp.gn;
+                sp.entering = (static_cast<uint32_t>(code) & kEnteringBit) != 0u;
+                const pt_face f = load_face(P.scene, static_cast<uint32_t>(code) & ~kEnteringBit);
+                sp.me = resolve_material(P.scene.materials[f.material_id]);
+            }
             sp.gmix = (Guided && P.gmix && sp.me.roughness >= 0.01f) ? P.gmix + static_cast<size_t>(i) * kGMix
                                                                      : nullptr;
             GuideVertex gv{sp.gmix, nullptr, P.galpha};
@@ -1111,11 +1254,22 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
                     })) return rc;
             }
             if (int rc = timed(1, [&] {
-                    if (P.gmix) k_shade_front<true><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
-                    else k_shade_front<false><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                    const bool tex = P.scene.num_textures > 0;
+                    if (P.gmix) {
+                        if (tex) k_shade_front<true, true><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                        else k_shade_front<true><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                    } else {
+                        if (tex) k_shade_front<false, true><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                        else k_shade_front<false><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                    }
                     if (d + 1 < P.max_depth) {
-                        if (P.gmix) k_shade_back<true><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
-                        else k_shade_back<false><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                        if (P.gmix) {
+                            if (tex) k_shade_back<true, true><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                            else k_shade_back<true><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                        } else {
+                            if (tex) k_shade_back<false, true><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                            else k_shade_back<false><<<wf.grid_shade, 128, 0, st>>>(P, q, d, s0);
+                        }
                     }
                 })) return rc;
             if (int rc = timed(2, [&] { k_shadow<<<wf.grid_shadow, 128, 0, st>>>(P); })) return rc;
@@ -1174,6 +1328,8 @@ DeviceScene device_view(const pt_scene* s) {
     v.env_tex = d.env_tex;
     v.punctual = static_cast<const pt_punctual_light*>(d.punctual);
     v.num_punctual = static_cast<uint32_t>(s->host.punctual.size());
+    v.textures = static_cast<const unsigned long long*>(d.tex_table);
+    v.num_textures = d.tex_table ? static_cast<uint32_t>(d.tex_objs.size()) : 0u;
     return v;
 }
 
@@ -1182,6 +1338,9 @@ void free_scene_device(pt_scene* s) {
     if (d.device >= 0) cudaSetDevice(d.device);
     if (d.env_tex) cudaDestroyTextureObject(static_cast<cudaTextureObject_t>(d.env_tex));
     if (d.env_array) cudaFreeArray(static_cast<cudaArray_t>(d.env_array));
+    for (unsigned long long t : d.tex_objs) if (t) cudaDestroyTextureObject(static_cast<cudaTextureObject_t>(t));
+    for (void* a : d.tex_arrays) if (a) cudaFreeArray(static_cast<cudaArray_t>(a));
+    if (d.tex_table) cudaFree(d.tex_table);
     void* bufs[] = {d.inner, d.tris, d.vertices, d.faces, d.materials, d.emissive, d.tri_pmf,
                     d.tri_alias, d.env_pmf, d.env_alias, d.punctual};
     for (void* b : bufs) if (b) cudaFree(b);
@@ -1212,6 +1371,60 @@ static void pin_host_arrays(pt_scene* s) {
     pin(s->tables.env_alias.data(), s->tables.env_alias.size() * sizeof(pt_alias_entry));
 }
 
+// GL wrap mode -> CUDA address mode (CudaTexture, Part_2/src/cuda/cuda_texture.cu:27-34).
+static cudaTextureAddressMode gl_wrap_mode(int gl) {
+    if (gl == 33071) return cudaAddressModeClamp;    // CLAMP_TO_EDGE
+    if (gl == 33648) return cudaAddressModeMirror;   // MIRRORED_REPEAT
+    return cudaAddressModeWrap;                      // REPEAT and anything else
+}
+
+// Material textures as the reference's CudaTexture (cuda_texture.cu:37-62):
+// float4 arrays, bilinear filtering, normalized coordinates, the sampler's wrap
+// modes; a texture without an image gets no object (lookups skip it).
+static int upload_textures(const HostScene& h, DeviceSceneBuffers& d) {
+    const size_t nt = h.textures.size();
+    d.tex_arrays.assign(nt, nullptr);
+    d.tex_objs.assign(nt, 0ull);
+    d.tex_sizes.assign(nt, 0);
+    d.tex_wraps.assign(nt, 0);
+    if (nt == 0) return PT_OK;
+    for (size_t i = 0; i < nt; ++i) {
+        const HostTextureImage& t = h.textures[i];
+        if (t.width <= 0 || t.height <= 0 || t.rgba.size() != size_t(t.width) * t.height * 4) continue;
+        cudaChannelFormatDesc ch = cudaCreateChannelDesc<float4>();
+        cudaArray_t arr = nullptr;
+        if (cudaMallocArray(&arr, &ch, t.width, t.height) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("texture " + std::to_string(i) + ": cannot allocate " + std::to_string(t.width) + "x" +
+                      std::to_string(t.height));
+            return PT_ERR_NOMEM;
+        }
+        d.tex_arrays[i] = arr;
+        const size_t pitch = static_cast<size_t>(t.width) * 4 * sizeof(float);
+        PT_CU(cudaMemcpy2DToArray(arr, 0, 0, t.rgba.data(), pitch, pitch, t.height, cudaMemcpyHostToDevice));
+        cudaResourceDesc rd;
+        std::memset(&rd, 0, sizeof(rd));
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = arr;
+        cudaTextureDesc td;
+        std::memset(&td, 0, sizeof(td));
+        td.addressMode[0] = gl_wrap_mode(t.wrap_s);
+        td.addressMode[1] = gl_wrap_mode(t.wrap_t);
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 1;
+        cudaTextureObject_t tex = 0;
+        PT_CU(cudaCreateTextureObject(&tex, &rd, &td, nullptr));
+        d.tex_objs[i] = tex;
+        d.tex_sizes[i] = size_t(t.width) * t.height;
+        d.tex_wraps[i] = (t.wrap_s << 16) ^ t.wrap_t;
+        d.bytes += static_cast<uint64_t>(t.width) * t.height * 16;
+    }
+    PT_CU(cudaMalloc(&d.tex_table, nt * sizeof(unsigned long long)));
+    PT_CU(cudaMemcpy(d.tex_table, d.tex_objs.data(), nt * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    return PT_OK;
+}
+
 int upload_scene(pt_scene* s, int device) {
     if (!s->tables.built) { set_error("scene not built: call pt_scene_build_accel first"); return PT_ERR_STATE; }
     const HostScene& hs = s->host;
@@ -1230,8 +1443,15 @@ int upload_scene(pt_scene* s, int device) {
                               hs.punctual.size() * sizeof(pt_punctual_light)};
     // Same device and the same buffer sizes: copy into the existing buffers.
     // The device addresses stay, so a render graph captured for them stays valid.
-    bool same = d.uploaded && d.device == device && d.env_w == hs.env_w && d.env_h == hs.env_h;
+    bool same = d.uploaded && d.device == device && d.env_w == hs.env_w && d.env_h == hs.env_h &&
+                d.tex_objs.size() == hs.textures.size();
     for (int i = 0; i < 11 && same; ++i) same = d.sizes[i] == sizes[i];
+    for (size_t i = 0; i < hs.textures.size() && same; ++i) {
+        const HostTextureImage& t = hs.textures[i];
+        const bool has = t.width > 0 && t.height > 0 && t.rgba.size() == size_t(t.width) * t.height * 4;
+        same = has == (d.tex_objs[i] != 0) && (!has || (d.tex_sizes[i] == size_t(t.width) * t.height &&
+                                                         d.tex_wraps[i] == ((t.wrap_s << 16) ^ t.wrap_t)));
+    }
     if (same) {
         if (int rc = ensure_device(device)) return rc;
         pin_host_arrays(s);
@@ -1241,6 +1461,13 @@ int upload_scene(pt_scene* s, int device) {
             const size_t pitch = static_cast<size_t>(hs.env_w) * 4 * sizeof(float);
             PT_CU(cudaMemcpy2DToArray(static_cast<cudaArray_t>(d.env_array), 0, 0, hs.env_rgba.data(), pitch, pitch,
                                       hs.env_h, cudaMemcpyHostToDevice));
+        }
+        for (size_t i = 0; i < hs.textures.size(); ++i) {
+            const HostTextureImage& t = hs.textures[i];
+            if (!d.tex_arrays[i]) continue;
+            const size_t pitch = static_cast<size_t>(t.width) * 4 * sizeof(float);
+            PT_CU(cudaMemcpy2DToArray(static_cast<cudaArray_t>(d.tex_arrays[i]), 0, 0, t.rgba.data(), pitch, pitch,
+                                      t.height, cudaMemcpyHostToDevice));
         }
         return PT_OK;
     }
@@ -1301,6 +1528,7 @@ int upload_scene(pt_scene* s, int device) {
         d.env_tex = tex;
         d.bytes += static_cast<uint64_t>(h.env_w) * h.env_h * 16;
     }
+    if (int rc2 = upload_textures(h, d)) return rc2;
     d.uploaded = true;
     return PT_OK;
 }

@@ -187,6 +187,9 @@ struct DeviceScene {
     unsigned long long     env_tex;         // cudaTextureObject_t (0 = none)
     const pt_punctual_light* punctual;
     uint32_t               num_punctual;
+    // material textures (float4, bilinear, normalized coordinates)
+    const unsigned long long* textures;     // cudaTextureObject_t per texture (0 = no image)
+    uint32_t               num_textures;
 };
 
 // Ray as stored in queues: origin (w unused) and direction (w = tmax for shadow rays).

@@ -25,6 +25,7 @@
 #include <unordered_map>
 
 #include "engine.h"
+#include "image_decode.h"
 
 namespace ptb {
 
@@ -621,8 +622,9 @@ bool load_obj(const std::string& path, int mat, const float xform[16],
 // specular, volume and anisotropy extensions and the alpha mode
 // (loadMaterials, gltf_loader.cpp:172-347); KHR_lights_punctual lights sit at
 // their node's origin looking down its -z.  Vertex attributes must be FLOAT
-// (the reference reads them as floats).  Files with textures or images are
-// rejected: this library has no image decoder and samples no textures.
+// (the reference reads them as floats).  Textures: the images (PNG or
+// baseline JPEG, decoded by image_decode.cpp) with their samplers' wrap
+// modes, and the materials' texture indices and KHR_texture_transform.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -706,8 +708,6 @@ GltfDoc read_gltf(const std::string& path) {
     }
     d.root = json::Parser(text).parse();
     if (d.root.kind != json::Value::Obj) throw json::Error{"glTF root must be an object"};
-    if ((d.root.has("images") && d.root["images"].size()) || (d.root.has("textures") && d.root["textures"].size()))
-        throw json::Error{"glTF textures are not supported (no image decoder in this library)"};
     if (d.root.has("buffers")) {
         const json::Value& bs = d.root["buffers"];
         d.owned.reserve(bs.size());
@@ -812,7 +812,84 @@ M4 gltf_node_transform(const json::Value& n) {
     return m4_mul(m4_mul(T, R), S);
 }
 
-void gltf_materials(const GltfDoc& d, std::vector<pt_material>& out, std::vector<std::string>& names) {
+// Texture index of a textureInfo object (index + the scene's texture offset), else -1.
+int gltf_tex_index(const json::Value& o, const char* key, int tex_offset) {
+    if (!o.has(key)) return -1;
+    const json::Value& info = o[key];
+    if (!info.has("index")) return -1;
+    const int i = json::as_int(info["index"]);
+    return i >= 0 ? i + tex_offset : -1;
+}
+
+// glTF textures (loadTextures, gltf_loader.cpp:112-147): each texture's image
+// (a bufferView, a data: URI or a file beside the glTF) decoded to 8-bit RGBA
+// and stored as value / 255, with its sampler's wrap modes; a texture without
+// a source image stays empty.
+void gltf_textures(const GltfDoc& d, const std::string& path, std::vector<HostTextureImage>& out) {
+    if (!d.root.has("textures")) return;
+    const json::Value& ts = d.root["textures"];
+    const size_t n_images = d.root.has("images") ? d.root["images"].size() : 0;
+    std::vector<DecodedImage> decoded(n_images);
+    std::vector<bool> done(n_images, false);
+    for (size_t i = 0; i < ts.size(); ++i) {
+        const json::Value& t = ts[i];
+        HostTextureImage img;
+        const int src = get_int(t, "source", -1);
+        if (src >= 0 && static_cast<size_t>(src) < n_images) {
+            if (!done[src]) {
+                const json::Value& im = d.root["images"][static_cast<size_t>(src)];
+                std::string owned;
+                const uint8_t* bytes = nullptr;
+                size_t size = 0;
+                if (im.has("bufferView")) {
+                    const int bvi = json::as_int(im["bufferView"]);
+                    const json::Value& bvs = d.root["bufferViews"];
+                    if (bvi < 0 || static_cast<size_t>(bvi) >= bvs.size()) throw json::Error{"image bufferView out of range"};
+                    const json::Value& bv = bvs[static_cast<size_t>(bvi)];
+                    const int bi = json::as_int(bv["buffer"]);
+                    if (bi < 0 || static_cast<size_t>(bi) >= d.buffers.size()) throw json::Error{"image buffer out of range"};
+                    const size_t off = static_cast<size_t>(get_int(bv, "byteOffset", 0));
+                    const size_t len = static_cast<size_t>(json::as_int(bv["byteLength"]));
+                    if (off + len > d.buffers[bi].size) throw json::Error{"image bufferView beyond its buffer"};
+                    bytes = reinterpret_cast<const uint8_t*>(d.buffers[bi].data) + off;
+                    size = len;
+                } else if (im.has("uri")) {
+                    const std::string& uri = json::as_string(im["uri"]);
+                    if (uri.compare(0, 5, "data:") == 0) {
+                        const size_t comma = uri.find(',');
+                        if (comma == std::string::npos) throw json::Error{"bad image data URI"};
+                        owned = base64_decode(uri, comma + 1);
+                    } else {
+                        owned = read_binary_file(resolve_relative(path, uri));
+                    }
+                    bytes = reinterpret_cast<const uint8_t*>(owned.data());
+                    size = owned.size();
+                } else {
+                    throw json::Error{"image " + std::to_string(src) + " has neither a bufferView nor a uri"};
+                }
+                std::string err;
+                if (!decode_image(bytes, size, decoded[src], err))
+                    throw json::Error{"image " + std::to_string(src) + ": " + err};
+                done[src] = true;
+            }
+            const DecodedImage& di = decoded[src];
+            img.width = di.width;
+            img.height = di.height;
+            img.rgba.resize(di.rgba.size());
+            for (size_t k = 0; k < di.rgba.size(); ++k) img.rgba[k] = static_cast<float>(di.rgba[k]) / 255.0f;
+        }
+        const int smp = get_int(t, "sampler", -1);
+        if (smp >= 0 && d.root.has("samplers") && static_cast<size_t>(smp) < d.root["samplers"].size()) {
+            const json::Value& sm = d.root["samplers"][static_cast<size_t>(smp)];
+            img.wrap_s = get_int(sm, "wrapS", 10497);
+            img.wrap_t = get_int(sm, "wrapT", 10497);
+        }
+        out.push_back(std::move(img));
+    }
+}
+
+void gltf_materials(const GltfDoc& d, std::vector<pt_material>& out, std::vector<std::string>& names,
+                    int tex_offset) {
     if (!d.root.has("materials")) return;
     const json::Value& ms = d.root["materials"];
     for (size_t i = 0; i < ms.size(); ++i) {
@@ -828,7 +905,28 @@ void gltf_materials(const GltfDoc& d, std::vector<pt_material>& out, std::vector
                 for (size_t k = 0; k < 4 && k < p["baseColorFactor"].size(); ++k) bc[k] = json::as_float(p["baseColorFactor"][k]);
             metallic = get_num(p, "metallicFactor", 1.0f);
             roughness = get_num(p, "roughnessFactor", 1.0f);
+            m.base_color_tex = gltf_tex_index(p, "baseColorTexture", tex_offset);
+            if (m.base_color_tex >= 0 && p["baseColorTexture"].has("extensions") &&
+                p["baseColorTexture"]["extensions"].has("KHR_texture_transform")) {
+                // readTextureTransform (gltf_loader.cpp:158-170)
+                const json::Value& tt = p["baseColorTexture"]["extensions"]["KHR_texture_transform"];
+                if (tt.has("offset") && tt["offset"].size() >= 2) {
+                    m.uv_offset_x = json::as_float(tt["offset"][0]);
+                    m.uv_offset_y = json::as_float(tt["offset"][1]);
+                }
+                if (tt.has("scale") && tt["scale"].size() >= 2) {
+                    m.uv_scale_x = json::as_float(tt["scale"][0]);
+                    m.uv_scale_y = json::as_float(tt["scale"][1]);
+                }
+                if (tt.has("rotation")) m.uv_rotation = json::as_float(tt["rotation"]);
+            }
+            m.metallic_roughness_tex = gltf_tex_index(p, "metallicRoughnessTexture", tex_offset);
         }
+        m.normal_tex = gltf_tex_index(g, "normalTexture", tex_offset);
+        if (m.normal_tex >= 0) m.normal_scale = get_num(g["normalTexture"], "scale", 1.0f);
+        m.emissive_tex = gltf_tex_index(g, "emissiveTexture", tex_offset);
+        m.occlusion_tex = gltf_tex_index(g, "occlusionTexture", tex_offset);
+        if (m.occlusion_tex >= 0) m.occlusion_strength = get_num(g["occlusionTexture"], "strength", 1.0f);
         m.base_color[0] = bc[0]; m.base_color[1] = bc[1]; m.base_color[2] = bc[2];
         m.base_alpha = bc[3];
         m.metallic = metallic;
@@ -846,12 +944,17 @@ void gltf_materials(const GltfDoc& d, std::vector<pt_material>& out, std::vector
                 if (e->has("emissiveStrength")) m.emissive_strength = json::as_float((*e)["emissiveStrength"]);
             if (const json::Value* e = ext("KHR_materials_ior"))
                 if (e->has("ior")) m.ior = json::as_float((*e)["ior"]);
-            if (const json::Value* e = ext("KHR_materials_transmission"))
+            if (const json::Value* e = ext("KHR_materials_transmission")) {
                 if (e->has("transmissionFactor")) m.spec_trans = json::as_float((*e)["transmissionFactor"]);
+                m.transmission_tex = gltf_tex_index(*e, "transmissionTexture", tex_offset);
+            }
             if (const json::Value* e = ext("KHR_materials_clearcoat")) {
                 if (e->has("clearcoatFactor")) m.clearcoat = json::as_float((*e)["clearcoatFactor"]);
                 if (e->has("clearcoatRoughnessFactor"))
                     m.clearcoat_roughness = json::as_float((*e)["clearcoatRoughnessFactor"]);
+                m.clearcoat_tex = gltf_tex_index(*e, "clearcoatTexture", tex_offset);
+                m.clearcoat_roughness_tex = gltf_tex_index(*e, "clearcoatRoughnessTexture", tex_offset);
+                m.clearcoat_normal_tex = gltf_tex_index(*e, "clearcoatNormalTexture", tex_offset);
             }
             if (const json::Value* e = ext("KHR_materials_sheen")) {
                 if (e->has("sheenRoughnessFactor")) m.sheen = json::as_float((*e)["sheenRoughnessFactor"]);
@@ -860,6 +963,8 @@ void gltf_materials(const GltfDoc& d, std::vector<pt_material>& out, std::vector
                     m.sheen_color_r = json::as_float(c[0]); m.sheen_color_g = json::as_float(c[1]);
                     m.sheen_color_b = json::as_float(c[2]);
                 }
+                m.sheen_color_tex = gltf_tex_index(*e, "sheenColorTexture", tex_offset);
+                m.sheen_roughness_tex = gltf_tex_index(*e, "sheenRoughnessTexture", tex_offset);
             }
             if (const json::Value* e = ext("KHR_materials_specular")) {
                 if (e->has("specularFactor")) m.specular_factor = json::as_float((*e)["specularFactor"]);
@@ -1049,8 +1154,10 @@ void gltf_nodes(const GltfDoc& d, int idx, const M4& parent, int mat_offset, con
 std::vector<std::string> load_gltf(const std::string& path, HostScene& hs, const GltfOptions& opt) {
     const GltfDoc d = read_gltf(path);
     const int mat_offset = static_cast<int>(hs.materials.size());
+    const int tex_offset = static_cast<int>(hs.textures.size());
+    gltf_textures(d, path, hs.textures);
     std::vector<std::string> names;
-    gltf_materials(d, hs.materials, names);
+    gltf_materials(d, hs.materials, names, tex_offset);
     if (hs.materials.empty()) hs.materials.push_back(default_material());
     std::vector<GltfLight> lights;
     if (d.root.has("extensions") && d.root["extensions"].has("KHR_lights_punctual") &&

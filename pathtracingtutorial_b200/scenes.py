@@ -37,11 +37,15 @@ class SceneArrays:
     sampler: int = SAMPLER_SOBOL
     pcg_seed: int = 0
     meta: dict = field(default_factory=dict)
+    # material textures: [{"rgba": (H, W, 4) float32 texels, "wrap_s": GL mode, "wrap_t": GL mode}]
+    textures: list = field(default_factory=list)
 
     def scene(self):
         """A SceneManager with these arrays and render settings (not yet built)."""
         from . import SceneManager
         s = SceneManager.from_arrays(self.vertices, self.faces, self.materials, self.camera, self.env)
+        for t in self.textures:
+            s.add_texture(t["rgba"], t.get("wrap_s", 10497), t.get("wrap_t", 10497))
         s.update_settings(spp=self.spp, sample_per_frame=self.sample_per_frame, max_depth=self.max_depth,
                           sampler_type=self.sampler, pcg_seed=self.pcg_seed)
         return s
@@ -187,6 +191,82 @@ def cornell_box(width: int = 512, height: int = 512, spp: int = 64, max_depth: i
     return SceneArrays("cornell_box_36tri", v, f, mats, cam, None, spp=spp, sample_per_frame=4,
                        max_depth=max_depth, sampler=SAMPLER_PCG, pcg_seed=pcg_seed,
                        meta={"triangles": 36})
+
+
+# ---------------------------------------------------------------------------
+# Textured Cornell box
+# ---------------------------------------------------------------------------
+def procedural_textures(seed: int = 5, size: int = 64):
+    """Four material textures as float RGBA arrays (glTF texels are 8-bit
+    values / 255): a coloured checker whose alpha holds a disc cut-out
+    (REPEAT), a metallic-roughness map (G roughness, B metallic; CLAMP), a
+    tangent-space bump normal map (REPEAT) and a value-noise map used for the
+    clearcoat, transmission and sheen channels (MIRRORED_REPEAT)."""
+    rng = np.random.default_rng(seed)
+    n = size
+    y, x = (np.mgrid[0:n, 0:n] + 0.5) / n
+    chk = ((np.floor(x * 8) + np.floor(y * 8)) % 2)[..., None]
+    col = np.where(chk > 0, np.array([0.85, 0.75, 0.3]), np.array([0.2, 0.45, 0.8]))
+    alpha = (((x - 0.5) ** 2 + (y - 0.5) ** 2) > 0.12).astype(np.float64)
+    base = np.concatenate([col, alpha[..., None]], -1)
+    mr = np.stack([np.zeros_like(x), 0.2 + 0.8 * x, (y > 0.5).astype(np.float64), np.ones_like(x)], -1)
+    hx, hy = np.sin(x * 6 * np.pi), np.sin(y * 6 * np.pi)
+    nrm = np.stack([-0.4 * np.cos(x * 6 * np.pi) * hy, -0.4 * hx * np.cos(y * 6 * np.pi), np.ones_like(x)], -1)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    nmap = np.concatenate([0.5 * (nrm + 1.0), np.ones_like(x)[..., None]], -1)
+    noise = rng.uniform(0, 1, (n // 8 + 1, n // 8 + 1))
+    noise = np.kron(noise, np.ones((8, 8)))[:n, :n]
+    misc = np.stack([noise, 1.0 - noise, 0.5 * noise + 0.25, noise], -1)
+
+    def q8(a):   # 8-bit texels as glTF images store them
+        return (np.round(np.clip(a, 0, 1) * 255.0) / 255.0).astype(np.float32)
+    return [{"rgba": q8(base), "wrap_s": 10497, "wrap_t": 10497},
+            {"rgba": q8(mr), "wrap_s": 33071, "wrap_t": 33071},
+            {"rgba": q8(nmap), "wrap_s": 10497, "wrap_t": 10497},
+            {"rgba": q8(misc), "wrap_s": 33648, "wrap_t": 33648}]
+
+
+def textured_cornell(width: int = 128, height: int = 128, spp: int = 16, max_depth: int = 8,
+                     sampler: int = SAMPLER_PCG, pcg_seed: int = 1) -> SceneArrays:
+    """The Cornell box with material textures on every path of the textured
+    shading: a checker base colour on the floor (KHR_texture_transform scale,
+    rotation and offset), a normal map and metallic-roughness map on the back
+    wall, clearcoat / sheen / transmission maps on the short box, an
+    alpha-MASK cut-out panel and an alpha-BLEND panel (baseAlpha 0.6 times the
+    texture's alpha) standing in the room."""
+    sa = cornell_box(width=width, height=height, spp=spp, max_depth=max_depth, pcg_seed=pcg_seed)
+    sa.sampler = sampler
+    mats = list(sa.materials)
+    floor = default_material(base_color=(0.9, 0.9, 0.9), roughness=0.8, base_color_tex=0,
+                             uv_scale_x=3.0, uv_scale_y=2.0, uv_rotation=0.35, uv_offset_x=0.1)
+    back = default_material(base_color=(0.8, 0.8, 0.8), roughness=1.0, metallic=1.0, normal_tex=2,
+                            normal_scale=1.5, metallic_roughness_tex=1)
+    short_box = default_material(base_color=(0.7, 0.6, 0.5), roughness=0.4, clearcoat=1.0, clearcoat_tex=3,
+                                 clearcoat_roughness=0.5, clearcoat_roughness_tex=3, sheen=1.0, sheen_roughness_tex=3,
+                                 sheen_color_tex=0, spec_trans=0.5, transmission_tex=3)
+    mask = default_material(base_color=(0.9, 0.3, 0.3), roughness=0.6, base_color_tex=0, alpha_mode=1,
+                            alpha_cutoff=0.5, double_sided=1)
+    blend = default_material(base_color=(0.3, 0.9, 0.4), roughness=0.5, base_color_tex=0, alpha_mode=2,
+                             base_alpha=0.6, double_sided=1)
+    first = len(mats)
+    mats += [floor, back, short_box, mask, blend]
+    m = _materials(mats)
+    f = sa.faces.copy()
+    f["material_id"][0:2] = first          # floor
+    f["material_id"][4:6] = first + 1      # back wall
+    f["material_id"][22:34] = first + 2    # short box (the second box)
+    b = _Builder()
+    b.add(quad((-0.35, 0.05, 0.25), (-0.05, 0.05, 0.25), (-0.05, 0.45, 0.25), (-0.35, 0.45, 0.25), first + 3))
+    b.add(quad((0.05, 0.35, 0.3), (0.4, 0.35, 0.3), (0.4, 0.7, 0.3), (0.05, 0.7, 0.3), first + 4))
+    pv, pf = b.arrays()
+    pf["v0"] += len(sa.vertices); pf["v1"] += len(sa.vertices); pf["v2"] += len(sa.vertices)
+    sa.vertices = np.concatenate([sa.vertices, pv])
+    sa.faces = np.concatenate([f, pf])
+    sa.materials = m
+    sa.textures = procedural_textures()
+    sa.name = f"textured_cornell_{len(sa.faces)}tri"
+    sa.meta = {"triangles": int(len(sa.faces)), "textures": len(sa.textures)}
+    return sa
 
 
 # ---------------------------------------------------------------------------

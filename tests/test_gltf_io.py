@@ -227,7 +227,9 @@ def test_gltf_scene_renders_after_device_and_host_builds(tmp_path):
     assert s.info()["num_faces"] == 4 + 3 + 1 + 1
 
 
-def test_gltf_with_textures_is_rejected(tmp_path):
+def test_gltf_with_a_missing_image_file_is_an_error(tmp_path):
+    """Textures load (tests/test_textures.py); an image file that is not
+    there fails the load with the file named."""
     g, blob = _gltf()
     g["images"] = [{"uri": "x.png"}]
     g["textures"] = [{"source": 0}]
@@ -235,7 +237,7 @@ def test_gltf_with_textures_is_rejected(tmp_path):
     g["buffers"][0]["uri"] = "m.bin"
     p = tmp_path / "t.gltf"
     p.write_text(json.dumps(g))
-    with pytest.raises(pt.PTError, match="textures"):
+    with pytest.raises(pt.PTError, match="x.png"):
         pt.SceneManager.load(str(p))
 
 
