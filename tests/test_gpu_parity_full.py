@@ -93,7 +93,7 @@ def test_cornell_full_config_per_pixel_noise_bound(oracle):
     frac_fail = 1.0 - float(pix_ok.mean())
     print(f"per-pixel 4-sigma bound: {frac_fail * 100:.4f} % of {pix_ok.size} pixels outside")
     assert frac_fail <= 1e-3, frac_fail
-    assert (m_o.sum(-1) > 0).mean() > 0.9 and np.median(sigma) > 0
+    assert (m_o.sum(-1) > 0).mean() > 0.8 and np.median(sigma) > 0
 
 
 # ---------------------------------------------------------------------------
