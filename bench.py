@@ -53,7 +53,9 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true",
                    help="skip the CPU baseline leg (profiling runs; the line then carries cpu_baseline null)")
     p.add_argument("--paths-in-flight", type=int, default=0,
-                   help="wavefront path slots of the render (0: the library default)")
+                   help="wavefront path slots of the render (0: the autotuner's choice)")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="render with the library defaults instead of the autotuner's choice")
     p.add_argument("--workload", choices=["render", "batch", "large", "build"], default="render",
                    help="render: the bench line; batch: the 64-scene uneven batch in one launch; large: the "
                         "20M-triangle 16-camera case; build: host vs GPU BVH build of the bench scene "
@@ -359,6 +361,21 @@ def convergence(local: int, stream, small: bool, plain_cap: int = 8192, guided_c
     rg.render_frames(train_spp // spf)
     sync()
     train_ms = (time.perf_counter() - t0) * 1e3
+    # stage breakdown of one chunk of each arm (CUDA events around every launch;
+    # a separate, untimed render)
+    breakdown = {}
+    for arm, mode in (("plain", pt.Guide.OFF), ("guided", pt.Guide.USE)):
+        g.attach(rg.integrator, mode)
+        scene.update_settings(flags=pt.FLAG_STAGE_TIMING | pt.FLAG_NO_GRAPH)
+        rg.integrator.reset_stats()
+        rg.reset_accumulation()
+        scene.set_frame_count(300_000)
+        rg.render_frames(chunk // spf)
+        sync()
+        st = rg.integrator.stats()
+        breakdown[arm] = {k: round(st[k], 2) for k in ("extend_ms", "shade_ms", "shadow_ms", "guide_ms", "other_ms")}
+        breakdown[arm]["rays"] = int(st["camera_rays"] + st["extension_rays"] + st["shadow_rays"])
+        scene.update_settings(flags=0)
     g.attach(rg.integrator, pt.Guide.OFF)
     rg.integrator.close()
     rg.film.close()
@@ -401,7 +418,8 @@ def convergence(local: int, stream, small: bool, plain_cap: int = 8192, guided_c
             "noise_corrected_time_ms": {"plain": None if tpc is None else round(tpc, 1),
                                         "guided": None if tgc is None else round(tgc, 1)},
             "guided_speedup": None if (tp is None or tg is None) else round(tp / tg, 3),
-            "target_speedup": 3.0}
+            "target_speedup": 3.0,
+            "stage_ms_per_chunk": breakdown}
 
 
 def build_leg(sa):
@@ -445,10 +463,15 @@ def ours(args):
     sa = workload(args.small)
     spp = args.spp
     scene = sa.scene()
-    if args.paths_in_flight > 0:
-        scene.update_settings(paths_in_flight=args.paths_in_flight)
     scene.build_accel()
     scene.upload_to_device(local)
+    # the library's autotuner picks the traversal shape and queue capacity
+    # (untimed; cached per device and scene class), unless fixed by the caller
+    tuned = None
+    if args.paths_in_flight > 0:
+        scene.update_settings(paths_in_flight=args.paths_in_flight)
+    elif not args.no_autotune:
+        tuned = scene.autotune()
     spf = sa.sample_per_frame
     batches = (spp + spf - 1) // spf
     stream = torch.cuda.Stream(device=local)
@@ -545,7 +568,11 @@ def ours(args):
         "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": config_of(sa, spp),
+        "config": dict(config_of(sa, spp), launch={
+            "paths_in_flight": scene.settings().paths_in_flight, "trace_block": scene.settings().trace_block,
+            "stack_depth": scene.settings().stack_depth,
+            "autotune": None if tuned is None else {k: tuned[k] for k in ("calib_spp", "best_ms", "default_ms",
+                                                                         "candidates")}}),
         "rays_per_step": total_rays / args.steps / world,
         "ray_classes": {"camera": st["camera_rays"] // args.steps, "extension": st["extension_rays"] // args.steps,
                         "shadow": st["shadow_rays"] // args.steps},

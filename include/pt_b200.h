@@ -153,6 +153,12 @@ typedef struct pt_render_settings {
     int32_t  paths_in_flight;   /* added: wavefront path slots (0 = 2^27); samples of a
                                    frame run concurrently while they fit.  Results do
                                    not depend on it. */
+    int32_t  trace_block;       /* added: threads per block of the traversal kernels,
+                                   64, 128 or 256 (0 = 128) */
+    int32_t  stack_depth;       /* added: traversal stack entries, 32 or 64 (0 = 64); a
+                                   value not above the tree's depth is raised to 64.
+                                   pt_autotune sets these three.  Results do not
+                                   depend on them. */
 } pt_render_settings;
 
 typedef struct pt_scene_info {
@@ -175,6 +181,7 @@ typedef struct pt_render_stats {
     double   extend_ms, shade_ms, shadow_ms, other_ms;   /* with PT_FLAG_STAGE_TIMING */
     double   total_ms;
     uint64_t kernel_launches;                            /* this library's kernels launched */
+    double   guide_ms;          /* guiding network (inference, training) with PT_FLAG_STAGE_TIMING */
 } pt_render_stats;
 
 typedef struct pt_hit {
@@ -342,6 +349,34 @@ int pt_scene_set_frame_count(pt_scene* scene, uint32_t frame_count);
  * concurrent pt_render calls are serialised. */
 int pt_render(pt_scene* scene, int32_t spp, float* out_rgba, int32_t out_is_device,
               pt_render_stats* stats);
+
+/* ---- autotuner (no reference counterpart: the reference has fixed launch
+ *      shapes).  Times calibration renders of the scene (the pt_render path,
+ *      the scene's own settings otherwise) and picks, by coordinate descent,
+ *      the traversal stack depth (64, and 32 when the tree is shallower), the
+ *      traversal kernels' block size (64, 128, 256) and the wavefront's queue
+ *      capacity (paths in flight: 2^24 .. 2^27, as the device holds them).
+ *      The choice is written into the scene's render settings (trace_block,
+ *      stack_depth, paths_in_flight), so pt_render and pt_render_batch use it,
+ *      and cached per device and scene class (triangles, pixels and depth,
+ *      each by its power of two; sampler; environment; textures): a later
+ *      call for a scene of the same class applies it without timing
+ *      (cached = 1).  calib_spp: samples per pixel of a calibration render
+ *      (0: enough to fill the largest queue once, at most 256).  Images do not
+ *      depend on any of the tuned values. */
+#define PT_TUNE_MAX_CANDIDATES 16
+typedef struct pt_tune_report {
+    int32_t paths_in_flight, trace_block, stack_depth;   /* the choice            */
+    int32_t cached;                                      /* 1: from the cache      */
+    int32_t calib_spp;                                   /* per calibration render */
+    int32_t candidates;                                  /* configurations timed   */
+    float   best_ms, default_ms;                         /* the choice, the defaults */
+    int32_t cand_paths[PT_TUNE_MAX_CANDIDATES];
+    int32_t cand_block[PT_TUNE_MAX_CANDIDATES];
+    int32_t cand_depth[PT_TUNE_MAX_CANDIDATES];
+    float   cand_ms[PT_TUNE_MAX_CANDIDATES];
+} pt_tune_report;
+int pt_autotune(pt_scene* scene, int32_t calib_spp, pt_tune_report* report);
 
 /* ---- batched rendering (no reference counterpart: the reference renders one
  *      scene per process).  Many scenes of uneven size and sample budget are

@@ -210,6 +210,14 @@ class SceneManager:
         check(lib().pt_scene_build_accel_device(self._h, device, C.byref(opt), C.byref(st)))
         return st.as_dict()
 
+    def autotune(self, calib_spp: int = 0) -> dict:
+        """pt_autotune: time calibration renders and keep the fastest traversal
+        stack depth, traversal block size and queue capacity in this scene's
+        settings (cached per device and scene class).  Returns the report."""
+        r = _ffi.TuneReport()
+        check(lib().pt_autotune(self._h, int(calib_spp), C.byref(r)))
+        return r.as_dict()
+
     def upload_to_device(self, device: int = 0) -> None:
         check(lib().pt_scene_upload(self._h, device))
 

@@ -70,7 +70,8 @@ class SceneParams(C.Structure):
 class RenderSettings(C.Structure):
     _fields_ = [("spp", C.c_int32), ("sample_per_frame", C.c_int32), ("max_depth", C.c_int32),
                 ("sampler_type", C.c_int32), ("pcg_seed", C.c_uint32), ("arg_order", C.c_int32),
-                ("flags", C.c_int32), ("paths_in_flight", C.c_int32)]
+                ("flags", C.c_int32), ("paths_in_flight", C.c_int32), ("trace_block", C.c_int32),
+                ("stack_depth", C.c_int32)]
 
 
 class BuildOptions(C.Structure):
@@ -100,13 +101,31 @@ class SceneInfo(C.Structure):
                 ("_pad", C.c_uint32)]
 
 
+class TuneReport(C.Structure):
+    _fields_ = [("paths_in_flight", C.c_int32), ("trace_block", C.c_int32), ("stack_depth", C.c_int32),
+                ("cached", C.c_int32), ("calib_spp", C.c_int32), ("candidates", C.c_int32),
+                ("best_ms", C.c_float), ("default_ms", C.c_float),
+                ("cand_paths", C.c_int32 * 16), ("cand_block", C.c_int32 * 16), ("cand_depth", C.c_int32 * 16),
+                ("cand_ms", C.c_float * 16)]
+
+    def as_dict(self) -> dict:
+        n = self.candidates
+        return {"paths_in_flight": self.paths_in_flight, "trace_block": self.trace_block,
+                "stack_depth": self.stack_depth, "cached": bool(self.cached), "calib_spp": self.calib_spp,
+                "best_ms": self.best_ms, "default_ms": self.default_ms,
+                "candidates": [{"paths_in_flight": self.cand_paths[k], "trace_block": self.cand_block[k],
+                                "stack_depth": self.cand_depth[k], "ms": round(self.cand_ms[k], 2)}
+                               for k in range(n)]}
+
+
 class RenderStats(C.Structure):
     _fields_ = [("camera_rays", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("node_visits", C.c_uint64), ("triangle_tests", C.c_uint64),
                 ("shadow_node_visits", C.c_uint64), ("shadow_triangle_tests", C.c_uint64),
                 ("paths", C.c_uint64), ("extend_launches", C.c_uint64),
                 ("extend_ms", C.c_double), ("shade_ms", C.c_double), ("shadow_ms", C.c_double),
-                ("other_ms", C.c_double), ("total_ms", C.c_double), ("kernel_launches", C.c_uint64)]
+                ("other_ms", C.c_double), ("total_ms", C.c_double), ("kernel_launches", C.c_uint64),
+                ("guide_ms", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -180,6 +199,7 @@ _SIGS = [
     ("pt_scene_set_frame_count", C.c_int, [_P, C.c_uint32]),
     ("pt_render", C.c_int, [_P, C.c_int32, _P, C.c_int32, C.POINTER(RenderStats)]),
     ("pt_render_batch", C.c_int, [_P, C.c_uint32, C.c_int32, C.POINTER(BatchConfig), C.POINTER(RenderStats)]),
+    ("pt_autotune", C.c_int, [_P, C.c_int32, C.POINTER(TuneReport)]),
     ("pt_guide_create", C.c_int, [_P, C.c_uint32, C.POINTER(_P)]),
     ("pt_guide_destroy", C.c_int, [_P]),
     ("pt_guide_set_learning_rate", C.c_int, [_P, C.c_float]),

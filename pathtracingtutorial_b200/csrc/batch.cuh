@@ -418,7 +418,9 @@ int batch_wavefront(const pt_batch_item* in, uint32_t n, int out_is_device, int6
     return PT_OK;
 }
 
-struct BatchTune { int block, blocks_per_sm, chunk_spp; double ms; int mode; };
+// The autotuner's choice for a batch class: the persistent kernel's block size
+// and blocks per SM, or wavefront mode with its queue capacity (paths).
+struct BatchTune { int block, blocks_per_sm, chunk_spp; double ms; int mode; int64_t paths; };
 std::mutex g_tune_mu;
 std::vector<std::pair<std::string, BatchTune>> g_tune_cache;
 
@@ -492,22 +494,25 @@ int render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batc
         req_mode = PT_BATCH_WAVEFRONT;
     }
     const int64_t budget = cfg && cfg->paths_in_flight > 0 ? cfg->paths_in_flight : kDefaultPathsInFlight;
-    auto run_wavefront = [&](float tuned_ms) -> int {
+    auto run_wavefront = [&](float tuned_ms, int64_t paths) -> int {
         float ms = 0.0f;
-        if (int rc = batch_wavefront(in, n, out_is_device, budget, true, st, &ms, stats)) return rc;
+        if (int rc = batch_wavefront(in, n, out_is_device, paths, true, st, &ms, stats)) return rc;
         if (cfg) {
             cfg->mode = PT_BATCH_WAVEFRONT;
-            cfg->paths_in_flight = static_cast<int32_t>(budget);
+            cfg->paths_in_flight = static_cast<int32_t>(paths);
             cfg->tuned_ms = tuned_ms;
         }
         return PT_OK;
     };
-    if (req_mode == PT_BATCH_WAVEFRONT) return run_wavefront(0.0f);
+    if (req_mode == PT_BATCH_WAVEFRONT) return run_wavefront(0.0f, budget);
 
     // ---- pick the mode and launch shape (autotuner) ----
+    // work units of the persistent kernel: chunk_spp samples of an item's
+    // pixels (16 unless fixed in cfg; the calibration batch caps every item at
+    // 8 spp, so the unit size is not among the timed candidates)
     BatchTune tune{cfg && cfg->block_size ? cfg->block_size : 128,
                    cfg && cfg->blocks_per_sm ? cfg->blocks_per_sm : 0,
-                   cfg && cfg->chunk_spp ? cfg->chunk_spp : 8, 0.0, PT_BATCH_PERSISTENT};
+                   cfg && cfg->chunk_spp ? cfg->chunk_spp : 16, 0.0, PT_BATCH_PERSISTENT, budget};
     const bool autotune = !cfg || cfg->autotune;
     const std::string key = tune_key(device, in, n) + ":" + std::to_string(req_mode);
     bool cached = false;
@@ -520,7 +525,7 @@ int render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batc
         std::vector<BatchTune> cands;
         for (int block : {64, 128, 256}) {
             const int mx = max_blocks_per_sm(block);
-            for (int bps : {mx, std::max(1, mx / 2)}) cands.push_back({block, bps, 8, 0.0});
+            for (int bps : {mx, std::max(1, mx / 2)}) cands.push_back({block, bps, 8, 0.0, PT_BATCH_PERSISTENT, budget});
         }
         BatchPlan cal = make_plan(in, n, 8, 8);
         BatchItemDev* d_items = static_cast<BatchItemDev*>(alloc(cal.items.size() * sizeof(BatchItemDev)));
@@ -549,30 +554,30 @@ int render_batch(const pt_batch_item* in, uint32_t n, int out_is_device, pt_batc
                 PT_CU(cudaEventElapsedTime(&ms, e0, e1));
                 c.ms = ms;   // second repetition counts (first is warm-up)
             }
-            if (c.ms < best) { best = c.ms; tune = c; }
+            if (c.ms < best) { best = c.ms; tune = c; tune.chunk_spp = cfg && cfg->chunk_spp ? cfg->chunk_spp : 16; }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        // the wavefront mode on the same calibration batch
+        // the wavefront mode on the same calibration batch, at three queue
+        // capacities (paths in flight shared by the items) unless fixed in cfg
         if (req_mode == PT_BATCH_AUTO) {
             std::vector<pt_batch_item> capped(in, in + n);
             for (pt_batch_item& it : capped) it.spp = std::min(it.spp, 8);
-            float wms = 0.0f;
-            for (int rep = 0; rep < 2; ++rep)
-                if (int rc = batch_wavefront(capped.data(), n, 0, budget, false, st, &wms, nullptr)) return rc;
-            if (wms < best) { best = wms; tune.mode = PT_BATCH_WAVEFRONT; tune.ms = wms; }
+            std::vector<int64_t> caps;
+            if (cfg && cfg->paths_in_flight > 0) caps.push_back(cfg->paths_in_flight);
+            else caps = {int64_t(1) << 25, int64_t(1) << 26, int64_t(1) << 27};
+            for (int64_t paths : caps) {
+                float wms = 0.0f;
+                for (int rep = 0; rep < 2; ++rep)
+                    if (int rc = batch_wavefront(capped.data(), n, 0, paths, false, st, &wms, nullptr)) return rc;
+                if (wms < best) { best = wms; tune.mode = PT_BATCH_WAVEFRONT; tune.ms = wms; tune.paths = paths; }
+            }
         }
-        // chunk size: larger chunks amortise the per-unit setup; bounded by the partial buffer
-        uint64_t pix = 0, spp_max = 0;
-        for (uint32_t k = 0; k < n; ++k) {
-            pix += static_cast<uint64_t>(in[k].scene->host.camera.width) * in[k].scene->host.camera.height;
-            spp_max = std::max<uint64_t>(spp_max, static_cast<uint64_t>(in[k].spp));
-        }
-        tune.chunk_spp = 16;
         std::lock_guard<std::mutex> lk(g_tune_mu);
         g_tune_cache.emplace_back(key, tune);
     }
-    if (tune.mode == PT_BATCH_WAVEFRONT && req_mode == PT_BATCH_AUTO) return run_wavefront(static_cast<float>(tune.ms));
+    if (tune.mode == PT_BATCH_WAVEFRONT && req_mode == PT_BATCH_AUTO)
+        return run_wavefront(static_cast<float>(tune.ms), tune.paths);
     if (tune.blocks_per_sm <= 0) tune.blocks_per_sm = max_blocks_per_sm(tune.block);
 
     // ---- the batch itself: one persistent launch + resolve, captured in a graph ----

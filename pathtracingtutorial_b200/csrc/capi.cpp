@@ -4,6 +4,7 @@
 // uploadToDevice -> Renderer::renderAll -> download
 // (Part_2/src/main.cpp:69-78,148-149), but every entry point returns a status
 // code instead of exiting, and the library owns all device memory.
+#include <chrono>
 #include <cmath>
 #include <algorithm>
 #include <cctype>
@@ -11,7 +12,9 @@
 #include <exception>
 #include <mutex>
 #include <new>
+#include <string>
 #include <unordered_map>
+#include <vector>
 
 #include "device_api.h"
 #include "engine.h"
@@ -215,6 +218,9 @@ int pt_scene_set_render_settings(pt_scene* s, const pt_render_settings* st) {
     PT_REQUIRE(st->max_depth >= 0, "max_depth must be non-negative");
     PT_REQUIRE(st->sampler_type == PT_SAMPLER_PCG || st->sampler_type == PT_SAMPLER_SOBOL, "unknown sampler");
     PT_REQUIRE(st->arg_order == PT_ARGS_LTR || st->arg_order == PT_ARGS_RTL, "unknown arg order");
+    PT_REQUIRE(st->trace_block == 0 || st->trace_block == 64 || st->trace_block == 128 || st->trace_block == 256,
+               "trace_block must be 0, 64, 128 or 256");
+    PT_REQUIRE(st->stack_depth == 0 || st->stack_depth == 32 || st->stack_depth == 64, "stack_depth must be 0, 32 or 64");
     s->host.settings = *st;
     return PT_OK;
 }
@@ -554,6 +560,128 @@ int pt_render(pt_scene* s, int32_t spp, float* out_rgba, int32_t out_is_device, 
     if (int rc = film_download(rcache.film, out_rgba, false, out_is_device == 0)) return rc;
     if (stats) integrator_stats(integ, stats);
     return device_sync(dev);
+    PT_GUARD_END
+}
+
+// ---- autotuner ----
+namespace {
+
+std::mutex g_tune_mu;
+std::unordered_map<std::string, pt_tune_report>& tune_cache() {
+    static std::unordered_map<std::string, pt_tune_report> c;
+    return c;
+}
+
+int log2_floor(uint64_t v) { int b = 0; while (v > 1) { v >>= 1; ++b; } return b; }
+
+// device : triangles : pixels : depth : sampler : environment : textures : shallow tree
+std::string tune_class(const pt_scene* s) {
+    const HostScene& h = s->host;
+    return std::to_string(s->dev.device) + ":" + std::to_string(log2_floor(h.faces.size())) + ":" +
+           std::to_string(log2_floor(uint64_t(h.camera.width) * uint64_t(h.camera.height))) + ":" +
+           std::to_string(h.settings.max_depth) + ":" + std::to_string(h.settings.sampler_type) + ":" +
+           std::to_string(h.env_w > 0 ? 1 : 0) + ":" + std::to_string(h.textures.empty() ? 0 : 1) + ":" +
+           std::to_string(s->tables.bvh_depth < 32 ? 1 : 0);
+}
+
+// One calibration render of `spp` samples per pixel with the scene's current
+// settings, through pt_render's film and integrator: wall milliseconds of the
+// second of two runs (the first captures its graph and sizes its arena).
+int calibration_ms(pt_scene* s, int spp, float* ms) {
+    const int w = s->host.camera.width, h = s->host.camera.height;
+    std::vector<float> img(static_cast<size_t>(w) * h * 4);
+    for (int rep = 0; rep < 2; ++rep) {
+        const auto t0 = std::chrono::steady_clock::now();
+        if (int rc = pt_render(s, spp, img.data(), 0, nullptr)) return rc;
+        *ms = static_cast<float>(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    }
+    return PT_OK;
+}
+
+}  // namespace
+
+int pt_autotune(pt_scene* s, int32_t calib_spp, pt_tune_report* report) {
+    PT_REQUIRE(s && report, "null argument");
+    PT_REQUIRE(calib_spp >= 0, "calib_spp must not be negative");
+    PT_GUARD_BEGIN
+    std::memset(report, 0, sizeof(*report));
+    if (!s->tables.built) {
+        if (int rc = pt_scene_build_accel(s)) return rc;
+    }
+    if (!s->dev.uploaded) {
+        int dev = 0;
+        if (int rc = current_device(&dev)) return rc;
+        if (int rc = upload_scene(s, dev)) return rc;
+    }
+    const std::string key = tune_class(s);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = tune_cache().find(key);
+        if (it != tune_cache().end()) {
+            *report = it->second;
+            report->cached = 1;
+            s->host.settings.paths_in_flight = report->paths_in_flight;
+            s->host.settings.trace_block = report->trace_block;
+            s->host.settings.stack_depth = report->stack_depth;
+            return PT_OK;
+        }
+    }
+    const uint64_t npix = uint64_t(s->host.camera.width) * uint64_t(s->host.camera.height);
+    PT_REQUIRE(npix > 0, "camera resolution must be positive");
+    int spp = calib_spp;
+    if (spp == 0) spp = static_cast<int>(std::min<uint64_t>(256, std::max<uint64_t>(8, ((1ull << 27) + npix - 1) / npix)));
+    report->calib_spp = spp;
+    const pt_render_settings saved = s->host.settings;
+    pt_render_settings best = saved;
+    best.paths_in_flight = saved.paths_in_flight > 0 ? saved.paths_in_flight : (1 << 27);
+    best.trace_block = 128;
+    best.stack_depth = 64;
+    float best_ms = 1e30f;
+    auto attempt = [&](int pif, int block, int depth) -> int {
+        if (report->candidates >= PT_TUNE_MAX_CANDIDATES) return PT_OK;
+        for (int k = 0; k < report->candidates; ++k)
+            if (report->cand_paths[k] == pif && report->cand_block[k] == block && report->cand_depth[k] == depth)
+                return PT_OK;
+        s->host.settings = saved;
+        s->host.settings.paths_in_flight = pif;
+        s->host.settings.trace_block = block;
+        s->host.settings.stack_depth = depth;
+        float ms = 0.0f;
+        if (int rc = calibration_ms(s, spp, &ms)) { s->host.settings = saved; return rc; }
+        const int k = report->candidates++;
+        report->cand_paths[k] = pif;
+        report->cand_block[k] = block;
+        report->cand_depth[k] = depth;
+        report->cand_ms[k] = ms;
+        if (k == 0) report->default_ms = ms;
+        if (ms < best_ms) { best_ms = ms; best = s->host.settings; }
+        return PT_OK;
+    };
+    // 1) stack depth, 2) block size, 3) queue capacity -- each at the best so far
+    const int pif0 = best.paths_in_flight;
+    if (int rc = attempt(pif0, 128, 64)) return rc;
+    if (s->tables.bvh_depth < 32)
+        if (int rc = attempt(pif0, 128, 32)) return rc;
+    const int depth = best.stack_depth;
+    for (int block : {64, 256})
+        if (int rc = attempt(pif0, block, depth)) return rc;
+    const int block = best.trace_block;
+    for (int lg = 24; lg <= 27; ++lg) {
+        const int pif = 1 << lg;
+        if (static_cast<uint64_t>(pif) < npix) continue;
+        if (int rc = attempt(pif, block, depth)) return rc;
+    }
+    s->host.settings = saved;
+    s->host.settings.paths_in_flight = best.paths_in_flight;
+    s->host.settings.trace_block = best.trace_block;
+    s->host.settings.stack_depth = best.stack_depth;
+    report->paths_in_flight = best.paths_in_flight;
+    report->trace_block = best.trace_block;
+    report->stack_depth = best.stack_depth;
+    report->best_ms = best_ms;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_cache()[key] = *report;
+    return PT_OK;
     PT_GUARD_END
 }
 

@@ -85,6 +85,8 @@ struct WaveParams {
     const float* gmix;   // queue-ordered mixtures, kGMix floats per entry
     float    galpha;     // probability of sampling the mixture (one-sample MIS)
     float4*  grec;       // training records [depth][npath][4]
+    // traversal kernel shape (threads per block, stack entries)
+    int      trace_block, stack_depth;
 };
 
 // ---------------------------------------------------------------------------
@@ -390,7 +392,8 @@ __device__ __forceinline__ void warp_count(unsigned long long* dst, uint32_t v) 
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, static_cast<unsigned long long>(v));
 }
 
-__global__ void __launch_bounds__(128) k_extend(WaveParams P, int q, int depth) {
+template <int Block, int Depth>
+__global__ void __launch_bounds__(Block) k_extend(WaveParams P, int q, int depth) {
     const uint32_t n = min(P.counts[q], static_cast<uint32_t>(P.npath));
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.counts[q ^ 1] = 0;
@@ -405,7 +408,7 @@ __global__ void __launch_bounds__(128) k_extend(WaveParams P, int q, int depth) 
     const float4* __restrict__ ro = P.ray_o[q];
     const float4* __restrict__ rd = P.ray_d[q];
     float4* __restrict__ hit = P.hit;
-    closest_loop(P.scene, blockIdx.x * blockDim.x + threadIdx.x, n, stride, watertight, err, tc,
+    closest_loop<Depth>(P.scene, blockIdx.x * blockDim.x + threadIdx.x, n, stride, watertight, err, tc,
                  [&](uint32_t i, RayInv& r) {
                      const float4 o = ro[i];
                      const float4 d = rd[i];
@@ -874,7 +877,8 @@ __global__ void __launch_bounds__(128, 6) k_shade_back(WaveParams P, int q, int 
     }
 }
 
-__global__ void __launch_bounds__(128) k_shadow(WaveParams P) {
+template <int Block, int Depth>
+__global__ void __launch_bounds__(Block) k_shadow(WaveParams P) {
     const uint32_t n = min(P.counts[2], static_cast<uint32_t>(P.npath) * static_cast<uint32_t>(P.n_slots));
     if (blockIdx.x == 0 && threadIdx.x == 0)
         atomicAdd(P.stats + kStatShadowRays, static_cast<unsigned long long>(n));
@@ -883,7 +887,7 @@ __global__ void __launch_bounds__(128) k_shadow(WaveParams P) {
     uint32_t err = 0;
     TraceCounters tc{0, 0};
     const uint32_t stride = gridDim.x * blockDim.x;
-    any_loop(P.scene, blockIdx.x * blockDim.x + threadIdx.x, n, stride, watertight, err, tc,
+    any_loop<Depth>(P.scene, blockIdx.x * blockDim.x + threadIdx.x, n, stride, watertight, err, tc,
              [&](uint32_t i, AnyWalk& w) {
                  const float4 o = P.sq_o[i];
                  const float4 d = P.sq_d[i];
@@ -1080,6 +1084,47 @@ __global__ void k_bsdf_eval(const pt_material* mats, uint32_t nmat, const float*
     }
 }
 
+// The traversal kernels' shapes: 64, 128 or 256 threads per block and a
+// stack of 32 or 64 entries (six instantiations of k_extend and k_shadow).
+inline int trace_shape_index(int block, int depth) {
+    return (block == 64 ? 0 : (block == 256 ? 2 : 1)) * 2 + (depth == 32 ? 0 : 1);
+}
+inline int trace_shape_block(int k) { return k < 2 ? 64 : (k < 4 ? 128 : 256); }
+inline int trace_shape_depth(int k) { return (k & 1) ? 64 : 32; }
+
+#define PT_TRACE_SHAPES(X) X(0, 64, 32) X(1, 64, 64) X(2, 128, 32) X(3, 128, 64) X(4, 256, 32) X(5, 256, 64)
+
+inline const void* extend_kernel(int k) {
+    switch (k) {
+#define PT_CASE(i, b, d) case i: return reinterpret_cast<const void*>(k_extend<b, d>);
+        PT_TRACE_SHAPES(PT_CASE)
+#undef PT_CASE
+    }
+    return reinterpret_cast<const void*>(k_extend<128, 64>);
+}
+inline const void* shadow_kernel(int k) {
+    switch (k) {
+#define PT_CASE(i, b, d) case i: return reinterpret_cast<const void*>(k_shadow<b, d>);
+        PT_TRACE_SHAPES(PT_CASE)
+#undef PT_CASE
+    }
+    return reinterpret_cast<const void*>(k_shadow<128, 64>);
+}
+inline void launch_extend(int k, int grid, cudaStream_t st, const WaveParams& P, int q, int d) {
+    switch (k) {
+#define PT_CASE(i, b, dd) case i: k_extend<b, dd><<<grid, b, 0, st>>>(P, q, d); return;
+        PT_TRACE_SHAPES(PT_CASE)
+#undef PT_CASE
+    }
+}
+inline void launch_shadow(int k, int grid, cudaStream_t st, const WaveParams& P) {
+    switch (k) {
+#define PT_CASE(i, b, d) case i: k_shadow<b, d><<<grid, b, 0, st>>>(P); return;
+        PT_TRACE_SHAPES(PT_CASE)
+#undef PT_CASE
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -1096,7 +1141,8 @@ struct Wavefront {
     cudaStream_t graph_stream = nullptr;
     // launch shapes
     int sms = 0;
-    int grid_raygen = 0, grid_extend = 0, grid_shade = 0, grid_shadow = 0, grid_finalize = 0;
+    int grid_raygen = 0, grid_shade = 0, grid_finalize = 0;
+    int grid_extend[6] = {}, grid_shadow[6] = {};   // per traversal shape (trace_shape_index)
     // stats
     unsigned long long host_stats[kStatCount] = {};
     double stage_ms[5] = {0, 0, 0, 0, 0};   // extend, shade, shadow, other, guide
@@ -1160,9 +1206,11 @@ int wavefront_prepare(Wavefront& wf, int device, int npath, int n_slots) {
         PT_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
         wf.sms = sms;
         wf.grid_raygen = grid_for(reinterpret_cast<const void*>(k_raygen), 256, sms);
-        wf.grid_extend = grid_for(reinterpret_cast<const void*>(k_extend), 128, sms);
         wf.grid_shade = grid_for(reinterpret_cast<const void*>(k_shade_front<false>), 128, sms);
-        wf.grid_shadow = grid_for(reinterpret_cast<const void*>(k_shadow), 128, sms);
+        for (int k = 0; k < 6; ++k) {
+            wf.grid_extend[k] = grid_for(extend_kernel(k), trace_shape_block(k), sms);
+            wf.grid_shadow[k] = grid_for(shadow_kernel(k), trace_shape_block(k), sms);
+        }
         wf.grid_finalize = grid_for(reinterpret_cast<const void*>(k_finalize), 256, sms);
         wf.device = device;
         wf.npath = 0;
@@ -1239,12 +1287,13 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
     };
     const int lanes = std::max(1, P.npath / std::max(P.npix, 1));
     const int total = static_cast<int>(total_samples);
+    const int tsi = trace_shape_index(P.trace_block, P.stack_depth);
     for (int s0 = 0; s0 < total; s0 += lanes) {
         const int count = std::min(lanes, total - s0);
         if (int rc = timed(3, [&] { k_raygen<<<wf.grid_raygen, 256, 0, st>>>(P, s0, count); })) return rc;
         for (int d = 0; d < P.max_depth; ++d) {
             const int q = d & 1;
-            if (int rc = timed(0, [&] { k_extend<<<wf.grid_extend, 128, 0, st>>>(P, q, d); })) return rc;
+            if (int rc = timed(0, [&] { launch_extend(tsi, wf.grid_extend[tsi], st, P, q, d); })) return rc;
             if (infer) {
                 if (int rc = timed(4, [&] {
                         k_guide_infer<<<wf.sms * kGInferBlocksPerSm, 32 * kGInferWarps, kGInferSmem, st>>>(
@@ -1272,7 +1321,7 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
                         }
                     }
                 })) return rc;
-            if (int rc = timed(2, [&] { k_shadow<<<wf.grid_shadow, 128, 0, st>>>(P); })) return rc;
+            if (int rc = timed(2, [&] { launch_shadow(tsi, wf.grid_shadow[tsi], st, P); })) return rc;
         }
         if (int rc = timed(3, [&] { k_finalize<<<wf.grid_finalize, 256, 0, st>>>(P, s0, count); })) return rc;
         if (train) {
@@ -1655,6 +1704,11 @@ int prepare_wave(pt_integrator* integ, pt_film* film, pt_scene* s, const pt_scen
         P.galpha = gs->alpha;
         P.grec = gs->mode == PT_GUIDE_TRAIN ? gs->rec : nullptr;
     }
+    // traversal shape: the settings' (the tuner's), 128 threads and 64 entries
+    // by default; a stack no deeper than the tree falls back to 64 entries
+    P.trace_block = rs.trace_block ? rs.trace_block : 128;
+    P.stack_depth = rs.stack_depth ? rs.stack_depth : kStackDepth;
+    if (P.stack_depth <= static_cast<int>(s->tables.bvh_depth)) P.stack_depth = kStackDepth;
     lanes_out = lanes;
     return PT_OK;
 }
@@ -1765,7 +1819,8 @@ int integrator_stats(const pt_integrator* integ, pt_render_stats* out) {
     out->extend_ms = wf->stage_ms[0];
     out->shade_ms = wf->stage_ms[1];
     out->shadow_ms = wf->stage_ms[2];
-    out->other_ms = wf->stage_ms[3] + wf->stage_ms[4];
+    out->other_ms = wf->stage_ms[3];
+    out->guide_ms = wf->stage_ms[4];
     out->total_ms = wf->total_ms;
     out->kernel_launches = wf->kernel_launches;
     return PT_OK;

@@ -332,9 +332,13 @@ PT_HD bool trace_any(const DeviceScene& s, const RayInv& ray, float tmax, bool w
 // its next ray (i + stride) at once instead of waiting for the warp's longest
 // ray.  All 32 lanes of the warp must call these loops.
 // ---------------------------------------------------------------------------
+// Deferred children of one walk; Depth entries (the tuner picks 32 or 64; a
+// tree needs more entries than its depth only never: the stack holds at most
+// one far child per level).
+template <int Depth = kStackDepth>
 struct StepStack {
-    uint32_t ref[kStackDepth];
-    float    t[kStackDepth];
+    uint32_t ref[Depth];
+    float    t[Depth];
 };
 
 struct ClosestWalk {
@@ -357,7 +361,8 @@ __device__ __forceinline__ bool closest_begin(const DeviceScene& s, ClosestWalk&
 }
 
 // Next deferred child that still passes against the current best; false at the end.
-__device__ __forceinline__ bool closest_pop(ClosestWalk& w, const StepStack& st) {
+template <int Depth>
+__device__ __forceinline__ bool closest_pop(ClosestWalk& w, const StepStack<Depth>& st) {
     while (w.sp > 0) {
         --w.sp;
         if (st.t[w.sp] <= w.best) { w.ref = st.ref[w.sp]; return true; }
@@ -366,7 +371,8 @@ __device__ __forceinline__ bool closest_pop(ClosestWalk& w, const StepStack& st)
 }
 
 // Inner node w.ref: both child boxes, then the next node; false at the end.
-__device__ __forceinline__ bool closest_inner(const DeviceScene& s, ClosestWalk& w, StepStack& st, uint32_t& err,
+template <int Depth>
+__device__ __forceinline__ bool closest_inner(const DeviceScene& s, ClosestWalk& w, StepStack<Depth>& st, uint32_t& err,
                                               TraceCounters& cnt) {
     ++cnt.inner;
     const float* nb = reinterpret_cast<const float*>(s.inner + w.ref);
@@ -390,7 +396,7 @@ __device__ __forceinline__ bool closest_inner(const DeviceScene& s, ClosestWalk&
     const float ef = right_first ? e0 : e1;
     if (hn) {
         if (hf) {
-            if (w.sp >= kStackDepth) { err |= kErrStackOverflow; return false; }
+            if (w.sp >= Depth) { err |= kErrStackOverflow; return false; }
             st.ref[w.sp] = fref; st.t[w.sp] = ef; ++w.sp;
         }
         w.ref = nref;
@@ -401,7 +407,8 @@ __device__ __forceinline__ bool closest_inner(const DeviceScene& s, ClosestWalk&
 }
 
 // Leaf w.ref: its triangles, then the next node; false at the end.
-__device__ __forceinline__ bool closest_leaf(const DeviceScene& s, ClosestWalk& w, StepStack& st, bool watertight,
+template <int Depth>
+__device__ __forceinline__ bool closest_leaf(const DeviceScene& s, ClosestWalk& w, StepStack<Depth>& st, bool watertight,
                                              TraceCounters& cnt) {
     uint32_t ti = w.ref & ~kLeafBit;
     for (;;) {
@@ -417,11 +424,11 @@ __device__ __forceinline__ bool closest_leaf(const DeviceScene& s, ClosestWalk& 
 
 // Closest hits of rays first, first + stride, ... < n.  fetch(i, RayInv&)
 // loads ray i; done(i, const ClosestWalk&) stores its result (prim < 0: miss).
-template <class Fetch, class Done>
+template <int Depth = kStackDepth, class Fetch, class Done>
 __device__ __forceinline__ void closest_loop(const DeviceScene& s, uint32_t i, uint32_t n, uint32_t stride,
                                              bool watertight, uint32_t& err, TraceCounters& cnt, Fetch&& fetch,
                                              Done&& done) {
-    StepStack st;
+    StepStack<Depth> st;
     ClosestWalk w;
     bool have = false;
     for (;;) {
@@ -462,6 +469,7 @@ __device__ __forceinline__ bool any_begin(const DeviceScene& s, AnyWalk& w) {
     return true;
 }
 
+template <int Depth>
 __device__ __forceinline__ bool any_inner(const DeviceScene& s, AnyWalk& w, uint32_t* stack, uint32_t& err,
                                           TraceCounters& cnt) {
     ++cnt.inner;
@@ -485,7 +493,7 @@ __device__ __forceinline__ bool any_inner(const DeviceScene& s, AnyWalk& w, uint
     const bool hf = right_first ? h0 : h1;
     if (hn) {
         if (hf) {
-            if (w.sp >= kStackDepth) { err |= kErrStackOverflow; return false; }
+            if (w.sp >= Depth) { err |= kErrStackOverflow; return false; }
             stack[w.sp++] = fref;
         }
         w.ref = nref;
@@ -515,11 +523,11 @@ __device__ __forceinline__ bool any_leaf(const DeviceScene& s, AnyWalk& w, uint3
 
 // Any-hit tests of rays first, first + stride, ... < n.  fetch(i, AnyWalk&)
 // sets r and tmax; done(i, bool occluded) consumes the result.
-template <class Fetch, class Done>
+template <int Depth = kStackDepth, class Fetch, class Done>
 __device__ __forceinline__ void any_loop(const DeviceScene& s, uint32_t i, uint32_t n, uint32_t stride,
                                          bool watertight, uint32_t& err, TraceCounters& cnt, Fetch&& fetch,
                                          Done&& done) {
-    uint32_t stack[kStackDepth];
+    uint32_t stack[Depth];
     AnyWalk w;
     bool have = false;
     for (;;) {
@@ -533,7 +541,7 @@ __device__ __forceinline__ void any_loop(const DeviceScene& s, uint32_t i, uint3
         bool fin = false;
         if (have) {
             while (!(w.ref & kLeafBit)) {
-                if (!any_inner(s, w, stack, err, cnt)) { fin = true; break; }
+                if (!any_inner<Depth>(s, w, stack, err, cnt)) { fin = true; break; }
             }
         }
         __syncwarp();
