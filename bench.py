@@ -361,21 +361,6 @@ def convergence(local: int, stream, small: bool, plain_cap: int = 8192, guided_c
     rg.render_frames(train_spp // spf)
     sync()
     train_ms = (time.perf_counter() - t0) * 1e3
-    # stage breakdown of one chunk of each arm (CUDA events around every launch;
-    # a separate, untimed render)
-    breakdown = {}
-    for arm, mode in (("plain", pt.Guide.OFF), ("guided", pt.Guide.USE)):
-        g.attach(rg.integrator, mode)
-        scene.update_settings(flags=pt.FLAG_STAGE_TIMING | pt.FLAG_NO_GRAPH)
-        rg.integrator.reset_stats()
-        rg.reset_accumulation()
-        scene.set_frame_count(300_000)
-        rg.render_frames(chunk // spf)
-        sync()
-        st = rg.integrator.stats()
-        breakdown[arm] = {k: round(st[k], 2) for k in ("extend_ms", "shade_ms", "shadow_ms", "guide_ms", "other_ms")}
-        breakdown[arm]["rays"] = int(st["camera_rays"] + st["extension_rays"] + st["shadow_rays"])
-        scene.update_settings(flags=0)
     g.attach(rg.integrator, pt.Guide.OFF)
     rg.integrator.close()
     rg.film.close()
@@ -392,6 +377,25 @@ def convergence(local: int, stream, small: bool, plain_cap: int = 8192, guided_c
         guided.append((spp, (time.perf_counter() - t0) * 1e3, e))
         if e <= TARGET_RELMSE:
             break
+    # stage breakdown of one chunk of each arm (CUDA events around every launch;
+    # separate renders after both clocks stopped)
+    breakdown = {}
+    rg = pt.Renderer(scene, device=local, stream=handle)
+    for arm, mode in (("plain", pt.Guide.OFF), ("guided", pt.Guide.USE)):
+        g.attach(rg.integrator, mode)
+        scene.update_settings(flags=pt.FLAG_STAGE_TIMING | pt.FLAG_NO_GRAPH)
+        rg.integrator.reset_stats()
+        rg.reset_accumulation()
+        scene.set_frame_count(300_000)
+        rg.render_frames(chunk // spf)
+        sync()
+        st = rg.integrator.stats()
+        breakdown[arm] = {k: round(st[k], 2) for k in ("extend_ms", "shade_ms", "shadow_ms", "guide_ms", "other_ms")}
+        breakdown[arm]["rays"] = int(st["camera_rays"] + st["extension_rays"] + st["shadow_rays"])
+        scene.update_settings(flags=0)
+    g.attach(rg.integrator, pt.Guide.OFF)
+    rg.integrator.close()
+    rg.film.close()
     g.close()
     tp_chk, tp = crossing_time(plain, TARGET_RELMSE)
     tg_chk, tg = crossing_time(guided, TARGET_RELMSE)

@@ -94,6 +94,8 @@ class Prepared:
 
     def __init__(self, vertices, faces, materials, nodes, depth, em_refs, tri_pmf, tri_alias, env, env_pmf,
                  env_alias, camera_frame, width, height, punctual=None, textures=None):
+        if np.asarray(materials).dtype.itemsize != 256:
+            raise ValueError("materials must be 256-byte records (pt_material)")
         self.vertices, self.faces, self.materials, self.nodes, self.depth = vertices, faces, materials, nodes, depth
         self.em_refs, self.tri_pmf, self.tri_alias = em_refs, tri_pmf, tri_alias
         self.env, self.env_pmf, self.env_alias = env, env_pmf, env_alias
@@ -208,6 +210,8 @@ class Oracle:
 
     def prepare(self, sa) -> Prepared:
         """Build a SceneArrays (pathtracingtutorial_b200.scenes) with the oracle's own prep."""
+        if np.asarray(sa.materials).dtype.itemsize != 256:
+            raise ValueError("materials must be 256-byte records (pt_material)")
         nodes, faces, depth = self.build_bvh(sa.vertices, sa.faces)
         refs, pmf, alias = self.emissive_tables(sa.vertices, faces, sa.materials)
         env_pmf, env_alias = self.env_tables(sa.env)

@@ -482,7 +482,7 @@ def large_scene(n_spheres: int = 3500, subdiv: int = 4, n_tets: int = 500_000, n
     cf["v0"] += len(v); cf["v1"] += len(v); cf["v2"] += len(v)
     v = np.concatenate([v, cv])
     f = np.concatenate([f, cf])
-    mats = np.concatenate([np.atleast_1d(m) for m in mats])
+    mats = _materials(mats)
     cams = []
     for k in range(n_cameras):
         a = 2 * np.pi * k / n_cameras
