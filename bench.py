@@ -370,7 +370,7 @@ def convergence(local: int, stream, small: bool, plain_cap: int = 8192, guided_c
     while spp < guided_cap:
         imgs, _, _ = pt.render_batch([(scene, chunk, spp // spf, None, g)], mode=pt.BATCH_WAVEFRONT,
                                      autotune=False)
-        img = imgs[0].astype(np.float64)
+        img = imgs[0][..., :3].astype(np.float64)
         acc = img if acc is None else acc + (img - acc) * (chunk / (spp + chunk))
         spp += chunk
         e = relmse(acc)

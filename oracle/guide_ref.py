@@ -8,8 +8,8 @@ tests/ import it.
 The model, for a position p in [0,1]^3 and a direction w:
   level l (16 levels): f = p * scale[l] + 1/2, trilinear over the 8 cell
       corners of table entries (2 features each); a corner index is
-      x + y*res + z*res^2 (res = floor(scale)+2) for dense levels and the
-      xor-prime hash x ^ 2654435761 y ^ 805459861 z otherwise, modulo T;
+      x + y*res + z*res^2 (res = floor(scale)+2) for dense levels and
+      x + (2654435761 y ^ 805459861 z) otherwise (32-bit products), modulo T;
   x = 32 features (feature 2l+f is level l, feature f);
   h1 = relu(W0 x), h2 = relu(W1 h1), h3 = relu(W2 h2), raw = W3 h3 (no biases);
   lobe k: mu = normalise(raw[5k:5k+3]), kappa = min(softplus(raw[5k+3]) + 1e-3, 5e3),
@@ -68,7 +68,7 @@ def _corners(params: dict, level: int, p: np.ndarray):
         if level < params["dense_limit"]:
             h = x + y * res + z * res * res
         else:
-            h = x ^ ((y * P1) & np.uint64(0xFFFFFFFF)) ^ ((z * P2) & np.uint64(0xFFFFFFFF))
+            h = x + (((y * P1) & np.uint64(0xFFFFFFFF)) ^ ((z * P2) & np.uint64(0xFFFFFFFF)))
         idx[:, c] = (h & np.uint64(table - 1)).astype(np.int64)
         wts[:, c] = (t[:, 0] if cx else 1 - t[:, 0]) * (t[:, 1] if cy else 1 - t[:, 1]) * \
                     (t[:, 2] if cz else 1 - t[:, 2])

@@ -442,15 +442,30 @@ class Guide:
     """Learned directional guide (hash grid + MLP + 8-lobe vMF mixture) for one scene."""
 
     OFF, USE, TRAIN = _ffi.GUIDE_OFF, _ffi.GUIDE_USE, _ffi.GUIDE_TRAIN
+    STEP_SAMPLES = 65536   # the library's default cap of training samples per optimiser step
 
-    def __init__(self, scene: SceneManager, seed: int = 1, lr: float | None = None, alpha: float | None = None):
+    def __init__(self, scene: SceneManager, seed: int = 1, lr: float | None = None, alpha: float | None = None,
+                 paths_per_step: int | None = None, samples_per_step: int | None = None):
         h = C.c_void_p()
         check(lib().pt_guide_create(scene.handle, seed, C.byref(h)))
         self._h = h
         if lr is not None:
             check(lib().pt_guide_set_learning_rate(self._h, float(lr)))
         if alpha is not None:
-            check(lib().pt_guide_set_alpha(self._h, float(alpha)))
+            self.set_alpha(alpha)
+        if paths_per_step is not None or samples_per_step is not None:
+            self.set_training(paths_per_step or 0,
+                              self.STEP_SAMPLES if samples_per_step is None else samples_per_step)
+
+    def set_alpha(self, alpha: float) -> None:
+        """Probability of drawing a continuation from the network (one-sample MIS)."""
+        check(lib().pt_guide_set_alpha(self._h, float(alpha)))
+
+    def set_training(self, paths_per_step: int = 0, samples_per_step: int = 65536) -> None:
+        """Online training: one optimiser step per `paths_per_step` paths of a
+        pass (0 = 32768), each on at most `samples_per_step` samples (0 = all;
+        65536 is the library's default)."""
+        check(lib().pt_guide_set_training(self._h, int(paths_per_step), int(samples_per_step)))
 
     def attach(self, integrator: PathIntegrator, mode: int) -> None:
         check(lib().pt_integrator_set_guide(integrator._h, self._h if mode else None, mode))

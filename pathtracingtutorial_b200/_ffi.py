@@ -114,7 +114,7 @@ class TuneReport(C.Structure):
                 "stack_depth": self.stack_depth, "cached": bool(self.cached), "calib_spp": self.calib_spp,
                 "best_ms": self.best_ms, "default_ms": self.default_ms,
                 "candidates": [{"paths_in_flight": self.cand_paths[k], "trace_block": self.cand_block[k],
-                                "stack_depth": self.cand_depth[k], "ms": round(self.cand_ms[k], 2)}
+                                "stack_depth": self.cand_depth[k], "ms": self.cand_ms[k]}
                                for k in range(n)]}
 
 
@@ -204,6 +204,7 @@ _SIGS = [
     ("pt_guide_destroy", C.c_int, [_P]),
     ("pt_guide_set_learning_rate", C.c_int, [_P, C.c_float]),
     ("pt_guide_set_alpha", C.c_int, [_P, C.c_float]),
+    ("pt_guide_set_training", C.c_int, [_P, C.c_int32, C.c_uint32]),
     ("pt_guide_info", C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     ("pt_guide_loss", C.c_int, [_P, C.POINTER(C.c_float)]),
     ("pt_integrator_set_guide", C.c_int, [_P, _P, C.c_int32]),

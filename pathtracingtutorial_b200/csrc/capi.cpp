@@ -714,6 +714,11 @@ int pt_guide_set_alpha(pt_guide* guide, float alpha) {
     guide_set_alpha(guide, alpha);
     return PT_OK;
 }
+int pt_guide_set_training(pt_guide* guide, int32_t paths_per_step, uint32_t samples_per_step) {
+    PT_REQUIRE(guide && paths_per_step >= 0, "invalid argument");
+    guide_set_training(guide, paths_per_step, samples_per_step);
+    return PT_OK;
+}
 int pt_guide_info(const pt_guide* guide, uint32_t* steps, uint32_t* last_samples) {
     PT_REQUIRE(guide, "null guide");
     return guide_info(guide, steps, last_samples);

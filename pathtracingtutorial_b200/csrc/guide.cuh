@@ -41,14 +41,20 @@ constexpr int kGHid = 64;
 constexpr int kGLobes = 8;
 constexpr int kGOut = 40;                 // used outputs
 constexpr int kGOutPad = 48;              // 6 n-tiles of 8
-constexpr int kGMix = 40;                 // floats per mixture: 8 x (mu xyz, kappa) + 8 weights
+constexpr int kGMix = 40;                 // floats per mixture record: 8 x (kappa mu xyz, log factor) + 8 weights
 constexpr float kGuideAlpha = 0.5f;        // default probability of sampling the mixture
 constexpr int kGuideMinibatchPaths = 1 << 15;
+// Training samples per optimiser step at most (an evenly spread subset of the
+// step's share of a pass).  On the hidden-light room (1024 x 1024, 64 training
+// spp) all samples (about 10^5 a step) cost 3.0 s of training and gave relMSE
+// 0.00214 at 256 guided spp; 65,536 a step cost 2.25 s for 0.00233; 32,768
+// cost 2.0 s for 0.0034.
+constexpr uint32_t kGuideStepSamples = 65536;
 
-// Optimiser steps per training pass of `paths` paths: one per 2^15 paths
-// (about 10^5 samples), 1 .. 32.
-inline int guide_minibatches(int64_t paths) {
-    return static_cast<int>(std::min<int64_t>(32, std::max<int64_t>(1, paths / kGuideMinibatchPaths)));
+// Optimiser steps per training pass of `paths` paths: one per
+// `paths_per_step` paths (2^15 by default, about 10^5 samples), 1 .. 32.
+inline int guide_minibatches(int64_t paths, int64_t paths_per_step = kGuideMinibatchPaths) {
+    return static_cast<int>(std::min<int64_t>(32, std::max<int64_t>(1, paths / std::max<int64_t>(1, paths_per_step))));
 }
 
 // layer l: out x in, row-major, rows padded to in + 8 bf16 in shared memory
@@ -66,7 +72,8 @@ __host__ __device__ constexpr int g_soff(int l) {
 constexpr int kGSmemW = kGHid * (kGIn + 8) + 2 * kGHid * (kGHid + 8) + kGOutPad * (kGHid + 8);   // bf16 elements
 
 struct GuideNet {
-    __half2*        grid;        // kGLevels * kGTable (inference copy)
+    uint2*          grid;        // kGLevels * kGTable FP16 pairs (inference copy): entry e holds the two
+                                 // features of e and of (e + 1) mod kGTable, the corner one step along x
     float2*         grid_master; // FP32 master
     unsigned long long* grid_grad;   // 2 per entry, fixed point (kGFix)
     float2*         grid_m;
@@ -150,10 +157,15 @@ __device__ __forceinline__ void relu_to_a(const float (&acc)[N / 8][4], uint32_t
 // ---------------------------------------------------------------------------
 // Hash-grid encoding
 // ---------------------------------------------------------------------------
+// Corner (x, y, z) of a level: x + y res + z res^2 on the dense levels, and
+// x + (y P1 xor z P2) on the hashed ones -- x is added outside the hash, so
+// the two corners of a cell edge along x are neighbouring table entries (one
+// 32-byte sector holds eight) and a cell's eight corners touch about four
+// sectors instead of eight.
 __device__ __forceinline__ uint32_t grid_index(const GuideNet& net, int level, uint32_t x, uint32_t y, uint32_t z) {
     const uint32_t res = static_cast<uint32_t>(net.scale[level]) + 2u;
     if (static_cast<uint32_t>(level) < net.dense_limit) return (x + y * res + z * res * res) & (kGTable - 1);
-    return (x ^ (y * 2654435761u) ^ (z * 805459861u)) & (kGTable - 1);
+    return (x + ((y * 2654435761u) ^ (z * 805459861u))) & (kGTable - 1);
 }
 
 // Trilinear features of one level at normalised position p.
@@ -163,15 +175,21 @@ __device__ __forceinline__ float2 encode_level(const GuideNet& net, int level, f
     const float bx = floorf(fx), by = floorf(fy), bz = floorf(fz);
     const float tx = fx - bx, ty = fy - by, tz = fz - bz;
     const uint32_t ix = static_cast<uint32_t>(bx), iy = static_cast<uint32_t>(by), iz = static_cast<uint32_t>(bz);
-    const __half2* tab = net.grid + static_cast<size_t>(level) * kGTable;
+    const uint2* tab = net.grid + static_cast<size_t>(level) * kGTable;
     float2 r = make_float2(0.0f, 0.0f);
+    // one 8-byte load per cell edge along x: both corners of the edge
 #pragma unroll
-    for (int cidx = 0; cidx < 8; ++cidx) {
-        const uint32_t cx = cidx & 1, cy = (cidx >> 1) & 1, cz = (cidx >> 2) & 1;
-        const float w = (cx ? tx : 1.0f - tx) * (cy ? ty : 1.0f - ty) * (cz ? tz : 1.0f - tz);
-        const float2 e = __half22float2(tab[grid_index(net, level, ix + cx, iy + cy, iz + cz)]);
-        r.x += w * e.x;
-        r.y += w * e.y;
+    for (int e = 0; e < 4; ++e) {
+        const uint32_t cy = e & 1, cz = e >> 1;
+        const uint2 pr = __ldg(tab + grid_index(net, level, ix, iy + cy, iz + cz));
+        const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&pr.x));
+        const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&pr.y));
+        const float w0 = (1.0f - tx) * (cy ? ty : 1.0f - ty) * (cz ? tz : 1.0f - tz);
+        const float w1 = tx * (cy ? ty : 1.0f - ty) * (cz ? tz : 1.0f - tz);
+        r.x += w0 * f0.x;
+        r.y += w0 * f0.y;
+        r.x += w1 * f1.x;
+        r.y += w1 * f1.y;
     }
     return r;
 }
@@ -252,23 +270,43 @@ __device__ __forceinline__ float vmf_pdf(float kappa, float c) {
     return kappa / (kTwoPi * (1.0f - expf(-2.0f * kappa))) * expf(kappa * (c - 1.0f));
 }
 
-__device__ __forceinline__ float mix_pdf(const float* mix, f3 w) {
+// The mixture as the shading kernels read it (kGMix floats per queue entry):
+// lobe k as float4(kappa_k mu_k, b_k) with b_k = log(pi_k kappa_k /
+// (2 pi (1 - e^{-2 kappa_k}))) - kappa_k, then the eight weights pi_k.  Then
+// pi_k vMF_k(w) = exp(kappa_k mu_k . w + b_k): one exponential per lobe.
+__device__ __forceinline__ void mixture_record(const float* raw, float* rec) {
+    float mix[kGMix];
+    raw_to_mixture(raw, mix);
+    for (int k = 0; k < kGLobes; ++k) {
+        const float kap = mix[4 * k + 3];   // >= 1e-3
+        rec[4 * k] = kap * mix[4 * k];
+        rec[4 * k + 1] = kap * mix[4 * k + 1];
+        rec[4 * k + 2] = kap * mix[4 * k + 2];
+        rec[4 * k + 3] = logf(mix[32 + k]) + logf(kap / (kTwoPi * -expm1f(-2.0f * kap))) - kap;
+        rec[32 + k] = mix[32 + k];
+    }
+}
+
+__device__ __forceinline__ float mix_pdf(const float* rec, f3 w) {
+    const float4* r4 = reinterpret_cast<const float4*>(rec);
     float q = 0.0f;
 #pragma unroll
-    for (int k = 0; k < kGLobes; ++k)
-        q += mix[32 + k] * vmf_pdf(mix[4 * k + 3], mix[4 * k] * w.x + mix[4 * k + 1] * w.y + mix[4 * k + 2] * w.z);
+    for (int k = 0; k < kGLobes; ++k) {
+        const float4 l = r4[k];
+        q += expf(fmaf(l.x, w.x, fmaf(l.y, w.y, fmaf(l.z, w.z, l.w))));
+    }
     return q;
 }
 
-__device__ __forceinline__ f3 mix_sample(const float* mix, float u0, float u1, float u2) {
+__device__ __forceinline__ f3 mix_sample(const float* rec, float u0, float u1, float u2) {
     int k = 0;
-    float acc = mix[32];
-    while (k < kGLobes - 1 && u0 >= acc) { ++k; acc += mix[32 + k]; }
-    const f3 mu = mk(mix[4 * k], mix[4 * k + 1], mix[4 * k + 2]);
-    const float kappa = mix[4 * k + 3];
-    float c;
-    if (kappa < 1e-4f) c = 1.0f - 2.0f * u1;
-    else c = fminf(fmaxf(1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * kappa)) / kappa, -1.0f), 1.0f);
+    float acc = rec[32];
+    while (k < kGLobes - 1 && u0 >= acc) { ++k; acc += rec[32 + k]; }
+    const float4 l = reinterpret_cast<const float4*>(rec)[k];
+    const f3 km = mk(l.x, l.y, l.z);
+    const float kappa = length(km);
+    const f3 mu = km / kappa;
+    const float c = fminf(fmaxf(1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * kappa)) / kappa, -1.0f), 1.0f);
     const float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
     const float phi = kTwoPi * u2;
     const Frame fr = make_frame(mu);
@@ -319,7 +357,7 @@ k_guide_infer(GuideNet net, const uint32_t* counts, int q, uint32_t cap,
             const uint32_t r = tile * 16 + lane;
             if (r < n) {
                 float mix[kGMix];
-                raw_to_mixture(my + lane * kGOutPad, mix);
+                mixture_record(my + lane * kGOutPad, mix);
                 float4* dst = reinterpret_cast<float4*>(mix_out + static_cast<size_t>(r) * kGMix);
 #pragma unroll
                 for (int k = 0; k < kGMix / 4; ++k) dst[k] = make_float4(mix[4 * k], mix[4 * k + 1], mix[4 * k + 2], mix[4 * k + 3]);
@@ -476,20 +514,27 @@ __device__ __forceinline__ void store_dy(const float (&acc)[N / 8][4], const __n
     }
 }
 
-// Minibatch mb of nmb over the first n samples takes samples mb, mb + nmb,
-// mb + 2 nmb, ...: the samples are collected in path (pixel) order, so
-// interleaving gives every optimiser step samples from the whole image
-// instead of one band of rows.
-__host__ __device__ __forceinline__ uint32_t minibatch_size(uint32_t n, int mb, int nmb) {
-    return n > static_cast<uint32_t>(mb) ? (n - static_cast<uint32_t>(mb) + static_cast<uint32_t>(nmb) - 1u) /
-                                               static_cast<uint32_t>(nmb)
-                                         : 0u;
+// Minibatch mb of nmb over the first n samples takes samples mb, mb + S,
+// mb + 2 S, ... with the stride S = nmb: the samples are collected in path
+// (pixel) order, so interleaving gives every optimiser step samples from the
+// whole image instead of one band of rows.  With a cap of `step_cap` samples
+// per step (0 = none) the stride grows to nmb * ceil(n / (nmb * step_cap)),
+// so a step takes an evenly spread subset and the samples between are skipped.
+__host__ __device__ __forceinline__ uint32_t minibatch_stride(uint32_t n, int nmb, uint32_t step_cap) {
+    if (step_cap == 0u) return static_cast<uint32_t>(nmb);
+    const uint64_t per = static_cast<uint64_t>(nmb) * step_cap;
+    const uint64_t k = (static_cast<uint64_t>(n) + per - 1u) / per;
+    return static_cast<uint32_t>(nmb) * static_cast<uint32_t>(k > 1u ? k : 1u);
+}
+__host__ __device__ __forceinline__ uint32_t minibatch_size(uint32_t n, int mb, int nmb, uint32_t step_cap) {
+    const uint32_t s = minibatch_stride(n, nmb, step_cap);
+    return n > static_cast<uint32_t>(mb) ? (n - static_cast<uint32_t>(mb) + s - 1u) / s : 0u;
 }
 
 // Optimiser steps taken for the first mb minibatches (the empty ones take none).
 __host__ __device__ __forceinline__ uint32_t steps_before(uint32_t n, int mb, int nmb) {
     uint32_t k = 0;
-    for (int i = 0; i < mb; ++i) k += minibatch_size(n, i, nmb) > 0u ? 1u : 0u;
+    for (int i = 0; i < mb; ++i) k += n > static_cast<uint32_t>(i) ? 1u : 0u;
     return k;
 }
 
@@ -498,12 +543,14 @@ __host__ __device__ __forceinline__ uint32_t steps_before(uint32_t n, int mb, in
 // weight gradient in shared memory for kGTrainWarps warps (one CTA per SM).
 constexpr int kGTrainWarps = 4;
 __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net, const GuideSample* __restrict__ samples_all,
-                                                     const uint32_t* count, uint32_t cap, int mb, int nmb) {
-    const uint32_t n = minibatch_size(min(*count, cap), mb, nmb);
+                                                     const uint32_t* count, uint32_t cap, int mb, int nmb,
+                                                     uint32_t step_cap) {
+    const uint32_t total = min(*count, cap);
+    const uint32_t n = minibatch_size(total, mb, nmb, step_cap);
     if (n == 0u) return;
-    // row r of this minibatch is sample mb + r * nmb
+    // row r of this minibatch is sample mb + r * stride
     const GuideSample* __restrict__ samples = samples_all + mb;
-    const uint32_t sstride = static_cast<uint32_t>(nmb);
+    const uint32_t sstride = minibatch_stride(total, nmb, step_cap);
     const float inv_n = 1.0f / static_cast<float>(n);
     extern __shared__ __align__(16) unsigned char g_smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(g_smem);                       // W  [out][in+8]
@@ -687,6 +734,8 @@ struct GuideState {
     int          mode = 0;            // 0 off, PT_GUIDE_USE, PT_GUIDE_TRAIN
     float        lr = 1e-2f;
     float        alpha = kGuideAlpha;
+    int          paths_per_step = kGuideMinibatchPaths;   // optimiser steps: one per this many paths of a pass
+    uint32_t     samples_per_step = kGuideStepSamples;    // cap of training samples per step (0 = all)
 };
 
 // After a pass's minibatches: advance the step counter by the steps taken
@@ -707,7 +756,7 @@ __global__ void k_guide_step(uint32_t* sample_count, uint32_t* step, float* loss
 __global__ void k_guide_adam(GuideNet net, const uint32_t* count, uint32_t cap, int mb, int nmb, const uint32_t* step,
                              float lr_w, float lr_g, float b1, float b2, float eps) {
     const uint32_t n = min(*count, cap);
-    if (minibatch_size(n, mb, nmb) == 0u) return;
+    if (n <= static_cast<uint32_t>(mb)) return;
     const float t = static_cast<float>(*step + steps_before(n, mb, nmb) + 1u);
     const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
     const size_t nw = kGWeights;
@@ -734,7 +783,11 @@ __global__ void k_guide_adam(GuideNet net, const uint32_t* count, uint32_t cap, 
             p.y -= lr_g * (m.y / bc1) / (sqrtf(v.y / bc2) + eps);
             net.grid_m[j] = m; net.grid_v[j] = v; net.grid_master[j] = p;
             reinterpret_cast<ulonglong2*>(net.grid_grad)[j] = make_ulonglong2(0ull, 0ull);
-            net.grid[j] = __floats2half2_rn(p.x, p.y);
+            // the FP16 pair table: this entry's own slot and the neighbour slot of the entry before it
+            const __half2 hp = __floats2half2_rn(p.x, p.y);
+            const size_t prev = (j & ~static_cast<size_t>(kGTable - 1)) | ((j + kGTable - 1) & (kGTable - 1));
+            reinterpret_cast<__half2*>(net.grid + j)[0] = hp;
+            reinterpret_cast<__half2*>(net.grid + prev)[1] = hp;
         }
     }
 }

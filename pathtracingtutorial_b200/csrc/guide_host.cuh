@@ -47,7 +47,7 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     }
     const size_t ng = static_cast<size_t>(kGLevels) * kGTable;
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    const size_t off_master = al(ng * sizeof(__half2));
+    const size_t off_master = al(ng * sizeof(uint2));
     const size_t off_grad = off_master + al(ng * sizeof(float2));       // 2 x u64 per entry
     const size_t off_m = off_grad + al(ng * 2 * sizeof(unsigned long long));
     const size_t off_v = off_m + al(ng * sizeof(float2));
@@ -61,7 +61,7 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     if (!guide_cuda_ok(cudaMalloc(&g.params, total), "parameter allocation")) return PT_ERR_NOMEM;
     g.param_bytes = total;
     char* base = static_cast<char*>(g.params);
-    g.net.grid = reinterpret_cast<__half2*>(base);
+    g.net.grid = reinterpret_cast<uint2*>(base);
     g.net.grid_master = reinterpret_cast<float2*>(base + off_master);
     g.net.grid_grad = reinterpret_cast<unsigned long long*>(base + off_grad);
     g.net.grid_m = reinterpret_cast<float2*>(base + off_m);
@@ -79,8 +79,12 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     std::vector<float> gm(2 * ng);
     std::uniform_real_distribution<float> uf(-1e-4f, 1e-4f);
     for (float& x : gm) x = uf(rng);
-    std::vector<__half2> gh(ng);
-    for (size_t i = 0; i < ng; ++i) gh[i] = __floats2half2_rn(gm[2 * i], gm[2 * i + 1]);
+    std::vector<__half2> gh(2 * ng);   // the pair table (see GuideNet::grid)
+    for (size_t i = 0; i < ng; ++i) {
+        const size_t next = (i & ~static_cast<size_t>(kGTable - 1)) | ((i + 1) & (kGTable - 1));
+        gh[2 * i] = __floats2half2_rn(gm[2 * i], gm[2 * i + 1]);
+        gh[2 * i + 1] = __floats2half2_rn(gm[2 * next], gm[2 * next + 1]);
+    }
     std::vector<float> w(kGWeights);
     std::vector<__nv_bfloat16> wb(kGWeights);
     for (int l = 0; l < 4; ++l) {
@@ -93,7 +97,7 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
         }
     }
     for (int i = 0; i < kGWeights; ++i) wb[i] = __float2bfloat16_rn(w[i]);
-    bool ok = guide_cuda_ok(cudaMemcpy(g.net.grid, gh.data(), ng * sizeof(__half2), cudaMemcpyHostToDevice), "upload") &&
+    bool ok = guide_cuda_ok(cudaMemcpy(g.net.grid, gh.data(), ng * sizeof(uint2), cudaMemcpyHostToDevice), "upload") &&
               guide_cuda_ok(cudaMemcpy(g.net.grid_master, gm.data(), ng * sizeof(float2), cudaMemcpyHostToDevice), "upload") &&
               guide_cuda_ok(cudaMemset(g.net.grid_grad, 0, off_w - off_grad), "clear") &&
               guide_cuda_ok(cudaMemcpy(g.net.w, wb.data(), kGWeights * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice), "upload") &&

@@ -1333,10 +1333,11 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
                     k_guide_collect<<<wf.grid_finalize, 256, 0, st>>>(P, np, gs->net, gs->samples, gs->scan_offsets,
                                                                       gs->counters, gs->sample_cap);
                     // optimiser steps over this pass's samples in minibatches
-                    const int nmb = guide_minibatches(P.npix * count);
+                    const int nmb = guide_minibatches(int64_t(P.npix) * count, gs->paths_per_step);
                     for (int mb = 0; mb < nmb; ++mb) {
                         k_guide_train<<<wf.sms, 32 * kGTrainWarps, kGTrainSmem, st>>>(gs->net, gs->samples, gs->counters,
-                                                                         gs->sample_cap, mb, nmb);
+                                                                         gs->sample_cap, mb, nmb,
+                                                                         gs->samples_per_step);
                         k_guide_adam<<<wf.sms * 8, 256, 0, st>>>(gs->net, gs->counters, gs->sample_cap, mb, nmb,
                                                                  gs->step, gs->lr, gs->lr, 0.9f, 0.99f, 1e-10f);
                     }
@@ -1752,10 +1753,15 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
         cudaEventDestroy(t1);
         if (rc) return rc;
     } else if (use_graph) {
-        std::vector<unsigned char> key(sizeof(WaveParams) + sizeof(cudaStream_t) + sizeof(int));
+        // everything the captured launches bake in: the parameters, the stream,
+        // the frame count and the guide's training settings
+        struct GuideKey { const void* params; float lr; int paths_per_step; uint32_t samples_per_step; } gk{};
+        if (gs) gk = GuideKey{gs->params, gs->lr, gs->paths_per_step, gs->samples_per_step};
+        std::vector<unsigned char> key(sizeof(WaveParams) + sizeof(cudaStream_t) + sizeof(int) + sizeof(GuideKey));
         std::memcpy(key.data(), &P, sizeof(WaveParams));
         std::memcpy(key.data() + sizeof(WaveParams), &st, sizeof(cudaStream_t));
         std::memcpy(key.data() + sizeof(WaveParams) + sizeof(cudaStream_t), &nframes, sizeof(int));
+        std::memcpy(key.data() + sizeof(WaveParams) + sizeof(cudaStream_t) + sizeof(int), &gk, sizeof(GuideKey));
         if (!wf.graph || key != wf.graph_key) {
             if (wf.graph) { cudaGraphExecDestroy(wf.graph); wf.graph = nullptr; }
             cudaGraph_t g = nullptr;
@@ -1778,7 +1784,7 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     if (!timing) wf.extend_launches += passes * static_cast<uint64_t>(P.max_depth);
     wf.kernel_launches += 1 + passes * (1 + 4 * static_cast<uint64_t>(P.max_depth));
     if (P.gmix)
-        wf.kernel_launches += passes * (P.max_depth + (P.grec ? 5 + 2 * guide_minibatches(P.npix * lanes) : 0));
+        wf.kernel_launches += passes * (P.max_depth + (P.grec ? 5 + 2 * guide_minibatches(int64_t(P.npix) * lanes, wf.guide->paths_per_step) : 0));
     return PT_OK;
 }
 
@@ -2020,8 +2026,8 @@ __global__ void __launch_bounds__(128) k_guide_eval(GuideNet net, const float* q
         __syncwarp();
         if (lane < 16 && tile * 16 + lane < n) {
             const uint32_t r = tile * 16 + lane;
-            float mix[kGMix];
-            raw_to_mixture(my + lane * kGOutPad, mix);
+            alignas(16) float mix[kGMix];
+            mixture_record(my + lane * kGOutPad, mix);
             out[r] = mix_pdf(mix, normalize(mk(qd[6 * r + 3], qd[6 * r + 4], qd[6 * r + 5])));
         }
         __syncwarp();
@@ -2044,6 +2050,10 @@ void guide_destroy(pt_guide* h) {
 
 void guide_set_lr(pt_guide* h, float lr) { h->g.lr = lr; }
 void guide_set_alpha(pt_guide* h, float alpha) { h->g.alpha = alpha; }
+void guide_set_training(pt_guide* h, int paths_per_step, uint32_t samples_per_step) {
+    h->g.paths_per_step = paths_per_step > 0 ? paths_per_step : kGuideMinibatchPaths;
+    h->g.samples_per_step = samples_per_step;
+}
 
 int guide_info(const pt_guide* h, uint32_t* steps, uint32_t* samples) {
     uint32_t c[2] = {0, 0};
@@ -2081,10 +2091,10 @@ int guide_get_params(const pt_guide* h, float* weights, float* grid, float* meta
     for (int i = 0; i < kGWeights; ++i) weights[i] = __bfloat162float(wb[i]);
     if (grid) {
         const size_t ng = static_cast<size_t>(kGLevels) * kGTable;
-        std::vector<__half2> gh(ng);
-        PT_CU(cudaMemcpy(gh.data(), h->g.net.grid, ng * sizeof(__half2), cudaMemcpyDeviceToHost));
+        std::vector<__half2> gh(2 * ng);
+        PT_CU(cudaMemcpy(gh.data(), h->g.net.grid, ng * sizeof(uint2), cudaMemcpyDeviceToHost));
         for (size_t i = 0; i < ng; ++i) {
-            const float2 v = __half22float2(gh[i]);
+            const float2 v = __half22float2(gh[2 * i]);
             grid[2 * i] = v.x;
             grid[2 * i + 1] = v.y;
         }
@@ -2111,7 +2121,7 @@ int guide_backward(pt_guide* h, const float* samples, uint32_t n, float* wgrad, 
     if (e == cudaSuccess) {
         GuideNet net = h->g.net;
         net.loss_fix = nullptr;   // leave the training-loss record alone
-        k_guide_train<<<148, 32 * kGTrainWarps, kGTrainSmem>>>(net, ds, dn, n, 0, 1);
+        k_guide_train<<<148, 32 * kGTrainWarps, kGTrainSmem>>>(net, ds, dn, n, 0, 1, 0u);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
     }

@@ -42,9 +42,9 @@ constexpr int kStackDepth = 64;
 // itself when the device cannot hold it).  Larger passes amortise the short
 // launches of the deep bounces: on the 1080p 256-spp workload 2^25 / 2^26 /
 // 2^27 slots render at 1621 / 1684 / 1719 Mrays/s.  A guide that samples
-// adds its mixture per path (160 B; 2.7 GB at 2^24 paths).
+// adds its mixture per path (160 B; 10.7 GB at 2^26 paths).
 constexpr int64_t kDefaultPathsInFlight = int64_t(1) << 27;
-constexpr int64_t kGuidedPathsInFlight = int64_t(1) << 24;
+constexpr int64_t kGuidedPathsInFlight = int64_t(1) << 26;
 // While a guide trains, passes stay small: every pass ends with optimiser
 // steps, so smaller passes mean more steps per sample.
 constexpr int64_t kTrainingPathsInFlight = int64_t(1) << 20;

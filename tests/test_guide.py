@@ -185,14 +185,17 @@ def test_guided_render_unbiased_and_lower_error():
     """Guided vs plain on the hidden-light room at equal samples per pixel
     (256): the image means agree with an 8192-spp plain render within four
     standard errors (estimated from eight independent 32-spp parts of each
-    render), and the trained guide lowers the relative MSE against it."""
+    render), and the trained guide lowers the relative MSE against it.  The
+    guide trains for 4096 spp: at 64 x 64 pixels that is 16M paths, 512
+    optimiser steps (one per 2^15 paths) -- about what 16 spp give at
+    1024 x 1024."""
     import pathtracingtutorial_b200 as pt
     from pathtracingtutorial_b200 import scenes
     sa = scenes.hidden_light_room(width=64, height=64, n_boxes=40, box_subdiv=2, spp=256, max_depth=10)
     s = _scene(sa)
     ref = _render_from(s, 8192, 1_000_000)[..., :3].astype(np.float64)
     g = pt.Guide(s, seed=1)
-    pt.render_guided(s, train_spp=256, spp=4, guide=g)
+    pt.render_guided(s, train_spp=4096, spp=4, guide=g)
     spf = sa.sample_per_frame
     parts_plain = [_render_from(s, 32, k * (32 // spf))[..., :3].astype(np.float64) for k in range(8)]
     parts_guided = [pt.render_batch([(s, 32, k * (32 // spf), None, g)])[0][0][..., :3].astype(np.float64)
