@@ -56,10 +56,13 @@ def parse_args():
                    help="wavefront path slots of the render (0: the autotuner's choice)")
     p.add_argument("--no-autotune", action="store_true",
                    help="render with the library defaults instead of the autotuner's choice")
-    p.add_argument("--workload", choices=["render", "batch", "large", "build"], default="render",
+    p.add_argument("--workload", choices=["render", "batch", "large", "build", "guided"], default="render",
                    help="render: the bench line; batch: the 64-scene uneven batch in one launch; large: the "
-                        "20M-triangle 16-camera case; build: host vs GPU BVH build of the bench scene "
-                        "(separate lines)")
+                        "20M-triangle 16-camera case; build: host vs GPU BVH build of the bench scene; "
+                        "guided: online training then a guided render of the hidden-light room at "
+                        "--room-size (a small case for profiling the guide's kernels) (separate lines)")
+    p.add_argument("--room-size", type=int, default=512, help="image side of --workload guided")
+    p.add_argument("--room-train-spp", type=int, default=4, help="training spp of --workload guided")
     p.add_argument("--large-spp", type=int, default=512, help="samples per pixel per camera of --workload large")
     p.add_argument("--large-train-spp", type=int, default=64, help="guide training spp of --workload large")
     p.add_argument("--builder", choices=["host", "device"], default="host",
@@ -796,9 +799,35 @@ def build_workload(args):
         "trace_ratio": round(dev_rate / host_rate, 3)}))
 
 
+def guided_workload(args):
+    """Online training for --room-train-spp, then --spp guided samples per
+    pixel of the hidden-light room at --room-size squared; stage times of the
+    guided render.  A profiling case for the guide's kernels."""
+    import pathtracingtutorial_b200 as pt
+    from pathtracingtutorial_b200 import scenes
+    sa = scenes.hidden_light_room(width=args.room_size, height=args.room_size)
+    s = sa.scene()
+    s.build_accel()
+    s.upload_to_device(0)
+    t0 = time.perf_counter()
+    img, g, st = pt.render_guided(s, train_spp=args.room_train_spp, spp=args.spp)
+    secs = time.perf_counter() - t0
+    info = g.info()
+    g.close()
+    print(json.dumps({
+        "metric": "guided render", "workload": f"{sa.name} {len(sa.faces)} tri, {args.room_size}^2, "
+                                              f"depth {sa.max_depth}",
+        "train_spp": args.room_train_spp, "spp": args.spp, "seconds": round(secs, 3),
+        "optimiser_steps": info["steps"], "mean": float(img[..., :3].mean()),
+        "rays": int(st["camera_rays"] + st["extension_rays"] + st["shadow_rays"]),
+        "kernel_launches": int(st["kernel_launches"])}))
+
+
 def main():
     args = parse_args()
-    if args.workload == "build":
+    if args.workload == "guided":
+        guided_workload(args)
+    elif args.workload == "build":
         build_workload(args)
     elif args.workload == "batch":
         batch_workload(args)

@@ -255,6 +255,30 @@ PT_HD BsdfEval disney_eval(const MatEval& m, f3 wo, f3 wi, f3 n, bool entering) 
     return r;
 }
 
+// Density with which disney_sample draws wi, given disney_eval's pdf of it.
+// The two differ in the clearcoat lobe: it is sampled from the visible
+// normals of its GGX distribution, while the eval pdf counts it with the
+// distribution of normals (D noh / (4 hol)); this swaps that term.  (The
+// reflections that total internal reflection gives the transmission branch
+// are not counted either way.)  The plain integrator only ever uses the eval
+// pdf, as the reference does; the guided mixture needs the sampler's own
+// density to keep the plain integrator's expectation.
+PT_HD float disney_sample_density(const MatEval& m, f3 wo, f3 wi, f3 n, float eval_pdf) {
+    if (m.clearcoat <= 0.0f) return eval_pdf;
+    const float nol = dot(n, wi);
+    const float nov = dot(n, wo);
+    if (nol < 1e-5f || nov < 1e-5f) return eval_pdf;
+    const f3 h = normalize(wo + wi);
+    const float noh = fmaxf(dot(n, h), 0.0f);
+    const float hol = fmaxf(dot(h, wi), 0.0f);
+    const Frame fr = make_frame(n);
+    const float ca = fmaxf(m.cc_roughness * m.cc_roughness, 0.001f);
+    const LobeWeights w = lobe_weights(m);
+    const float ndf = ggx_d(noh, ca) * noh / (4.0f * hol + 1e-7f);
+    const float vis = pdf_vndf(to_local(fr, wo), to_local(fr, h), ca, ca) / (4.0f * hol + 1e-7f);
+    return fmaxf(eval_pdf + w.cc * (vis - ndf), 0.0f);
+}
+
 struct BsdfSample { f3 wi; f3 weight; float pdf; bool delta; bool valid; };
 
 #if defined(__CUDA_ARCH__)

@@ -4,10 +4,12 @@
 // A position-conditioned directional distribution q(w | x) is learned online
 // from the tracer's own samples and mixed with BSDF sampling by one-sample MIS:
 // with probability alpha the direction is drawn from q, otherwise from the
-// BSDF, and every sample is weighted by f / (alpha q + (1 - alpha) p_bsdf), so
-// the estimator keeps the expectation of the BSDF-only integrator wherever
-// p_bsdf > 0.  Vertices that can produce delta samples (roughness < 0.01) are
-// never guided.
+// BSDF's sampler (density pB), and the plain integrator's weight f / pdf is
+// scaled by pB / (alpha q + (1 - alpha) pB), so the estimator keeps the
+// expectation of the BSDF-only integrator wherever pB > 0 -- also where the
+// BSDF's pdf is not its sampler's density.  Light samples and emitter hits
+// keep the plain integrator's MIS weights.  Vertices that can produce delta
+// samples (roughness < 0.01) are never guided.
 //
 // Network: multi-resolution hash-grid encoding of the position (16 levels x 2
 // features, 2^19 FP16 entries per level, trilinear) -> 3 hidden layers of 64

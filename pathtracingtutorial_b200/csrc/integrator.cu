@@ -284,18 +284,13 @@ __device__ __forceinline__ uint32_t sample_alias(const pt_alias_entry* t, uint32
     return (u2 < e.x) ? i : __float_as_uint(e.y);
 }
 // evaluateDirectLight (direct_lighting.cuh:204-218) without the visibility term.
-// At a guided vertex the directional strategy is the guide/BSDF mixture, so
-// its pdf (alpha q + (1 - alpha) p_bsdf) enters the power heuristic.
-template <bool Guided>
-__device__ __forceinline__ f3 direct_term(const MatEval& me, f3 wo, f3 wi, f3 n, f3 radiance, float light_pdf,
-                                          const float* gmix, float galpha) {
+// A guided vertex weighs its light samples exactly as the plain integrator
+// does (power heuristic against the BSDF's pdf), so the light sample and the
+// directional sample together keep the plain integrator's expectation.
+__device__ __forceinline__ f3 direct_term(const MatEval& me, f3 wo, f3 wi, f3 n, f3 radiance, float light_pdf) {
     const BsdfEval b = PT_BSDF_EVAL(me, wo, wi, n, true);
     if (b.pdf <= 0.0f) return mk(0.0f);
-    float dir_pdf = b.pdf;
-    if constexpr (Guided) {
-        if (gmix) dir_pdf = galpha * mix_pdf(gmix, wi) + (1.0f - galpha) * b.pdf;
-    }
-    const float mis = power_heuristic(light_pdf, dir_pdf);
+    const float mis = power_heuristic(light_pdf, b.pdf);
     return radiance * b.f * (mis / (light_pdf + 1e-7f));
 }
 
@@ -561,7 +556,7 @@ __device__ int shade_front(const DeviceScene& s, int arg_rtl, int depth, f3 ro, 
             }
             if (ok) {
                 const f3 le = material_emission(s.materials[lf.material_id]);
-                contrib = T * direct_term<Guided>(me, wo, wi, N, le, pdf, gmix, gv.alpha);
+                contrib = T * direct_term(me, wo, wi, N, le, pdf);
                 ok = !is_zero(contrib);
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
@@ -584,7 +579,7 @@ __device__ int shade_front(const DeviceScene& s, int arg_rtl, int depth, f3 ro, 
             f3 contrib = mk(0.0f);
             if (ok) { pdf = env_pdf(s, wi); ok = pdf > 0.0f; }
             if (ok) {
-                contrib = T * direct_term<Guided>(me, wo, wi, N, env_radiance(s, wi), pdf, gmix, gv.alpha);
+                contrib = T * direct_term(me, wo, wi, N, env_radiance(s, wi), pdf);
                 ok = !is_zero(contrib);
             }
             const float sg = dot(wi, N) >= 0.0f ? 1.0f : -1.0f;
@@ -649,27 +644,33 @@ __device__ bool shade_back(int arg_rtl, int depth, f3 rd, const ShadePoint& sp, 
     const float* gmix = Guided ? sp.gmix : nullptr;
     BsdfSample bs;
     float plain_w = 0.0f;   // guided: max3(f cos / p_bsdf) of this vertex, for the roulette
+    float mix_p = 0.0f;     // guided: the density the direction was drawn with (training records)
     if (Guided && gmix) {
-        // one-sample MIS between the learned mixture and the BSDF
+        // One-sample MIS between the learned mixture q and the BSDF's own
+        // sampler (density pB): the direction comes from q with probability
+        // alpha, else from the BSDF, and the plain integrator's weight f / pdf
+        // is scaled by pB / (alpha q + (1 - alpha) pB).  Its expectation is
+        // the plain integrator's, including where the reference's pdf is not
+        // the sampler's density (disney_sample_density).  bs.pdf stays the
+        // BSDF's pdf, for the emitter hit's power heuristic.
         const float sel = rng_next(rng);
         if (sel < gv.alpha) {
             const float u0 = rng_next(rng), u1 = rng_next(rng), u2 = rng_next(rng);
             bs.wi = mix_sample(gmix, u0, u1, u2);
             const BsdfEval ev = PT_BSDF_EVAL(me, wo, bs.wi, N, entering);
-            const float p = gv.alpha * mix_pdf(gmix, bs.wi) + (1.0f - gv.alpha) * ev.pdf;
-            bs.valid = p > 0.0f && !is_zero(ev.f);
-            bs.pdf = p;
-            bs.weight = bs.valid ? ev.f / p : mk(0.0f);
+            bs.pdf = ev.pdf;
             bs.delta = false;
-            plain_w = ev.pdf > 0.0f ? max3(ev.f) / ev.pdf : max3(bs.weight);
+            bs.valid = ev.pdf > 0.0f && !is_zero(ev.f);
+            bs.weight = ev.f / (ev.pdf + 1e-7f);   // the plain integrator's weight
         } else {
             bs = PT_BSDF_SAMPLE(me, wo, N, rng, arg_rtl, entering);
+        }
+        if (bs.valid) {
+            const float pB = disney_sample_density(me, wo, bs.wi, N, bs.pdf);
+            mix_p = gv.alpha * mix_pdf(gmix, bs.wi) + (1.0f - gv.alpha) * pB;
+            bs.valid = mix_p > 0.0f && pB > 0.0f;
             plain_w = max3(bs.weight);
-            if (bs.valid) {
-                const float p = gv.alpha * mix_pdf(gmix, bs.wi) + (1.0f - gv.alpha) * bs.pdf;
-                bs.weight = bs.weight * ((bs.pdf + 1e-7f) / p);
-                bs.pdf = p;
-            }
+            bs.weight = bs.weight * (pB / fmaxf(mix_p, 1e-30f));
         }
     } else {
         bs = PT_BSDF_SAMPLE(me, wo, N, rng, arg_rtl, entering);
@@ -706,7 +707,7 @@ __device__ bool shade_back(int arg_rtl, int depth, f3 rd, const ShadePoint& sp, 
     if (Guided && gv.rec && !bs.delta) {
         // training record: where, which way, with which pdf, the throughput
         // that scales everything found along this direction, |cos| to the normal
-        gv.rec[0] = make_float4(hp.x, hp.y, hp.z, bs.pdf);
+        gv.rec[0] = make_float4(hp.x, hp.y, hp.z, mix_p);
         gv.rec[1] = make_float4(nd.x, nd.y, nd.z, 1.0f);
         gv.rec[2] = make_float4(T.x, T.y, T.z, fabsf(dot(N, nd)));
     }
