@@ -11,9 +11,10 @@
 //   sampleDisneyBsdf         disney_bsdf.cuh:325-410
 //   GGX/Smith/Fresnel/VNDF   Part_2/src/materials/microfacet.cuh:10-113
 // The tangent argument of the reference's eval/sample is never read (both
-// build their frame from N alone), so it is not carried here.  Texture ids are
-// not resolved: the JSON scene format cannot reference textures (only the glTF
-// importer sets them), so every material is evaluated untextured.
+// build their frame from N alone), so it is not carried here.  Texture lookups
+// (fetchMaterial's textured parameters) happen before this, in the shading
+// kernels (resolve_material_textured in integrator.cu); MatEval holds the
+// resolved values.
 #pragma once
 
 #include "pt_internal.h"
