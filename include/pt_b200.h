@@ -433,8 +433,8 @@ int pt_guide_set_learning_rate(pt_guide* guide, float lr);
 int pt_guide_set_alpha(pt_guide* guide, float alpha);
 /* online training: one optimiser step per `paths_per_step` paths of a pass
    (0 = 32768; at most 32 steps per pass), each on at most `samples_per_step`
-   training samples spread evenly over the pass's (0 = all of them).  The
-   defaults are 32768 and 65536. */
+   training samples spread evenly over the pass's (0 or more than 131072:
+   131072, the most one step takes).  The defaults are 32768 and 65536. */
 int pt_guide_set_training(pt_guide* guide, int32_t paths_per_step, uint32_t samples_per_step);
 /* steps taken and samples used by the last step (synchronises the device) */
 int pt_guide_info(const pt_guide* guide, uint32_t* steps, uint32_t* last_samples);

@@ -463,8 +463,8 @@ class Guide:
 
     def set_training(self, paths_per_step: int = 0, samples_per_step: int = 65536) -> None:
         """Online training: one optimiser step per `paths_per_step` paths of a
-        pass (0 = 32768), each on at most `samples_per_step` samples (0 = all;
-        65536 is the library's default)."""
+        pass (0 = 32768), each on at most `samples_per_step` samples (0 = the
+        most a step takes, 131072; 65536 is the library's default)."""
         check(lib().pt_guide_set_training(self._h, int(paths_per_step), int(samples_per_step)))
 
     def attach(self, integrator: PathIntegrator, mode: int) -> None:

@@ -23,11 +23,13 @@
 // incident radiance to q with the one-sample estimate
 // -L_in(w) |cos| / p(w) * log q(w | x)  per recorded path vertex, in
 // minibatches interleaved over the whole image; the backward pass runs on the
-// tensor cores too (dX = dY W and dW = dY^T X per warp tile), and Adam
+// tensor cores too (dX = dY W per warp tile in the forward/backward kernel,
+// dW = dY^T X as a split-K GEMM over the step's rows in k_guide_dw), and Adam
 // updates FP32 master copies.  Training is deterministic: the samples are
-// stored in path order (count, scan, write), and every gradient sum is
-// accumulated in 64-bit fixed point (units of 2^-40) with integer atomics,
-// whose result does not depend on the order in which they land.
+// stored in path order (count, scan, write), the weight gradient is summed in
+// fixed row chunks in a fixed order, and the hash-grid gradient is scattered
+// in 64-bit fixed point (units of 2^-40) with integer atomics, whose result
+// does not depend on the order in which they land.
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -439,33 +441,33 @@ __device__ __forceinline__ void store_t(const uint32_t (&a)[K / 16][4], __nv_bfl
     }
 }
 
-// dW[out][in] += DYT[out][16] . XT[in][16]^T  (K = the warp's 16 rows), into the
-// fixed-point shared dW.
-template <int OUT, int IN>
-__device__ __forceinline__ void accum_dw(const __nv_bfloat16* DYT, const __nv_bfloat16* XT, unsigned long long* sdw) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+// The weight gradient dW_l = DY_l^T X_l is a GEMM over the minibatch's rows;
+// the forward/backward kernel stores each layer's input X_l and upstream
+// gradient DY_l transposed ([column][row], rows contiguous, bf16) in global
+// memory, and k_guide_dw sums them in fixed row chunks (deterministic, no
+// atomics).  Row block: kGTrainRows rows per matrix.
+constexpr int kGTrainRows = 1 << 17;      // rows (training samples) of one optimiser step at most
+constexpr int kGDwChunk = 512;            // rows per partial sum of k_guide_dw
+constexpr int kGDwChunks = kGTrainRows / kGDwChunk;
+// bf16 element offsets of X_l ([IN_l][R]) and DY_l ([OUT_l][R]) in the row store
+__host__ __device__ constexpr size_t g_rx(int l) {
+    return static_cast<size_t>(l == 0 ? 0 : kGIn + (l - 1) * kGHid) * kGTrainRows;
+}
+__host__ __device__ constexpr size_t g_rdy(int l) {
+    return static_cast<size_t>(kGIn + 3 * kGHid + (l == 3 ? 0 : kGOutPad + (2 - l) * kGHid)) * kGTrainRows;
+}
+constexpr size_t kGRowStoreElems = static_cast<size_t>(kGIn + 3 * kGHid + kGOutPad + 3 * kGHid) * kGTrainRows;
+
+// Copy a warp's transposed [N][16] tile (row stride `ld` bf16) to columns
+// r0 .. r0 + 15 of a [N][kGTrainRows] matrix: two 16-byte stores per row.
+template <int N>
+__device__ __forceinline__ void store_rows(const __nv_bfloat16* T, int ld, __nv_bfloat16* dst, uint32_t r0) {
+    const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int mt = 0; mt < OUT / 16; ++mt) {
-        uint32_t a[4];
-        const __nv_bfloat16* r0 = DYT + (mt * 16 + g) * 24 + 2 * c;
-        const __nv_bfloat16* r1 = DYT + (mt * 16 + g + 8) * 24 + 2 * c;
-        a[0] = *reinterpret_cast<const uint32_t*>(r0);
-        a[1] = *reinterpret_cast<const uint32_t*>(r1);
-        a[2] = *reinterpret_cast<const uint32_t*>(r0 + 8);
-        a[3] = *reinterpret_cast<const uint32_t*>(r1 + 8);
-#pragma unroll
-        for (int nt = 0; nt < IN / 8; ++nt) {
-            const __nv_bfloat16* xb = XT + (nt * 8 + g) * 16 + 2 * c;
-            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(xb);
-            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(xb + 8);
-            float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            mma_bf16(acc, a, b0, b1);
-            const int m0 = mt * 16 + g, n0 = nt * 8 + 2 * c;
-            atomicAdd(&sdw[m0 * IN + n0], g_fix(acc[0]));
-            atomicAdd(&sdw[m0 * IN + n0 + 1], g_fix(acc[1]));
-            atomicAdd(&sdw[(m0 + 8) * IN + n0], g_fix(acc[2]));
-            atomicAdd(&sdw[(m0 + 8) * IN + n0 + 1], g_fix(acc[3]));
-        }
+    for (int k = lane; k < 2 * N; k += 32) {
+        const int row = k >> 1, half = k & 1;
+        const uint4 v = *reinterpret_cast<const uint4*>(T + row * ld + 8 * half);
+        *reinterpret_cast<uint4*>(dst + static_cast<size_t>(row) * kGTrainRows + r0 + 8 * half) = v;
     }
 }
 
@@ -528,6 +530,11 @@ __host__ __device__ __forceinline__ uint32_t minibatch_stride(uint32_t n, int nm
     const uint64_t k = (static_cast<uint64_t>(n) + per - 1u) / per;
     return static_cast<uint32_t>(nmb) * static_cast<uint32_t>(k > 1u ? k : 1u);
 }
+// The per-step sample cap the kernels use: the caller's, within the row store.
+__host__ __device__ __forceinline__ uint32_t guide_step_cap(uint32_t samples_per_step) {
+    return (samples_per_step == 0u || samples_per_step > static_cast<uint32_t>(kGTrainRows)) ? kGTrainRows
+                                                                                           : samples_per_step;
+}
 __host__ __device__ __forceinline__ uint32_t minibatch_size(uint32_t n, int mb, int nmb, uint32_t step_cap) {
     const uint32_t s = minibatch_stride(n, nmb, step_cap);
     return n > static_cast<uint32_t>(mb) ? (n - static_cast<uint32_t>(mb) + s - 1u) / s : 0u;
@@ -540,13 +547,15 @@ __host__ __device__ __forceinline__ uint32_t steps_before(uint32_t n, int mb, in
     return k;
 }
 
-// Gradient of the mean loss over minibatch mb (of nmb) of the collected samples.
-// Training CTAs hold one copy of both weight layouts and the fixed-point
-// weight gradient in shared memory for kGTrainWarps warps (one CTA per SM).
-constexpr int kGTrainWarps = 4;
+// Forward and backward of minibatch mb (of nmb) of the collected samples:
+// the loss gradient of every row, the hash-grid gradient (fixed-point
+// atomics), and each layer's input and upstream gradient in the row store
+// for k_guide_dw.  CTAs of kGTrainWarps warps share one copy of both weight
+// layouts (one CTA per SM).
+constexpr int kGTrainWarps = 8;
 __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net, const GuideSample* __restrict__ samples_all,
                                                      const uint32_t* count, uint32_t cap, int mb, int nmb,
-                                                     uint32_t step_cap) {
+                                                     uint32_t step_cap, __nv_bfloat16* __restrict__ rows) {
     const uint32_t total = min(*count, cap);
     const uint32_t n = minibatch_size(total, mb, nmb, step_cap);
     if (n == 0u) return;
@@ -557,8 +566,7 @@ __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net,
     extern __shared__ __align__(16) unsigned char g_smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(g_smem);                       // W  [out][in+8]
     __nv_bfloat16* swt = sw + kGSmemW;                                                 // WT [in][out+8]
-    unsigned long long* sdw = reinterpret_cast<unsigned long long*>(swt + kGSmemW + 64);   // dW fixed point, packed
-    unsigned char* scratch0 = reinterpret_cast<unsigned char*>(sdw + kGWeights);
+    unsigned char* scratch0 = reinterpret_cast<unsigned char*>(swt + kGSmemW + 64);
     load_weights_smem(net, sw);
     // transposed weights: layer l, WT[in][out] with row length out + 8
     for (int l = 0; l < 4; ++l) {
@@ -570,7 +578,6 @@ __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net,
             swt[woff + k * (out + 8) + o] = net.w[g_woff(l) + i];
         }
     }
-    for (int i = threadIdx.x; i < kGWeights; i += blockDim.x) sdw[i] = 0ull;
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
     unsigned char* my = scratch0 + warp * kGWarpScratch;
@@ -648,26 +655,30 @@ __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net,
         }
         __syncwarp();
         // layer 3 (48 x 64)
-        accum_dw<kGOutPad, kGHid>(DYT, HT3, sdw + g_woff(3));
+        store_rows<kGOutPad>(DYT, 24, rows + g_rdy(3), tile * 16);
+        store_rows<kGHid>(HT3, 16, rows + g_rx(3), tile * 16);
         float dh[8][4];
         back_dx<kGOutPad, kGHid>(DY, WT3, dh);
         __syncwarp();
         store_dy<kGHid>(dh, HT3, DY, DYT);
         __syncwarp();
         // layer 2
-        accum_dw<kGHid, kGHid>(DYT, HT2, sdw + g_woff(2));
+        store_rows<kGHid>(DYT, 24, rows + g_rdy(2), tile * 16);
+        store_rows<kGHid>(HT2, 16, rows + g_rx(2), tile * 16);
         back_dx<kGHid, kGHid>(DY, WT2, dh);
         __syncwarp();
         store_dy<kGHid>(dh, HT2, DY, DYT);
         __syncwarp();
         // layer 1
-        accum_dw<kGHid, kGHid>(DYT, HT1, sdw + g_woff(1));
+        store_rows<kGHid>(DYT, 24, rows + g_rdy(1), tile * 16);
+        store_rows<kGHid>(HT1, 16, rows + g_rx(1), tile * 16);
         back_dx<kGHid, kGHid>(DY, WT1, dh);
         __syncwarp();
         store_dy<kGHid>(dh, HT1, DY, DYT);
         __syncwarp();
         // layer 0: dW0 and the gradient of the encoding
-        accum_dw<kGHid, kGIn>(DYT, XT0, sdw + g_woff(0));
+        store_rows<kGHid>(DYT, 24, rows + g_rdy(0), tile * 16);
+        store_rows<kGIn>(XT0, 16, rows + g_rx(0), tile * 16);
         float dx[4][4];
         back_dx<kGHid, kGIn>(DY, WT0, dx);
         __syncwarp();
@@ -698,19 +709,77 @@ __global__ void __launch_bounds__(32 * kGTrainWarps) k_guide_train(GuideNet net,
         }
         __syncwarp();
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kGWeights; i += blockDim.x)
-        if (sdw[i] != 0ull) atomicAdd(&net.w_grad[i], sdw[i]);
+}
+
+// dW_l = DY_l^T X_l over the minibatch's rows: block (chunk, l) sums rows
+// chunk * kGDwChunk .. + kGDwChunk (up to the tile-padded row count) of layer
+// l into partial[chunk][l's weights]; warp w takes output rows 16 w .. 16 w
+// + 15 (every column) on mma.sync m16n8k16, rows as the reduction dimension.
+__global__ void __launch_bounds__(128) k_guide_dw(const uint32_t* count, uint32_t cap, int mb, int nmb,
+                                                  uint32_t step_cap, const __nv_bfloat16* __restrict__ rows,
+                                                  float* __restrict__ partial) {
+    const uint32_t n = minibatch_size(min(*count, cap), mb, nmb, step_cap);
+    const uint32_t rpad = (n + 15u) & ~15u;
+    const uint32_t k0 = blockIdx.x * kGDwChunk;
+    if (k0 >= rpad) return;
+    const uint32_t k1 = min(rpad, k0 + kGDwChunk);
+    const int l = blockIdx.y;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+    const int out = g_out(l), in = g_in(l);
+    if (warp * 16 >= out) return;
+    const __nv_bfloat16* dy = rows + g_rdy(l) + static_cast<size_t>(warp * 16) * kGTrainRows;
+    const __nv_bfloat16* x = rows + g_rx(l);
+    float acc[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
+    for (uint32_t k = k0; k < k1; k += 16) {
+        uint32_t a[4];
+        const __nv_bfloat16* r0 = dy + static_cast<size_t>(g) * kGTrainRows + k + 2 * c;
+        const __nv_bfloat16* r1 = r0 + static_cast<size_t>(8) * kGTrainRows;
+        a[0] = *reinterpret_cast<const uint32_t*>(r0);
+        a[1] = *reinterpret_cast<const uint32_t*>(r1);
+        a[2] = *reinterpret_cast<const uint32_t*>(r0 + 8);
+        a[3] = *reinterpret_cast<const uint32_t*>(r1 + 8);
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            if (nt * 8 >= in) break;
+            const __nv_bfloat16* xb = x + static_cast<size_t>(nt * 8 + g) * kGTrainRows + k + 2 * c;
+            mma_bf16(acc[nt], a, *reinterpret_cast<const uint32_t*>(xb), *reinterpret_cast<const uint32_t*>(xb + 8));
+        }
+    }
+    float* dst = partial + static_cast<size_t>(blockIdx.x) * kGWeights + g_woff(l);
+    const int m0 = warp * 16 + g;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+        if (nt * 8 >= in) break;
+        const int n0 = nt * 8 + 2 * c;
+        dst[m0 * in + n0] = acc[nt][0];
+        dst[m0 * in + n0 + 1] = acc[nt][1];
+        dst[(m0 + 8) * in + n0] = acc[nt][2];
+        dst[(m0 + 8) * in + n0 + 1] = acc[nt][3];
+    }
+}
+
+// Sums the partials of k_guide_dw in chunk order into the weight gradient
+// (fixed point, as the optimiser reads it).
+__global__ void k_guide_dw_reduce(const uint32_t* count, uint32_t cap, int mb, int nmb, uint32_t step_cap,
+                                  const float* __restrict__ partial, unsigned long long* w_grad) {
+    const uint32_t n = minibatch_size(min(*count, cap), mb, nmb, step_cap);
+    const uint32_t chunks = (((n + 15u) & ~15u) + kGDwChunk - 1u) / kGDwChunk;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGWeights; i += gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        for (uint32_t ch = 0; ch < chunks; ++ch) s += partial[static_cast<size_t>(ch) * kGWeights + i];
+        if (chunks) w_grad[i] += g_fix(s);
+    }
 }
 
 // Adam on the MLP weights (FP32 master -> BF16 copy) and the hash grid
 // (FP32 master -> FP16 copy); gradients are cleared.
 // dynamic shared memory of the two network kernels (4 warps per CTA)
 constexpr int kGInferSmem = kGSmemW * 2 + kGInferWarps * 16 * kGOutPad * 4;
-constexpr int kGTrainSmem = (2 * kGSmemW + 64) * 2 + kGWeights * 8 + kGTrainWarps * kGWarpScratch;
+constexpr int kGTrainSmem = (2 * kGSmemW + 64) * 2 + kGTrainWarps * kGWarpScratch;
 static_assert(kGTrainSmem <= 227 * 1024, "training kernel shared memory");
-static_assert(((2 * kGSmemW + 64) * 2) % 16 == 0 && (kGWeights * 8) % 16 == 0 && kGWarpScratch % 16 == 0,
-              "shared memory carve alignment");
+static_assert(((2 * kGSmemW + 64) * 2) % 16 == 0 && kGWarpScratch % 16 == 0, "shared memory carve alignment");
 
 // Host-side state of one guide: the network, its optimiser state and the
 // buffers the wavefront fills (mixtures per queue entry, training records and
@@ -732,6 +801,8 @@ struct GuideState {
     uint32_t*    scan_offsets = nullptr;  // their exclusive prefix sums
     void*        scan_tmp = nullptr;      // the scan's temporary storage
     size_t       scan_tmp_bytes = 0;
+    __nv_bfloat16* rows = nullptr;    // training row store (kGRowStoreElems) for the weight gradient
+    float*       partial = nullptr;   // k_guide_dw's partial sums (kGDwChunks x kGWeights)
     uint32_t*    step = nullptr;      // optimiser steps taken (with the parameters: survives work resizes)
     int          mode = 0;            // 0 off, PT_GUIDE_USE, PT_GUIDE_TRAIN
     float        lr = 1e-2f;

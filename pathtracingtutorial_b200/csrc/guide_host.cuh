@@ -20,6 +20,8 @@ inline void guide_free(GuideState& g) {
     if (g.params) cudaFree(g.params);
     if (g.work) cudaFree(g.work);
     g.params = g.work = nullptr;
+    g.rows = nullptr;
+    g.partial = nullptr;
     g.step = g.counters = nullptr;
     g.param_bytes = g.work_bytes = 0;
     g.npix = g.depth = 0;
@@ -131,14 +133,18 @@ inline int guide_prepare_work(GuideState& g, int npix, int depth, bool records) 
                        "scan size"))
         return PT_ERR_CUDA;
     const size_t b_scan = records ? 2 * al((P + 1) * sizeof(uint32_t)) + al(scan_tmp) : 0;
-    const size_t total = b_mix + b_rec + b_smp + b_scan + 256;
+    const size_t b_rows = records ? al(kGRowStoreElems * sizeof(__nv_bfloat16)) : 0;
+    const size_t b_part = records ? al(static_cast<size_t>(kGDwChunks) * kGWeights * sizeof(float)) : 0;
+    const size_t total = b_mix + b_rec + b_smp + b_scan + b_rows + b_part + 256;
     if (!guide_cuda_ok(cudaMalloc(&g.work, total), "work allocation")) return PT_ERR_NOMEM;
     g.work_bytes = total;
     char* base = static_cast<char*>(g.work);
     g.mix = reinterpret_cast<float*>(base);
     g.rec = records ? reinterpret_cast<float4*>(base + b_mix) : nullptr;
     g.samples = records ? reinterpret_cast<GuideSample*>(base + b_mix + b_rec) : nullptr;
-    g.counters = reinterpret_cast<uint32_t*>(base + b_mix + b_rec + b_smp + b_scan);
+    g.counters = reinterpret_cast<uint32_t*>(base + b_mix + b_rec + b_smp + b_scan + b_rows + b_part);
+    g.rows = records ? reinterpret_cast<__nv_bfloat16*>(base + b_mix + b_rec + b_smp + b_scan) : nullptr;
+    g.partial = records ? reinterpret_cast<float*>(base + b_mix + b_rec + b_smp + b_scan + b_rows) : nullptr;
     g.scan_counts = records ? reinterpret_cast<uint32_t*>(base + b_mix + b_rec + b_smp) : nullptr;
     g.scan_offsets = records ? reinterpret_cast<uint32_t*>(base + b_mix + b_rec + b_smp + al((P + 1) * 4)) : nullptr;
     g.scan_tmp = records ? base + b_mix + b_rec + b_smp + 2 * al((P + 1) * 4) : nullptr;

@@ -1335,10 +1335,15 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
                                                                       gs->counters, gs->sample_cap);
                     // optimiser steps over this pass's samples in minibatches
                     const int nmb = guide_minibatches(int64_t(P.npix) * count, gs->paths_per_step);
+                    const uint32_t step_cap = guide_step_cap(gs->samples_per_step);
                     for (int mb = 0; mb < nmb; ++mb) {
                         k_guide_train<<<wf.sms, 32 * kGTrainWarps, kGTrainSmem, st>>>(gs->net, gs->samples, gs->counters,
-                                                                         gs->sample_cap, mb, nmb,
-                                                                         gs->samples_per_step);
+                                                                         gs->sample_cap, mb, nmb, step_cap, gs->rows);
+                        k_guide_dw<<<dim3(kGDwChunks, 4), 128, 0, st>>>(gs->counters, gs->sample_cap, mb, nmb, step_cap,
+                                                                        gs->rows, gs->partial);
+                        k_guide_dw_reduce<<<(kGWeights + 255) / 256, 256, 0, st>>>(gs->counters, gs->sample_cap, mb, nmb,
+                                                                                   step_cap, gs->partial,
+                                                                                   gs->net.w_grad);
                         k_guide_adam<<<wf.sms * 8, 256, 0, st>>>(gs->net, gs->counters, gs->sample_cap, mb, nmb,
                                                                  gs->step, gs->lr, gs->lr, 0.9f, 0.99f, 1e-10f);
                     }
@@ -1785,7 +1790,7 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     if (!timing) wf.extend_launches += passes * static_cast<uint64_t>(P.max_depth);
     wf.kernel_launches += 1 + passes * (1 + 4 * static_cast<uint64_t>(P.max_depth));
     if (P.gmix)
-        wf.kernel_launches += passes * (P.max_depth + (P.grec ? 5 + 2 * guide_minibatches(int64_t(P.npix) * lanes, wf.guide->paths_per_step) : 0));
+        wf.kernel_launches += passes * (P.max_depth + (P.grec ? 5 + 4 * guide_minibatches(int64_t(P.npix) * lanes, wf.guide->paths_per_step) : 0));
     return PT_OK;
 }
 
@@ -2109,11 +2114,22 @@ int guide_get_params(const pt_guide* h, float* weights, float* grid, float* meta
 }
 
 int guide_backward(pt_guide* h, const float* samples, uint32_t n, float* wgrad, float* ggrad) {
+    if (n > static_cast<uint32_t>(kGTrainRows)) {
+        set_error("guide backward: at most " + std::to_string(kGTrainRows) + " samples");
+        return PT_ERR_INVALID;
+    }
     if (int rc = ensure_device(h->g.device)) return rc;
     GuideSample* ds = nullptr;
     uint32_t* dn = nullptr;
+    void* store = nullptr;   // the row store and the partial sums of the weight gradient
     PT_CU(cudaMalloc(&ds, std::max<size_t>(n, 1) * sizeof(GuideSample)));
-    if (cudaMalloc(&dn, 4) != cudaSuccess) { cudaFree(ds); cudaGetLastError(); set_error("alloc"); return PT_ERR_NOMEM; }
+    if (cudaMalloc(&dn, 4) != cudaSuccess ||
+        cudaMalloc(&store, kGRowStoreElems * sizeof(__nv_bfloat16) +
+                               static_cast<size_t>(kGDwChunks) * kGWeights * sizeof(float)) != cudaSuccess) {
+        cudaFree(ds); cudaFree(dn); cudaGetLastError(); set_error("alloc"); return PT_ERR_NOMEM;
+    }
+    __nv_bfloat16* rows = static_cast<__nv_bfloat16*>(store);
+    float* partial = reinterpret_cast<float*>(rows + kGRowStoreElems);
     const size_t ng = static_cast<size_t>(kGLevels) * kGTable;
     cudaError_t e = cudaMemcpy(ds, samples, static_cast<size_t>(n) * sizeof(GuideSample), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(dn, &n, 4, cudaMemcpyHostToDevice);
@@ -2122,7 +2138,12 @@ int guide_backward(pt_guide* h, const float* samples, uint32_t n, float* wgrad, 
     if (e == cudaSuccess) {
         GuideNet net = h->g.net;
         net.loss_fix = nullptr;   // leave the training-loss record alone
-        k_guide_train<<<148, 32 * kGTrainWarps, kGTrainSmem>>>(net, ds, dn, n, 0, 1, 0u);
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->g.device);
+        const uint32_t cap = guide_step_cap(0u);
+        k_guide_train<<<sms, 32 * kGTrainWarps, kGTrainSmem>>>(net, ds, dn, n, 0, 1, cap, rows);
+        k_guide_dw<<<dim3(kGDwChunks, 4), 128>>>(dn, n, 0, 1, cap, rows, partial);
+        k_guide_dw_reduce<<<(kGWeights + 255) / 256, 256>>>(dn, n, 0, 1, cap, partial, net.w_grad);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
     }
@@ -2142,6 +2163,7 @@ int guide_backward(pt_guide* h, const float* samples, uint32_t n, float* wgrad, 
     cudaMemset(h->g.net.grid_grad, 0, ng * 2 * sizeof(unsigned long long));
     cudaFree(ds);
     cudaFree(dn);
+    cudaFree(store);
     if (e != cudaSuccess) { set_error(std::string("guide backward: ") + cudaGetErrorString(e)); return PT_ERR_CUDA; }
     return PT_OK;
 }
