@@ -63,6 +63,9 @@ def parse_args():
                         "--room-size (a small case for profiling the guide's kernels) (separate lines)")
     p.add_argument("--room-size", type=int, default=512, help="image side of --workload guided")
     p.add_argument("--room-train-spp", type=int, default=4, help="training spp of --workload guided")
+    p.add_argument("--guide-infer", choices=["default", "fused", "split_mma", "split_tc", "all"], default="default",
+                   help="network evaluation kernels of --workload guided (all: train with the default, then "
+                        "time every kind on the same guided render)")
     p.add_argument("--large-spp", type=int, default=512, help="samples per pixel per camera of --workload large")
     p.add_argument("--large-train-spp", type=int, default=64, help="guide training spp of --workload large")
     p.add_argument("--builder", choices=["host", "device"], default="host",
@@ -799,28 +802,58 @@ def build_workload(args):
         "trace_ratio": round(dev_rate / host_rate, 3)}))
 
 
+GUIDE_INFER = {"default": 0, "fused": 1, "split_mma": 2, "split_tc": 3}
+
+
 def guided_workload(args):
     """Online training for --room-train-spp, then --spp guided samples per
     pixel of the hidden-light room at --room-size squared; stage times of the
-    guided render.  A profiling case for the guide's kernels."""
+    guided render.  A profiling case for the guide's kernels.  With
+    --guide-infer all, the trained guide then renders the same --spp samples
+    once per inference kind with per-stage CUDA events (the network's stage
+    time of each kind, and the image mean)."""
+    import torch
     import pathtracingtutorial_b200 as pt
     from pathtracingtutorial_b200 import scenes
     sa = scenes.hidden_light_room(width=args.room_size, height=args.room_size)
     s = sa.scene()
     s.build_accel()
     s.upload_to_device(0)
+    kinds = list(GUIDE_INFER)[1:] if args.guide_infer == "all" else [args.guide_infer]
+    g = pt.Guide(s, seed=1, inference=GUIDE_INFER[kinds[0]])
     t0 = time.perf_counter()
-    img, g, st = pt.render_guided(s, train_spp=args.room_train_spp, spp=args.spp)
+    img, g, st = pt.render_guided(s, train_spp=args.room_train_spp, spp=args.spp, guide=g)
     secs = time.perf_counter() - t0
     info = g.info()
+    per_kind = {}
+    if len(kinds) > 1:
+        r = pt.Renderer(s, device=0)
+        g.attach(r.integrator, pt.Guide.USE)
+        s.update_settings(flags=pt.FLAG_STAGE_TIMING | pt.FLAG_NO_GRAPH)
+        spf = sa.sample_per_frame
+        for kind in kinds * 2:   # the second round is the one kept (the first warms up)
+            g.set_inference(GUIDE_INFER[kind])
+            r.integrator.reset_stats()
+            r.reset_accumulation()
+            s.set_frame_count(0)
+            r.render_frames((args.spp + spf - 1) // spf)
+            torch.cuda.synchronize()
+            k = r.integrator.stats()
+            per_kind[kind] = {"guide_ms": round(k["guide_ms"], 2), "extend_ms": round(k["extend_ms"], 2),
+                              "shade_ms": round(k["shade_ms"], 2), "shadow_ms": round(k["shadow_ms"], 2),
+                              "mean": round(float(r.download_current_image()[..., :3].mean()), 6)}
+        s.update_settings(flags=0)
+        g.attach(r.integrator, pt.Guide.OFF)
+        r.integrator.close()
+        r.film.close()
     g.close()
     print(json.dumps({
         "metric": "guided render", "workload": f"{sa.name} {len(sa.faces)} tri, {args.room_size}^2, "
                                               f"depth {sa.max_depth}",
         "train_spp": args.room_train_spp, "spp": args.spp, "seconds": round(secs, 3),
-        "optimiser_steps": info["steps"], "mean": float(img[..., :3].mean()),
+        "inference": kinds[0], "optimiser_steps": info["steps"], "mean": float(img[..., :3].mean()),
         "rays": int(st["camera_rays"] + st["extension_rays"] + st["shadow_rays"]),
-        "kernel_launches": int(st["kernel_launches"])}))
+        "kernel_launches": int(st["kernel_launches"]), "per_inference_kind": per_kind or None}))
 
 
 def main():

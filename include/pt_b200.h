@@ -436,6 +436,20 @@ int pt_guide_set_alpha(pt_guide* guide, float alpha);
    training samples spread evenly over the pass's (0 or more than 131072:
    131072, the most one step takes).  The defaults are 32768 and 65536. */
 int pt_guide_set_training(pt_guide* guide, int32_t paths_per_step, uint32_t samples_per_step);
+/* How the network is evaluated while rendering (and by pt_guide_eval); all
+ * kinds give the same densities up to FP32 accumulation order.
+ *   FUSED      one kernel: hash-grid encoding and the MLP on mma.sync, 16
+ *              queries per warp;
+ *   SPLIT_MMA  the encoding as its own kernel (one thread per query and level),
+ *              then the MLP on mma.sync;
+ *   SPLIT_TC   the encoding kernel, then the MLP on the tcgen05 tensor cores
+ *              (128-query tiles, accumulators in tensor memory).
+ * 0 selects the library default. */
+#define PT_GUIDE_INFER_DEFAULT   0
+#define PT_GUIDE_INFER_FUSED     1
+#define PT_GUIDE_INFER_SPLIT_MMA 2
+#define PT_GUIDE_INFER_SPLIT_TC  3
+int pt_guide_set_inference(pt_guide* guide, int32_t kind);
 /* steps taken and samples used by the last step (synchronises the device) */
 int pt_guide_info(const pt_guide* guide, uint32_t* steps, uint32_t* last_samples);
 /* mean training loss -w log q(dir | pos) over the last training pass (synchronises) */

@@ -442,13 +442,19 @@ class Guide:
     """Learned directional guide (hash grid + MLP + 8-lobe vMF mixture) for one scene."""
 
     OFF, USE, TRAIN = _ffi.GUIDE_OFF, _ffi.GUIDE_USE, _ffi.GUIDE_TRAIN
+    # how the network is evaluated (pt_guide_set_inference)
+    INFER_DEFAULT, INFER_FUSED, INFER_SPLIT_MMA, INFER_SPLIT_TC = (
+        _ffi.GUIDE_INFER_DEFAULT, _ffi.GUIDE_INFER_FUSED, _ffi.GUIDE_INFER_SPLIT_MMA, _ffi.GUIDE_INFER_SPLIT_TC)
     STEP_SAMPLES = 65536   # the library's default cap of training samples per optimiser step
 
     def __init__(self, scene: SceneManager, seed: int = 1, lr: float | None = None, alpha: float | None = None,
-                 paths_per_step: int | None = None, samples_per_step: int | None = None):
+                 paths_per_step: int | None = None, samples_per_step: int | None = None,
+                 inference: int | None = None):
         h = C.c_void_p()
         check(lib().pt_guide_create(scene.handle, seed, C.byref(h)))
         self._h = h
+        if inference is not None:
+            self.set_inference(inference)
         if lr is not None:
             check(lib().pt_guide_set_learning_rate(self._h, float(lr)))
         if alpha is not None:
@@ -460,6 +466,12 @@ class Guide:
     def set_alpha(self, alpha: float) -> None:
         """Probability of drawing a continuation from the network (one-sample MIS)."""
         check(lib().pt_guide_set_alpha(self._h, float(alpha)))
+
+    def set_inference(self, kind: int) -> None:
+        """Network evaluation kernels: INFER_FUSED (encoding and MLP in one
+        mma.sync kernel), INFER_SPLIT_MMA / INFER_SPLIT_TC (encoding kernel,
+        then the MLP on mma.sync / on the tcgen05 tensor cores)."""
+        check(lib().pt_guide_set_inference(self._h, int(kind)))
 
     def set_training(self, paths_per_step: int = 0, samples_per_step: int = 65536) -> None:
         """Online training: one optimiser step per `paths_per_step` paths of a

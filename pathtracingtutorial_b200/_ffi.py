@@ -19,6 +19,7 @@ SAMPLER_PCG, SAMPLER_SOBOL = 0, 1
 FLAG_WATERTIGHT, FLAG_STAGE_TIMING, FLAG_NO_GRAPH, FLAG_COUNT_TRAVERSAL = 1, 2, 4, 8
 ARGS_LTR, ARGS_RTL = 0, 1
 GUIDE_OFF, GUIDE_USE, GUIDE_TRAIN = 0, 1, 2
+GUIDE_INFER_DEFAULT, GUIDE_INFER_FUSED, GUIDE_INFER_SPLIT_MMA, GUIDE_INFER_SPLIT_TC = 0, 1, 2, 3
 
 VERTEX_DTYPE = np.dtype([("position", "<f4", 3), ("_pad0", "<f4"), ("normal", "<f4", 3), ("_pad1", "<f4"),
                          ("uv", "<f4", 2), ("_pad2", "<f4", 2), ("tangent", "<f4", 4)])
@@ -205,6 +206,7 @@ _SIGS = [
     ("pt_guide_set_learning_rate", C.c_int, [_P, C.c_float]),
     ("pt_guide_set_alpha", C.c_int, [_P, C.c_float]),
     ("pt_guide_set_training", C.c_int, [_P, C.c_int32, C.c_uint32]),
+    ("pt_guide_set_inference", C.c_int, [_P, C.c_int32]),
     ("pt_guide_info", C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     ("pt_guide_loss", C.c_int, [_P, C.POINTER(C.c_float)]),
     ("pt_integrator_set_guide", C.c_int, [_P, _P, C.c_int32]),

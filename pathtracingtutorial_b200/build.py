@@ -23,7 +23,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 CXX_SOURCES = ["host_prep.cpp", "scene_io.cpp", "image_decode.cpp", "capi.cpp"]
 CU_SOURCES = ["integrator.cu", "static_trace.cu", "lbvh.cu"]
-HEADERS = ["image_decode.h", "pt_internal.h", "sampler.h", "bsdf.h", "traverse.h", "engine.h", "device_api.h", "batch.cuh", "guide.cuh", "guide_host.cuh"]
+HEADERS = ["image_decode.h", "pt_internal.h", "sampler.h", "bsdf.h", "traverse.h", "engine.h", "device_api.h", "batch.cuh", "guide.cuh", "guide_tc.cuh", "guide_host.cuh"]
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXXFLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-Wall",

@@ -317,6 +317,7 @@ int batch_wavefront(const pt_batch_item* in, uint32_t n, int out_is_device, int6
             v.step = g.step;
             v.alpha = g.alpha;
             v.lr = g.lr;
+            v.infer = g.infer;
             v.mode = PT_GUIDE_USE;
             gs_k = &v;
         }

@@ -719,6 +719,11 @@ int pt_guide_set_training(pt_guide* guide, int32_t paths_per_step, uint32_t samp
     guide_set_training(guide, paths_per_step, samples_per_step);
     return PT_OK;
 }
+int pt_guide_set_inference(pt_guide* guide, int32_t kind) {
+    PT_REQUIRE(guide && kind >= PT_GUIDE_INFER_DEFAULT && kind <= PT_GUIDE_INFER_SPLIT_TC, "unknown inference kind");
+    guide_set_inference(guide, kind);
+    return PT_OK;
+}
 int pt_guide_info(const pt_guide* guide, uint32_t* steps, uint32_t* last_samples) {
     PT_REQUIRE(guide, "null guide");
     return guide_info(guide, steps, last_samples);

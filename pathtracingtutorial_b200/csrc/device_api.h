@@ -37,6 +37,7 @@ void guide_destroy(pt_guide* g);
 void guide_set_lr(pt_guide* g, float lr);
 void guide_set_alpha(pt_guide* g, float alpha);
 void guide_set_training(pt_guide* g, int paths_per_step, uint32_t samples_per_step);
+void guide_set_inference(pt_guide* g, int kind);
 int  guide_info(const pt_guide* g, uint32_t* steps, uint32_t* samples);
 int  guide_loss(const pt_guide* g, float* loss);
 int  integrator_set_guide(pt_integrator* integ, pt_guide* g, int mode);

@@ -54,6 +54,11 @@ constexpr int kGuideMinibatchPaths = 1 << 15;
 // 0.00214 at 256 guided spp; 65,536 a step cost 2.25 s for 0.00233; 32,768
 // cost 2.0 s for 0.0034.
 constexpr uint32_t kGuideStepSamples = 65536;
+// Inference kind used unless pt_guide_set_inference chooses another.  Network
+// stage time of a 64-spp guided render of the hidden-light room at 1024 x 1024
+// (about 3.3M queries a bounce): fused 160.5 ms, encoding + mma.sync MLP 152.0
+// ms, encoding + tcgen05 MLP 114.6 ms.
+constexpr int kGuideInferDefault = PT_GUIDE_INFER_SPLIT_TC;
 
 // Optimiser steps per training pass of `paths` paths: one per
 // `paths_per_step` paths (2^15 by default, about 10^5 samples), 1 .. 32.
@@ -804,6 +809,8 @@ struct GuideState {
     __nv_bfloat16* rows = nullptr;    // training row store (kGRowStoreElems) for the weight gradient
     float*       partial = nullptr;   // k_guide_dw's partial sums (kGDwChunks x kGWeights)
     uint32_t*    step = nullptr;      // optimiser steps taken (with the parameters: survives work resizes)
+    unsigned char* feat = nullptr;    // encoded features of one queue (split inference kinds), 8 KB per 128 entries
+    int          infer = kGuideInferDefault;   // PT_GUIDE_INFER_*
     int          mode = 0;            // 0 off, PT_GUIDE_USE, PT_GUIDE_TRAIN
     float        lr = 1e-2f;
     float        alpha = kGuideAlpha;

@@ -22,6 +22,7 @@ inline void guide_free(GuideState& g) {
     g.params = g.work = nullptr;
     g.rows = nullptr;
     g.partial = nullptr;
+    g.feat = nullptr;
     g.step = g.counters = nullptr;
     g.param_bytes = g.work_bytes = 0;
     g.npix = g.depth = 0;
@@ -107,7 +108,9 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
               guide_cuda_ok(cudaMemset(g.net.w_grad, 0, wg + 2 * wf), "clear") &&
               guide_cuda_ok(cudaMemset(g.step, 0, 256), "clear") &&
               guide_cuda_ok(cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kGTrainSmem), "smem") &&
-              guide_cuda_ok(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kGInferSmem), "smem");
+              guide_cuda_ok(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kGInferSmem), "smem") &&
+              guide_cuda_ok(cudaFuncSetAttribute(k_guide_mlp_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, kGInferSmem), "smem") &&
+              guide_cuda_ok(cudaFuncSetAttribute(k_guide_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kGTcSmem), "smem");
     return ok ? PT_OK : PT_ERR_CUDA;
 }
 
@@ -124,6 +127,7 @@ inline int guide_prepare_work(GuideState& g, int npix, int depth, bool records) 
     const size_t P = static_cast<size_t>(npix), D = static_cast<size_t>(std::max(depth, 1));
     const size_t cap = records ? std::min<size_t>(P * D, size_t(1) << 24) : 0;
     const size_t b_mix = al(P * kGMix * sizeof(float));
+    const size_t b_feat = al(static_cast<size_t>(guide_feat_rows(static_cast<uint32_t>(P))) * kGIn * sizeof(__nv_bfloat16));
     const size_t b_rec = records ? al(D * P * 4 * sizeof(float4)) : 0;
     const size_t b_smp = al(cap * sizeof(GuideSample));
     size_t scan_tmp = 0;
@@ -135,7 +139,7 @@ inline int guide_prepare_work(GuideState& g, int npix, int depth, bool records) 
     const size_t b_scan = records ? 2 * al((P + 1) * sizeof(uint32_t)) + al(scan_tmp) : 0;
     const size_t b_rows = records ? al(kGRowStoreElems * sizeof(__nv_bfloat16)) : 0;
     const size_t b_part = records ? al(static_cast<size_t>(kGDwChunks) * kGWeights * sizeof(float)) : 0;
-    const size_t total = b_mix + b_rec + b_smp + b_scan + b_rows + b_part + 256;
+    const size_t total = b_mix + b_rec + b_smp + b_scan + b_rows + b_part + 256 + b_feat;
     if (!guide_cuda_ok(cudaMalloc(&g.work, total), "work allocation")) return PT_ERR_NOMEM;
     g.work_bytes = total;
     char* base = static_cast<char*>(g.work);
@@ -149,6 +153,7 @@ inline int guide_prepare_work(GuideState& g, int npix, int depth, bool records) 
     g.scan_offsets = records ? reinterpret_cast<uint32_t*>(base + b_mix + b_rec + b_smp + al((P + 1) * 4)) : nullptr;
     g.scan_tmp = records ? base + b_mix + b_rec + b_smp + 2 * al((P + 1) * 4) : nullptr;
     g.scan_tmp_bytes = records ? scan_tmp : 0;
+    g.feat = reinterpret_cast<unsigned char*>(base + b_mix + b_rec + b_smp + b_scan + b_rows + b_part + 256);
     g.sample_cap = static_cast<uint32_t>(cap);
     g.npix = npix;
     g.depth = depth;

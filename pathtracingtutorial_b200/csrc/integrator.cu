@@ -33,6 +33,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include "guide.cuh"
+#include "guide_tc.cuh"
 #include "guide_host.cuh"
 
 namespace ptb {
@@ -1268,6 +1269,26 @@ struct StageEvent { int kind; cudaEvent_t a, b; };
 
 // Enqueues `total` samples per pixel, counted from the first sample of frame
 // P.pass->frame, as passes of the wavefront's lanes.
+// Guide inference over queue q (the hit points of its rays) into the guide's
+// mixture buffer, by the guide's inference kind.
+void launch_guide_infer(const GuideState& g, const WaveParams& P, int q, int sms, cudaStream_t st) {
+    const uint32_t cap = static_cast<uint32_t>(P.npath);
+    if (g.infer == PT_GUIDE_INFER_FUSED) {
+        k_guide_infer<<<sms * kGInferBlocksPerSm, 32 * kGInferWarps, kGInferSmem, st>>>(g.net, P.counts, q, cap,
+                                                                                      P.ray_o[q], P.ray_d[q], P.hit,
+                                                                                      g.mix);
+        return;
+    }
+    k_guide_encode<<<sms * 8, 256, 0, st>>>(g.net, P.counts, q, cap, P.ray_o[q], P.ray_d[q], P.hit, nullptr, 0u,
+                                            g.feat);
+    if (g.infer == PT_GUIDE_INFER_SPLIT_MMA)
+        k_guide_mlp_mma<<<sms * kGInferBlocksPerSm, 32 * kGInferWarps, kGInferSmem, st>>>(g.net, P.counts, q, cap, 0u,
+                                                                                        g.feat, g.mix);
+    else
+        k_guide_mlp_tc<<<sms * kGTcBlocksPerSm, kGTcThreads, kGTcSmem, st>>>(g.net, P.counts, q, cap, 0u, g.feat,
+                                                                             g.mix, P.err);
+}
+
 int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cudaStream_t st,
                   std::vector<StageEvent>* ev, GuideState* gs = nullptr) {
     const bool infer = gs && gs->mode != 0 && P.gmix;
@@ -1296,12 +1317,7 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
             const int q = d & 1;
             if (int rc = timed(0, [&] { launch_extend(tsi, wf.grid_extend[tsi], st, P, q, d); })) return rc;
             if (infer) {
-                if (int rc = timed(4, [&] {
-                        k_guide_infer<<<wf.sms * kGInferBlocksPerSm, 32 * kGInferWarps, kGInferSmem, st>>>(
-                                                                            gs->net, P.counts, q,
-                                                                            static_cast<uint32_t>(P.npath), P.ray_o[q],
-                                                                            P.ray_d[q], P.hit, gs->mix);
-                    })) return rc;
+                if (int rc = timed(4, [&] { launch_guide_infer(*gs, P, q, wf.sms, st); })) return rc;
             }
             if (int rc = timed(1, [&] {
                     const bool tex = P.scene.num_textures > 0;
@@ -1761,8 +1777,8 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     } else if (use_graph) {
         // everything the captured launches bake in: the parameters, the stream,
         // the frame count and the guide's training settings
-        struct GuideKey { const void* params; float lr; int paths_per_step; uint32_t samples_per_step; } gk{};
-        if (gs) gk = GuideKey{gs->params, gs->lr, gs->paths_per_step, gs->samples_per_step};
+        struct GuideKey { const void* params; const void* feat; float lr; int paths_per_step; uint32_t samples_per_step; int infer; } gk{};
+        if (gs) gk = GuideKey{gs->params, gs->feat, gs->lr, gs->paths_per_step, gs->samples_per_step, gs->infer};
         std::vector<unsigned char> key(sizeof(WaveParams) + sizeof(cudaStream_t) + sizeof(int) + sizeof(GuideKey));
         std::memcpy(key.data(), &P, sizeof(WaveParams));
         std::memcpy(key.data() + sizeof(WaveParams), &st, sizeof(cudaStream_t));
@@ -1790,7 +1806,8 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     if (!timing) wf.extend_launches += passes * static_cast<uint64_t>(P.max_depth);
     wf.kernel_launches += 1 + passes * (1 + 4 * static_cast<uint64_t>(P.max_depth));
     if (P.gmix)
-        wf.kernel_launches += passes * (P.max_depth + (P.grec ? 5 + 4 * guide_minibatches(int64_t(P.npix) * lanes, wf.guide->paths_per_step) : 0));
+        wf.kernel_launches += passes * ((wf.guide->infer == PT_GUIDE_INFER_FUSED ? 1 : 2) * P.max_depth +
+                                        (P.grec ? 5 + 4 * guide_minibatches(int64_t(P.npix) * lanes, wf.guide->paths_per_step) : 0));
     return PT_OK;
 }
 
@@ -1805,6 +1822,7 @@ int integrator_check(pt_integrator* integ, bool sync) {
         std::string m = "device error word 0x" + std::to_string(err) + ":";
         if (err & kErrStackOverflow) m += " traversal stack overflow;";
         if (err & kErrQueueOverflow) m += " queue overflow;";
+        if (err & kErrGuideTimeout) m += " guide network wait timed out;";
         set_error(m);
         PT_CU(cudaMemset(wf->base.err, 0, 4));
         return PT_ERR_DEVICE;
@@ -2056,6 +2074,7 @@ void guide_destroy(pt_guide* h) {
 
 void guide_set_lr(pt_guide* h, float lr) { h->g.lr = lr; }
 void guide_set_alpha(pt_guide* h, float alpha) { h->g.alpha = alpha; }
+void guide_set_inference(pt_guide* h, int kind) { h->g.infer = kind == PT_GUIDE_INFER_DEFAULT ? kGuideInferDefault : kind; }
 void guide_set_training(pt_guide* h, int paths_per_step, uint32_t samples_per_step) {
     h->g.paths_per_step = paths_per_step > 0 ? paths_per_step : kGuideMinibatchPaths;
     h->g.samples_per_step = samples_per_step;
@@ -2168,21 +2187,56 @@ int guide_backward(pt_guide* h, const float* samples, uint32_t n, float* wgrad, 
     return PT_OK;
 }
 
+// q(dir | pos) of query r from its mixture record (split inference kinds).
+__global__ void __launch_bounds__(256) k_guide_mix_pdf(const float* __restrict__ mix, const float* __restrict__ qd,
+                                                       uint32_t n, float* __restrict__ out) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+        out[r] = mix_pdf(mix + static_cast<size_t>(r) * kGMix, normalize(mk(qd[6 * r + 3], qd[6 * r + 4], qd[6 * r + 5])));
+}
+
 int guide_eval(pt_guide* h, const float* qd, uint32_t n, float* out) {
     if (int rc = ensure_device(h->g.device)) return rc;
     if (n == 0) return PT_OK;
-    float *dq = nullptr, *dout = nullptr;
-    PT_CU(cudaMalloc(&dq, static_cast<size_t>(n) * 24));
-    if (cudaMalloc(&dout, static_cast<size_t>(n) * 4) != cudaSuccess) { cudaFree(dq); cudaGetLastError(); set_error("alloc"); return PT_ERR_NOMEM; }
+    const GuideState& g = h->g;
+    const bool split = g.infer != PT_GUIDE_INFER_FUSED;
+    int sms = 0;
+    PT_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device));
+    // queries, densities, and for the split kinds the feature tiles, the
+    // mixture records and an error word: one allocation
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t b_q = al(static_cast<size_t>(n) * 24), b_out = al(static_cast<size_t>(n) * 4);
+    const size_t b_feat = split ? al(static_cast<size_t>(guide_feat_rows(n)) * kGIn * 2) : 0;
+    const size_t b_mix = split ? al(static_cast<size_t>(n) * kGMix * 4) : 0;
+    char* buf = nullptr;
+    PT_CU(cudaMalloc(&buf, b_q + b_out + b_feat + b_mix + 256));
+    float* dq = reinterpret_cast<float*>(buf);
+    float* dout = reinterpret_cast<float*>(buf + b_q);
+    unsigned char* feat = reinterpret_cast<unsigned char*>(buf + b_q + b_out);
+    float* mix = reinterpret_cast<float*>(buf + b_q + b_out + b_feat);
+    uint32_t* derr = reinterpret_cast<uint32_t*>(buf + b_q + b_out + b_feat + b_mix);
     cudaError_t e = cudaMemcpy(dq, qd, static_cast<size_t>(n) * 24, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(derr, 0, 4);
     if (e == cudaSuccess) {
-        k_guide_eval<<<148, 128, kGEvalSmem>>>(h->g.net, dq, n, dout);
+        if (!split) {
+            k_guide_eval<<<sms, 128, kGEvalSmem>>>(g.net, dq, n, dout);
+        } else {
+            k_guide_encode<<<sms * 8, 256>>>(g.net, nullptr, 0, 0u, nullptr, nullptr, nullptr, dq, n, feat);
+            if (g.infer == PT_GUIDE_INFER_SPLIT_MMA)
+                k_guide_mlp_mma<<<sms * kGInferBlocksPerSm, 32 * kGInferWarps, kGInferSmem>>>(g.net, nullptr, 0, 0u, n,
+                                                                                          feat, mix);
+            else
+                k_guide_mlp_tc<<<sms * kGTcBlocksPerSm, kGTcThreads, kGTcSmem>>>(g.net, nullptr, 0, 0u, n, feat, mix,
+                                                                               derr);
+            k_guide_mix_pdf<<<sms * 4, 256>>>(mix, dq, n, dout);
+        }
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpy(out, dout, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost);
     }
-    cudaFree(dq);
-    cudaFree(dout);
+    uint32_t err = 0;
+    if (e == cudaSuccess && split) e = cudaMemcpy(&err, derr, 4, cudaMemcpyDeviceToHost);
+    cudaFree(buf);
     if (e != cudaSuccess) { set_error(std::string("guide eval: ") + cudaGetErrorString(e)); return PT_ERR_CUDA; }
+    if (err) { set_error("guide eval: the network's tensor-core wait timed out"); return PT_ERR_DEVICE; }
     return PT_OK;
 }
 

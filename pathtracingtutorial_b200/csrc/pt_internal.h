@@ -54,6 +54,7 @@ enum : uint32_t {
     kErrStackOverflow = 1u << 0,
     kErrQueueOverflow = 1u << 1,
     kErrNanRadiance   = 1u << 2,
+    kErrGuideTimeout  = 1u << 3,   // a tensor-core wait of the guide's network gave up
 };
 
 // ---------------------------------------------------------------------------

@@ -248,3 +248,44 @@ def test_guided_render_keeps_plain_expectation_with_clearcoat_and_sky():
     print(f"plain {mp.mean():.6f} guided {mg.mean():.6f} se {se:.2e}")
     assert abs(mp.mean() - mg.mean()) < 4 * se, (mp.mean(), mg.mean(), se)
     g.close()
+
+
+@pytest.mark.gpu
+def test_guide_inference_kinds_agree_with_oracle():
+    """The three ways of evaluating the network while rendering -- one fused
+    mma.sync kernel, the encoding kernel then the MLP on mma.sync, and the
+    encoding kernel then the MLP on the tcgen05 tensor cores -- give the
+    FP64 oracle's densities (with the kernels' BF16 storage points) within
+    the fused kernel's bounds; the two mma.sync kinds agree to FP32 rounding,
+    and guided renders with each kind agree with the fused kind's."""
+    import pathtracingtutorial_b200 as pt
+    from pathtracingtutorial_b200 import scenes
+    sa = scenes.hidden_light_room(width=64, height=64, n_boxes=40, box_subdiv=2, spp=8, max_depth=8)
+    s = _scene(sa)
+    _, g, _ = pt.render_guided(s, train_spp=64, spp=4)
+    prm = g.params()
+    rng = np.random.default_rng(7)
+    lo, inv = prm["lo"].astype(np.float64), prm["inv_extent"].astype(np.float64)
+    # 5000 queries: several 128-query tiles and a ragged last one
+    p01 = rng.uniform(0.02, 0.98, (5000, 3)).astype(np.float32)
+    world = (lo + p01 / inv).astype(np.float32)
+    d = rng.normal(size=(5000, 3)); d /= np.linalg.norm(d, axis=1, keepdims=True)
+    pn = np.clip((world - prm["lo"]) * prm["inv_extent"], 0, 1).astype(np.float32)
+    q_ref = guide_ref.pdf(prm, pn, d, bf16=True)
+    q, img = {}, {}
+    for kind in (pt.Guide.INFER_FUSED, pt.Guide.INFER_SPLIT_MMA, pt.Guide.INFER_SPLIT_TC):
+        g.set_inference(kind)
+        q[kind] = g.pdf(world, d.astype(np.float32)).astype(np.float64)
+        rel = np.abs(q[kind] - q_ref) / q_ref
+        assert np.median(rel) < 1e-3 and np.quantile(rel, 0.99) < 1e-2, (kind, np.median(rel), np.quantile(rel, 0.99))
+        img[kind] = pt.render_batch([(s, 16, 1000, None, g)])[0][0][..., :3].astype(np.float64)
+    assert np.max(np.abs(q[pt.Guide.INFER_SPLIT_MMA] - q[pt.Guide.INFER_FUSED]) / q[pt.Guide.INFER_FUSED]) < 1e-5
+    rel_tc = np.abs(q[pt.Guide.INFER_SPLIT_TC] - q[pt.Guide.INFER_FUSED]) / q[pt.Guide.INFER_FUSED]
+    assert np.median(rel_tc) < 1e-4 and np.max(rel_tc) < 1e-2, (np.median(rel_tc), np.max(rel_tc))
+    base = img[pt.Guide.INFER_FUSED]
+    for kind in (pt.Guide.INFER_SPLIT_MMA, pt.Guide.INFER_SPLIT_TC):
+        # same sample streams: only directions whose lobe or density choice sits
+        # on an FP32 rounding boundary can differ
+        assert abs(img[kind].mean() - base.mean()) < 0.01 * base.mean(), (kind, img[kind].mean(), base.mean())
+        assert np.mean(np.abs(img[kind] - base)) < 0.02 * base.mean(), (kind, np.mean(np.abs(img[kind] - base)))
+    g.close()
