@@ -325,9 +325,11 @@ def convergence(local: int, stream, small: bool, plain_cap: int = 8192, guided_c
     spf = sa.sample_per_frame
     handle = stream.cuda_stream
 
-    def relmse(img):
-        c = img[y0:y1, x0:x1, :3].astype(np.float64)
+    def relmse_crop(c):
         return float(np.mean((c - ref) ** 2 / (ref * ref + eps)))
+
+    def relmse(img):
+        return relmse_crop(img[y0:y1, x0:x1, :3].astype(np.float64))
 
     def sync():
         torch.cuda.synchronize(local)
@@ -376,10 +378,11 @@ def convergence(local: int, stream, small: bool, plain_cap: int = 8192, guided_c
     while spp < guided_cap:
         imgs, _, _ = pt.render_batch([(scene, chunk, spp // spf, None, g)], mode=pt.BATCH_WAVEFRONT,
                                      autotune=False)
-        img = imgs[0][..., :3].astype(np.float64)
+        # the whole image is read back; only the scored crop is averaged on the host
+        img = imgs[0][y0:y1, x0:x1, :3].astype(np.float64)
         acc = img if acc is None else acc + (img - acc) * (chunk / (spp + chunk))
         spp += chunk
-        e = relmse(acc)
+        e = relmse_crop(acc)
         guided.append((spp, (time.perf_counter() - t0) * 1e3, e))
         if e <= TARGET_RELMSE:
             break

@@ -55,9 +55,10 @@ constexpr int kGuideMinibatchPaths = 1 << 15;
 // cost 2.0 s for 0.0034.
 constexpr uint32_t kGuideStepSamples = 65536;
 // Inference kind used unless pt_guide_set_inference chooses another.  Network
-// stage time of a 64-spp guided render of the hidden-light room at 1024 x 1024
-// (about 3.3M queries a bounce): fused 160.5 ms, encoding + mma.sync MLP 152.0
-// ms, encoding + tcgen05 MLP 114.6 ms.
+// stage time of a 64-spp guided render of the hidden-light room at 1024 x 1024:
+// fused 124.0 ms, encoding + mma.sync MLP 118.6 ms, encoding + tcgen05 MLP
+// 104.9 ms (with the exactly rounded exponentials and logarithms in the
+// mixture records: 160.5 / 152.0 / 114.6 ms).
 constexpr int kGuideInferDefault = PT_GUIDE_INFER_SPLIT_TC;
 
 // Optimiser steps per training pass of `paths` paths: one per
@@ -177,7 +178,9 @@ __device__ __forceinline__ uint32_t grid_index(const GuideNet& net, int level, u
     return (x + ((y * 2654435761u) ^ (z * 805459861u))) & (kGTable - 1);
 }
 
-// Trilinear features of one level at normalised position p.
+// Trilinear features of one level at normalised position p.  (Gathers that
+// bypass L1, ld.global.cg, made the encoding kernel 1.3x slower: 18 % of its
+// gathers hit in L1.)
 __device__ __forceinline__ float2 encode_level(const GuideNet& net, int level, f3 p) {
     const float s = net.scale[level];
     const float fx = p.x * s + 0.5f, fy = p.y * s + 0.5f, fz = p.z * s + 0.5f;
@@ -283,26 +286,57 @@ __device__ __forceinline__ float vmf_pdf(float kappa, float c) {
 // lobe k as float4(kappa_k mu_k, b_k) with b_k = log(pi_k kappa_k /
 // (2 pi (1 - e^{-2 kappa_k}))) - kappa_k, then the eight weights pi_k.  Then
 // pi_k vMF_k(w) = exp(kappa_k mu_k . w + b_k): one exponential per lobe.
+// The same function as raw_to_mixture followed by the record's algebra, with
+// the hardware's approximate exponential and logarithm: log pi_k = (logit_k
+// - max) - log(sum), one logarithm per row; the normalisation factor as
+// log(kappa / (1 - e^{-2 kappa})) - log(2 pi).  About a quarter of the
+// instructions of the exactly rounded library functions; the densities agree
+// with the FP64 oracle to about 1e-6 relative.
 __device__ __forceinline__ void mixture_record(const float* raw, float* rec) {
-    float mix[kGMix];
-    raw_to_mixture(raw, mix);
+    float mx = -1e30f;
+#pragma unroll
+    for (int k = 0; k < kGLobes; ++k) mx = fmaxf(mx, raw[5 * k + 4]);
+    float e[kGLobes];
+    float sum = 0.0f;
+#pragma unroll
     for (int k = 0; k < kGLobes; ++k) {
-        const float kap = mix[4 * k + 3];   // >= 1e-3
-        rec[4 * k] = kap * mix[4 * k];
-        rec[4 * k + 1] = kap * mix[4 * k + 1];
-        rec[4 * k + 2] = kap * mix[4 * k + 2];
-        rec[4 * k + 3] = logf(mix[32 + k]) + logf(kap / (kTwoPi * -expm1f(-2.0f * kap))) - kap;
-        rec[32 + k] = mix[32 + k];
+        e[k] = __expf(raw[5 * k + 4] - mx);
+        sum += e[k];
+    }
+    const float inv_sum = 1.0f / sum, log_sum = __logf(sum);
+    constexpr float kLog2Pi = 1.83787706640934548356f;
+#pragma unroll
+    for (int k = 0; k < kGLobes; ++k) {
+        const float mxx = raw[5 * k], myy = raw[5 * k + 1], mzz = raw[5 * k + 2];
+        const float l2 = mxx * mxx + myy * myy + mzz * mzz;
+        const float r = raw[5 * k + 3];
+        const float sp = r > 15.0f ? r : __logf(1.0f + __expf(r));
+        const float kap = fminf(sp + 1e-3f, 5e3f);   // >= 1e-3
+        if (l2 > 1e-24f) {
+            const float s = kap * rsqrtf(l2);
+            rec[4 * k] = s * mxx;
+            rec[4 * k + 1] = s * myy;
+            rec[4 * k + 2] = s * mzz;
+        } else {
+            rec[4 * k] = 0.0f;
+            rec[4 * k + 1] = 0.0f;
+            rec[4 * k + 2] = kap;
+        }
+        rec[4 * k + 3] = (raw[5 * k + 4] - mx) - log_sum + __logf(__fdividef(kap, 1.0f - __expf(-2.0f * kap))) -
+                         kLog2Pi - kap;
+        rec[32 + k] = e[k] * inv_sum;
     }
 }
 
+// q(w) = sum_k exp(kappa_k mu_k . w + b_k), with the hardware exponential
+// (relative error about 1e-6 at the exponents met here).
 __device__ __forceinline__ float mix_pdf(const float* rec, f3 w) {
     const float4* r4 = reinterpret_cast<const float4*>(rec);
     float q = 0.0f;
 #pragma unroll
     for (int k = 0; k < kGLobes; ++k) {
         const float4 l = r4[k];
-        q += expf(fmaf(l.x, w.x, fmaf(l.y, w.y, fmaf(l.z, w.z, l.w))));
+        q += __expf(fmaf(l.x, w.x, fmaf(l.y, w.y, fmaf(l.z, w.z, l.w))));
     }
     return q;
 }
@@ -315,7 +349,7 @@ __device__ __forceinline__ f3 mix_sample(const float* rec, float u0, float u1, f
     const f3 km = mk(l.x, l.y, l.z);
     const float kappa = length(km);
     const f3 mu = km / kappa;
-    const float c = fminf(fmaxf(1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * kappa)) / kappa, -1.0f), 1.0f);
+    const float c = fminf(fmaxf(1.0f + __logf(u1 + (1.0f - u1) * __expf(-2.0f * kappa)) / kappa, -1.0f), 1.0f);
     const float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
     const float phi = kTwoPi * u2;
     const Frame fr = make_frame(mu);

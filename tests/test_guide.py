@@ -289,3 +289,4 @@ def test_guide_inference_kinds_agree_with_oracle():
         assert abs(img[kind].mean() - base.mean()) < 0.01 * base.mean(), (kind, img[kind].mean(), base.mean())
         assert np.mean(np.abs(img[kind] - base)) < 0.02 * base.mean(), (kind, np.mean(np.abs(img[kind] - base)))
     g.close()
+
