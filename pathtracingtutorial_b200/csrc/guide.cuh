@@ -56,8 +56,8 @@ constexpr int kGuideMinibatchPaths = 1 << 15;
 constexpr uint32_t kGuideStepSamples = 65536;
 // Inference kind used unless pt_guide_set_inference chooses another.  Network
 // stage time of a 64-spp guided render of the hidden-light room at 1024 x 1024:
-// fused 124.0 ms, encoding + mma.sync MLP 118.6 ms, encoding + tcgen05 MLP
-// 104.9 ms (with the exactly rounded exponentials and logarithms in the
+// fused 123.5 ms, encoding + mma.sync MLP 118.0 ms, encoding + tcgen05 MLP
+// 101.5 ms (with the exactly rounded exponentials and logarithms in the
 // mixture records: 160.5 / 152.0 / 114.6 ms).
 constexpr int kGuideInferDefault = PT_GUIDE_INFER_SPLIT_TC;
 

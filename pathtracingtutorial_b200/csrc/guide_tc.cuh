@@ -216,29 +216,44 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
-// The network on tcgen05: one 128-query tile at a time per CTA of 4 warps.
-// Shared memory: the four weight matrices (B operands, 26 KB), the feature
-// tile (A of layer 0, 8 KB, refilled by the bulk-copy engine while layers 1-3
-// run), the hidden tile (A of layers 1-3, 16 KB) and two mbarriers.  Tensor
-// memory: 64 columns of FP32 accumulators, row i in lane i, so thread i of
-// the CTA (warp i / 32 reads lanes 32 (i / 32) ..) owns query row i through
-// the ReLU epilogues and the mixture record.  4 CTAs per SM (50.5 KB of
-// shared memory and 64 tensor-memory columns each, up to 128 registers).
+// The network on tcgen05.  A CTA holds one copy of the four weight matrices
+// (B operands, 26 KB of shared memory) and runs kGTcGroups independent tile
+// groups of 4 warps; a group takes one 128-query tile at a time through the
+// four layers.  Per group: the feature tile (A of layer 0, 8 KB, refilled by
+// the bulk-copy engine while layers 1-3 run), the hidden tile (A of layers
+// 1-3, 16 KB), two mbarriers and 64 tensor-memory columns of FP32
+// accumulators with row i in lane i, so thread i of the group (its warp i / 32
+// reads lanes 32 (i / 32) ..) owns query row i through the ReLU epilogues and
+// the mixture record.  While one group's warps run an epilogue, the tensor
+// core serves the others.  The output layer's rows are reordered (the eight
+// logits first, then each lobe's mean and concentration) so that the mixture
+// epilogue streams its row out of tensor memory in 8-column pieces.
+// 2 CTAs of 3 groups per SM: 24 warps, 2 x 100 KB of shared memory, 2 x 256
+// tensor-memory columns, at most 85 registers a thread.
 // ---------------------------------------------------------------------------
-constexpr int kGTcThreads = 128;
-constexpr int kGTcBlocksPerSm = 4;
-constexpr uint32_t kGTcCols = 64;                                  // tensor-memory columns allocated
+constexpr int kGTcGroups = 3;
+constexpr int kGTcThreads = 128 * kGTcGroups;
+constexpr int kGTcBlocksPerSm = 2;
+constexpr uint32_t kGTcCols = 256;                                 // tensor-memory columns allocated (power of 2)
+static_assert(64 * kGTcGroups <= static_cast<int>(kGTcCols), "accumulator columns");
 __host__ __device__ constexpr int g_tc_woff(int l) {              // byte offset of layer l's B operand
     return l == 0 ? 0 : (l == 1 ? kGHid * kGIn * 2 : (l == 2 ? kGHid * kGIn * 2 + kGHid * kGHid * 2
                                                               : kGHid * kGIn * 2 + 2 * kGHid * kGHid * 2));
 }
-constexpr int kGTcF = g_tc_woff(3) + kGOutPad * kGHid * 2;        // 26,624: feature tile
-constexpr int kGTcH = kGTcF + kGFeatTileBytes;                      // 34,816: hidden tile
-constexpr int kGTcBar = kGTcH + kGTcRows * kGHid * 2;              // 51,200: barriers, TMEM address
-constexpr int kGTcSmem = kGTcBar + 32;
-static_assert(kGTcSmem * kGTcBlocksPerSm + 1024 * kGTcBlocksPerSm <= 228 * 1024, "tcgen05 MLP occupancy");
+constexpr int kGTcW = g_tc_woff(3) + kGOutPad * kGHid * 2;        // 26,624 bytes of weights
+constexpr int kGTcGroupBytes = kGFeatTileBytes + kGTcRows * kGHid * 2;   // feature + hidden tile: 24 KB
+constexpr int kGTcBar = kGTcW + kGTcGroups * kGTcGroupBytes;      // barriers, TMEM address
+constexpr int kGTcSmem = kGTcBar + 16 * kGTcGroups + 16;
+static_assert((kGTcSmem + 1024) * kGTcBlocksPerSm <= 228 * 1024, "tcgen05 MLP occupancy");
 static_assert(kGTcCols * kGTcBlocksPerSm <= 512, "tensor memory of the resident CTAs");
-static_assert(kGTcF % 16 == 0 && kGTcH % 16 == 0 && kGTcBar % 8 == 0, "operand alignment");
+static_assert(kGTcW % 16 == 0 && kGTcGroupBytes % 16 == 0 && kGTcBar % 8 == 0, "operand alignment");
+
+// Output row of the network that feeds accumulator column o: logits first
+// (column k = logit of lobe k), then lobe k's mean xyz and concentration in
+// columns 8 + 4 k .. 8 + 4 k + 3, then the padding rows.
+__host__ __device__ constexpr int g_tc_out_row(int o) {
+    return o < kGLobes ? 5 * o + 4 : (o < kGLobes + 4 * kGLobes ? 5 * ((o - kGLobes) / 4) + (o - kGLobes) % 4 : o);
+}
 
 // Issue the K / 16 MMAs of one layer: D[128 x N] = A[128 x K] B[N x K]^T.
 template <int K, int N>
@@ -250,6 +265,12 @@ __device__ __forceinline__ void tc_layer(uint32_t tmem, uint32_t a_saddr, uint32
         const uint64_t bd = umma_desc(b_saddr + s * 256u, 128u, K * 16u);
         umma_bf16(tmem, ad, bd, idesc, s > 0 ? 1u : 0u);
     }
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
 }
 
 // Accumulator row (64 columns) of this thread -> ReLU -> BF16 row of the hidden tile.
@@ -271,35 +292,75 @@ __device__ __forceinline__ void tc_relu_to_hidden(uint32_t tmem_row, unsigned ch
     }
 }
 
+// One lobe's record (mixture_record's algebra) from its four accumulator
+// columns: float4(kappa mu, b) with b = log pi - kappa + log(kappa / (2 pi (1 - e^{-2 kappa}))).
+__device__ __forceinline__ float4 tc_lobe_record(const uint32_t* v, float log_pi) {
+    const float mxx = __uint_as_float(v[0]), myy = __uint_as_float(v[1]), mzz = __uint_as_float(v[2]);
+    const float r = __uint_as_float(v[3]);
+    const float l2 = mxx * mxx + myy * myy + mzz * mzz;
+    const float sp = r > 15.0f ? r : __logf(1.0f + __expf(r));
+    const float kap = fminf(sp + 1e-3f, 5e3f);
+    constexpr float kLog2Pi = 1.83787706640934548356f;
+    const float b = log_pi + __logf(__fdividef(kap, 1.0f - __expf(-2.0f * kap))) - kLog2Pi - kap;
+    if (l2 > 1e-24f) {
+        const float sc = kap * rsqrtf(l2);
+        return make_float4(sc * mxx, sc * myy, sc * mzz, b);
+    }
+    return make_float4(0.0f, 0.0f, kap, b);
+}
+
+// Group-wide barrier over the group's 128 threads (named barrier 1 + g, an
+// immediate, so that the kernel reserves barriers 0-3 only) with an AND vote.
+template <int Id>
+__device__ __forceinline__ bool bar_red_and(bool v) {
+    uint32_t out;
+    asm volatile(
+        "{\n.reg .pred p, q;\n"
+        "setp.ne.u32 p, %1, 0;\n"
+        "bar.red.and.pred q, %2, 128, p;\n"
+        "selp.u32 %0, 1, 0, q;\n}"
+        : "=r"(out)
+        : "r"(v ? 1u : 0u), "n"(Id)
+        : "memory");
+    return out != 0u;
+}
+__device__ __forceinline__ bool group_sync_and(int g, bool v) {
+    static_assert(kGTcGroups == 3, "one named barrier per group");
+    return g == 0 ? bar_red_and<1>(v) : (g == 1 ? bar_red_and<2>(v) : bar_red_and<3>(v));
+}
+
 __global__ void __launch_bounds__(kGTcThreads, kGTcBlocksPerSm)
 k_guide_mlp_tc(GuideNet net, const uint32_t* counts, int q, uint32_t cap, uint32_t qn,
                const unsigned char* __restrict__ feat, float* __restrict__ mix_out, uint32_t* err) {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     const uint32_t n = counts ? min(counts[q], cap) : qn;
     const uint32_t tiles = (n + kGTcRows - 1) / kGTcRows;
-    if (blockIdx.x >= tiles) return;   // uniform: before any barrier or allocation
-    uint64_t* bar_feat = reinterpret_cast<uint64_t*>(tc_smem + kGTcBar);
-    uint64_t* bar_mma = bar_feat + 1;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_feat + 2);
+    if (blockIdx.x * kGTcGroups >= tiles) return;   // uniform: before any barrier or allocation
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int grp = warp >> 2, gtid = tid & 127, gwarp = warp & 3;
+    uint64_t* bar_feat = reinterpret_cast<uint64_t*>(tc_smem + kGTcBar) + 2 * grp;
+    uint64_t* bar_mma = bar_feat + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + kGTcBar + 16 * kGTcGroups);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
                      "r"(kGTcCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    if (tid == 0) {
+    if (gtid == 0) {
         mbar_init(bar_feat, 1);
         mbar_init(bar_mma, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // weights -> the canonical operand layout, 16 bytes (8 inputs of one output) at a time
+    // weights -> the canonical operand layout, 16 bytes (8 inputs of one output) at a time;
+    // the output layer's rows in accumulator-column order
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
         const int in = g_in(l), chunks = g_out(l) * in / 8;
         for (int c = tid; c < chunks; c += kGTcThreads) {
             const int o = c / (in / 8), j = c % (in / 8);
-            const uint4 v = *reinterpret_cast<const uint4*>(net.w + g_woff(l) + o * in + j * 8);
+            const int src = l == 3 ? g_tc_out_row(o) : o;
+            const uint4 v = *reinterpret_cast<const uint4*>(net.w + g_woff(l) + src * in + j * 8);
             *reinterpret_cast<uint4*>(tc_smem + g_tc_woff(l) + umma_off(o, 8 * j, in)) = v;
         }
     }
@@ -307,24 +368,28 @@ k_guide_mlp_tc(GuideNet net, const uint32_t* counts, int q, uint32_t cap, uint32
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t tmem_row = tmem + (static_cast<uint32_t>(32 * warp) << 16);   // this warp's lane quadrant
+    const uint32_t tmem = *tmem_slot + 64u * grp;                                  // this group's columns
+    const uint32_t tmem_row = tmem + (static_cast<uint32_t>(32 * gwarp) << 16);   // this warp's lane quadrant
     const uint32_t s_base = smem_addr(tc_smem);
-    unsigned char* H = tc_smem + kGTcH;
+    unsigned char* F = tc_smem + kGTcW + grp * kGTcGroupBytes;
+    unsigned char* H = F + kGFeatTileBytes;
+    const uint32_t sF = smem_addr(F), sH = smem_addr(H);
+    const uint32_t tstride = gridDim.x * kGTcGroups;
     uint32_t feat_phase = 0, mma_phase = 0;
     bool ok = true;
-    uint32_t tile = blockIdx.x;
-    if (tid == 0) bulk_load(tc_smem + kGTcF, feat + static_cast<size_t>(tile) * kGFeatTileBytes, kGFeatTileBytes, bar_feat);
-    // Every decision to stop is taken on a CTA-wide vote (__syncthreads_and),
-    // so all threads leave the loop together and meet the same barriers.
-    for (; tile < tiles; tile += gridDim.x) {
+    uint32_t tile = blockIdx.x * kGTcGroups + grp;
+    if (gtid == 0 && tile < tiles)
+        bulk_load(F, feat + static_cast<size_t>(tile) * kGFeatTileBytes, kGFeatTileBytes, bar_feat);
+    // Every decision to stop is taken on a group-wide vote, so the group's
+    // threads leave the loop together and meet the same barriers.
+    for (; tile < tiles; tile += tstride) {
         // layer 0 once the features have landed
-        ok = __syncthreads_and(mbar_wait(bar_feat, feat_phase)) != 0;
+        ok = group_sync_and(grp, mbar_wait(bar_feat, feat_phase));
         feat_phase ^= 1u;
         if (!ok) break;
-        if (tid == 0) {
+        if (gtid == 0) {
             tc_fence_after();
-            tc_layer<kGIn, kGHid>(tmem, s_base + kGTcF, s_base + g_tc_woff(0));
+            tc_layer<kGIn, kGHid>(tmem, sF, s_base + g_tc_woff(0));
             umma_commit(bar_mma);
         }
         // layers 0..2: wait, ReLU into the hidden tile, next layer
@@ -333,18 +398,17 @@ k_guide_mlp_tc(GuideNet net, const uint32_t* counts, int q, uint32_t cap, uint32
             ok = __all_sync(0xffffffffu, mbar_wait(bar_mma, mma_phase));   // tcgen05.ld wants whole warps
             mma_phase ^= 1u;
             tc_fence_after();
-            if (l == 0 && tid == 0 && ok && tile + gridDim.x < tiles)   // the feature tile is free again
-                bulk_load(tc_smem + kGTcF, feat + static_cast<size_t>(tile + gridDim.x) * kGFeatTileBytes,
-                          kGFeatTileBytes, bar_feat);
-            if (ok) tc_relu_to_hidden(tmem_row, H, static_cast<uint32_t>(tid));
+            if (l == 0 && gtid == 0 && ok && tile + tstride < tiles)   // the feature tile is free again
+                bulk_load(F, feat + static_cast<size_t>(tile + tstride) * kGFeatTileBytes, kGFeatTileBytes, bar_feat);
+            if (ok) tc_relu_to_hidden(tmem_row, H, static_cast<uint32_t>(gtid));
             fence_async_smem();
             tc_fence_before();
-            ok = __syncthreads_and(ok) != 0;
+            ok = group_sync_and(grp, ok);
             if (!ok) break;
-            if (tid == 0) {
+            if (gtid == 0) {
                 tc_fence_after();
-                if (l < 2) tc_layer<kGHid, kGHid>(tmem, s_base + kGTcH, s_base + g_tc_woff(l + 1));
-                else tc_layer<kGHid, kGOutPad>(tmem, s_base + kGTcH, s_base + g_tc_woff(3));
+                if (l < 2) tc_layer<kGHid, kGHid>(tmem, sH, s_base + g_tc_woff(l + 1));
+                else tc_layer<kGHid, kGOutPad>(tmem, sH, s_base + g_tc_woff(3));
                 umma_commit(bar_mma);
             }
         }
@@ -352,26 +416,47 @@ k_guide_mlp_tc(GuideNet net, const uint32_t* counts, int q, uint32_t cap, uint32
         ok = __all_sync(0xffffffffu, mbar_wait(bar_mma, mma_phase));
         mma_phase ^= 1u;
         tc_fence_after();
-        float raw[kGOutPad];
+        const uint32_t r = tile * kGTcRows + static_cast<uint32_t>(gtid);
+        float4* dst = reinterpret_cast<float4*>(mix_out + static_cast<size_t>(r) * kGMix);
         if (ok) {
-            uint32_t v0[32], v1[16];
-            tmem_ld32(tmem_row, v0);
-            tmem_ld16(tmem_row + 32u, v1);
+            // mixture record, streamed: logits (8 columns), then two lobes (8 columns) at a time
+            uint32_t lg[8];
+            tmem_ld8(tmem_row, lg);
             tmem_wait_ld();
+            float mx = -1e30f;
 #pragma unroll
-            for (int j = 0; j < 32; ++j) raw[j] = __uint_as_float(v0[j]);
+            for (int k = 0; k < kGLobes; ++k) mx = fmaxf(mx, __uint_as_float(lg[k]));
+            float e[kGLobes], sum = 0.0f;
 #pragma unroll
-            for (int j = 0; j < 16; ++j) raw[32 + j] = __uint_as_float(v1[j]);
+            for (int k = 0; k < kGLobes; ++k) {
+                e[k] = __expf(__uint_as_float(lg[k]) - mx);
+                sum += e[k];
+            }
+            const float log_sum = __logf(sum), inv_sum = 1.0f / sum;
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {   // lobes 2h, 2h + 1: columns 8 + 8h .. 8 + 8h + 7
+                uint32_t v[8];
+                tmem_ld8(tmem_row + 8u + 8u * h, v);
+                tmem_wait_ld();
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const int lobe = 2 * h + k;
+                    const float4 rec = tc_lobe_record(v + 4 * k, (__uint_as_float(lg[lobe]) - mx) - log_sum);
+                    if (r < n) dst[lobe] = rec;
+                }
+            }
+            if (r < n) {
+                dst[8] = make_float4(e[0] * inv_sum, e[1] * inv_sum, e[2] * inv_sum, e[3] * inv_sum);
+                dst[9] = make_float4(e[4] * inv_sum, e[5] * inv_sum, e[6] * inv_sum, e[7] * inv_sum);
+            }
         }
-        // every thread has its row out of tensor memory before the next tile's MMAs
+        // every thread has its row out of tensor memory before the group's next MMAs
         tc_fence_before();
-        ok = __syncthreads_and(ok) != 0;
+        ok = group_sync_and(grp, ok);
         if (!ok) break;
-        const uint32_t r = tile * kGTcRows + static_cast<uint32_t>(tid);
-        if (r < n) store_mixture(raw, mix_out + static_cast<size_t>(r) * kGMix);
     }
     if (!ok) {
-        if (tid == 0) atomicOr(err, kErrGuideTimeout);
+        if (gtid == 0) atomicOr(err, kErrGuideTimeout);
         // let whatever is still in flight finish (bounded) before the memory goes
         mbar_wait(bar_mma, mma_phase);
         mbar_wait(bar_feat, feat_phase);
@@ -380,7 +465,8 @@ k_guide_mlp_tc(GuideNet net, const uint32_t* counts, int q, uint32_t cap, uint32
     __syncthreads();
     tc_fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kGTcCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kGTcCols)
+                     : "memory");
 }
 
 }  // namespace ptb
