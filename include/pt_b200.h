@@ -429,6 +429,14 @@ int pt_render_batch(const pt_batch_item* items, uint32_t n, int32_t out_is_devic
 int pt_guide_create(pt_scene* scene, uint32_t seed, pt_guide** out);   /* scene must be uploaded */
 int pt_guide_destroy(pt_guide* guide);
 int pt_guide_set_learning_rate(pt_guide* guide, float lr);
+/* Training schedule.  ema > 0: renders sample with a copy of the network made
+ * from an exponential moving average of its parameters (factor ema per
+ * optimiser step; 0.995 by default), updated after every step, while training
+ * continues on the parameters themselves (0: off; averaging switched on later
+ * starts from the current parameters).  lr_half_life > 0: the learning rate
+ * halves every lr_half_life optimiser steps, down to lr_floor times its set
+ * value (0: constant, the default). */
+int pt_guide_set_schedule(pt_guide* guide, float ema, float lr_half_life, float lr_floor);
 /* probability of drawing the continuation from the network (default 0.5) */
 int pt_guide_set_alpha(pt_guide* guide, float alpha);
 /* online training: one optimiser step per `paths_per_step` paths of a pass
@@ -458,7 +466,8 @@ int pt_integrator_set_guide(pt_integrator* integ, pt_guide* guide, int32_t mode)
 /* Evaluate the learned directional density q(dir | pos) for n queries
  * (pos[3], dir[3] floats each) -> out[n].  Diagnostic / checkpoint check. */
 int pt_guide_eval(pt_guide* guide, const float* pos_dir, uint32_t n, float* out_pdf);
-/* Parameters as used by the kernels: weights (13312 floats: layers 32->64,
+/* Parameters as the renders' inference kernels use them (the averaged copy
+ * while averaging is on, see pt_guide_set_schedule): weights (13312 floats: layers 32->64,
  * 64->64, 64->64, 64->48 row-major [out][in], BF16 values) and, if grid is not
  * NULL, the hash grid (16 levels x 2^19 entries x 2 features, FP16 values);
  * meta = {lo[3], inv_extent[3], scale[16], dense_limit}. */
@@ -466,7 +475,8 @@ int pt_guide_get_params(const pt_guide* guide, float* weights, float* grid, floa
 /* One backward pass (no optimiser step) over n samples given as n x 8 floats
  * (normalised position[3], weight, direction[3], 0); returns the weight
  * gradient (13312 floats) and, if grid_grad is not NULL, the hash-grid
- * gradient (16 x 2^19 x 2 floats). */
+ * gradient (16 x 2^19 x 2 floats), both at the parameters training runs on
+ * (those pt_guide_get_params returns once averaging is off). */
 int pt_guide_backward(pt_guide* guide, const float* samples, uint32_t n, float* weight_grad, float* grid_grad);
 
 /* ---- diagnostics used by the parity tests (same kernels as the render path) ---- */

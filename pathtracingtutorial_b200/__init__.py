@@ -467,6 +467,12 @@ class Guide:
         """Probability of drawing a continuation from the network (one-sample MIS)."""
         check(lib().pt_guide_set_alpha(self._h, float(alpha)))
 
+    def set_schedule(self, ema: float = 0.0, lr_half_life: float = 0.0, lr_floor: float = 0.1) -> None:
+        """Parameter averaging for the renders (ema: factor per optimiser step,
+        0 = off) and learning-rate halving every lr_half_life steps down to
+        lr_floor of the set rate (0 = constant)."""
+        check(lib().pt_guide_set_schedule(self._h, float(ema), float(lr_half_life), float(lr_floor)))
+
     def set_inference(self, kind: int) -> None:
         """Network evaluation kernels: INFER_FUSED (encoding and MLP in one
         mma.sync kernel), INFER_SPLIT_MMA / INFER_SPLIT_TC (encoding kernel,

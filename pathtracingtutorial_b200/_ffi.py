@@ -207,6 +207,7 @@ _SIGS = [
     ("pt_guide_set_alpha", C.c_int, [_P, C.c_float]),
     ("pt_guide_set_training", C.c_int, [_P, C.c_int32, C.c_uint32]),
     ("pt_guide_set_inference", C.c_int, [_P, C.c_int32]),
+    ("pt_guide_set_schedule", C.c_int, [_P, C.c_float, C.c_float, C.c_float]),
     ("pt_guide_info", C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     ("pt_guide_loss", C.c_int, [_P, C.POINTER(C.c_float)]),
     ("pt_integrator_set_guide", C.c_int, [_P, _P, C.c_int32]),

@@ -709,6 +709,11 @@ int pt_guide_set_learning_rate(pt_guide* guide, float lr) {
     guide_set_lr(guide, lr);
     return PT_OK;
 }
+int pt_guide_set_schedule(pt_guide* guide, float ema, float lr_half_life, float lr_floor) {
+    PT_REQUIRE(guide && ema >= 0.0f && ema < 1.0f && lr_half_life >= 0.0f && lr_floor >= 0.0f && lr_floor <= 1.0f,
+               "invalid argument");
+    return guide_set_schedule(guide, ema, lr_half_life, lr_floor);
+}
 int pt_guide_set_alpha(pt_guide* guide, float alpha) {
     PT_REQUIRE(guide && alpha > 0.0f && alpha < 1.0f, "alpha must be in (0, 1)");
     guide_set_alpha(guide, alpha);

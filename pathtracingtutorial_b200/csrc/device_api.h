@@ -35,6 +35,7 @@ void batch_forget_scene(const pt_scene* s);
 int  guide_create(pt_scene* s, uint32_t seed, pt_guide** out);
 void guide_destroy(pt_guide* g);
 void guide_set_lr(pt_guide* g, float lr);
+int  guide_set_schedule(pt_guide* g, float ema, float lr_half_life, float lr_floor);
 void guide_set_alpha(pt_guide* g, float alpha);
 void guide_set_training(pt_guide* g, int paths_per_step, uint32_t samples_per_step);
 void guide_set_inference(pt_guide* g, int kind);

@@ -54,6 +54,13 @@ constexpr int kGuideMinibatchPaths = 1 << 15;
 // 0.00214 at 256 guided spp; 65,536 a step cost 2.25 s for 0.00233; 32,768
 // cost 2.0 s for 0.0034.
 constexpr uint32_t kGuideStepSamples = 65536;
+// Parameter averaging factor per optimiser step unless pt_guide_set_schedule
+// sets another.  Measured on the hidden-light room (1024 x 1024, 64 training
+// spp, time to relMSE 1e-3 against the FP64 crop, six network seeds each):
+// no averaging 7.21 s (relMSE x spp after training 0.65, sd 0.09), 0.99 6.89
+// s (0.62, sd 0.14), 0.995 6.61 s (0.58, sd 0.05), 0.998 7.40 s (0.71, three
+// seeds); a halving learning rate (every 512 steps) 7.81 s.
+constexpr float kGuideEma = 0.995f;
 // Inference kind used unless pt_guide_set_inference chooses another.  Network
 // stage time of a 64-spp guided render of the hidden-light room at 1024 x 1024:
 // fused 123.5 ms, encoding + mma.sync MLP 118.0 ms, encoding + tcgen05 MLP
@@ -99,7 +106,23 @@ struct GuideNet {
     uint32_t        dense_limit; // levels with (res+1)^3 <= table use direct indexing
     float*          loss;        // [2] mean loss of the last pass
     unsigned long long* loss_fix;    // [0] sum of w (-log q) (kGLossFix units), [1] samples
+    // Parameter averaging (ema > 0): renders sample with copies made from an
+    // exponential moving average of the parameters, updated after every
+    // optimiser step, while training runs on the parameters themselves.
+    float           ema;         // averaging factor (0: off)
+    float2*         grid_ema;    // averages (FP32)
+    float*          w_ema;
+    uint2*          grid_inf;    // FP16 pair table and BF16 weights made from the averages
+    __nv_bfloat16*  w_inf;
 };
+
+// The network as the renders' inference kernels read it: the averaged copies
+// when averaging is on, else the parameters the training kernels use.
+__host__ __device__ inline GuideNet guide_infer_view(const GuideNet& n) {
+    GuideNet v = n;
+    if (n.ema > 0.0f) { v.grid = n.grid_inf; v.w = n.w_inf; }
+    return v;
+}
 
 // Fixed-point gradient sums: a contribution x is added as round(x * 2^40)
 // (clamped to +-2^20, far above any gradient of a mean loss), so a sum holds
@@ -847,6 +870,8 @@ struct GuideState {
     int          infer = kGuideInferDefault;   // PT_GUIDE_INFER_*
     int          mode = 0;            // 0 off, PT_GUIDE_USE, PT_GUIDE_TRAIN
     float        lr = 1e-2f;
+    float        lr_half_life = 0.0f;  // optimiser steps per halving of the learning rate (0: constant)
+    float        lr_floor = 0.1f;      // the learning rate stays above this fraction of lr
     float        alpha = kGuideAlpha;
     int          paths_per_step = kGuideMinibatchPaths;   // optimiser steps: one per this many paths of a pass
     uint32_t     samples_per_step = kGuideStepSamples;    // cap of training samples per step (0 = all)
@@ -868,11 +893,17 @@ __global__ void k_guide_step(uint32_t* sample_count, uint32_t* step, float* loss
 // Adam step for minibatch mb (skipped when it is empty); the step number is
 // the counter plus the non-empty minibatches before it, plus one.
 __global__ void k_guide_adam(GuideNet net, const uint32_t* count, uint32_t cap, int mb, int nmb, const uint32_t* step,
-                             float lr_w, float lr_g, float b1, float b2, float eps) {
+                             float lr_w, float lr_g, float b1, float b2, float eps, float lr_half_life, float lr_floor) {
     const uint32_t n = min(*count, cap);
     if (n <= static_cast<uint32_t>(mb)) return;
     const float t = static_cast<float>(*step + steps_before(n, mb, nmb) + 1u);
     const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
+    if (lr_half_life > 0.0f) {   // learning rate halving every lr_half_life steps, down to lr_floor of it
+        const float f = fmaxf(lr_floor, exp2f(-t / lr_half_life));
+        lr_w *= f;
+        lr_g *= f;
+    }
+    const float ea = net.ema, eb = 1.0f - net.ema;
     const size_t nw = kGWeights;
     const size_t ng = static_cast<size_t>(kGLevels) * kGTable;
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < nw + ng;
@@ -885,6 +916,11 @@ __global__ void k_guide_adam(GuideNet net, const uint32_t* count, uint32_t cap, 
             const float p = net.w_master[i] - lr_w * (m / bc1) / (sqrtf(v / bc2) + eps);
             net.w_master[i] = p;
             net.w[i] = __float2bfloat16_rn(p);
+            if (ea > 0.0f) {
+                const float e = ea * net.w_ema[i] + eb * p;
+                net.w_ema[i] = e;
+                net.w_inf[i] = __float2bfloat16_rn(e);
+            }
         } else {
             const size_t j = i - nw;
             const ulonglong2 gi = reinterpret_cast<const ulonglong2*>(net.grid_grad)[j];
@@ -902,6 +938,15 @@ __global__ void k_guide_adam(GuideNet net, const uint32_t* count, uint32_t cap, 
             const size_t prev = (j & ~static_cast<size_t>(kGTable - 1)) | ((j + kGTable - 1) & (kGTable - 1));
             reinterpret_cast<__half2*>(net.grid + j)[0] = hp;
             reinterpret_cast<__half2*>(net.grid + prev)[1] = hp;
+            if (ea > 0.0f) {
+                float2 e = net.grid_ema[j];
+                e.x = ea * e.x + eb * p.x;
+                e.y = ea * e.y + eb * p.y;
+                net.grid_ema[j] = e;
+                const __half2 he = __floats2half2_rn(e.x, e.y);
+                reinterpret_cast<__half2*>(net.grid_inf + j)[0] = he;
+                reinterpret_cast<__half2*>(net.grid_inf + prev)[1] = he;
+            }
         }
     }
 }

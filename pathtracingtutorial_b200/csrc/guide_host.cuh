@@ -60,7 +60,12 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     const size_t off_wg = off_wm + wf;                                    // u64 per weight
     const size_t wg = al(kGWeights * sizeof(unsigned long long));
     const size_t off_step = off_wg + wg + 2 * wf;
-    const size_t total = off_step + 256;
+    // parameter averages and the copies made from them
+    const size_t off_gema = off_step + 256;
+    const size_t off_ginf = off_gema + al(ng * sizeof(float2));
+    const size_t off_wema = off_ginf + al(ng * sizeof(uint2));
+    const size_t off_winf = off_wema + wf;
+    const size_t total = off_winf + al(kGWeights * sizeof(__nv_bfloat16));
     if (!guide_cuda_ok(cudaMalloc(&g.params, total), "parameter allocation")) return PT_ERR_NOMEM;
     g.param_bytes = total;
     char* base = static_cast<char*>(g.params);
@@ -77,6 +82,11 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     g.step = reinterpret_cast<uint32_t*>(base + off_step);
     g.net.loss = reinterpret_cast<float*>(base + off_step + 16);
     g.net.loss_fix = reinterpret_cast<unsigned long long*>(base + off_step + 32);
+    g.net.ema = kGuideEma;
+    g.net.grid_ema = reinterpret_cast<float2*>(base + off_gema);
+    g.net.grid_inf = reinterpret_cast<uint2*>(base + off_ginf);
+    g.net.w_ema = reinterpret_cast<float*>(base + off_wema);
+    g.net.w_inf = reinterpret_cast<__nv_bfloat16*>(base + off_winf);
     // host-side initial values
     std::mt19937 rng(seed);
     std::vector<float> gm(2 * ng);
@@ -107,6 +117,10 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
               guide_cuda_ok(cudaMemcpy(g.net.w_master, w.data(), kGWeights * sizeof(float), cudaMemcpyHostToDevice), "upload") &&
               guide_cuda_ok(cudaMemset(g.net.w_grad, 0, wg + 2 * wf), "clear") &&
               guide_cuda_ok(cudaMemset(g.step, 0, 256), "clear") &&
+              guide_cuda_ok(cudaMemcpy(g.net.grid_inf, gh.data(), ng * sizeof(uint2), cudaMemcpyHostToDevice), "upload") &&
+              guide_cuda_ok(cudaMemcpy(g.net.grid_ema, gm.data(), ng * sizeof(float2), cudaMemcpyHostToDevice), "upload") &&
+              guide_cuda_ok(cudaMemcpy(g.net.w_inf, wb.data(), kGWeights * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice), "upload") &&
+              guide_cuda_ok(cudaMemcpy(g.net.w_ema, w.data(), kGWeights * sizeof(float), cudaMemcpyHostToDevice), "upload") &&
               guide_cuda_ok(cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kGTrainSmem), "smem") &&
               guide_cuda_ok(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kGInferSmem), "smem") &&
               guide_cuda_ok(cudaFuncSetAttribute(k_guide_mlp_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, kGInferSmem), "smem") &&

@@ -1271,8 +1271,10 @@ struct StageEvent { int kind; cudaEvent_t a, b; };
 // P.pass->frame, as passes of the wavefront's lanes.
 // Guide inference over queue q (the hit points of its rays) into the guide's
 // mixture buffer, by the guide's inference kind.
-void launch_guide_infer(const GuideState& g, const WaveParams& P, int q, int sms, cudaStream_t st) {
+void launch_guide_infer(const GuideState& gs, const WaveParams& P, int q, int sms, cudaStream_t st) {
     const uint32_t cap = static_cast<uint32_t>(P.npath);
+    GuideState g = gs;
+    g.net = guide_infer_view(gs.net);
     if (g.infer == PT_GUIDE_INFER_FUSED) {
         k_guide_infer<<<sms * kGInferBlocksPerSm, 32 * kGInferWarps, kGInferSmem, st>>>(g.net, P.counts, q, cap,
                                                                                       P.ray_o[q], P.ray_d[q], P.hit,
@@ -1361,7 +1363,8 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
                                                                                    step_cap, gs->partial,
                                                                                    gs->net.w_grad);
                         k_guide_adam<<<wf.sms * 8, 256, 0, st>>>(gs->net, gs->counters, gs->sample_cap, mb, nmb,
-                                                                 gs->step, gs->lr, gs->lr, 0.9f, 0.99f, 1e-10f);
+                                                                 gs->step, gs->lr, gs->lr, 0.9f, 0.99f, 1e-10f,
+                                                                 gs->lr_half_life, gs->lr_floor);
                     }
                     k_guide_step<<<1, 1, 0, st>>>(gs->counters, gs->step, gs->net.loss, gs->net.loss_fix,
                                                   gs->sample_cap, nmb);
@@ -1777,8 +1780,12 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     } else if (use_graph) {
         // everything the captured launches bake in: the parameters, the stream,
         // the frame count and the guide's training settings
-        struct GuideKey { const void* params; const void* feat; float lr; int paths_per_step; uint32_t samples_per_step; int infer; } gk{};
-        if (gs) gk = GuideKey{gs->params, gs->feat, gs->lr, gs->paths_per_step, gs->samples_per_step, gs->infer};
+        struct GuideKey {
+            const void* params; const void* feat; float lr, lr_half_life, lr_floor, ema;
+            int paths_per_step; uint32_t samples_per_step; int infer;
+        } gk{};
+        if (gs) gk = GuideKey{gs->params, gs->feat, gs->lr, gs->lr_half_life, gs->lr_floor, gs->net.ema,
+                              gs->paths_per_step, gs->samples_per_step, gs->infer};
         std::vector<unsigned char> key(sizeof(WaveParams) + sizeof(cudaStream_t) + sizeof(int) + sizeof(GuideKey));
         std::memcpy(key.data(), &P, sizeof(WaveParams));
         std::memcpy(key.data() + sizeof(WaveParams), &st, sizeof(cudaStream_t));
@@ -2073,6 +2080,23 @@ void guide_destroy(pt_guide* h) {
 }
 
 void guide_set_lr(pt_guide* h, float lr) { h->g.lr = lr; }
+int guide_set_schedule(pt_guide* h, float ema, float lr_half_life, float lr_floor) {
+    GuideNet& n = h->g.net;
+    if (ema > 0.0f && n.ema == 0.0f) {
+        // averaging starts from the current parameters
+        if (int rc = ensure_device(h->g.device)) return rc;
+        const size_t ng = static_cast<size_t>(kGLevels) * kGTable;
+        PT_CU(cudaDeviceSynchronize());
+        PT_CU(cudaMemcpy(n.grid_ema, n.grid_master, ng * sizeof(float2), cudaMemcpyDeviceToDevice));
+        PT_CU(cudaMemcpy(n.grid_inf, n.grid, ng * sizeof(uint2), cudaMemcpyDeviceToDevice));
+        PT_CU(cudaMemcpy(n.w_ema, n.w_master, kGWeights * sizeof(float), cudaMemcpyDeviceToDevice));
+        PT_CU(cudaMemcpy(n.w_inf, n.w, kGWeights * sizeof(__nv_bfloat16), cudaMemcpyDeviceToDevice));
+    }
+    n.ema = ema;
+    h->g.lr_half_life = lr_half_life;
+    h->g.lr_floor = lr_floor;
+    return PT_OK;
+}
 void guide_set_alpha(pt_guide* h, float alpha) { h->g.alpha = alpha; }
 void guide_set_inference(pt_guide* h, int kind) { h->g.infer = kind == PT_GUIDE_INFER_DEFAULT ? kGuideInferDefault : kind; }
 void guide_set_training(pt_guide* h, int paths_per_step, uint32_t samples_per_step) {
@@ -2111,13 +2135,14 @@ int integrator_set_guide(pt_integrator* integ, pt_guide* h, int mode) {
 int guide_get_params(const pt_guide* h, float* weights, float* grid, float* meta) {
     if (int rc = ensure_device(h->g.device)) return rc;
     PT_CU(cudaDeviceSynchronize());
+    const GuideNet net = guide_infer_view(h->g.net);
     std::vector<__nv_bfloat16> wb(kGWeights);
-    PT_CU(cudaMemcpy(wb.data(), h->g.net.w, kGWeights * sizeof(__nv_bfloat16), cudaMemcpyDeviceToHost));
+    PT_CU(cudaMemcpy(wb.data(), net.w, kGWeights * sizeof(__nv_bfloat16), cudaMemcpyDeviceToHost));
     for (int i = 0; i < kGWeights; ++i) weights[i] = __bfloat162float(wb[i]);
     if (grid) {
         const size_t ng = static_cast<size_t>(kGLevels) * kGTable;
         std::vector<__half2> gh(2 * ng);
-        PT_CU(cudaMemcpy(gh.data(), h->g.net.grid, ng * sizeof(uint2), cudaMemcpyDeviceToHost));
+        PT_CU(cudaMemcpy(gh.data(), net.grid, ng * sizeof(uint2), cudaMemcpyDeviceToHost));
         for (size_t i = 0; i < ng; ++i) {
             const float2 v = __half22float2(gh[2 * i]);
             grid[2 * i] = v.x;
@@ -2197,7 +2222,8 @@ __global__ void __launch_bounds__(256) k_guide_mix_pdf(const float* __restrict__
 int guide_eval(pt_guide* h, const float* qd, uint32_t n, float* out) {
     if (int rc = ensure_device(h->g.device)) return rc;
     if (n == 0) return PT_OK;
-    const GuideState& g = h->g;
+    GuideState g = h->g;
+    g.net = guide_infer_view(h->g.net);
     const bool split = g.infer != PT_GUIDE_INFER_FUSED;
     int sms = 0;
     PT_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device));

@@ -127,6 +127,7 @@ def test_guide_gradients_match_fp64_oracle_at_init():
     from pathtracingtutorial_b200 import scenes
     s = _scene(scenes.cornell_box(width=32, height=32, spp=4))
     g = pt.Guide(s, seed=5)
+    g.set_schedule(ema=0.0)   # the parameters read back are then the ones training runs on
     _check_gradients(g, 11, False)
     g.close()
 
@@ -137,7 +138,9 @@ def test_guide_forward_and_gradients_after_training():
     from pathtracingtutorial_b200 import scenes
     sa = scenes.hidden_light_room(width=64, height=64, n_boxes=40, box_subdiv=2, spp=8, max_depth=8)
     s = _scene(sa)
-    img, g, _ = pt.render_guided(s, train_spp=64, spp=8)
+    g = pt.Guide(s, seed=1)
+    g.set_schedule(ema=0.0)   # the parameters read back are then the ones training runs on
+    img, g, _ = pt.render_guided(s, train_spp=64, spp=8, guide=g)
     assert g.info()["steps"] > 0
     prm = g.params()
     # forward: pdf at world positions inside the scene bounds
