@@ -556,11 +556,17 @@ def ours(args):
     per_launch_ms = ist["extend_ms"] / launches
     achieved = alg_bytes / launches / (per_launch_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = None
+    traffic = units = None
     tp = os.path.join(ROOT, "profiles", "extend_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+            prof = json.load(f)
+        traffic = prof.get("dram_bytes_per_launch")
+        u = prof.get("units_small_case")
+        if u:   # the L2 / L1 / issue fractions beside the HBM one (ncu, small case)
+            units = {k: u[k] for k in ("l2_throughput_of_peak", "l1tex_throughput_of_peak", "dram_throughput_of_peak",
+                                       "issue_active_of_peak", "lanes_per_warp_instruction")}
+            units["source"] = "profiles/extend_traffic.json (ncu --set full, 4-spp case)"
     stage_total = ist["extend_ms"] + ist["shade_ms"] + ist["shadow_ms"] + ist["other_ms"]
 
     if rank != 0:
@@ -594,7 +600,7 @@ def ours(args):
                 "path": "pt_scene_upload + pt_render (host arrays -> device, 256 spp, image -> host)"},
         "roofline": {"kernel": "k_extend (closest-hit traversal)", "bound": "hbm", "achieved": round(achieved, 1),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes / launches,
+                     "traffic": traffic, "units": units, "algorithmic_bytes_per_launch": alg_bytes / launches,
                      "avg_launch_ms": round(per_launch_ms, 4), "launches": launches,
                      "stage_ms": {"extend": round(ist["extend_ms"], 2), "shade": round(ist["shade_ms"], 2),
                                   "shadow": round(ist["shadow_ms"], 2), "other": round(ist["other_ms"], 2)},
