@@ -74,7 +74,8 @@ struct WaveParams {
     float4*  sq_o;      // w = slot (bits)
     float4*  sq_d;      // w = tmax
     float4*  sq_c;
-    uint32_t* counts;   // [0], [1] path queues, [2] shadow queue
+    uint32_t* counts;   // [0], [1] path queues, [2] shadow queue, [4] sampling list
+    uint32_t* slist;    // queue entries that continue by sampling (k_shade_front -> k_shade_back)
     unsigned long long* stats;
     uint32_t* err;
     PassState* pass;
@@ -394,6 +395,7 @@ __global__ void __launch_bounds__(Block) k_extend(WaveParams P, int q, int depth
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.counts[q ^ 1] = 0;
         P.counts[2] = 0;
+        P.counts[4] = 0;
         atomicAdd(P.stats + (depth == 0 ? kStatCameraRays : kStatExtRays), static_cast<unsigned long long>(n));
     }
     const bool watertight = (P.flags & PT_FLAG_WATERTIGHT) != 0;
@@ -807,6 +809,11 @@ __global__ void __launch_bounds__(128, 6) k_shade_front(WaveParams P, int q, int
                                                                thr.w, lo.w != 0.0f, L, rng, no, nd, sink, gv, sp);
         P.lo[p] = f4of(L, lo.w);
         P.rng[p] = rng.s;
+        // the back kernel takes only the entries that continue by sampling, so
+        // its warps start full
+        const bool samp = r == 1 && !last;
+        const uint32_t js = warp_append(P.counts + 4, samp);
+        if (samp) P.slist[js] = i;
         if (Textured) {
             // the back kernel recomputes the surface from the untouched hit and
             // ray; a negative primitive tells it that this path needs no sampling
@@ -825,10 +832,11 @@ __global__ void __launch_bounds__(128, 6) k_shade_front(WaveParams P, int q, int
 template <bool Guided, bool Textured = false>
 __global__ void __launch_bounds__(128, 6) k_shade_back(WaveParams P, int q, int depth, int s0) {
     const uint32_t cap = static_cast<uint32_t>(P.npath);
-    const uint32_t n = min(P.counts[q], cap);
+    const uint32_t n = min(P.counts[4], cap);
     const uint32_t sidx0 = P.pass->frame * static_cast<uint32_t>(P.spf) + static_cast<uint32_t>(s0);
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const uint32_t i = P.slist[j];
         const float4 h = P.hit[i];
         const int code = Textured ? __float_as_int(h.y) : __float_as_int(h.w);
         bool cont = false;
@@ -1191,6 +1199,7 @@ size_t arena_size(int npath, int n_slots) {
     b += S * 4 + 256;                // sq_path
     b += 3 * (S * 16 + 256);         // sq_o, sq_d, sq_c
     b += 64 * 4 + 256;               // counts
+    b += P * 4 + 256;                // slist
     b += kStatCount * 8 + 256;       // stats
     b += 4 * 4 + 256;                // err
     b += sizeof(PassState) + 256;
@@ -1250,6 +1259,7 @@ int wavefront_prepare(Wavefront& wf, int device, int npath, int n_slots) {
     b.sq_d = carve<float4>(cur, S);
     b.sq_c = carve<float4>(cur, S);
     b.counts = carve<uint32_t>(cur, 64);
+    b.slist = carve<uint32_t>(cur, P);
     b.stats = carve<unsigned long long>(cur, kStatCount);
     b.err = carve<uint32_t>(cur, 4);
     b.pass = carve<PassState>(cur, 1);
