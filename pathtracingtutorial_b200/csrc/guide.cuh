@@ -63,9 +63,10 @@ constexpr uint32_t kGuideStepSamples = 65536;
 constexpr float kGuideEma = 0.995f;
 // Inference kind used unless pt_guide_set_inference chooses another.  Network
 // stage time of a 64-spp guided render of the hidden-light room at 1024 x 1024:
-// fused 123.5 ms, encoding + mma.sync MLP 118.0 ms, encoding + tcgen05 MLP
-// 101.5 ms (with the exactly rounded exponentials and logarithms in the
-// mixture records: 160.5 / 152.0 / 114.6 ms).
+// fused 124.7 ms, encoding + mma.sync MLP 114.6 ms, encoding + tcgen05 MLP
+// 98.2 ms (with the exactly rounded exponentials and logarithms in the
+// mixture records and without the dense levels' four-corner table: 160.5 /
+// 152.0 / 114.6 ms).
 constexpr int kGuideInferDefault = PT_GUIDE_INFER_SPLIT_TC;
 
 // Optimiser steps per training pass of `paths` paths: one per
@@ -104,6 +105,13 @@ struct GuideNet {
     float           inv_ext[3];
     float           scale[kGLevels];
     uint32_t        dense_limit; // levels with (res+1)^3 <= table use direct indexing
+    // Four-corner table of the dense levels for the encoding kernel: entry
+    // x + y res + z res^2 of level l (at quad + quad_off[l]) holds the FP16
+    // feature pairs of corners (x, y), (x + 1, y), (x, y + 1), (x + 1, y + 1)
+    // of layer z, 16 bytes, made from the pair table before each inference
+    // (k_guide_quad); null: the encoding reads the pair table.
+    uint4*          quad;
+    uint32_t        quad_off[kGLevels];
     float*          loss;        // [2] mean loss of the last pass
     unsigned long long* loss_fix;    // [0] sum of w (-log q) (kGLossFix units), [1] samples
     // Parameter averaging (ema > 0): renders sample with copies made from an

@@ -65,7 +65,14 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     const size_t off_ginf = off_gema + al(ng * sizeof(float2));
     const size_t off_wema = off_ginf + al(ng * sizeof(uint2));
     const size_t off_winf = off_wema + wf;
-    const size_t total = off_winf + al(kGWeights * sizeof(__nv_bfloat16));
+    const size_t off_quad = off_winf + al(kGWeights * sizeof(__nv_bfloat16));
+    uint32_t quad_entries = 0;
+    for (uint32_t l = 0; l < g.net.dense_limit; ++l) {
+        const uint32_t res = static_cast<uint32_t>(g.net.scale[l]) + 2u;
+        g.net.quad_off[l] = quad_entries;
+        quad_entries += res * res * res;
+    }
+    const size_t total = off_quad + al(static_cast<size_t>(quad_entries) * sizeof(uint4));
     if (!guide_cuda_ok(cudaMalloc(&g.params, total), "parameter allocation")) return PT_ERR_NOMEM;
     g.param_bytes = total;
     char* base = static_cast<char*>(g.params);
@@ -87,6 +94,7 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     g.net.grid_inf = reinterpret_cast<uint2*>(base + off_ginf);
     g.net.w_ema = reinterpret_cast<float*>(base + off_wema);
     g.net.w_inf = reinterpret_cast<__nv_bfloat16*>(base + off_winf);
+    g.net.quad = quad_entries ? reinterpret_cast<uint4*>(base + off_quad) : nullptr;
     // host-side initial values
     std::mt19937 rng(seed);
     std::vector<float> gm(2 * ng);

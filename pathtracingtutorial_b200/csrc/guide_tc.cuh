@@ -32,6 +32,52 @@ __host__ __device__ __forceinline__ uint32_t guide_feat_rows(uint32_t n) {
     return (n + kGTcRows - 1u) / kGTcRows * kGTcRows;
 }
 
+// The four-corner table of the dense levels from the pair table `net.grid`.
+__global__ void __launch_bounds__(256) k_guide_quad(GuideNet net) {
+    for (uint32_t l = 0; l < net.dense_limit; ++l) {
+        const uint32_t res = static_cast<uint32_t>(net.scale[l]) + 2u;
+        const uint32_t n = res * res * res;
+        const uint2* tab = net.grid + static_cast<size_t>(l) * kGTable;
+        uint4* dst = net.quad + net.quad_off[l];
+        for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+            const uint2 a = tab[e], b = tab[(e + res) & (kGTable - 1)];
+            dst[e] = make_uint4(a.x, a.y, b.x, b.y);
+        }
+    }
+}
+
+// encode_level for a dense level from the four-corner table: two 16-byte
+// gathers (layers z and z + 1) instead of four 8-byte ones, the same
+// products summed in the same order.
+__device__ __forceinline__ float2 encode_level_quad(const GuideNet& net, int level, f3 p) {
+    const float s = net.scale[level];
+    const float fx = p.x * s + 0.5f, fy = p.y * s + 0.5f, fz = p.z * s + 0.5f;
+    const float bx = floorf(fx), by = floorf(fy), bz = floorf(fz);
+    const float tx = fx - bx, ty = fy - by, tz = fz - bz;
+    const uint32_t ix = static_cast<uint32_t>(bx), iy = static_cast<uint32_t>(by), iz = static_cast<uint32_t>(bz);
+    const uint32_t res = static_cast<uint32_t>(s) + 2u;
+    const uint4* tab = net.quad + net.quad_off[level];
+    const uint32_t e0 = ix + iy * res + iz * res * res;
+    float2 r = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int cz = 0; cz < 2; ++cz) {
+        const uint4 qd = __ldg(tab + e0 + static_cast<uint32_t>(cz) * res * res);
+#pragma unroll
+        for (int cy = 0; cy < 2; ++cy) {
+            const uint32_t u0 = cy ? qd.z : qd.x, u1 = cy ? qd.w : qd.y;
+            const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&u0));
+            const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&u1));
+            const float w0 = (1.0f - tx) * (cy ? ty : 1.0f - ty) * (cz ? tz : 1.0f - tz);
+            const float w1 = tx * (cy ? ty : 1.0f - ty) * (cz ? tz : 1.0f - tz);
+            r.x += w0 * f0.x;
+            r.y += w0 * f0.y;
+            r.x += w1 * f1.x;
+            r.y += w1 * f1.y;
+        }
+    }
+    return r;
+}
+
 // ---------------------------------------------------------------------------
 // Encoding: thread (row r, level l); 16 lanes per query, 2 queries per warp.
 // Rows between n and the end of the last tile get zero features.  Positions
@@ -57,7 +103,9 @@ __global__ void __launch_bounds__(256) k_guide_encode(GuideNet net, const uint32
                 const float t = __float_as_int(h.y) >= 0 ? h.x : 0.0f;
                 x = mk(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
             }
-            e = encode_level(net, level, guide_normalise(net, x));
+            const f3 pn = guide_normalise(net, x);
+            e = (net.quad && static_cast<uint32_t>(level) < net.dense_limit) ? encode_level_quad(net, level, pn)
+                                                                             : encode_level(net, level, pn);
         }
         unsigned char* tile = feat + static_cast<size_t>(r / kGTcRows) * kGFeatTileBytes;
         *reinterpret_cast<uint32_t*>(tile + umma_off(r % kGTcRows, 2u * level, kGIn)) = pack_bf16(e.x, e.y);

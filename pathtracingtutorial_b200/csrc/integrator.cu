@@ -1291,6 +1291,7 @@ void launch_guide_infer(const GuideState& gs, const WaveParams& P, int q, int sm
                                                                                       g.mix);
         return;
     }
+    if (g.net.quad) k_guide_quad<<<sms * 2, 256, 0, st>>>(g.net);
     k_guide_encode<<<sms * 8, 256, 0, st>>>(g.net, P.counts, q, cap, P.ray_o[q], P.ray_d[q], P.hit, nullptr, 0u,
                                             g.feat);
     if (g.infer == PT_GUIDE_INFER_SPLIT_MMA)
@@ -1823,7 +1824,7 @@ int integrator_launch(pt_integrator* integ, pt_film* film, pt_scene* s, const pt
     if (!timing) wf.extend_launches += passes * static_cast<uint64_t>(P.max_depth);
     wf.kernel_launches += 1 + passes * (1 + 4 * static_cast<uint64_t>(P.max_depth));
     if (P.gmix)
-        wf.kernel_launches += passes * ((wf.guide->infer == PT_GUIDE_INFER_FUSED ? 1 : 2) * P.max_depth +
+        wf.kernel_launches += passes * ((wf.guide->infer == PT_GUIDE_INFER_FUSED ? 1 : 3) * P.max_depth +
                                         (P.grec ? 5 + 4 * guide_minibatches(int64_t(P.npix) * lanes, wf.guide->paths_per_step) : 0));
     return PT_OK;
 }
@@ -2256,6 +2257,7 @@ int guide_eval(pt_guide* h, const float* qd, uint32_t n, float* out) {
         if (!split) {
             k_guide_eval<<<sms, 128, kGEvalSmem>>>(g.net, dq, n, dout);
         } else {
+            if (g.net.quad) k_guide_quad<<<sms * 2, 256>>>(g.net);
             k_guide_encode<<<sms * 8, 256>>>(g.net, nullptr, 0, 0u, nullptr, nullptr, nullptr, dq, n, feat);
             if (g.infer == PT_GUIDE_INFER_SPLIT_MMA)
                 k_guide_mlp_mma<<<sms * kGInferBlocksPerSm, 32 * kGInferWarps, kGInferSmem>>>(g.net, nullptr, 0, 0u, n,
