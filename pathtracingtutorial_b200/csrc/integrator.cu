@@ -389,7 +389,10 @@ __device__ __forceinline__ void warp_count(unsigned long long* dst, uint32_t v) 
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, static_cast<unsigned long long>(v));
 }
 
-template <int Block, int Depth>
+// Closest hits of queue q.  Packet: the queue holds camera rays, 32
+// neighbouring pixels of one sample per warp, walked as packets
+// (closest_packet_loop); else lane by lane with refill (closest_loop).
+template <int Block, int Depth, bool Packet = false>
 __global__ void __launch_bounds__(Block) k_extend(WaveParams P, int q, int depth) {
     const uint32_t n = min(P.counts[q], static_cast<uint32_t>(P.npath));
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -406,16 +409,22 @@ __global__ void __launch_bounds__(Block) k_extend(WaveParams P, int q, int depth
     const float4* __restrict__ ro = P.ray_o[q];
     const float4* __restrict__ rd = P.ray_d[q];
     float4* __restrict__ hit = P.hit;
-    closest_loop<Depth>(P.scene, blockIdx.x * blockDim.x + threadIdx.x, n, stride, watertight, err, tc,
-                 [&](uint32_t i, RayInv& r) {
-                     const float4 o = ro[i];
-                     const float4 d = rd[i];
-                     r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
-                 },
-                 [&](uint32_t i, const ClosestWalk& w) {
-                     hit[i] = w.prim >= 0 ? make_float4(w.best, __int_as_float(w.prim), w.bu, w.bv)
-                                          : make_float4(FLT_MAX, __int_as_float(-1), 0.0f, 0.0f);
-                 });
+    auto fetch = [&](uint32_t i, RayInv& r) {
+        const float4 o = ro[i];
+        const float4 d = rd[i];
+        r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+    };
+    auto done = [&](uint32_t i, const ClosestWalk& w) {
+        hit[i] = w.prim >= 0 ? make_float4(w.best, __int_as_float(w.prim), w.bu, w.bv)
+                             : make_float4(FLT_MAX, __int_as_float(-1), 0.0f, 0.0f);
+    };
+    if (Packet) {
+        closest_packet_loop<Depth>(P.scene, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, stride >> 5, n, watertight,
+                                   err, tc, fetch, done);
+    } else {
+        closest_loop<Depth>(P.scene, blockIdx.x * blockDim.x + threadIdx.x, n, stride, watertight, err, tc, fetch,
+                            done);
+    }
     if (err) atomicOr(P.err, err);
     if (count) {
         warp_count(P.stats + kStatNodes, tc.inner);
@@ -1122,7 +1131,11 @@ inline const void* shadow_kernel(int k) {
 }
 inline void launch_extend(int k, int grid, cudaStream_t st, const WaveParams& P, int q, int d) {
     switch (k) {
-#define PT_CASE(i, b, dd) case i: k_extend<b, dd><<<grid, b, 0, st>>>(P, q, d); return;
+#define PT_CASE(i, b, dd)                                                   \
+    case i:                                                                 \
+        if (d == 0) k_extend<b, dd, true><<<grid, b, 0, st>>>(P, q, d);     \
+        else k_extend<b, dd><<<grid, b, 0, st>>>(P, q, d);                  \
+        return;
         PT_TRACE_SHAPES(PT_CASE)
 #undef PT_CASE
     }

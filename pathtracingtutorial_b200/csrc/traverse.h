@@ -451,6 +451,121 @@ __device__ __forceinline__ void closest_loop(const DeviceScene& s, uint32_t i, u
     }
 }
 
+// Packet walk of the rays of one warp whose direction signs agree (sgn3: the
+// shared sign bits x | y << 1 | z << 2).  The child order of every inner
+// node depends only on the parent's axis and the ray's sign along it, so all
+// lanes share one depth-first order, and the warp walks it together: every
+// lane tests the boxes of the node in hand against its own best distance,
+// the warp descends where any lane needs to, and a lane is active in exactly
+// the nodes its own walk (closest_inner / closest_leaf) would visit, in the
+// same order and with the same best distance at each -- so hits, distances
+// and counters equal the per-lane walk's.  Stacked far children keep each
+// lane's entry distance (+inf for lanes that do not need them); a pop takes
+// the next entry some lane still needs.  Node and triangle loads are the same
+// address on every lane.  `act` is false for lanes without a live ray.
+template <int Depth>
+__device__ __forceinline__ void closest_packet(const DeviceScene& s, ClosestWalk& w, bool act, int sgn3,
+                                               StepStack<Depth>& st, bool watertight, uint32_t& err,
+                                               TraceCounters& cnt) {
+    uint32_t ref = s.root_ref;
+    int sp = 0;
+    for (;;) {
+        if (!(ref & kLeafBit)) {
+            if (act) ++cnt.inner;
+            const float* nb = reinterpret_cast<const float*>(s.inner + ref);
+            const float4 q0 = PT_LDG4(nb);
+            const float4 q1 = PT_LDG4(nb + 4);
+            const float4 q2 = PT_LDG4(nb + 8);
+            const uint4  q3 = PT_LDGU4(nb + 12);
+            float e0, x0, e1, x1;
+            box_span(w.r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, e0, x0);
+            box_span(w.r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, e1, x1);
+            const bool h0 = act && e0 <= w.best && e0 <= x0;
+            const bool h1 = act && e1 <= w.best && e1 <= x1;
+            const uint32_t axis = q3.z & 3u;
+            const int lt = static_cast<int>((q3.z >> 2) & 1u);
+            const bool right_first = ((sgn3 >> axis) & 1) == lt;
+            const uint32_t nref = right_first ? q3.y : q3.x;
+            const uint32_t fref = right_first ? q3.x : q3.y;
+            const bool hn = right_first ? h1 : h0;
+            const bool hf = right_first ? h0 : h1;
+            const float ef = right_first ? e0 : e1;
+            const bool any_n = __any_sync(0xffffffffu, hn), any_f = __any_sync(0xffffffffu, hf);
+            if (any_n) {
+                if (any_f) {
+                    if (sp >= Depth) { err |= kErrStackOverflow; break; }
+                    st.ref[sp] = fref;
+                    st.t[sp] = hf ? ef : INFINITY;
+                    ++sp;
+                }
+                act = hn;
+                ref = nref;
+                continue;
+            }
+            if (any_f) { act = hf; ref = fref; continue; }
+        } else if (act) {
+            uint32_t ti = ref & ~kLeafBit;
+            for (;;) {
+                float u, v; bool last;
+                const float t = tri_test(s, w.r, ti, false, watertight, u, v, last);
+                ++cnt.tris;
+                if (t >= 0.0f && t < w.best) { w.best = t; w.prim = static_cast<int>(ti); w.bu = u; w.bv = v; }
+                if (last) break;
+                ++ti;
+            }
+        }
+        // the next stacked node some lane still needs
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            const bool need = st.t[sp] <= w.best;
+            if (__any_sync(0xffffffffu, need)) { act = need; ref = st.ref[sp]; found = true; break; }
+        }
+        if (!found) break;
+    }
+}
+
+// Closest hits of rays 32 t .. 32 t + 31 for the warp's tiles t = warp,
+// warp + warps, ... (< n rays): a tile whose live rays share their direction
+// signs is walked as a packet (closest_packet), any other lane by lane.  For
+// coherent rays (camera rays of neighbouring pixels).  All 32 lanes call it.
+template <int Depth = kStackDepth, class Fetch, class Done>
+__device__ __forceinline__ void closest_packet_loop(const DeviceScene& s, uint32_t warp, uint32_t warps, uint32_t n,
+                                                    bool watertight, uint32_t& err, TraceCounters& cnt,
+                                                    Fetch&& fetch, Done&& done) {
+    const uint32_t lane = threadIdx.x & 31u;
+    StepStack<Depth> st;
+    for (uint32_t base = warp * 32u; base < n; base += warps * 32u) {
+        const uint32_t i = base + lane;
+        const bool have = i < n;
+        ClosestWalk w;
+        w.best = FLT_MAX; w.prim = -1; w.bu = 0.0f; w.bv = 0.0f; w.sp = 0;
+        bool alive = false;
+        if (have) {
+            fetch(i, w.r);
+            w.r.xs = exit_scale(watertight);
+            alive = closest_begin(s, w);
+        }
+        const int sgn3 = alive ? (w.r.sx | (w.r.sy << 1) | (w.r.sz << 2)) : -1;
+        const uint32_t live = __ballot_sync(0xffffffffu, alive);
+        if (live) {
+            const int lead = __shfl_sync(0xffffffffu, sgn3, __ffs(live) - 1);
+            if (__all_sync(0xffffffffu, !alive || sgn3 == lead)) {
+                closest_packet<Depth>(s, w, alive, lead, st, watertight, err, cnt);
+            } else if (alive) {
+                for (;;) {
+                    if (w.ref & kLeafBit) {
+                        if (!closest_leaf(s, w, st, watertight, cnt)) break;
+                    } else if (!closest_inner(s, w, st, err, cnt)) {
+                        break;
+                    }
+                }
+            }
+        }
+        if (have) done(i, w);
+    }
+}
+
 struct AnyWalk {
     RayInv   r;
     float    tmax;
