@@ -896,7 +896,10 @@ __global__ void __launch_bounds__(128, 6) k_shade_back(WaveParams P, int q, int 
     }
 }
 
-template <int Block, int Depth>
+// Any-hit tests of the shadow queue.  Packet: the queue holds the shadow rays
+// of the camera bounce, emitted warp by warp from neighbouring pixels, tested
+// as packets where a tile's directions share their signs (any_packet_loop).
+template <int Block, int Depth, bool Packet = false>
 __global__ void __launch_bounds__(Block) k_shadow(WaveParams P) {
     const uint32_t n = min(P.counts[2], static_cast<uint32_t>(P.npath) * static_cast<uint32_t>(P.n_slots));
     if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -906,27 +909,31 @@ __global__ void __launch_bounds__(Block) k_shadow(WaveParams P) {
     uint32_t err = 0;
     TraceCounters tc{0, 0};
     const uint32_t stride = gridDim.x * blockDim.x;
-    any_loop<Depth>(P.scene, blockIdx.x * blockDim.x + threadIdx.x, n, stride, watertight, err, tc,
-             [&](uint32_t i, AnyWalk& w) {
-                 const float4 o = P.sq_o[i];
-                 const float4 d = P.sq_d[i];
-                 w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
-                 w.tmax = d.w;
-             },
-             [&](uint32_t i, bool occluded) {
-                 if (occluded) return;
-                 const uint32_t slot = __float_as_uint(P.sq_o[i].w);
-                 const uint32_t path = P.sq_path[i];
-                 if (slot < static_cast<uint32_t>(P.n_slots) && path < static_cast<uint32_t>(P.npath)) {
-                     float4* acc = P.nee + static_cast<size_t>(slot) * P.npath + path;
-                     const float4 c = P.sq_c[i];
-                     float4 a = *acc;
-                     a.x += c.x; a.y += c.y; a.z += c.z;
-                     *acc = a;
-                 } else {
-                     err |= kErrQueueOverflow;
-                 }
-             });
+    auto fetch = [&](uint32_t i, AnyWalk& w) {
+        const float4 o = P.sq_o[i];
+        const float4 d = P.sq_d[i];
+        w.r = make_ray_inv(o.x, o.y, o.z, d.x, d.y, d.z);
+        w.tmax = d.w;
+    };
+    auto done = [&](uint32_t i, bool occluded) {
+        if (occluded) return;
+        const uint32_t slot = __float_as_uint(P.sq_o[i].w);
+        const uint32_t path = P.sq_path[i];
+        if (slot < static_cast<uint32_t>(P.n_slots) && path < static_cast<uint32_t>(P.npath)) {
+            float4* acc = P.nee + static_cast<size_t>(slot) * P.npath + path;
+            const float4 c = P.sq_c[i];
+            float4 a = *acc;
+            a.x += c.x; a.y += c.y; a.z += c.z;
+            *acc = a;
+        } else {
+            err |= kErrQueueOverflow;
+        }
+    };
+    if (Packet)
+        any_packet_loop<Depth>(P.scene, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, stride >> 5, n, watertight, err,
+                               tc, fetch, done);
+    else
+        any_loop<Depth>(P.scene, blockIdx.x * blockDim.x + threadIdx.x, n, stride, watertight, err, tc, fetch, done);
     if (err) atomicOr(P.err, err);
     if (count) {
         warp_count(P.stats + kStatShadowNodes, tc.inner);
@@ -1140,9 +1147,13 @@ inline void launch_extend(int k, int grid, cudaStream_t st, const WaveParams& P,
 #undef PT_CASE
     }
 }
-inline void launch_shadow(int k, int grid, cudaStream_t st, const WaveParams& P) {
+inline void launch_shadow(int k, int grid, cudaStream_t st, const WaveParams& P, int depth) {
     switch (k) {
-#define PT_CASE(i, b, d) case i: k_shadow<b, d><<<grid, b, 0, st>>>(P); return;
+#define PT_CASE(i, b, d)                                                    \
+    case i:                                                                 \
+        if (depth == 0) k_shadow<b, d, true><<<grid, b, 0, st>>>(P);        \
+        else k_shadow<b, d><<<grid, b, 0, st>>>(P);                         \
+        return;
         PT_TRACE_SHAPES(PT_CASE)
 #undef PT_CASE
     }
@@ -1364,7 +1375,7 @@ int enqueue_batch(Wavefront& wf, const WaveParams& P, int64_t total_samples, cud
                         }
                     }
                 })) return rc;
-            if (int rc = timed(2, [&] { launch_shadow(tsi, wf.grid_shadow[tsi], st, P); })) return rc;
+            if (int rc = timed(2, [&] { launch_shadow(tsi, wf.grid_shadow[tsi], st, P, d); })) return rc;
         }
         if (int rc = timed(3, [&] { k_finalize<<<wf.grid_finalize, 256, 0, st>>>(P, s0, count); })) return rc;
         if (train) {

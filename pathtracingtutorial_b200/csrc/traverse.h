@@ -664,6 +664,112 @@ __device__ __forceinline__ void any_loop(const DeviceScene& s, uint32_t i, uint3
         if (fin) { done(i, w.hit); i += stride; have = false; }
     }
 }
+// Any-hit packet walk of one warp (see closest_packet): the warp walks the
+// depth-first order of the sign bits sgn3; a lane takes part in the nodes
+// whose box it passes on its own ray, and leaves once it finds an occluder.
+// The answer does not depend on the visit order.  A stacked node records, per
+// lane, whether that lane passed its box (bit sp of need).
+template <int Depth>
+__device__ __forceinline__ void any_packet(const DeviceScene& s, AnyWalk& w, bool act, int sgn3, uint32_t* stack,
+                                           bool watertight, uint32_t& err, TraceCounters& cnt) {
+    static_assert(Depth <= 64, "one bit per stack entry");
+    uint32_t ref = s.root_ref;
+    int sp = 0;
+    unsigned long long need = 0ull;
+    for (;;) {
+        if (!(ref & kLeafBit)) {
+            if (act) ++cnt.inner;
+            const float* nb = reinterpret_cast<const float*>(s.inner + ref);
+            const float4 q0 = PT_LDG4(nb);
+            const float4 q1 = PT_LDG4(nb + 4);
+            const float4 q2 = PT_LDG4(nb + 8);
+            const uint4  q3 = PT_LDGU4(nb + 12);
+            float e0, x0, e1, x1;
+            box_span(w.r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, e0, x0);
+            box_span(w.r, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, e1, x1);
+            const bool h0 = act && e0 <= w.tmax && e0 <= x0;
+            const bool h1 = act && e1 <= w.tmax && e1 <= x1;
+            const uint32_t axis = q3.z & 3u;
+            const int lt = static_cast<int>((q3.z >> 2) & 1u);
+            const bool right_first = ((sgn3 >> axis) & 1) == lt;
+            const uint32_t nref = right_first ? q3.y : q3.x;
+            const uint32_t fref = right_first ? q3.x : q3.y;
+            const bool hn = right_first ? h1 : h0;
+            const bool hf = right_first ? h0 : h1;
+            const bool any_n = __any_sync(0xffffffffu, hn), any_f = __any_sync(0xffffffffu, hf);
+            if (any_n) {
+                if (any_f) {
+                    if (sp >= Depth) { err |= kErrStackOverflow; break; }
+                    stack[sp] = fref;
+                    if (hf) need |= 1ull << sp;
+                    else need &= ~(1ull << sp);
+                    ++sp;
+                }
+                act = hn;
+                ref = nref;
+                continue;
+            }
+            if (any_f) { act = hf; ref = fref; continue; }
+        } else if (act) {
+            uint32_t ti = ref & ~kLeafBit;
+            for (;;) {
+                float u, v; bool last;
+                const float t = tri_test(s, w.r, ti, true, watertight, u, v, last);
+                ++cnt.tris;
+                if (t > 0.0f && t < w.tmax) { w.hit = true; break; }
+                if (last) break;
+                ++ti;
+            }
+        }
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            const bool nd = !w.hit && ((need >> sp) & 1ull);
+            if (__any_sync(0xffffffffu, nd)) { act = nd; ref = stack[sp]; found = true; break; }
+        }
+        if (!found) break;
+    }
+}
+
+// Any-hit tests of the warp's tiles of 32 rays (see closest_packet_loop):
+// a tile whose live rays share their direction signs walks as a packet, any
+// other lane by lane.  fetch(i, AnyWalk&) sets r and tmax; done(i, occluded).
+template <int Depth = kStackDepth, class Fetch, class Done>
+__device__ __forceinline__ void any_packet_loop(const DeviceScene& s, uint32_t warp, uint32_t warps, uint32_t n,
+                                                bool watertight, uint32_t& err, TraceCounters& cnt, Fetch&& fetch,
+                                                Done&& done) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t stack[Depth];
+    for (uint32_t base = warp * 32u; base < n; base += warps * 32u) {
+        const uint32_t i = base + lane;
+        const bool have = i < n;
+        AnyWalk w;
+        w.sp = 0; w.hit = false;
+        bool alive = false;
+        if (have) {
+            fetch(i, w);
+            w.r.xs = exit_scale(watertight);
+            alive = any_begin(s, w);
+        }
+        const int sgn3 = alive ? (w.r.sx | (w.r.sy << 1) | (w.r.sz << 2)) : -1;
+        const uint32_t live = __ballot_sync(0xffffffffu, alive);
+        if (live) {
+            const int lead = __shfl_sync(0xffffffffu, sgn3, __ffs(live) - 1);
+            if (__all_sync(0xffffffffu, !alive || sgn3 == lead)) {
+                any_packet<Depth>(s, w, alive, lead, stack, watertight, err, cnt);
+            } else if (alive) {
+                for (;;) {
+                    if (w.ref & kLeafBit) {
+                        if (!any_leaf(s, w, stack, watertight, cnt)) break;
+                    } else if (!any_inner<Depth>(s, w, stack, err, cnt)) {
+                        break;
+                    }
+                }
+            }
+        }
+        if (have) done(i, w.hit);
+    }
+}
 #endif  // __CUDACC__
 
 }  // namespace ptb
