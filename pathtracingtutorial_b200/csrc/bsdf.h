@@ -294,12 +294,13 @@ __device__ __noinline__ BsdfEval disney_eval_call(const MatEval& m, f3 wo, f3 wi
 #  define PT_BSDF_EVAL disney_eval
 #endif
 
-// One-lobe importance sample.  Draws 1 + 2 dimensions, none when N.V < 1e-5
-// (the reference returns before its first draw, disney_bsdf.cuh:332-333).
-PT_HD BsdfSample disney_sample(const MatEval& m, f3 wo, f3 n, PathRng& rng, int rtl, bool entering) {
-    BsdfSample r; r.wi = mk(0.0f); r.weight = mk(0.0f); r.pdf = 0.0f; r.delta = false; r.valid = false;
+// The direction of disney_sample: draws 1 + 2 dimensions, none when N.V <
+// 1e-5 (the reference returns before its first draw, disney_bsdf.cuh:332-333);
+// false when the sample is rejected (below the surface).
+PT_HD bool disney_sample_dir(const MatEval& m, f3 wo, f3 n, PathRng& rng, int rtl, bool entering, f3& wi_out,
+                             bool& delta_out) {
     const float nov = dot(n, wo);
-    if (nov < 1e-5f) return r;
+    if (nov < 1e-5f) return false;
     const LobeWeights w = lobe_weights(m);
     const float choice = rng_next(rng);
     const Frame fr = make_frame(n);
@@ -317,25 +318,37 @@ PT_HD BsdfSample disney_sample(const MatEval& m, f3 wo, f3 n, PathRng& rng, int 
     } else if (choice < w.diff + w.sheen + w.spec) {
         const f3 h = to_world(fr, sample_vndf(wol, ax, ay, u1, u2));
         wi = reflect(-wo, h);
-        if (dot(wi, n) <= 0.0f) return r;
+        if (dot(wi, n) <= 0.0f) return false;
         delta = m.roughness < 0.01f;
     } else if (choice < w.diff + w.sheen + w.spec + w.cc) {
         const float ca = fmaxf(m.cc_roughness * m.cc_roughness, 0.001f);
         const f3 h = to_world(fr, sample_vndf(wol, ca, ca, u1, u2));
         wi = reflect(-wo, h);
-        if (dot(wi, n) <= 0.0f) return r;
+        if (dot(wi, n) <= 0.0f) return false;
     } else {
         const f3 h = to_world(fr, sample_vndf(wol, ax, ay, u1, u2));
         const float eta = entering ? (1.0f / m.ior) : m.ior;
         f3 wt;
         if (!refract_dir(wo, h, eta, wt)) {
             wi = reflect(-wo, h);
-            if (dot(wi, n) <= 0.0f) return r;
+            if (dot(wi, n) <= 0.0f) return false;
         } else {
             wi = normalize(wt);
             delta = m.roughness < 0.01f;
         }
     }
+    wi_out = wi;
+    delta_out = delta;
+    return true;
+}
+
+// One-lobe importance sample (disney_bsdf.cuh:325-410): the direction, then
+// the full BSDF there.
+PT_HD BsdfSample disney_sample(const MatEval& m, f3 wo, f3 n, PathRng& rng, int rtl, bool entering) {
+    BsdfSample r; r.wi = mk(0.0f); r.weight = mk(0.0f); r.pdf = 0.0f; r.delta = false; r.valid = false;
+    f3 wi;
+    bool delta = false;
+    if (!disney_sample_dir(m, wo, n, rng, rtl, entering, wi, delta)) return r;
     const BsdfEval ev = PT_BSDF_EVAL(m, wo, wi, n, entering);
     if (ev.pdf <= 0.0f) return r;
     r.wi = wi; r.pdf = ev.pdf; r.delta = delta; r.valid = true;

@@ -665,17 +665,28 @@ __device__ bool shade_back(int arg_rtl, int depth, f3 rd, const ShadePoint& sp, 
         // the plain integrator's, including where the reference's pdf is not
         // the sampler's density (disney_sample_density).  bs.pdf stays the
         // BSDF's pdf, for the emitter hit's power heuristic.
+        // Either branch only picks the direction; the BSDF is then evaluated
+        // once for the whole warp (a lane that drew from q and one that drew
+        // from the BSDF would otherwise each run an evaluation in turn).  No
+        // guided vertex has a delta lobe, so both weights are f / pdf.
         const float sel = rng_next(rng);
-        if (sel < gv.alpha) {
+        const bool from_q = sel < gv.alpha;
+        bool have_dir;
+        bool delta = false;
+        if (from_q) {
             const float u0 = rng_next(rng), u1 = rng_next(rng), u2 = rng_next(rng);
             bs.wi = mix_sample(gmix, u0, u1, u2);
+            have_dir = true;
+        } else {
+            have_dir = disney_sample_dir(me, wo, N, rng, arg_rtl, entering, bs.wi, delta);
+        }
+        bs.valid = false;
+        bs.delta = false;
+        if (have_dir) {
             const BsdfEval ev = PT_BSDF_EVAL(me, wo, bs.wi, N, entering);
             bs.pdf = ev.pdf;
-            bs.delta = false;
-            bs.valid = ev.pdf > 0.0f && !is_zero(ev.f);
+            bs.valid = ev.pdf > 0.0f && (!from_q || !is_zero(ev.f));
             bs.weight = ev.f / (ev.pdf + 1e-7f);   // the plain integrator's weight
-        } else {
-            bs = PT_BSDF_SAMPLE(me, wo, N, rng, arg_rtl, entering);
         }
         if (bs.valid) {
             const float pB = disney_sample_density(me, wo, bs.wi, N, bs.pdf);
