@@ -70,7 +70,7 @@ inline int guide_init(GuideState& g, int device, const float lo[3], const float 
     for (uint32_t l = 0; l < g.net.dense_limit; ++l) {
         const uint32_t res = static_cast<uint32_t>(g.net.scale[l]) + 2u;
         g.net.quad_off[l] = quad_entries;
-        quad_entries += res * res * res;
+        quad_entries += guide_quad_level_entries(res);
     }
     const size_t total = off_quad + al(static_cast<size_t>(quad_entries) * sizeof(uint4));
     if (!guide_cuda_ok(cudaMalloc(&g.params, total), "parameter allocation")) return PT_ERR_NOMEM;

@@ -32,15 +32,22 @@ __host__ __device__ __forceinline__ uint32_t guide_feat_rows(uint32_t n) {
     return (n + kGTcRows - 1u) / kGTcRows * kGTcRows;
 }
 
+// Entries of a dense level's four-corner table: res^3 plus one layer (res^2),
+// so that a cell in the last layer (a position at the top of the unit cube,
+// where floor(scale * p + 0.5) can reach res - 1) reads the same pair-table
+// entries as encode_level does (the index wraps on into the next layers
+// there, as the dense index arithmetic does).
+__host__ __device__ inline uint32_t guide_quad_level_entries(uint32_t res) { return res * res * res + res * res; }
+
 // The four-corner table of the dense levels from the pair table `net.grid`.
 __global__ void __launch_bounds__(256) k_guide_quad(GuideNet net) {
     for (uint32_t l = 0; l < net.dense_limit; ++l) {
         const uint32_t res = static_cast<uint32_t>(net.scale[l]) + 2u;
-        const uint32_t n = res * res * res;
+        const uint32_t n = guide_quad_level_entries(res);
         const uint2* tab = net.grid + static_cast<size_t>(l) * kGTable;
         uint4* dst = net.quad + net.quad_off[l];
         for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-            const uint2 a = tab[e], b = tab[(e + res) & (kGTable - 1)];
+            const uint2 a = tab[e & (kGTable - 1)], b = tab[(e + res) & (kGTable - 1)];
             dst[e] = make_uint4(a.x, a.y, b.x, b.y);
         }
     }

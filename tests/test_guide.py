@@ -269,10 +269,13 @@ def test_guide_inference_kinds_agree_with_oracle():
     prm = g.params()
     rng = np.random.default_rng(7)
     lo, inv = prm["lo"].astype(np.float64), prm["inv_extent"].astype(np.float64)
-    # 5000 queries: several 128-query tiles and a ragged last one
-    p01 = rng.uniform(0.02, 0.98, (5000, 3)).astype(np.float32)
+    # 5512 queries: several 128-query tiles and a ragged last one; 512 of them
+    # at the top of the unit cube and beyond it (clamped), where the dense
+    # levels' cells reach the last layer of their index range
+    p01 = np.concatenate([rng.uniform(0.02, 0.98, (5000, 3)),
+                          rng.uniform(0.985, 1.02, (512, 3))]).astype(np.float32)
     world = (lo + p01 / inv).astype(np.float32)
-    d = rng.normal(size=(5000, 3)); d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d = rng.normal(size=(len(p01), 3)); d /= np.linalg.norm(d, axis=1, keepdims=True)
     pn = np.clip((world - prm["lo"]) * prm["inv_extent"], 0, 1).astype(np.float32)
     q_ref = guide_ref.pdf(prm, pn, d, bf16=True)
     q, img = {}, {}
